@@ -1,0 +1,306 @@
+// Oracle driver around the reference hmat-oss library (test infrastructure only).
+//
+// Runs the reference's own public C API on a point cloud given as a binary file:
+//   hmat_create_clustering_median + hmat_create_clustering_max_dof   (c_default_interface.cpp:35,73)
+//   hmat_create_cluster_tree                                          (c_default_interface.cpp:101)
+//   hmat_create_admissibility_standard                                (c_default_interface.cpp:215)
+//   hmat_create_compression_aca_plus                                  (compression.hpp:137)
+//   hi.create_empty_hmatrix_admissibility / set_low_rank_epsilon /
+//   assemble_generic (simple_compute callback) / gemv / get_info      (c_wrapping.hpp:41-96,233-252)
+// and dumps what the parity tests compare: the cluster permutation, the leaf list,
+// the leaf payloads (optional), the gemv result and wall-clock timings.
+//
+// Usage: ref_driver <params file>   (key=value lines, see parse_params below)
+//
+// The kernel callbacks are evaluated in double with a fixed operation order and no
+// contraction (this file is compiled without -ffast-math), so the device kernels can
+// reproduce the same entries.
+#include "hmat/hmat.h"
+#include "hmat_cpp_interface.hpp"
+#include "h_matrix.hpp"
+#include "rk_matrix.hpp"
+#include "full_matrix.hpp"
+
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace {
+
+struct Params {
+  std::map<std::string, std::string> kv;
+  std::string get(const std::string& k, const std::string& d = "") const {
+    auto it = kv.find(k);
+    return it == kv.end() ? d : it->second;
+  }
+  double num(const std::string& k, double d) const {
+    auto it = kv.find(k);
+    return it == kv.end() ? d : atof(it->second.c_str());
+  }
+};
+
+Params parse_params(const char* path) {
+  Params p;
+  FILE* f = fopen(path, "r");
+  if (!f) { perror(path); exit(2); }
+  char line[4096];
+  while (fgets(line, sizeof line, f)) {
+    char* eq = strchr(line, '=');
+    if (!eq) continue;
+    *eq = 0;
+    std::string k(line), v(eq + 1);
+    while (!v.empty() && (v.back() == '\n' || v.back() == '\r' || v.back() == ' ')) v.pop_back();
+    p.kv[k] = v;
+  }
+  fclose(f);
+  return p;
+}
+
+std::vector<char> read_file(const std::string& path) {
+  FILE* f = fopen(path.c_str(), "rb");
+  if (!f) { perror(path.c_str()); exit(2); }
+  fseek(f, 0, SEEK_END);
+  long n = ftell(f);
+  fseek(f, 0, SEEK_SET);
+  std::vector<char> buf(n);
+  if (n && fread(buf.data(), 1, n, f) != (size_t)n) { perror("read"); exit(2); }
+  fclose(f);
+  return buf;
+}
+
+void write_file(const std::string& path, const void* data, size_t bytes) {
+  FILE* f = fopen(path.c_str(), "wb");
+  if (!f) { perror(path.c_str()); exit(2); }
+  if (bytes && fwrite(data, 1, bytes, f) != bytes) { perror("write"); exit(2); }
+  fclose(f);
+}
+
+// Kernel context passed to the simple_compute callback.
+struct KernelCtx {
+  const double* pts;  // N x 3, point-major
+  int kind;           // 0 laplace_reg, 1 exp_cov, 2 helmholtz_reg
+  double delta;       // regularisation of 1/(4 pi (r + delta))
+  double ell;         // correlation length of exp(-r/ell)
+  double nugget;      // added on the diagonal (row == col) of exp_cov
+  double wavenumber;  // k of exp(i k r)
+};
+
+const double kFourPi = 4.0 * M_PI;
+
+inline double dist(const double* a, const double* b) {
+  double dx = a[0] - b[0];
+  double dy = a[1] - b[1];
+  double dz = a[2] - b[2];
+  double s = dx * dx;
+  s = s + dy * dy;
+  s = s + dz * dz;
+  return std::sqrt(s);
+}
+
+void real_kernel(void* vctx, int row, int col, void* result) {
+  const KernelCtx* c = (const KernelCtx*)vctx;
+  double r = dist(c->pts + 3 * (size_t)row, c->pts + 3 * (size_t)col);
+  double v;
+  if (c->kind == 0) {
+    v = 1.0 / (kFourPi * (r + c->delta));
+  } else {
+    v = std::exp(-r / c->ell);
+    if (row == col) v += c->nugget;
+  }
+  *(double*)result = v;
+}
+
+void complex_kernel(void* vctx, int row, int col, void* result) {
+  const KernelCtx* c = (const KernelCtx*)vctx;
+  double r = dist(c->pts + 3 * (size_t)row, c->pts + 3 * (size_t)col);
+  double s = 1.0 / (kFourPi * (r + c->delta));
+  double kr = c->wavenumber * r;
+  double* out = (double*)result;
+  out[0] = std::cos(kr) * s;
+  out[1] = std::sin(kr) * s;
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct LeafRec {
+  int row_off, row_size, col_off, col_size, type, rank;
+};
+
+template <typename T>
+void walk(const hmat::HMatrix<T>* h, std::vector<LeafRec>& leaves, std::vector<T>& payload, bool dump) {
+  if (!h) return;
+  if (!h->isLeaf()) {
+    for (int i = 0; i < h->nrChild(); ++i) walk(h->getChild(i), leaves, payload, dump);
+    return;
+  }
+  LeafRec r;
+  r.row_off = h->rows()->offset();
+  r.row_size = h->rows()->size();
+  r.col_off = h->cols()->offset();
+  r.col_size = h->cols()->size();
+  if (h->isRkMatrix()) {
+    r.type = 1;
+    r.rank = h->rank();
+    if (dump && r.rank > 0) {
+      const hmat::RkMatrix<T>* rk = h->rk();
+      for (int j = 0; j < r.rank; ++j)
+        for (int i = 0; i < r.row_size; ++i) payload.push_back(rk->a->get(i, j));
+      for (int j = 0; j < r.rank; ++j)
+        for (int i = 0; i < r.col_size; ++i) payload.push_back(rk->b->get(i, j));
+    }
+  } else {
+    r.type = 0;
+    r.rank = -1;
+    const hmat::FullMatrix<T>* f = h->isFullMatrix() ? h->full() : nullptr;
+    if (dump && f) {
+      for (int j = 0; j < r.col_size; ++j)
+        for (int i = 0; i < r.row_size; ++i) payload.push_back(f->data.get(i, j));
+    }
+    if (!f) r.rank = -2;  // full leaf without storage (empty block)
+  }
+  leaves.push_back(r);
+}
+
+template <typename T>
+int run(const Params& p, hmat_value_t vt) {
+  const int n = (int)p.num("n", 0);
+  std::vector<char> pbuf = read_file(p.get("points"));
+  if ((int)(pbuf.size() / (3 * sizeof(double))) != n) {
+    fprintf(stderr, "points file holds %zu bytes, expected %d points\n", pbuf.size(), n);
+    return 2;
+  }
+  std::vector<double> pts(3 * (size_t)n);
+  memcpy(pts.data(), pbuf.data(), pbuf.size());
+  const std::string out = p.get("out");
+
+  hmat_settings_t settings;
+  hmat_get_parameters(&settings);
+  settings.compressionMinLeafSize = (int)p.num("min_leaf", 0);
+  hmat_set_parameters(&settings);
+
+  hmat_interface_t hi;
+  hmat_init_default_interface(&hi, vt);
+
+  double t0 = now_s();
+  hmat_clustering_algorithm_t* median = hmat_create_clustering_median();
+  hmat_clustering_algorithm_t* algo = hmat_create_clustering_max_dof(median, (int)p.num("leaf", 64));
+  hmat_cluster_tree_t* ct = hmat_create_cluster_tree(pts.data(), 3, n, algo);
+  hmat_admissibility_t* adm = hmat_create_admissibility_standard(p.num("eta", 2.0));
+  hmat_matrix_t* M = hi.create_empty_hmatrix_admissibility(ct, ct, 0, adm);
+  const double eps = p.num("eps", 1e-4);
+  hi.set_low_rank_epsilon(M, eps);
+  double t_build = now_s() - t0;
+
+  KernelCtx kctx;
+  kctx.pts = pts.data();
+  const std::string kname = p.get("kernel", "laplace");
+  kctx.kind = kname == "laplace" ? 0 : (kname == "expcov" ? 1 : 2);
+  kctx.delta = p.num("delta", 0.01);
+  kctx.ell = p.num("ell", 0.3);
+  kctx.nugget = p.num("nugget", 0.0);
+  kctx.wavenumber = p.num("wavenumber", 0.0);
+
+  hmat_assemble_context_t ctx;
+  hmat_assemble_context_init(&ctx);
+  ctx.compression = hmat_create_compression_aca_plus(eps);
+  ctx.user_context = &kctx;
+  ctx.simple_compute = (vt == HMAT_DOUBLE_COMPLEX || vt == HMAT_SIMPLE_COMPLEX) ? complex_kernel : real_kernel;
+  ctx.lower_symmetric = 0;
+  ctx.factorization = hmat_factorization_none;
+  t0 = now_s();
+  int rc = hi.assemble_generic(M, &ctx);
+  double t_assemble = now_s() - t0;
+  if (rc) {
+    fprintf(stderr, "assemble_generic failed\n");
+    return 3;
+  }
+
+  // Cluster permutation (internal -> client).
+  const int* perm = hmat_cluster_get_indices(ct);
+  write_file(out + ".perm", perm, sizeof(int) * (size_t)n);
+
+  // Leaves.
+  hmat::HMatInterface<T>* hm = (hmat::HMatInterface<T>*)M;
+  std::vector<LeafRec> leaves;
+  std::vector<T> payload;
+  const bool dump = p.num("dump_factors", 0) != 0;
+  walk<T>(hm->engine().hmat, leaves, payload, dump);
+  write_file(out + ".leaves", leaves.data(), leaves.size() * sizeof(LeafRec));
+  if (dump) write_file(out + ".payload", payload.data(), payload.size() * sizeof(T));
+
+  hmat_info_t info;
+  memset(&info, 0, sizeof info);
+  hi.get_info(M, &info);
+
+  // gemv in client numbering, alpha = 1, beta = 0.
+  const int nrhs = (int)p.num("nrhs", 1);
+  const std::string trans = p.get("trans", "N");
+  const int reps = (int)p.num("gemv_reps", 1);
+  double t_gemv_first = 0, t_gemv_mean = 0;
+  if (!p.get("x").empty()) {
+    std::vector<char> xb = read_file(p.get("x"));
+    if (xb.size() != sizeof(T) * (size_t)n * nrhs) {
+      fprintf(stderr, "x file holds %zu bytes, expected %zu\n", xb.size(), sizeof(T) * (size_t)n * nrhs);
+      return 2;
+    }
+    std::vector<T> x((size_t)n * nrhs), y((size_t)n * nrhs);
+    T alpha = T(1), beta = T(0);
+    for (int rep = 0; rep <= reps; ++rep) {
+      memcpy(x.data(), xb.data(), xb.size());
+      std::fill(y.begin(), y.end(), T(0));
+      t0 = now_s();
+      rc = hi.gemv(trans[0], &alpha, M, x.data(), &beta, y.data(), nrhs);
+      double dt = now_s() - t0;
+      if (rc) { fprintf(stderr, "gemv failed\n"); return 4; }
+      if (rep == 0) t_gemv_first = dt; else t_gemv_mean += dt / reps;
+    }
+    write_file(out + ".y", y.data(), y.size() * sizeof(T));
+  }
+
+  FILE* js = fopen((out + ".json").c_str(), "w");
+  fprintf(js,
+          "{\"n\": %d, \"leaves\": %zu, \"t_build\": %.9g, \"t_assemble\": %.9g, \"t_gemv_first\": %.9g, "
+          "\"t_gemv_mean\": %.9g, \"gemv_reps\": %d, \"nrhs\": %d, \"full_count\": %zu, \"rk_count\": %zu, "
+          "\"full_size\": %zu, \"rk_size\": %zu, \"compressed_size\": %zu, \"uncompressed_size\": %zu, "
+          "\"nr_block_clusters\": %d, \"largest_rk_dim_rows\": %d, \"largest_rk_dim_cols\": %d, "
+          "\"largest_rk_mem_rows\": %d, \"largest_rk_mem_cols\": %d, \"largest_rk_mem_rank\": %d}\n",
+          n, leaves.size(), t_build, t_assemble, t_gemv_first, t_gemv_mean, reps, nrhs, info.full_count,
+          info.rk_count, info.full_size, info.rk_size, info.compressed_size, info.uncompressed_size,
+          info.nr_block_clusters, info.largest_rk_dim_rows, info.largest_rk_dim_cols, info.largest_rk_mem_rows,
+          info.largest_rk_mem_cols, info.largest_rk_mem_rank);
+  fclose(js);
+
+  hi.destroy(M);
+  hmat_delete_cluster_tree(ct);
+  hmat_delete_admissibility(adm);
+  hmat_delete_compression(ctx.compression);
+  hmat_delete_clustering(algo);
+  hmat_delete_clustering(median);
+  hi.finalize();
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc != 2) {
+    fprintf(stderr, "usage: %s <params file>\n", argv[0]);
+    return 2;
+  }
+  Params p = parse_params(argv[1]);
+  const std::string s = p.get("scalar", "D");
+  if (s == "D") return run<hmat::D_t>(p, HMAT_DOUBLE_PRECISION);
+  if (s == "S") return run<hmat::S_t>(p, HMAT_SIMPLE_PRECISION);
+  if (s == "Z") return run<hmat::Z_t>(p, HMAT_DOUBLE_COMPLEX);
+  if (s == "C") return run<hmat::C_t>(p, HMAT_SIMPLE_COMPLEX);
+  fprintf(stderr, "unknown scalar type %s\n", s.c_str());
+  return 2;
+}
