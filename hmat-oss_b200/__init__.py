@@ -1,0 +1,399 @@
+"""Python mirror of the hmat-oss C interface, backed by the B200 engine.
+
+The product is ``libhmat_b200.so`` (C ABI declared in ``include/hmat_b200.h``); this
+module binds it with ctypes and mirrors the reference's C entry points with the same
+names and argument meaning (``hmat_init_default_interface``, ``create_empty_hmatrix_admissibility``,
+``set_low_rank_epsilon``, ``assemble_generic``, ``gemv``, ``get_info``, ``destroy``, ...), so
+that host programs and tests read like the reference's own examples
+(examples/c-simple-cylinder.c, examples/c-simple-kriging.c).  There is no CPU fallback: if
+the shared library is missing, importing the bindings raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhmat_b200.so")
+
+HMAT_SIMPLE_PRECISION = 0
+HMAT_DOUBLE_PRECISION = 1
+HMAT_SIMPLE_COMPLEX = 2
+HMAT_DOUBLE_COMPLEX = 3
+
+DTYPES = {
+    HMAT_SIMPLE_PRECISION: np.float32,
+    HMAT_DOUBLE_PRECISION: np.float64,
+    HMAT_SIMPLE_COMPLEX: np.complex64,
+    HMAT_DOUBLE_COMPLEX: np.complex128,
+}
+
+LAPLACE_REG = 0
+EXP_COV = 1
+HELMHOLTZ_REG = 2
+
+hmat_factorization_none = -1
+
+
+class KernelDesc(C.Structure):
+    _fields_ = [("kind", C.c_int), ("delta", C.c_double), ("ell", C.c_double), ("nugget", C.c_double),
+                ("wavenumber", C.c_double)]
+
+
+class AssembleContext(C.Structure):
+    """hmat_assemble_context_t (reference: include/hmat/hmat.h:516-622)."""
+    _fields_ = [("assembly", C.c_void_p), ("simple_compute", C.c_void_p), ("block_compute", C.c_void_p),
+                ("advanced_compute", C.c_void_p), ("user_context", C.c_void_p), ("prepare", C.c_void_p),
+                ("compression", C.c_void_p), ("lower_symmetric", C.c_int), ("factorization", C.c_int),
+                ("progress", C.c_void_p)]
+
+
+class Info(C.Structure):
+    """hmat_info_t (reference: include/hmat/hmat.h:404-439)."""
+    _fields_ = [("full_zeros", C.c_int), ("full_size", C.c_size_t), ("rk_size", C.c_size_t),
+                ("full_count", C.c_size_t), ("rk_count", C.c_size_t), ("compressed_size", C.c_size_t),
+                ("uncompressed_size", C.c_size_t), ("nr_block_clusters", C.c_int),
+                ("largest_rk_dim_rows", C.c_int), ("largest_rk_dim_cols", C.c_int),
+                ("largest_rk_mem_rows", C.c_int), ("largest_rk_mem_cols", C.c_int),
+                ("largest_rk_mem_rank", C.c_int)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Settings(C.Structure):
+    """hmat_settings_t (reference: include/hmat/hmat.h:1107-1131)."""
+    _fields_ = [("compressionMinLeafSize", C.c_int), ("coarseningEpsilon", C.c_double), ("maxLeafSize", C.c_int),
+                ("coarsening", C.c_int), ("validateNullRowCol", C.c_int), ("validateCompression", C.c_int),
+                ("validateRecompression", C.c_int), ("dumpTrace", C.c_int), ("validationReRun", C.c_int),
+                ("validationDump", C.c_int), ("validationErrorThreshold", C.c_double)]
+
+
+# Slot order of hmat_interface_t (reference: include/hmat/hmat.h:717-1103).
+_SLOTS = ["create_empty_hmatrix_admissibility", "own_cluster_trees", "set_low_rank_epsilon", "assemble_generic",
+          "copy", "copy_struct", "norm", "logdet", "inverse", "factorize_generic", "destroy", "get_child",
+          "destroy_child", "solve_generic", "solve_mat", "solve_systems", "solve_dense", "transpose", "scale",
+          "truncate", "vector_reorder", "vector_restore", "gemm", "axpy", "trsm", "gemv", "gemm_scalar",
+          "full_gemm", "gemm_dense", "add_identity", "init", "finalize", "get_info", "get_profile", "get_ratio",
+          "FPcompress", "FPdecompress", "GetFPCompressionSettings", "SetFPCompressionSettings",
+          "SetFPCompressionSettingsParams", "dump_info", "get_cluster_trees", "set_cluster_trees",
+          "extract_diagonal", "solve_lower_triangular", "solve_lower_triangular_dense", "get_block",
+          "get_values", "walk", "apply_on_leaf", "value_type", "internal", "read_struct", "write_struct",
+          "read_data", "write_data", "set_progressbar", "extract_diagonal_block"]
+
+
+class InterfaceTable(C.Structure):
+    _fields_ = [(s, C.c_int if s == "value_type" else C.c_void_p) for s in _SLOTS]
+
+
+_P = C.c_void_p
+_PROTOS = {
+    "create_empty_hmatrix_admissibility": C.CFUNCTYPE(_P, _P, _P, C.c_int, _P),
+    "own_cluster_trees": C.CFUNCTYPE(None, _P, C.c_int, C.c_int),
+    "set_low_rank_epsilon": C.CFUNCTYPE(None, _P, C.c_double),
+    "assemble_generic": C.CFUNCTYPE(C.c_int, _P, C.POINTER(AssembleContext)),
+    "destroy": C.CFUNCTYPE(C.c_int, _P),
+    "gemv": C.CFUNCTYPE(C.c_int, C.c_char, _P, _P, _P, _P, _P, C.c_int),
+    "get_info": C.CFUNCTYPE(C.c_int, _P, C.POINTER(Info)),
+    "vector_reorder": C.CFUNCTYPE(C.c_int, _P, _P, C.c_int, _P, C.c_int),
+    "vector_restore": C.CFUNCTYPE(C.c_int, _P, _P, C.c_int, _P, C.c_int),
+    "truncate": C.CFUNCTYPE(C.c_int, _P),
+    "gemm_dense": C.CFUNCTYPE(C.c_int, C.c_char, C.c_char, C.c_char, _P, _P, _P, _P, _P, C.c_int),
+    "solve_systems": C.CFUNCTYPE(C.c_int, _P, _P, C.c_int),
+    "init": C.CFUNCTYPE(C.c_int),
+    "finalize": C.CFUNCTYPE(C.c_int),
+}
+
+_lib = None
+
+# Entry points declared in include/hmat_b200.h; the tests check that every one is exported.
+EXPORTED = [
+    "hmat_create_clustering_median", "hmat_create_clustering_max_dof", "hmat_delete_clustering",
+    "hmat_set_clustering_divider", "hmat_create_cluster_tree", "hmat_delete_cluster_tree", "hmat_tree_nodes_count",
+    "hmat_cluster_get_info", "hmat_cluster_get_indices", "hmat_init_admissibility_param",
+    "hmat_create_admissibility", "hmat_update_admissibility", "hmat_create_admissibility_standard",
+    "hmat_delete_admissibility", "hmat_create_compression_aca_plus", "hmat_create_compression_aca_partial",
+    "hmat_create_compression_svd", "hmat_create_compression_aca_full", "hmat_create_compression_aca_random",
+    "hmat_create_compression_rrqr", "hmat_delete_compression", "hmat_default_progress",
+    "hmat_assemble_context_init", "hmat_factorization_context_init", "hmat_solve_context_init",
+    "hmat_init_default_interface", "hmat_get_parameters", "hmat_set_parameters", "hmat_get_version",
+    "hmat_b200_create_assembly", "hmat_b200_delete_assembly", "hmat_b200_gemv_device", "hmat_b200_leaf_count",
+    "hmat_b200_leaf_table", "hmat_b200_leaf_payload", "hmat_b200_leaf_arenas", "hmat_b200_leaf_gradients",
+    "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_last_error",
+]
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Loads libhmat_b200.so (built in-tree by `make -C hmat-oss_b200`).  Raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `make -C hmat-oss_b200` (no CPU fallback exists)")
+    lib = C.CDLL(path)
+    sig = {
+        "hmat_create_clustering_median": (_P, []),
+        "hmat_create_clustering_max_dof": (_P, [_P, C.c_int]),
+        "hmat_delete_clustering": (None, [_P]),
+        "hmat_create_cluster_tree": (_P, [_P, C.c_int, C.c_int, _P]),
+        "hmat_delete_cluster_tree": (None, [_P]),
+        "hmat_tree_nodes_count": (C.c_int, [_P]),
+        "hmat_cluster_get_indices": (C.POINTER(C.c_int), [_P]),
+        "hmat_create_admissibility_standard": (_P, [C.c_double]),
+        "hmat_delete_admissibility": (None, [_P]),
+        "hmat_create_compression_aca_plus": (_P, [C.c_double]),
+        "hmat_create_compression_aca_partial": (_P, [C.c_double]),
+        "hmat_create_compression_svd": (_P, [C.c_double]),
+        "hmat_delete_compression": (None, [_P]),
+        "hmat_assemble_context_init": (None, [C.POINTER(AssembleContext)]),
+        "hmat_init_default_interface": (None, [C.POINTER(InterfaceTable), C.c_int]),
+        "hmat_get_parameters": (None, [C.POINTER(Settings)]),
+        "hmat_set_parameters": (C.c_int, [C.POINTER(Settings)]),
+        "hmat_get_version": (C.c_char_p, []),
+        "hmat_b200_create_assembly": (_P, [C.POINTER(KernelDesc), _P, C.c_int]),
+        "hmat_b200_delete_assembly": (None, [_P]),
+        "hmat_b200_gemv_device": (C.c_int, [_P, C.c_char, _P, _P, _P, _P, C.c_int, _P]),
+        "hmat_b200_leaf_count": (C.c_int, [_P]),
+        "hmat_b200_leaf_table": (C.c_int, [_P, _P]),
+        "hmat_b200_leaf_payload": (C.c_longlong, [_P, C.c_int, _P]),
+        "hmat_b200_leaf_arenas": (C.c_int, [_P, C.POINTER(_P), C.POINTER(C.c_longlong), C.POINTER(_P),
+                                            C.POINTER(C.c_longlong), _P]),
+        "hmat_b200_leaf_gradients": (C.c_int, [_P, _P, _P, C.c_int, _P, _P, C.c_int, _P]),
+        "hmat_b200_phase_times": (C.c_int, [_P, _P]),
+        "hmat_b200_gemv_profile": (C.c_int, [_P, C.c_char, _P, _P, C.c_int, _P, _P]),
+        "hmat_b200_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+class HMatError(RuntimeError):
+    pass
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        msg = load_library().hmat_b200_last_error().decode()
+        raise HMatError(f"{what} failed: {msg}")
+
+
+def get_parameters() -> Settings:
+    s = Settings()
+    load_library().hmat_get_parameters(C.byref(s))
+    return s
+
+
+def set_parameters(**kw):
+    s = get_parameters()
+    for k, v in kw.items():
+        setattr(s, k, v)
+    _check(load_library().hmat_set_parameters(C.byref(s)), "hmat_set_parameters")
+
+
+class HMatInterface:
+    """The function table of one value type (hmat_init_default_interface)."""
+
+    def __init__(self, value_type: int):
+        lib = load_library()
+        self.value_type = value_type
+        self.table = InterfaceTable()
+        lib.hmat_init_default_interface(C.byref(self.table), value_type)
+        self._fns = {}
+
+    def fn(self, slot: str):
+        if slot not in self._fns:
+            self._fns[slot] = _PROTOS[slot](getattr(self.table, slot))
+        return self._fns[slot]
+
+    def create_empty_hmatrix_admissibility(self, rows_tree, cols_tree, lower_symmetric, cond):
+        return self.fn("create_empty_hmatrix_admissibility")(rows_tree, cols_tree, lower_symmetric, cond)
+
+    def set_low_rank_epsilon(self, m, eps):
+        self.fn("set_low_rank_epsilon")(m, eps)
+
+    def assemble_generic(self, m, ctx: AssembleContext) -> int:
+        return self.fn("assemble_generic")(m, C.byref(ctx))
+
+    def gemv(self, trans, alpha, m, x, beta, y, nrhs) -> int:
+        return self.fn("gemv")(trans, alpha, m, x, beta, y, nrhs)
+
+    def get_info(self, m) -> Info:
+        info = Info()
+        _check(self.fn("get_info")(m, C.byref(info)), "get_info")
+        return info
+
+    def destroy(self, m) -> int:
+        return self.fn("destroy")(m)
+
+
+class HMatrix:
+    """One H-matrix on the B200 engine, built the way the reference's examples build theirs:
+    median clustering with a maximum leaf size, standard admissibility, ACA+ compression at
+    `epsilon`, low-rank epsilon `low_rank_epsilon` (defaults to `epsilon`)."""
+
+    def __init__(self, points: np.ndarray, kernel: KernelDesc, *, value_type: int = HMAT_DOUBLE_PRECISION,
+                 leaf_size: int = 64, eta: float = 2.0, epsilon: float = 1e-4, low_rank_epsilon: float | None = None,
+                 compression: str = "aca_plus", assemble: bool = True, leaf_size_cols: int | None = None):
+        lib = load_library()
+        self.lib = lib
+        self.points = np.ascontiguousarray(points, dtype=np.float64)
+        self.n = int(self.points.shape[0])
+        self.value_type = value_type
+        self.dtype = DTYPES[value_type]
+        self.hi = HMatInterface(value_type)
+        self._median = lib.hmat_create_clustering_median()
+        self._algo = lib.hmat_create_clustering_max_dof(self._median, leaf_size)
+        self.tree = lib.hmat_create_cluster_tree(self.points.ctypes.data, 3, self.n, self._algo)
+        if not self.tree:
+            raise HMatError("hmat_create_cluster_tree failed: " + lib.hmat_b200_last_error().decode())
+        self._algo_c = self.tree_cols = None
+        if leaf_size_cols:
+            self._algo_c = lib.hmat_create_clustering_max_dof(self._median, leaf_size_cols)
+            self.tree_cols = lib.hmat_create_cluster_tree(self.points.ctypes.data, 3, self.n, self._algo_c)
+        self._adm = lib.hmat_create_admissibility_standard(eta)
+        self.m = self.hi.create_empty_hmatrix_admissibility(self.tree, self.tree_cols or self.tree, 0, self._adm)
+        if not self.m:
+            raise HMatError("create_empty_hmatrix_admissibility failed: " + lib.hmat_b200_last_error().decode())
+        self.hi.set_low_rank_epsilon(self.m, epsilon if low_rank_epsilon is None else low_rank_epsilon)
+        make = {"aca_plus": lib.hmat_create_compression_aca_plus,
+                "aca_partial": lib.hmat_create_compression_aca_partial,
+                "svd": lib.hmat_create_compression_svd}[compression]
+        self._comp = make(epsilon)
+        self._kernel = kernel
+        self._assembly = lib.hmat_b200_create_assembly(C.byref(kernel), self.points.ctypes.data, self.n)
+        if not self._assembly:
+            raise HMatError("hmat_b200_create_assembly failed: " + lib.hmat_b200_last_error().decode())
+        if assemble:
+            self.assemble()
+
+    # -- reference-shaped operations --
+    def assemble(self):
+        ctx = AssembleContext()
+        self.lib.hmat_assemble_context_init(C.byref(ctx))
+        ctx.assembly = self._assembly
+        ctx.compression = self._comp
+        ctx.factorization = hmat_factorization_none
+        _check(self.hi.assemble_generic(self.m, ctx), "assemble_generic")
+
+    def gemv(self, x: np.ndarray, trans: str = "N", alpha=1.0, beta=0.0, y: np.ndarray | None = None) -> np.ndarray:
+        """y = alpha op(H) x + beta y through the C table's gemv (host buffers)."""
+        x = np.asfortranarray(x, dtype=self.dtype)
+        nrhs = 1 if x.ndim == 1 else x.shape[1]
+        if y is None:
+            y = np.zeros_like(x)
+        else:
+            y = np.asfortranarray(y, dtype=self.dtype).copy()
+        a = np.array([alpha], dtype=self.dtype)
+        b = np.array([beta], dtype=self.dtype)
+        _check(self.hi.gemv(trans.encode(), a.ctypes.data, self.m, x.ctypes.data, b.ctypes.data, y.ctypes.data,
+                            nrhs), "gemv")
+        return y
+
+    def gemv_device(self, x_ptr: int, y_ptr: int, nrhs: int, trans: str = "N", alpha=1.0, beta=0.0, stream=0):
+        a = np.array([alpha], dtype=self.dtype)
+        b = np.array([beta], dtype=self.dtype)
+        _check(self.lib.hmat_b200_gemv_device(self.m, trans.encode(), a.ctypes.data, C.c_void_p(x_ptr),
+                                              b.ctypes.data, C.c_void_p(y_ptr), nrhs, C.c_void_p(stream)),
+               "hmat_b200_gemv_device")
+
+    def info(self) -> dict:
+        return self.hi.get_info(self.m).as_dict()
+
+    def perm(self, cols: bool = False) -> np.ndarray:
+        p = self.lib.hmat_cluster_get_indices(self.tree_cols if (cols and self.tree_cols) else self.tree)
+        return np.ctypeslib.as_array(p, shape=(self.n,)).copy()
+
+    def leaf_table(self) -> np.ndarray:
+        n = self.lib.hmat_b200_leaf_count(self.m)
+        out = np.zeros((n, 6), dtype=np.int32)
+        _check(self.lib.hmat_b200_leaf_table(self.m, out.ctypes.data), "hmat_b200_leaf_table")
+        return out
+
+    def leaf_payload(self, i: int) -> np.ndarray:
+        r0, m, c0, n, t, k = self.leaf_table()[i]
+        size = m * n if t == 0 else max(k, 0) * (m + n)
+        out = np.zeros(max(size, 1), dtype=self.dtype)
+        got = self.lib.hmat_b200_leaf_payload(self.m, i, out.ctypes.data)
+        if got < 0:
+            raise HMatError("hmat_b200_leaf_payload failed")
+        return out[:got]
+
+    def leaf_block(self, i: int) -> np.ndarray:
+        """The dense block of leaf i (F, or A B^T), in cluster numbering."""
+        r0, m, c0, n, t, k = self.leaf_table()[i]
+        p = self.leaf_payload(i)
+        if t == 0:
+            return p.reshape(n, m).T
+        if k <= 0:
+            return np.zeros((m, n), dtype=self.dtype)
+        A = p[:k * m].reshape(k, m).T
+        B = p[k * m:].reshape(k, n).T
+        return A @ B.T
+
+    def arenas(self):
+        n = self.lib.hmat_b200_leaf_count(self.m)
+        full, rk = C.c_void_p(), C.c_void_p()
+        fe, re = C.c_longlong(), C.c_longlong()
+        offs = np.zeros(n, dtype=np.int64)
+        _check(self.lib.hmat_b200_leaf_arenas(self.m, C.byref(full), C.byref(fe), C.byref(rk), C.byref(re),
+                                              offs.ctypes.data), "hmat_b200_leaf_arenas")
+        return (full.value or 0, fe.value, rk.value or 0, re.value, offs)
+
+    def leaf_gradients(self, x_ptr, r_ptr, nrhs, gfull_ptr, grk_ptr, accumulate=False, stream=0):
+        _check(self.lib.hmat_b200_leaf_gradients(self.m, C.c_void_p(x_ptr), C.c_void_p(r_ptr), nrhs,
+                                                 C.c_void_p(gfull_ptr), C.c_void_p(grk_ptr), int(accumulate),
+                                                 C.c_void_p(stream)), "hmat_b200_leaf_gradients")
+
+    def gemv_profile(self, x_ptr: int, y_ptr: int, nrhs: int, trans: str = "N"):
+        ms = np.zeros(3)
+        by = np.zeros(3)
+        _check(self.lib.hmat_b200_gemv_profile(self.m, trans.encode(), C.c_void_p(x_ptr), C.c_void_p(y_ptr), nrhs,
+                                               ms.ctypes.data, by.ctypes.data), "hmat_b200_gemv_profile")
+        return {"ms": dict(zip(("gather", "zphase", "yphase"), ms)),
+                "bytes": dict(zip(("gather", "zphase", "yphase"), by))}
+
+    def phase_times(self) -> dict:
+        out = np.zeros(4, dtype=np.float64)
+        _check(self.lib.hmat_b200_phase_times(self.m, out.ctypes.data), "hmat_b200_phase_times")
+        return {"full_ms": out[0], "aca_ms": out[1], "truncate_ms": out[2], "gemv_ms": out[3]}
+
+    def gemv_bytes(self, nrhs: int) -> int:
+        """Algorithmic bytes of one product: every stored leaf scalar read once, x read and
+        y written once."""
+        t = self.leaf_table()
+        s = np.dtype(self.dtype).itemsize
+        full = t[t[:, 4] == 0]
+        rk = t[(t[:, 4] == 1) & (t[:, 5] > 0)]
+        stored = int((full[:, 1].astype(np.int64) * full[:, 3]).sum() +
+                     (rk[:, 5].astype(np.int64) * (rk[:, 1] + rk[:, 3])).sum())
+        return stored * s + 2 * self.n * nrhs * s
+
+    def close(self):
+        lib = self.lib
+        if getattr(self, "m", None):
+            self.hi.destroy(self.m)
+            self.m = None
+        for attr, fn in (("_assembly", lib.hmat_b200_delete_assembly), ("_comp", lib.hmat_delete_compression),
+                         ("_adm", lib.hmat_delete_admissibility), ("tree", lib.hmat_delete_cluster_tree),
+                         ("tree_cols", lib.hmat_delete_cluster_tree), ("_algo", lib.hmat_delete_clustering),
+                         ("_algo_c", lib.hmat_delete_clustering), ("_median", lib.hmat_delete_clustering)):
+            v = getattr(self, attr, None)
+            if v:
+                fn(v)
+                setattr(self, attr, None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def kernel(kind: int, delta: float = 0.01, ell: float = 0.3, nugget: float = 0.0, wavenumber: float = 0.0):
+    return KernelDesc(kind, delta, ell, nugget, wavenumber)

@@ -1,0 +1,428 @@
+// Batched ACA+ compression of admissible leaves, one CTA per leaf, persistent grid fed
+// by a device work counter over leaves sorted by decreasing cost.
+//
+// The control flow is hmat-oss's doCompressionAcaPlus (compression.cpp:553-724) with its
+// helpers findCol / findMinRow / findMinCol / updateRow / updateCol (compression.cpp:81-220)
+// and the partial-ACA delegate doCompressionAcaPartial (compression.cpp:382-533), taken
+// when cols * 100 < rows (compression.cpp:557-560).  Pivot selection keeps the BLAS
+// i?amax rule (first index of the largest |x|, |Re|+|Im| for complex) and the
+// strict-minimum / strict-maximum first-index rules of the scalar loops, so the FP64
+// engine picks the reference's pivots.  Residual updates are per-element sequential in
+// the rank index with one FMA per term, like the axpy sequence they restate.
+//
+// Vectors of a leaf live in its workspace slot (global memory, L1/L2 resident while the
+// CTA works on it); FP64 accumulators carry the Frobenius-norm estimate for every T.
+#include "block_reduce.cuh"
+#include "kernels.h"
+
+namespace hmatb200 {
+namespace {
+
+constexpr int kAcaThreads = 128;
+
+template <typename T>
+struct Aca {
+  typedef typename Traits<T>::wide W;
+  KernelParams kp;
+  Points P;
+  int row_off, m, col_off, n, kcap;
+  T* A;  // m x kcap
+  T* B;  // n x kcap
+  T* aRef;
+  T* bRef;
+  unsigned char* rowFree;
+  unsigned char* colFree;
+  T* coef;  // shared [kcap]
+  W* da;    // shared [kcap]
+  W* db;    // shared [kcap]
+  RedScratch* rs;
+
+  __device__ T entry(int i, int j) const { return KernelEval<T>::eval(kp, P, row_off + i, col_off + j); }
+
+  // out[j] = K(i, j) - sum_{l<k} A[i, l] B[j, l]   (getRow + updateRow)
+  __device__ void fill_row(int i, int k, T* out) {
+    __syncthreads();
+    for (int l = threadIdx.x; l < k; l += blockDim.x) coef[l] = -A[(size_t)l * m + i];
+    __syncthreads();
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      T v = entry(i, j);
+      for (int l = 0; l < k; ++l) v = fmadd(coef[l], B[(size_t)l * n + j], v);
+      out[j] = v;
+    }
+    __syncthreads();
+  }
+  // out[i] = K(i, j) - sum_{l<k} B[j, l] A[i, l]   (getCol + updateCol)
+  __device__ void fill_col(int j, int k, T* out) {
+    __syncthreads();
+    for (int l = threadIdx.x; l < k; l += blockDim.x) coef[l] = -B[(size_t)l * n + j];
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      T v = entry(i, j);
+      for (int l = 0; l < k; ++l) v = fmadd(coef[l], A[(size_t)l * m + i], v);
+      out[i] = v;
+    }
+    __syncthreads();
+  }
+  __device__ void scale(T* v, int len, T s) {
+    for (int e = threadIdx.x; e < len; e += blockDim.x) v[e] = v[e] * s;
+    __syncthreads();
+  }
+  // v += a * x
+  __device__ void axpy(T a, const T* x, T* v, int len) {
+    for (int e = threadIdx.x; e < len; e += blockDim.x) v[e] = fmadd(a, x[e], v[e]);
+    __syncthreads();
+  }
+  __device__ bool is_zero(const T* v, int len) {
+    bool nz = false;
+    for (int e = threadIdx.x; e < len; e += blockDim.x) nz |= !is_zero_val(v[e]);
+    return !block_any(nz, *rs);
+  }
+  __device__ int iamax(const T* v, int len) {
+    KeyIdx b{-1.0, -1};
+    for (int e = threadIdx.x; e < len; e += blockDim.x) {
+      double kk = amax_key(v[e]);
+      if (kk > b.key) { b.key = kk; b.idx = e; }
+    }
+    return block_arg<true>(b, *rs).idx;
+  }
+  // first index of the strict minimum of |v|^2 over free entries (DBL_MAX start)
+  __device__ int argmin_free(const T* v, const unsigned char* fr, int len) {
+    KeyIdx b{DBL_MAX, -1};
+    for (int e = threadIdx.x; e < len; e += blockDim.x) {
+      if (fr[e]) {
+        double kk = abs2(v[e]);
+        if (kk < b.key) { b.key = kk; b.idx = e; }
+      }
+    }
+    return block_arg<false>(b, *rs).idx;
+  }
+  // first index of the strict maximum of |v|^2 over free entries (0 start), -1 if none
+  __device__ int argmax_free_pos(const T* v, const unsigned char* fr, int len) {
+    KeyIdx b{0.0, -1};
+    for (int e = threadIdx.x; e < len; e += blockDim.x) {
+      if (fr[e]) {
+        double kk = abs2(v[e]);
+        if (kk > b.key) { b.key = kk; b.idx = e; }
+      }
+    }
+    return block_arg<true>(b, *rs).idx;
+  }
+  __device__ void clear_flag(unsigned char* fr, int idx) {
+    __syncthreads();
+    if (threadIdx.x == 0) fr[idx] = 0;
+    __syncthreads();
+  }
+
+  // findCol: first free column that is not identically zero (raw, not updated)
+  __device__ int find_col(T* out) {
+    for (int j = 0; j < n; ++j) {
+      if (colFree[j]) {
+        fill_col(j, 0, out);
+        clear_flag(colFree, j);
+        if (!is_zero(out, m)) return j;
+      }
+    }
+    return -1;
+  }
+  __device__ int find_min_row(int k, const T* ref, T* out) {
+    for (;;) {
+      int i = argmin_free(ref, rowFree, m);
+      if (i < 0) return -1;
+      fill_row(i, k, out);
+      clear_flag(rowFree, i);
+      if (!is_zero(out, n)) return i;
+    }
+  }
+  __device__ int find_min_col(int k, const T* ref, T* out) {
+    for (;;) {
+      int j = argmin_free(ref, colFree, n);
+      if (j < 0) return -1;
+      fill_col(j, k, out);
+      clear_flag(colFree, j);
+      if (!is_zero(out, m)) return j;
+    }
+  }
+
+  // Gram terms of the new pair (a_k, b_k) against the previous ones, in FP64:
+  // returns ||a_k||^2 ||b_k||^2 and adds 2 sum_l Re(<a_k,a_l><b_k,b_l>) + that to est.
+  __device__ double update_estimate(int k, double& est) {
+    const T* a = A + (size_t)k * m;
+    const T* b = B + (size_t)k * n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __shared__ double s_norm[2];
+    for (int t = warp; t < 2 * k + 2; t += nw) {
+      const bool isA = (t < k) || (t == 2 * k);
+      const T* x = isA ? a : b;
+      const T* y = t < k ? A + (size_t)t * m : (t < 2 * k ? B + (size_t)(t - k) * n : x);
+      const int len = isA ? m : n;
+      W acc = zero<W>();
+      for (int e = lane; e < len; e += 32) acc = acc + widen(conjg(x[e])) * widen(y[e]);
+      acc = warp_sum(acc);
+      if (lane == 0) {
+        if (t < k) da[t] = acc;
+        else if (t < 2 * k) db[t - k] = acc;
+        else s_norm[t - 2 * k] = real_part(acc);
+      }
+    }
+    __syncthreads();
+    double ne = 0.0;
+    for (int l = 0; l < k; ++l) ne += real_part(da[l] * db[l]);
+    est += 2.0 * ne;
+    double ab = s_norm[0] * s_norm[1];
+    est += ab;
+    __syncthreads();
+    return ab;
+  }
+
+  __device__ void init_flags() {
+    for (int e = threadIdx.x; e < m; e += blockDim.x) rowFree[e] = 1;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) colFree[e] = 1;
+    __syncthreads();
+  }
+
+  // doCompressionAcaPartial, no random pivots.  Returns the rank; sets *overflow when the
+  // slot capacity is reached first.
+  __device__ int partial(double eps, bool* overflow) {
+    const int maxK = min(m, n);
+    init_flags();
+    double est = 0.0;
+    int row_index = 0, J = 0, k = 0, rowPivotCount = 0;
+    do {
+      if (k >= kcap) { *overflow = true; break; }
+      T* bCol = B + (size_t)k * n;
+      fill_row(row_index, k, bCol);
+      clear_flag(rowFree, row_index);
+      int jj = argmax_free_pos(bCol, colFree, n);
+      if (jj >= 0) J = jj;
+      T bj = bCol[J];
+      if (is_zero_val(bj)) {
+        row_index = 0;
+        while (row_index < m && !rowFree[row_index]) row_index++;
+      } else {
+        scale(bCol, n, recip(bj));
+        T* aCol = A + (size_t)k * m;
+        fill_col(J, k, aCol);
+        clear_flag(colFree, J);
+        int ii = argmax_free_pos(aCol, rowFree, m);
+        if (ii >= 0) row_index = ii;
+        double ab = update_estimate(k, est);
+        k++;
+        if (ab < eps * eps * est) break;
+      }
+      rowPivotCount++;
+    } while (rowPivotCount < maxK && row_index < m);
+    return k;
+  }
+
+  // doCompressionAcaPlus.
+  __device__ int plus(double eps, bool* overflow) {
+    const int maxK = min(m, n);
+    init_flags();
+    double est = 0.0;
+    int k = 0;
+    int j_ref = find_col(aRef);
+    if (j_ref < 0) return 0;
+    int i_ref = find_min_row(0, aRef, bRef);
+    if (i_ref < 0) return 0;  // cannot happen once a non-zero column exists; keeps indices valid
+    do {
+      if (k >= kcap) { *overflow = true; break; }
+      T* aVec = A + (size_t)k * m;
+      T* bVec = B + (size_t)k * n;
+      KeyIdx ka{-1.0, -1}, kb{-1.0, -1};
+      for (int e = threadIdx.x; e < m; e += blockDim.x) {
+        double kk = amax_key(aRef[e]);
+        if (kk > ka.key) { ka.key = kk; ka.idx = e; }
+      }
+      for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        double kk = amax_key(bRef[e]);
+        if (kk > kb.key) { kb.key = kk; kb.idx = e; }
+      }
+      block_argmax2(ka, kb, *rs);
+      int i_star = ka.idx, j_star = kb.idx;
+      if (abs2(aRef[i_star]) > abs2(bRef[j_star])) {
+        fill_row(i_star, k, bVec);
+        j_star = iamax(bVec, n);
+        T pivot = bVec[j_star];
+        fill_col(j_star, k, aVec);
+        if (!is_zero_val(pivot)) scale(aVec, m, recip(pivot));
+      } else {
+        fill_col(j_star, k, aVec);
+        i_star = iamax(aVec, m);
+        T pivot = aVec[i_star];
+        fill_row(i_star, k, bVec);
+        if (!is_zero_val(pivot)) scale(bVec, n, recip(pivot));
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        rowFree[i_star] = 0;
+        colFree[j_star] = 0;
+      }
+      double ab = update_estimate(k, est);
+      k++;
+      if (ab < eps * eps * est) break;
+
+      // aRef -= b_k[j_ref] a_k ; bRef -= a_k[i_ref] b_k
+      T ca = -bVec[j_ref];
+      T cb = -aVec[i_ref];
+      axpy(ca, aVec, aRef, m);
+      axpy(cb, bVec, bRef, n);
+      const bool needNewA = (j_star == j_ref) || is_zero(aRef, m);
+      const bool needNewB = (i_star == i_ref) || is_zero(bRef, n);
+      if (needNewA && needNewB) {
+        bool found = false;
+        while (!found) {
+          j_ref = find_col(aRef);
+          if (j_ref < 0) break;
+          fill_col(j_ref, k, aRef);
+          found = !is_zero(aRef, m);
+        }
+        if (!found) break;
+        i_ref = find_min_row(k, aRef, bRef);
+        if (i_ref < 0) break;
+      } else if (needNewB) {
+        i_ref = find_min_row(k, aRef, bRef);
+        if (i_ref < 0) break;
+      } else if (needNewA) {
+        j_ref = find_min_col(k, bRef, aRef);
+        if (j_ref < 0) break;
+      }
+    } while (k < maxK);
+    return k;
+  }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kAcaThreads) aca_kernel(const RkLeafDesc* __restrict__ leaves,
+                                                          const int* __restrict__ order, int nleaves,
+                                                          KernelParams kp, Points pts, double eps, T* ws,
+                                                          unsigned char* flags, int* ranks, int* status,
+                                                          int* counter, int kcap_max) {
+  typedef typename Traits<T>::wide W;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  W* da = reinterpret_cast<W*>(smem_raw);
+  W* db = da + kcap_max;
+  T* coef = reinterpret_cast<T*>(db + kcap_max);
+  __shared__ RedScratch rs;
+  __shared__ int s_item;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= nleaves) break;
+    const int leaf = order[item];
+    const RkLeafDesc d = leaves[leaf];
+    Aca<T> c;
+    c.kp = kp;
+    c.P = pts;
+    c.row_off = d.row_off;
+    c.m = d.m;
+    c.col_off = d.col_off;
+    c.n = d.n;
+    c.kcap = d.kcap;
+    T* slot = ws + d.ws_off;
+    c.A = slot;
+    c.B = slot + (size_t)d.m * d.kcap;
+    c.aRef = c.B + (size_t)d.n * d.kcap;
+    c.bRef = c.aRef + d.m;
+    c.rowFree = flags + d.fl_off;
+    c.colFree = c.rowFree + d.m;
+    c.coef = coef;
+    c.da = da;
+    c.db = db;
+    c.rs = &rs;
+    bool overflow = false;
+    int k;
+    if (d.n * 100 < d.m) k = c.partial(eps, &overflow);
+    else k = c.plus(eps, &overflow);
+    if (threadIdx.x == 0) {
+      ranks[leaf] = k;
+      status[leaf] = overflow ? kLeafAcaCapacity : kLeafOk;
+    }
+  }
+}
+
+// Dense-SVD compression of small admissible blocks (doCompressionSVD, compression.cpp:241-251):
+// the block M is written into the slot as a trivially exact factorisation M = A B^T
+// (A = M, B = I when m >= n; A = I, B = M^T otherwise, rank min(m, n)), so the truncation
+// phase, whose core is the SVD of Ra Rb^T, computes the truncated SVD of M.
+template <typename T>
+__global__ void dense_to_rk_kernel(const RkLeafDesc* __restrict__ leaves, const int* __restrict__ order,
+                                   int nleaves, KernelParams kp, Points pts, T* ws, int* ranks, int* status) {
+  const int item = blockIdx.x;
+  if (item >= nleaves) return;
+  const int leaf = order[item];
+  const RkLeafDesc d = leaves[leaf];
+  const int m = d.m, n = d.n, k = min(m, n);
+  T* A = ws + d.ws_off;
+  T* B = A + (size_t)m * d.kcap;
+  if (d.kcap < k) {
+    if (threadIdx.x == 0) {
+      ranks[leaf] = 0;
+      status[leaf] = kLeafBadShape;
+    }
+    return;
+  }
+  for (int e = threadIdx.x; e < m * n; e += blockDim.x) {
+    const int i = e % m, j = e / m;
+    const T v = KernelEval<T>::eval(kp, pts, d.row_off + i, d.col_off + j);
+    if (m >= n) A[(size_t)j * m + i] = v;  // A = M (m x n)
+    else B[(size_t)i * n + j] = v;         // B = M^T (n x m)
+  }
+  if (m >= n) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) B[e] = (e % (n + 1) == 0) ? one<T>() : zero<T>();
+  } else {
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) A[e] = (e % (m + 1) == 0) ? one<T>() : zero<T>();
+  }
+  if (threadIdx.x == 0) {
+    ranks[leaf] = k;
+    status[leaf] = kLeafOk;
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_dense_to_rk(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, const KernelParams& kp,
+                        Points pts, T* ws, int* ranks, int* status, cudaStream_t s) {
+  if (nleaves <= 0) return;
+  dense_to_rk_kernel<T><<<nleaves, 256, 0, s>>>(d_leaves, d_order, nleaves, kp, pts, ws, ranks, status);
+}
+
+int persistent_grid(int blocks_per_sm) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms * blocks_per_sm;
+}
+
+template <typename T>
+void launch_aca(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, const KernelParams& kp, Points pts,
+                double epsilon, T* ws, unsigned char* flags, int* ranks, int* status, int* counter, int kcap_max,
+                int grid, cudaStream_t s) {
+  if (nleaves <= 0) return;
+  typedef typename Traits<T>::wide W;
+  size_t smem = (size_t)kcap_max * (2 * sizeof(W) + sizeof(T));
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(aca_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int g = grid < nleaves ? grid : nleaves;
+  aca_kernel<T><<<g, kAcaThreads, smem, s>>>(d_leaves, d_order, nleaves, kp, pts, epsilon, ws, flags, ranks,
+                                             status, counter, kcap_max);
+}
+
+#define HB_INST(T)                                                                                           \
+  template void launch_aca<T>(const RkLeafDesc*, const int*, int, const KernelParams&, Points, double, T*, \
+                              unsigned char*, int*, int*, int*, int, int, cudaStream_t);                    \
+  template void launch_dense_to_rk<T>(const RkLeafDesc*, const int*, int, const KernelParams&, Points, T*, \
+                                      int*, int*, cudaStream_t);
+HB_INST(float)
+HB_INST(double)
+HB_INST(cfloat)
+HB_INST(cdouble)
+#undef HB_INST
+
+}  // namespace hmatb200

@@ -1,0 +1,43 @@
+// Dense assembly of the non-admissible (full) leaves: every entry of every full leaf is
+// one kernel evaluation, written once, column-major, into the full-leaf arena.  Restates
+// the full branch of AssemblyFunction::assemble / SimpleFunction::assemble
+// (assembly.cpp:66-91) with the interaction evaluated on the device.
+#include "kernels.h"
+
+namespace hmatb200 {
+namespace {
+
+template <typename T>
+__global__ void __launch_bounds__(256) assemble_full_kernel(const FullLeafDesc* __restrict__ leaves, int nleaves,
+                                                            KernelParams kp, Points pts, T* __restrict__ arena) {
+  for (int leaf = blockIdx.x; leaf < nleaves; leaf += gridDim.x) {
+    const FullLeafDesc d = leaves[leaf];
+    T* F = arena + d.off;
+    const int mn = d.m * d.n;
+    for (int e = threadIdx.x; e < mn; e += blockDim.x) {
+      const int i = e % d.m, j = e / d.m;
+      F[e] = KernelEval<T>::eval(kp, pts, d.row_off + i, d.col_off + j);
+    }
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_assemble_full(const FullLeafDesc* d_leaves, int nleaves, const KernelParams& kp, Points pts,
+                          T* arena, cudaStream_t s) {
+  if (nleaves <= 0) return;
+  int grid = persistent_grid(8);
+  if (grid > nleaves) grid = nleaves;
+  assemble_full_kernel<T><<<grid, 256, 0, s>>>(d_leaves, nleaves, kp, pts, arena);
+}
+
+#define HB_INST(T) \
+  template void launch_assemble_full<T>(const FullLeafDesc*, int, const KernelParams&, Points, T*, cudaStream_t);
+HB_INST(float)
+HB_INST(double)
+HB_INST(cfloat)
+HB_INST(cdouble)
+#undef HB_INST
+
+}  // namespace hmatb200

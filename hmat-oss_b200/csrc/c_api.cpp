@@ -1,0 +1,643 @@
+// C ABI of the B200 engine: the hmat-oss C entry points on the leaf-level path (same
+// names, argument meaning and 0 / non-zero return convention as c_default_interface.cpp
+// and c_wrapping.hpp) plus the hmat_b200_* extensions declared in include/hmat_b200.h.
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "hmat_b200.h"
+#include "host.h"
+
+using namespace hmatb200;
+
+struct hmat_clustering_algorithm {
+  ClusteringAlgo a;
+};
+struct hmat_cluster_tree_struct {
+  std::unique_ptr<ClusterTree> t;
+};
+struct hmat_admissibility_condition {
+  Admissibility a;
+};
+struct hmat_compression_algorithm_struct {
+  hmat_compress_t method;
+  double eps;
+};
+struct hmat_matrix_struct {
+  int vt = 1;
+  const hmat_cluster_tree_t* rows_h = nullptr;
+  const hmat_cluster_tree_t* cols_h = nullptr;
+  bool own_rows = false, own_cols = false;
+  BlockTree bt;
+  double low_rank_eps = 1e-4;  // LocalSettings default (h_matrix.cpp:151)
+  std::unique_ptr<EngineBase> engine;
+};
+
+namespace {
+
+const unsigned kAssemblyMagic = 0xB200A55Eu;
+struct AssemblyObj {
+  unsigned magic = kAssemblyMagic;
+  AssemblyDesc d;
+};
+
+thread_local std::string g_last_error;
+
+// Global settings with the reference's defaults (hmat_cpp_interface.hpp:88-95).
+hmat_settings_t g_settings = {100, 1e-4, 200, 0, 0, 0, 0, 0, 0, 0, 0.0};
+
+// The device side of a matrix is created on first use, so that the host-only parts
+// (clustering, block tree, leaf table) work without a GPU.
+EngineBase& engine_of(hmat_matrix_t* m) {
+  if (!m->engine) m->engine = make_engine(m->vt, m->rows_h->t.get(), m->cols_h->t.get(), &m->bt);
+  return *m->engine;
+}
+
+int leaf_rank(const hmat_matrix_t* m, size_t i) {
+  if (m->engine) return m->engine->ranks[i];
+  return m->bt.leaves[i].type == 1 ? 0 : -1;
+}
+
+int fail(const char* where, const std::string& msg) {
+  g_last_error = std::string(where) + ": " + msg;
+  fprintf(stderr, "%s\n", g_last_error.c_str());
+  return 1;
+}
+
+#define HB_TRY(where, ...)            \
+  try {                               \
+    __VA_ARGS__;                      \
+  } catch (const std::exception& e) { \
+    return fail(where, e.what());     \
+  }
+
+
+// ---- table entries on the path ----
+
+hmat_matrix_t* create_empty(const hmat_cluster_tree_t* rows, const hmat_cluster_tree_t* cols, int lower_sym,
+                            hmat_admissibility_t* cond, int vt) {
+  try {
+    if (!rows || !cols || !cond) throw Error("null argument");
+    if (lower_sym) throw Error("lower-symmetric storage is not supported by the B200 engine");
+    std::unique_ptr<hmat_matrix_t> m(new hmat_matrix_t());
+    m->vt = vt;
+    m->rows_h = rows;
+    m->cols_h = cols;
+    m->bt = build_block_tree(*rows->t, *cols->t, cond->a);
+    return m.release();
+  } catch (const std::exception& e) {
+    fail("create_empty_hmatrix_admissibility", e.what());
+    return nullptr;
+  }
+}
+template <int VT>
+hmat_matrix_t* create_empty_t(const hmat_cluster_tree_t* rows, const hmat_cluster_tree_t* cols, int lower_sym,
+                              hmat_admissibility_t* cond) {
+  return create_empty(rows, cols, lower_sym, cond, VT);
+}
+
+void own_cluster_trees(hmat_matrix_t* m, int owns_row, int owns_col) {
+  if (!m) return;
+  m->own_rows = owns_row != 0;
+  m->own_cols = owns_col != 0;
+}
+
+void set_low_rank_epsilon(hmat_matrix_t* m, double eps) {
+  if (m) m->low_rank_eps = eps;
+}
+
+int assemble_generic(hmat_matrix_t* m, hmat_assemble_context_t* ctx) {
+  HB_TRY("assemble_generic", {
+    if (!m || !ctx) throw Error("null argument");
+    if (ctx->lower_symmetric) throw Error("lower-symmetric assembly is not supported by the B200 engine");
+    if (!ctx->compression) throw Error("No compression algorithm defined in hmat_assemble_context_t");
+    if (ctx->factorization != hmat_factorization_none)
+      throw Error("factorization is outside the B200 engine's path");
+    if (ctx->simple_compute || ctx->block_compute || ctx->advanced_compute)
+      throw Error("host interaction callbacks cannot run on the device; pass hmat_b200_create_assembly() in "
+                  "the 'assembly' field");
+    const AssemblyObj* a = (const AssemblyObj*)ctx->assembly;
+    if (!a || a->magic != kAssemblyMagic) throw Error("'assembly' is not a descriptor from hmat_b200_create_assembly");
+    int method;
+    switch (ctx->compression->method) {
+      case hmat_compress_aca_plus: method = 0; break;
+      case hmat_compress_aca_partial: method = 1; break;
+      default: throw Error("only ACA+ and partial-ACA compression are implemented by the B200 engine");
+    }
+    const int svd_below = g_settings.compressionMinLeafSize;
+    engine_of(m).assemble(a->d, method, ctx->compression->eps, m->low_rank_eps, svd_below);
+  });
+  return 0;
+}
+
+int destroy(hmat_matrix_t* m) {
+  if (!m) return 0;
+  const hmat_cluster_tree_t* r = m->own_rows ? m->rows_h : nullptr;
+  const hmat_cluster_tree_t* c = m->own_cols ? m->cols_h : nullptr;
+  delete m;
+  if (r) hmat_delete_cluster_tree(r);
+  if (c && c != r) hmat_delete_cluster_tree(c);
+  return 0;
+}
+
+int gemv(char trans, void* alpha, hmat_matrix_t* m, void* x, void* beta, void* y, int nrhs) {
+  HB_TRY("gemv", {
+    if (!m || !alpha || !beta || (nrhs > 0 && (!x || !y))) throw Error("null argument");
+    engine_of(m).gemv_host(trans, alpha, x, beta, y, nrhs);
+  });
+  return 0;
+}
+
+template <int VT>
+int gemv_t(char trans, void* alpha, hmat_matrix_t* m, void* x, void* beta, void* y, int nrhs) {
+  if (m && m->vt != VT) return fail("gemv", "matrix value type does not match this interface");
+  return gemv(trans, alpha, m, x, beta, y, nrhs);
+}
+
+template <typename T>
+void permute(T* v, const std::vector<int>& idx, int rows, int cols, int axis, bool restore) {
+  const int n = axis == 0 ? rows : cols;
+  std::vector<T> tmp(n);
+  const int outer = axis == 0 ? cols : rows;
+  for (int o = 0; o < outer; ++o) {
+    for (int i = 0; i < n; ++i) {
+      size_t a = axis == 0 ? (size_t)o * rows + i : (size_t)i * rows + o;
+      size_t b = axis == 0 ? (size_t)o * rows + idx[i] : (size_t)idx[i] * rows + o;
+      if (restore) tmp[idx[i]] = v[a];
+      else tmp[i] = v[b];
+    }
+    for (int i = 0; i < n; ++i) v[axis == 0 ? (size_t)o * rows + i : (size_t)i * rows + o] = tmp[i];
+  }
+}
+
+// reorderVector / restoreVectorOrder over a rows x cols column-major array
+// (h_matrix.cpp:75-141, c_wrapping.hpp:455-500).
+template <typename T>
+int reorder_impl(void* vec, const hmat_cluster_tree_t* rct, int rows, const hmat_cluster_tree_t* cct, int cols,
+                 bool restore) {
+  HB_TRY(restore ? "vector_restore" : "vector_reorder", {
+    if (!rct && rows == 0) throw Error("either row cluster tree or rows must be non null");
+    if (!cct && cols == 0) throw Error("either col cluster tree or cols must be non null");
+    const int nr = rct ? rct->t->n : rows, nc = cct ? cct->t->n : cols;
+    if (rct) permute((T*)vec, rct->t->perm, nr, nc, 0, restore);
+    if (cct) permute((T*)vec, cct->t->perm, nr, nc, 1, restore);
+  });
+  return 0;
+}
+template <typename T>
+int vector_reorder_t(void* v, const hmat_cluster_tree_t* r, int rows, const hmat_cluster_tree_t* c, int cols) {
+  return reorder_impl<T>(v, r, rows, c, cols, false);
+}
+template <typename T>
+int vector_restore_t(void* v, const hmat_cluster_tree_t* r, int rows, const hmat_cluster_tree_t* c, int cols) {
+  return reorder_impl<T>(v, r, rows, c, cols, true);
+}
+
+// HMatrix::info (h_matrix.cpp:464-502) over the flattened leaves.
+int get_info(hmat_matrix_t* m, hmat_info_t* info) {
+  HB_TRY("get_info", {
+    if (!m || !info) throw Error("null argument");
+    memset(info, 0, sizeof(*info));
+    info->nr_block_clusters = m->bt.nr_block_clusters;
+    const auto& L = m->bt.leaves;
+    for (size_t i = 0; i < L.size(); ++i) {
+      const size_t r = L[i].m, c = L[i].n;
+      if (!r || !c) continue;
+      const size_t s = r * c;
+      info->uncompressed_size += s;
+      if (L[i].type == 1) {
+        const int k = leaf_rank(m, i);
+        const size_t mem = (size_t)k * (r + c);
+        info->compressed_size += mem;
+        if ((int)(r + c) > info->largest_rk_dim_cols + info->largest_rk_dim_rows) {
+          info->largest_rk_dim_cols = (int)c;
+          info->largest_rk_dim_rows = (int)r;
+        }
+        const size_t old =
+            ((size_t)info->largest_rk_mem_cols + info->largest_rk_mem_rows) * info->largest_rk_mem_rank;
+        if (mem > old) {
+          info->largest_rk_mem_cols = (int)c;
+          info->largest_rk_mem_rows = (int)r;
+          info->largest_rk_mem_rank = k;
+        }
+        info->rk_count++;
+        info->rk_size += s;
+      } else {
+        info->compressed_size += s;
+        info->full_count++;
+        info->full_size += s;
+      }
+    }
+  });
+  return 0;
+}
+
+int get_cluster_trees(hmat_matrix_t* m, const hmat_cluster_tree_t** rows, const hmat_cluster_tree_t** cols) {
+  if (!m) return fail("get_cluster_trees", "null matrix");
+  if (rows) *rows = m->rows_h;
+  if (cols) *cols = m->cols_h;
+  return 0;
+}
+
+int init_fn(void) { return 0; }
+int finalize_fn(void) { return 0; }
+
+// ---- slots outside the path: explicit failures ----
+int unsupported(const char* name) {
+  return fail(name, "not supported by the B200 engine (outside the leaf-level assembly / gemv path)");
+}
+hmat_matrix_t* u_copy(hmat_matrix_t*) {
+  unsupported("copy");
+  return nullptr;
+}
+hmat_matrix_t* u_copy_struct(hmat_matrix_t*) {
+  unsupported("copy_struct");
+  return nullptr;
+}
+double u_norm(hmat_matrix_t*) {
+  unsupported("norm");
+  return -1.0;
+}
+int u_logdet(hmat_matrix_t*, double*) { return unsupported("logdet"); }
+int u_inverse(hmat_matrix_t*) { return unsupported("inverse"); }
+int u_factorize(hmat_matrix_t*, hmat_factorization_context_t*) { return unsupported("factorize_generic"); }
+hmat_matrix_t* u_get_child(hmat_matrix_t*, int, int) {
+  unsupported("get_child");
+  return nullptr;
+}
+int u_destroy_child(hmat_matrix_t*) { return unsupported("destroy_child"); }
+int u_solve_generic(hmat_matrix_t*, const struct hmat_solve_context_t*) { return unsupported("solve_generic"); }
+int u_solve_mat(hmat_matrix_t*, hmat_matrix_t*) { return unsupported("solve_mat"); }
+int u_solve_systems(hmat_matrix_t*, void*, int) { return unsupported("solve_systems"); }
+int u_solve_dense(hmat_matrix_t*, void*, int) { return unsupported("solve_dense"); }
+int u_transpose(hmat_matrix_t*) { return unsupported("transpose"); }
+int u_scale(void*, hmat_matrix_t*) { return unsupported("scale"); }
+int u_truncate(hmat_matrix_t*) { return unsupported("truncate"); }
+int u_gemm(char, char, const void*, hmat_matrix_t*, hmat_matrix_t*, const void*, hmat_matrix_t*) {
+  return unsupported("gemm");
+}
+int u_axpy(void*, hmat_matrix_t*, hmat_matrix_t*) { return unsupported("axpy"); }
+int u_trsm(char, char, char, char, int, int, void*, hmat_matrix_t*, int, void*) { return unsupported("trsm"); }
+int u_gemm_scalar(char, void*, hmat_matrix_t*, void*, void*, void*, int) { return unsupported("gemm_scalar"); }
+int u_full_gemm(char, char, int, int, void*, void*, void*, hmat_matrix_t*, void*) { return unsupported("full_gemm"); }
+int u_gemm_dense(char, char, char, const void*, hmat_matrix_t*, void*, const void*, void*, int) {
+  return unsupported("gemm_dense");
+}
+int u_add_identity(hmat_matrix_t*, void*) { return unsupported("add_identity"); }
+int u_get_profile(hmat_matrix_t*, hmat_profile_t*) { return unsupported("get_profile"); }
+int u_get_ratio(hmat_matrix_t*, hmat_FPCompressionRatio_t*) { return unsupported("get_ratio"); }
+int u_fpcompress(hmat_matrix_t*) { return unsupported("FPcompress"); }
+int u_fpdecompress(hmat_matrix_t*) { return unsupported("FPdecompress"); }
+hmat_fp_settings_t u_get_fp(hmat_matrix_t*) {
+  unsupported("GetFPCompressionSettings");
+  hmat_fp_settings_t s;
+  memset(&s, 0, sizeof(s));
+  return s;
+}
+int u_set_fp(hmat_matrix_t*, hmat_fp_settings_t) { return unsupported("SetFPCompressionSettings"); }
+int u_set_fp_params(hmat_matrix_t*, float, int, hmat_FPcompress_t, bool, bool) {
+  return unsupported("SetFPCompressionSettingsParams");
+}
+int u_dump_info(hmat_matrix_t*, char*) { return unsupported("dump_info"); }
+int u_set_cluster_trees(hmat_matrix_t*, const hmat_cluster_tree_t*, const hmat_cluster_tree_t*) {
+  return unsupported("set_cluster_trees");
+}
+int u_extract_diagonal(hmat_matrix_t*, void*, int) { return unsupported("extract_diagonal"); }
+int u_solve_lower(hmat_matrix_t*, int, void*, int) { return unsupported("solve_lower_triangular"); }
+int u_solve_lower_dense(hmat_matrix_t*, int, void*, int) { return unsupported("solve_lower_triangular_dense"); }
+int u_get_block(struct hmat_get_values_context_t*) { return unsupported("get_block"); }
+int u_get_values(struct hmat_get_values_context_t*) { return unsupported("get_values"); }
+int u_walk(hmat_matrix_t*, hmat_procedure_t*) { return unsupported("walk"); }
+int u_apply_on_leaf(hmat_matrix_t*, const hmat_leaf_procedure_t*) { return unsupported("apply_on_leaf"); }
+hmat_matrix_t* u_read_struct(hmat_iostream, void*) {
+  unsupported("read_struct");
+  return nullptr;
+}
+void u_write_struct(hmat_matrix_t*, hmat_iostream, void*) { unsupported("write_struct"); }
+void u_read_data(hmat_matrix_t*, hmat_iostream, void*) { unsupported("read_data"); }
+void u_write_data(hmat_matrix_t*, hmat_iostream, void*) { unsupported("write_data"); }
+void u_set_progressbar(hmat_matrix_t*, hmat_progress_t*) {}
+int u_extract_diagonal_block(hmat_matrix_t*, int, void*) { return unsupported("extract_diagonal_block"); }
+
+template <int VT, typename T>
+void fill_table(hmat_interface_t* i) {
+  i->create_empty_hmatrix_admissibility = create_empty_t<VT>;
+  i->own_cluster_trees = own_cluster_trees;
+  i->set_low_rank_epsilon = set_low_rank_epsilon;
+  i->assemble_generic = assemble_generic;
+  i->copy = u_copy;
+  i->copy_struct = u_copy_struct;
+  i->norm = u_norm;
+  i->logdet = u_logdet;
+  i->inverse = u_inverse;
+  i->factorize_generic = u_factorize;
+  i->destroy = destroy;
+  i->get_child = u_get_child;
+  i->destroy_child = u_destroy_child;
+  i->solve_generic = u_solve_generic;
+  i->solve_mat = u_solve_mat;
+  i->solve_systems = u_solve_systems;
+  i->solve_dense = u_solve_dense;
+  i->transpose = u_transpose;
+  i->scale = u_scale;
+  i->truncate = u_truncate;
+  i->vector_reorder = vector_reorder_t<T>;
+  i->vector_restore = vector_restore_t<T>;
+  i->gemm = u_gemm;
+  i->axpy = u_axpy;
+  i->trsm = u_trsm;
+  i->gemv = gemv_t<VT>;
+  i->gemm_scalar = u_gemm_scalar;
+  i->full_gemm = u_full_gemm;
+  i->gemm_dense = u_gemm_dense;
+  i->add_identity = u_add_identity;
+  i->init = init_fn;
+  i->finalize = finalize_fn;
+  i->get_info = get_info;
+  i->get_profile = u_get_profile;
+  i->get_ratio = u_get_ratio;
+  i->FPcompress = u_fpcompress;
+  i->FPdecompress = u_fpdecompress;
+  i->GetFPCompressionSettings = u_get_fp;
+  i->SetFPCompressionSettings = u_set_fp;
+  i->SetFPCompressionSettingsParams = u_set_fp_params;
+  i->dump_info = u_dump_info;
+  i->get_cluster_trees = get_cluster_trees;
+  i->set_cluster_trees = u_set_cluster_trees;
+  i->extract_diagonal = u_extract_diagonal;
+  i->solve_lower_triangular = u_solve_lower;
+  i->solve_lower_triangular_dense = u_solve_lower_dense;
+  i->get_block = u_get_block;
+  i->get_values = u_get_values;
+  i->walk = u_walk;
+  i->apply_on_leaf = u_apply_on_leaf;
+  i->internal = nullptr;
+  i->read_struct = u_read_struct;
+  i->write_struct = u_write_struct;
+  i->read_data = u_read_data;
+  i->write_data = u_write_data;
+  i->set_progressbar = u_set_progressbar;
+  i->extract_diagonal_block = u_extract_diagonal_block;
+}
+
+}  // namespace
+
+extern "C" {
+
+hmat_clustering_algorithm_t* hmat_create_clustering_median(void) { return new hmat_clustering_algorithm(); }
+
+hmat_clustering_algorithm_t* hmat_create_clustering_max_dof(const hmat_clustering_algorithm_t* algo, int max_dof) {
+  if (!algo) return nullptr;
+  hmat_clustering_algorithm* r = new hmat_clustering_algorithm(*algo);
+  r->a.max_leaf = max_dof;
+  return r;
+}
+
+void hmat_delete_clustering(hmat_clustering_algorithm_t* algo) { delete algo; }
+
+void hmat_set_clustering_divider(hmat_clustering_algorithm_t* algo, int divider) {
+  if (algo) algo->a.divider = divider;
+}
+
+hmat_cluster_tree_t* hmat_create_cluster_tree(double* coord, int dimension, int size,
+                                              hmat_clustering_algorithm_t* algo) {
+  try {
+    if (!coord || !algo) throw Error("null argument");
+    if (dimension != 3) throw Error("the B200 engine clusters 3-D points only");
+    if (algo->a.divider != 2) throw Error("only bisection (divider 2) is supported");
+    const int leaf = algo->a.max_leaf >= 0 ? algo->a.max_leaf : g_settings.maxLeafSize;
+    hmat_cluster_tree_t* t = new hmat_cluster_tree_t();
+    t->t = build_cluster_tree(coord, size, leaf);
+    return t;
+  } catch (const std::exception& e) {
+    fail("hmat_create_cluster_tree", e.what());
+    return nullptr;
+  }
+}
+
+void hmat_delete_cluster_tree(const hmat_cluster_tree_t* tree) { delete tree; }
+
+int hmat_tree_nodes_count(const hmat_cluster_tree_t* tree) { return tree ? (int)tree->t->nodes.size() : 0; }
+
+int hmat_cluster_get_info(hmat_cluster_tree_t* tree, hmat_cluster_info_t* info) {
+  if (!tree || !info) return fail("hmat_cluster_get_info", "null argument");
+  info->spatial_dimension = 3;
+  info->dimension = tree->t->n;
+  info->nr_tree_nodes = tree->t->nodes.size();
+  return 0;
+}
+
+const int* hmat_cluster_get_indices(const hmat_cluster_tree_t* tree) { return tree ? tree->t->perm.data() : nullptr; }
+
+void hmat_init_admissibility_param(hmat_admissibility_param_t* p) {
+  if (!p) return;
+  p->eta = 2;
+  p->ratio = 0.0;
+  p->max_width = (size_t)-1;
+  p->scale = -1;
+}
+
+hmat_admissibility_t* hmat_create_admissibility(hmat_admissibility_param_t* p) {
+  if (!p) return nullptr;
+  hmat_admissibility_condition* c = new hmat_admissibility_condition();
+  c->a.eta = p->eta;
+  c->a.ratio = p->ratio;
+  c->a.max_width = p->max_width;
+  return c;
+}
+
+void hmat_update_admissibility(hmat_admissibility_t* cond, hmat_admissibility_param_t* p) {
+  if (!cond || !p) return;
+  cond->a.eta = p->eta;
+  cond->a.ratio = p->ratio;
+  cond->a.max_width = p->max_width;
+}
+
+hmat_admissibility_t* hmat_create_admissibility_standard(double eta) {
+  hmat_admissibility_condition* c = new hmat_admissibility_condition();
+  c->a.eta = eta;
+  return c;
+}
+
+void hmat_delete_admissibility(hmat_admissibility_t* cond) { delete cond; }
+
+static hmat_compression_algorithm_t* make_compression(hmat_compress_t m, double eps) {
+  hmat_compression_algorithm_t* c = new hmat_compression_algorithm_t();
+  c->method = m;
+  c->eps = eps;
+  return c;
+}
+hmat_compression_algorithm_t* hmat_create_compression_aca_plus(double e) {
+  return make_compression(hmat_compress_aca_plus, e);
+}
+hmat_compression_algorithm_t* hmat_create_compression_aca_partial(double e) {
+  return make_compression(hmat_compress_aca_partial, e);
+}
+hmat_compression_algorithm_t* hmat_create_compression_svd(double e) { return make_compression(hmat_compress_svd, e); }
+hmat_compression_algorithm_t* hmat_create_compression_aca_full(double e) {
+  return make_compression(hmat_compress_aca_full, e);
+}
+hmat_compression_algorithm_t* hmat_create_compression_aca_random(double e) {
+  return make_compression(hmat_compress_aca_random, e);
+}
+hmat_compression_algorithm_t* hmat_create_compression_rrqr(double e) {
+  return make_compression(hmat_compress_rrqr, e);
+}
+void hmat_delete_compression(const hmat_compression_algorithm_t* algo) { delete algo; }
+
+void hmat_assemble_context_init(hmat_assemble_context_t* c) {
+  if (!c) return;
+  memset(c, 0, sizeof(*c));
+  c->factorization = hmat_factorization_none;
+}
+
+void hmat_factorization_context_init(hmat_factorization_context_t* c) {
+  if (!c) return;
+  c->factorization = hmat_factorization_lu;
+  c->progress = nullptr;
+}
+
+void hmat_solve_context_init(struct hmat_solve_context_t* c) {
+  if (!c) return;
+  memset(c, 0, sizeof(*c));
+}
+
+hmat_progress_t* hmat_default_progress(void) {
+  static hmat_progress_t p = {0, 0, nullptr, nullptr};
+  return &p;
+}
+
+void hmat_init_default_interface(hmat_interface_t* i, hmat_value_t type) {
+  if (!i) return;
+  memset(i, 0, sizeof(*i));
+  i->value_type = type;
+  switch (type) {
+    case HMAT_SIMPLE_PRECISION: fill_table<0, float>(i); break;
+    case HMAT_DOUBLE_PRECISION: fill_table<1, double>(i); break;
+    case HMAT_SIMPLE_COMPLEX: fill_table<2, std::complex<float>>(i); break;
+    case HMAT_DOUBLE_COMPLEX: fill_table<3, std::complex<double>>(i); break;
+    default: fail("hmat_init_default_interface", "unknown value type");
+  }
+}
+
+void hmat_get_parameters(hmat_settings_t* s) {
+  if (s) *s = g_settings;
+}
+
+int hmat_set_parameters(hmat_settings_t* s) {
+  if (!s) return fail("hmat_set_parameters", "null settings");
+  g_settings = *s;
+  return 0;
+}
+
+const char* hmat_get_version(void) { return "1.11.1-b200"; }
+
+// ---------------------------------------------------------------------------------
+
+void* hmat_b200_create_assembly(const hmat_b200_kernel_t* k, const double* coord, int n) {
+  if (!k || !coord || n <= 0) {
+    fail("hmat_b200_create_assembly", "bad argument");
+    return nullptr;
+  }
+  if (k->kind < HMAT_B200_LAPLACE_REG || k->kind > HMAT_B200_HELMHOLTZ_REG) {
+    fail("hmat_b200_create_assembly", "unknown kernel kind");
+    return nullptr;
+  }
+  if (k->kind == HMAT_B200_EXP_COV && !(k->ell > 0)) {
+    fail("hmat_b200_create_assembly", "exp_cov needs ell > 0");
+    return nullptr;
+  }
+  AssemblyObj* a = new AssemblyObj();
+  a->d.kp.kind = (int)k->kind;
+  a->d.kp.delta = k->delta;
+  a->d.kp.ell = k->ell;
+  a->d.kp.nugget = k->nugget;
+  a->d.kp.wavenumber = k->wavenumber;
+  a->d.pts.assign(coord, coord + 3 * (size_t)n);
+  return a;
+}
+
+void hmat_b200_delete_assembly(void* a) {
+  AssemblyObj* o = (AssemblyObj*)a;
+  if (o && o->magic == kAssemblyMagic) {
+    o->magic = 0;
+    delete o;
+  }
+}
+
+int hmat_b200_gemv_device(hmat_matrix_t* m, char trans, const void* alpha, const void* x, const void* beta, void* y,
+                          int nrhs, void* stream) {
+  HB_TRY("hmat_b200_gemv_device", {
+    if (!m || !alpha || !beta || (nrhs > 0 && (!x || !y))) throw Error("null argument");
+    engine_of(m).gemv_device(trans, alpha, x, beta, y, nrhs, (cudaStream_t)stream);
+  });
+  return 0;
+}
+
+int hmat_b200_leaf_count(hmat_matrix_t* m) { return m ? (int)m->bt.leaves.size() : -1; }
+
+int hmat_b200_leaf_table(hmat_matrix_t* m, int* out) {
+  if (!m || !out) return fail("hmat_b200_leaf_table", "null argument");
+  const auto& L = m->bt.leaves;
+  for (size_t i = 0; i < L.size(); ++i) {
+    out[6 * i + 0] = L[i].row_off;
+    out[6 * i + 1] = L[i].m;
+    out[6 * i + 2] = L[i].col_off;
+    out[6 * i + 3] = L[i].n;
+    out[6 * i + 4] = L[i].type;
+    out[6 * i + 5] = leaf_rank(m, i);
+  }
+  return 0;
+}
+
+long long hmat_b200_leaf_payload(hmat_matrix_t* m, int leaf, void* out) {
+  try {
+    if (!m || !out) throw Error("null argument");
+    return engine_of(m).leaf_payload(leaf, out);
+  } catch (const std::exception& e) {
+    fail("hmat_b200_leaf_payload", e.what());
+    return -1;
+  }
+}
+
+int hmat_b200_leaf_arenas(hmat_matrix_t* m, void** full, long long* full_elems, void** rk, long long* rk_elems,
+                          long long* offsets) {
+  HB_TRY("hmat_b200_leaf_arenas", {
+    if (!m) throw Error("null matrix");
+    if (!engine_of(m).assembled) throw Error("matrix is not assembled");
+    m->engine->arenas(full, full_elems, rk, rk_elems, offsets);
+  });
+  return 0;
+}
+
+int hmat_b200_leaf_gradients(hmat_matrix_t* m, const void* x, const void* r, int nrhs, void* gfull, void* grk,
+                             int accumulate, void* stream) {
+  HB_TRY("hmat_b200_leaf_gradients", {
+    if (!m || !x || !r) throw Error("null argument");
+    engine_of(m).leaf_gradients(x, r, nrhs, gfull, grk, accumulate != 0, (cudaStream_t)stream);
+  });
+  return 0;
+}
+
+int hmat_b200_gemv_profile(hmat_matrix_t* m, char trans, const void* x_dev, void* y_dev, int nrhs, double* ms3,
+                           double* bytes3) {
+  HB_TRY("hmat_b200_gemv_profile", {
+    if (!m || !x_dev || !y_dev || !ms3 || !bytes3) throw Error("null argument");
+    engine_of(m).profile_gemv(trans, x_dev, y_dev, nrhs, ms3, bytes3);
+  });
+  return 0;
+}
+
+int hmat_b200_phase_times(hmat_matrix_t* m, double* out4) {
+  if (!m || !out4) return fail("hmat_b200_phase_times", "null argument");
+  for (int i = 0; i < 4; ++i) out4[i] = m->engine ? m->engine->times_ms[i] : 0.0;
+  return 0;
+}
+
+const char* hmat_b200_last_error(void) { return g_last_error.c_str(); }
+
+}  // extern "C"

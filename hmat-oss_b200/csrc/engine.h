@@ -1,0 +1,54 @@
+// The B200 engine: device residency and phase orchestration for one H-matrix.
+//
+// Plays the role of the reference's IEngine<T> / DefaultEngine<T> pair
+// (iengine.hpp:31-98, default_engine.cpp:94-141) for the leaf-level path: assembly and
+// gemv.  The block tree is built on the host (host.h); this class flattens it into
+// device-resident leaf descriptors, runs the assembly phases and keeps the gemv
+// schedule and its CUDA graph.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "host.h"
+
+namespace hmatb200 {
+
+struct AssemblyDesc {
+  KernelParams kp;
+  std::vector<double> pts;  // client numbering, point-major
+};
+
+struct LeafGrad;
+
+class EngineBase {
+ public:
+  virtual ~EngineBase() {}
+  // method: 0 ACA+, 1 partial ACA.  eps_aca is the compression's epsilon, eps_trunc the
+  // matrix's low-rank epsilon; admissible blocks with max(m, n) < svd_below are
+  // compressed by dense SVD instead.
+  virtual void assemble(const AssemblyDesc& a, int method, double eps_aca, double eps_trunc, int svd_below) = 0;
+  virtual void gemv_device(char trans, const void* alpha, const void* x, const void* beta, void* y, int nrhs,
+                           cudaStream_t user_stream) = 0;
+  virtual void gemv_host(char trans, const void* alpha, const void* x, const void* beta, void* y, int nrhs) = 0;
+  virtual long long leaf_payload(int leaf, void* out) = 0;
+  virtual void arenas(void** full, long long* full_elems, void** rk, long long* rk_elems,
+                      long long* offsets) = 0;
+  virtual void leaf_gradients(const void* x, const void* r, int nrhs, void* gfull, void* grk, bool accumulate,
+                              cudaStream_t user_stream) = 0;
+  virtual void retruncate(double eps) = 0;
+  // One eager product on device buffers with events between its phases: device ms of
+  // [gather, z-phase, y-phase] and their algorithmic bytes (nrhs <= 16).
+  virtual void profile_gemv(char trans, const void* x, void* y, int nrhs, double* ms3, double* bytes3) = 0;
+
+  bool assembled = false;
+  std::vector<int> ranks;  // per leaf, -1 for full leaves
+  double times_ms[4] = {0, 0, 0, 0};
+};
+
+std::unique_ptr<EngineBase> make_engine(int value_type, const ClusterTree* rows, const ClusterTree* cols,
+                                        const BlockTree* bt);
+
+}  // namespace hmatb200

@@ -1,0 +1,82 @@
+// Host-side launch interface of the B200 engine's device phases.  Plain types only; the
+// engine (engine.cu) owns the device buffers and calls these launchers on its stream.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace hmatb200 {
+
+// One admissible leaf as the ACA and truncation phases see it.
+struct RkLeafDesc {
+  int row_off, m;     // rows [row_off, row_off + m) in cluster order
+  int col_off, n;     // cols [col_off, col_off + n)
+  long long ws_off;   // element offset of the leaf's slot in the ACA workspace
+  long long fl_off;   // byte offset of the leaf's pivot flags (m + n bytes)
+  int kcap;           // rank capacity of the slot
+  int pad;
+};
+// Workspace slot layout (elements of T, from ws_off): A (m x kcap), B (n x kcap),
+// aRef (m), bRef (n).
+inline long long rk_slot_elems(int m, int n, int kcap) { return (long long)(m + n) * (kcap + 1); }
+
+// One dense (non-admissible) leaf.
+struct FullLeafDesc {
+  int row_off, m, col_off, n;
+  long long off;  // element offset in the full-leaf arena (column-major m x n)
+};
+
+// ---- assembly ----
+template <typename T>
+void launch_assemble_full(const FullLeafDesc* d_leaves, int nleaves, const KernelParams& kp, Points pts,
+                          T* arena, cudaStream_t s);
+
+// ACA+ (compression.cpp:553-724), delegating to partial ACA when n * 100 < m.  Leaves are
+// taken in `order` from a device work counter that must be zero at launch.
+template <typename T>
+void launch_aca(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, const KernelParams& kp, Points pts,
+                double epsilon, T* ws, unsigned char* flags, int* ranks, int* status, int* counter, int kcap_max,
+                int grid, cudaStream_t s);
+
+// Dense block written as an exact rank-min(m, n) factorisation, for the SVD compression
+// of small blocks (the truncation phase then performs the SVD).
+template <typename T>
+void launch_dense_to_rk(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, const KernelParams& kp,
+                        Points pts, T* ws, int* ranks, int* status, cudaStream_t s);
+
+// Truncation (rk_matrix.cpp:490-585): replaces A, B in each slot by the recompressed
+// factors (first new-rank columns, same slot) and rewrites ranks.  `scratch` holds
+// `grid` per-CTA FP64 slabs of `slab_elems` wide elements each.
+template <typename T>
+void launch_truncate(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, double epsilon, T* ws,
+                     int* ranks, int* status, int* counter, typename Traits<T>::wide* scratch,
+                     long long slab_elems, int grid, cudaStream_t s);
+template <typename T>
+long long truncate_slab_elems(int max_m, int max_n, int max_k);
+
+// Copies the truncated factors of each leaf from its workspace slot into the compact
+// Rk arena at dst_off[leaf] (A then B, column-major).
+template <typename T>
+void launch_compact(const RkLeafDesc* d_leaves, int nleaves, const T* ws, const int* ranks,
+                    const long long* dst_off, T* arena, cudaStream_t s);
+
+// ---- gemv ----
+}  // namespace hmatb200
+#include "gemv_plan.h"
+namespace hmatb200 {
+template <typename T>
+void launch_gemv(const GemvPlan& p, char trans, int nrhs, T alpha, T beta, const T* x_client, T* y_client,
+                 T* x_rm, T* zpart, T* z, cudaStream_t s, const GemvTiming* timing = nullptr);
+
+// Leaf-factor gradients of y = H x for the output gradient r (real types; x, r device,
+// client numbering, nrhs <= 16): dF = r_I x_J^T, dA = r_I (B^T x_J)^T, dB = x_J (A^T r_I)^T,
+// written (or added) into gradient arenas laid out like the leaf arenas.
+template <typename T>
+void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, T* x_rm, T* r_rm, T* zx, T* zr,
+                           T* gfull, T* grk, bool accumulate, cudaStream_t s);
+
+// Grid size of a persistent launch: a multiple of the SM count.
+int persistent_grid(int blocks_per_sm);
+
+}  // namespace hmatb200

@@ -1,0 +1,419 @@
+/*
+ * hmat_b200.h -- C ABI of the B200 engine for hmat-oss's leaf-level path.
+ *
+ * The engine is a drop-in for the reference's `hmat_init_default_interface` path: the
+ * library exports the same C entry points (same names, same argument meaning, 0 on
+ * success and non-zero on failure), and `hmat_interface_t` has the reference's field
+ * order so that a program compiled against either header calls the same slots.  Linking
+ * libhmat_b200.so in place of libhmat.so selects the engine.
+ *
+ * What runs on the GPU: dense assembly of full leaves, ACA+ (partial-ACA for very tall
+ * blocks) of admissible leaves, Rk truncation, and the H-matrix-vector product
+ * ('N', 'T', 'C', any number of right-hand sides).  What stays on the host: median
+ * clustering, bounding boxes, the Hackbusch admissibility test and the block tree, all
+ * with the reference's arithmetic so the partitions match bit for bit.
+ *
+ * Precision: HMAT_DOUBLE_PRECISION / HMAT_DOUBLE_COMPLEX run everything in FP64.
+ * HMAT_SIMPLE_PRECISION / HMAT_SIMPLE_COMPLEX run assembly, ACA and gemv in FP32 and
+ * keep FP64 for the ACA stopping-norm estimate and the QR/SVD of the truncation.
+ *
+ * Table slots outside this path (factorizations, solves, H-matrix products, copies,
+ * serialisation, ...) are filled with functions that print an error and return a
+ * failure value (non-zero, or NULL for constructors), which is how the reference's C
+ * layer reports an unsupported operation.
+ *
+ * Interaction functions: the device cannot call host callbacks, so `simple_compute`,
+ * `block_compute` and `advanced_compute` are rejected by assemble_generic (it returns 1).
+ * Put a descriptor made by hmat_b200_create_assembly() in the context's `assembly` field
+ * instead (the reference's "Assembly object" scenario, hmat.h:526-536).
+ */
+#ifndef HMAT_B200_H
+#define HMAT_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- value types and enums (reference: include/hmat/hmat.h:57-107) ---- */
+typedef enum {
+  HMAT_SIMPLE_PRECISION = 0,
+  HMAT_DOUBLE_PRECISION = 1,
+  HMAT_SIMPLE_COMPLEX = 2,
+  HMAT_DOUBLE_COMPLEX = 3
+} hmat_value_t;
+
+typedef enum {
+  hmat_compress_svd,
+  hmat_compress_aca_full,
+  hmat_compress_aca_partial,
+  hmat_compress_aca_plus,
+  hmat_compress_aca_random,
+  hmat_compress_rrqr
+} hmat_compress_t;
+
+typedef enum { DEFAULT_COMPRESSOR = 0, ZFP_COMPRESSOR = 1, SZ_COMPRESSOR = 2, SZ3_COMPRESSOR = 3 } hmat_FPcompress_t;
+
+typedef enum { hmat_block_full, hmat_block_null, hmat_block_sparse } hmat_block_t;
+
+typedef enum {
+  hmat_factorization_none = -1,
+  hmat_factorization_lu,
+  hmat_factorization_ldlt,
+  hmat_factorization_llt,
+  hmat_factorization_hodlr,
+  hmat_factorization_hodlrsym
+} hmat_factorization_t;
+
+/* ---- user callback types (reference: hmat.h:118-200); accepted in the context for
+ *      layout compatibility, rejected at assembly time ---- */
+typedef struct hmat_block_info_struct {
+  hmat_block_t block_type;
+  void* user_data;
+  void (*release_user_data)(void* user_data);
+  char (*is_guaranteed_null_row)(const struct hmat_block_info_struct* block_info, int block_row_offset, int stratum);
+  char (*is_guaranteed_null_col)(const struct hmat_block_info_struct* block_info, int block_col_offset, int stratum);
+  size_t needed_memory;
+  int number_of_strata;
+} hmat_block_info_t;
+
+typedef struct hmat_fp_settings_struct {
+  hmat_FPcompress_t compressor;
+  int nb_blocs;
+  float epsilonFP;
+  bool compressFull;
+  bool compressRk;
+} hmat_fp_settings_t;
+
+typedef void (*hmat_prepare_func_t)(int row_start, int row_count, int col_start, int col_count, int* row_hmat2client,
+                                    int* row_client2hmat, int* col_hmat2client, int* col_client2hmat, void* context,
+                                    hmat_block_info_t* block_info);
+typedef void (*hmat_compute_func_t)(void* v_data, int block_row_start, int block_row_count, int block_col_start,
+                                    int block_col_count, void* block);
+typedef void (*hmat_interaction_func_t)(void* user_context, int row, int col, void* result);
+
+/* ---- clustering (reference: hmat.h:206-330; c_default_interface.cpp:35-193) ---- */
+typedef struct hmat_clustering_algorithm hmat_clustering_algorithm_t;
+typedef struct hmat_cluster_tree_struct hmat_cluster_tree_t;
+
+/* Median bisection (MedianBisectionAlgorithm, clustering.cpp:257-301). */
+hmat_clustering_algorithm_t* hmat_create_clustering_median(void);
+/* Copy of `algo` with at most `max_dof` points per leaf (c_default_interface.cpp:73-78). */
+hmat_clustering_algorithm_t* hmat_create_clustering_max_dof(const hmat_clustering_algorithm_t* algo, int max_dof);
+void hmat_delete_clustering(hmat_clustering_algorithm_t* algo);
+/* Only divider 2 (bisection) is supported; other values make tree creation fail. */
+void hmat_set_clustering_divider(hmat_clustering_algorithm_t* algo, int divider);
+/* Cluster tree over `size` points given point-major in `coord` (c_default_interface.cpp:101-115).
+ * Only dimension 3 is supported. Returns NULL on error. */
+hmat_cluster_tree_t* hmat_create_cluster_tree(double* coord, int dimension, int size, hmat_clustering_algorithm_t* algo);
+void hmat_delete_cluster_tree(const hmat_cluster_tree_t* tree);
+int hmat_tree_nodes_count(const hmat_cluster_tree_t* tree);
+
+typedef struct {
+  int spatial_dimension;
+  int dimension;
+  size_t nr_tree_nodes;
+} hmat_cluster_info_t;
+int hmat_cluster_get_info(hmat_cluster_tree_t* tree, hmat_cluster_info_t* info);
+/* internal -> client permutation of the tree (c_default_interface.cpp:191-193) */
+const int* hmat_cluster_get_indices(const hmat_cluster_tree_t* tree);
+
+/* ---- admissibility (reference: hmat.h:332-372; c_default_interface.cpp:195-240) ---- */
+typedef struct {
+  double eta;
+  double ratio;
+  size_t max_width;
+  double scale;
+} hmat_admissibility_param_t;
+typedef struct hmat_admissibility_condition hmat_admissibility_t;
+void hmat_init_admissibility_param(hmat_admissibility_param_t* p);
+hmat_admissibility_t* hmat_create_admissibility(hmat_admissibility_param_t* p);
+void hmat_update_admissibility(hmat_admissibility_t* cond, hmat_admissibility_param_t* p);
+/* Hackbusch condition min(diam) <= eta * dist (admissibility.cpp:109-117). */
+hmat_admissibility_t* hmat_create_admissibility_standard(double eta);
+void hmat_delete_admissibility(hmat_admissibility_t* cond);
+
+/* ---- compression (reference: hmat.h:376-394) ---- */
+typedef struct hmat_compression_algorithm_struct hmat_compression_algorithm_t;
+/* ACA+ with partial-ACA delegate (compression.hpp:134-148). */
+hmat_compression_algorithm_t* hmat_create_compression_aca_plus(double epsilon);
+/* Partial ACA (compression.cpp:382-533). */
+hmat_compression_algorithm_t* hmat_create_compression_aca_partial(double epsilon);
+/* Dense SVD, ACA-full, ACA-random and RRQR: objects are created, assembly with them fails. */
+hmat_compression_algorithm_t* hmat_create_compression_svd(double epsilon);
+hmat_compression_algorithm_t* hmat_create_compression_aca_full(double epsilon);
+hmat_compression_algorithm_t* hmat_create_compression_aca_random(double epsilon);
+hmat_compression_algorithm_t* hmat_create_compression_rrqr(double epsilon);
+void hmat_delete_compression(const hmat_compression_algorithm_t* algo);
+
+/* ---- info / settings (reference: hmat.h:404-470, 1107-1142) ---- */
+typedef struct {
+  int full_zeros;
+  size_t full_size;
+  size_t rk_size;
+  size_t full_count;
+  size_t rk_count;
+  size_t compressed_size;
+  size_t uncompressed_size;
+  int nr_block_clusters;
+  int largest_rk_dim_rows;
+  int largest_rk_dim_cols;
+  int largest_rk_mem_rows;
+  int largest_rk_mem_cols;
+  int largest_rk_mem_rank;
+} hmat_info_t;
+
+typedef struct {
+  int wip;
+} hmat_profile_t;
+
+typedef struct hmat_matrix_struct hmat_matrix_t;
+
+typedef struct hmat_progress_struct {
+  int max;
+  int current;
+  void (*update)(struct hmat_progress_struct* context);
+  void* user_data;
+} hmat_progress_t;
+hmat_progress_t* hmat_default_progress(void);
+
+typedef struct {
+  double rkRatio;
+  size_t size_Rk;
+  size_t size_Rk_compressed;
+  double fullRatio;
+  size_t size_Full;
+  size_t size_Full_compressed;
+  double ratio;
+} hmat_FPCompressionRatio_t;
+
+typedef void (*hmat_iostream)(void* buffer, size_t n, void* user_data);
+
+struct hmat_block_compute_context_t {
+  void* user_data;
+  int row_start, row_count, col_start, col_count;
+  int stratum;
+  void* block;
+};
+
+/* Assembly context (reference: hmat.h:516-622).  Exactly one of `assembly`,
+ * `simple_compute`, `block_compute`, `advanced_compute` is set; this engine accepts
+ * only `assembly` = a descriptor from hmat_b200_create_assembly(). */
+typedef struct {
+  void* assembly;
+  hmat_interaction_func_t simple_compute;
+  hmat_compute_func_t block_compute;
+  void (*advanced_compute)(struct hmat_block_compute_context_t*);
+  void* user_context;
+  hmat_prepare_func_t prepare;
+  const hmat_compression_algorithm_t* compression;
+  int lower_symmetric;
+  hmat_factorization_t factorization;
+  hmat_progress_t* progress;
+} hmat_assemble_context_t;
+void hmat_assemble_context_init(hmat_assemble_context_t* context);
+
+typedef struct {
+  hmat_factorization_t factorization;
+  hmat_progress_t* progress;
+} hmat_factorization_context_t;
+void hmat_factorization_context_init(hmat_factorization_context_t* context);
+
+struct hmat_get_values_context_t {
+  hmat_matrix_t* matrix;
+  void* values;
+  int row_offset, col_offset;
+  int row_size, col_size;
+  int *row_indices, *col_indices;
+  int renumber_rows : 1;
+};
+
+struct hmat_solve_context_t {
+  void* values;
+  int nr_rhs;
+  int no_permutation;
+  int lower;
+  int upper;
+  hmat_progress_t* progress;
+};
+void hmat_solve_context_init(struct hmat_solve_context_t* context);
+
+typedef struct {
+  hmat_value_t value_type;
+  void* internal;
+} hmat_procedure_t;
+typedef struct {
+  hmat_value_t value_type;
+  const void* internal;
+} hmat_leaf_procedure_t;
+
+/* Function table (reference: hmat.h:717-1103), same slot order. */
+typedef struct {
+  hmat_matrix_t* (*create_empty_hmatrix_admissibility)(const hmat_cluster_tree_t* rows_tree,
+                                                       const hmat_cluster_tree_t* cols_tree, int lower_symmetric,
+                                                       hmat_admissibility_t* cond);
+  void (*own_cluster_trees)(hmat_matrix_t* hmatrix, int owns_row, int owns_col);
+  void (*set_low_rank_epsilon)(hmat_matrix_t* hmatrix, double epsilon);
+  int (*assemble_generic)(hmat_matrix_t* matrix, hmat_assemble_context_t* context);
+  hmat_matrix_t* (*copy)(hmat_matrix_t* hmatrix);
+  hmat_matrix_t* (*copy_struct)(hmat_matrix_t* hmatrix);
+  double (*norm)(hmat_matrix_t* hmatrix);
+  int (*logdet)(hmat_matrix_t* hmatrix, double* result);
+  int (*inverse)(hmat_matrix_t* hmatrix);
+  int (*factorize_generic)(hmat_matrix_t* matrix, hmat_factorization_context_t* context);
+  int (*destroy)(hmat_matrix_t* hmatrix);
+  hmat_matrix_t* (*get_child)(hmat_matrix_t* hmatrix, int i, int j);
+  int (*destroy_child)(hmat_matrix_t* hmatrix);
+  int (*solve_generic)(hmat_matrix_t* matrix, const struct hmat_solve_context_t* context);
+  int (*solve_mat)(hmat_matrix_t* hmatrix, hmat_matrix_t* hmatrixB);
+  int (*solve_systems)(hmat_matrix_t* hmatrix, void* b, int nrhs);
+  int (*solve_dense)(hmat_matrix_t* hmatrix, void* b, int nrhs);
+  int (*transpose)(hmat_matrix_t* hmatrix);
+  int (*scale)(void* alpha, hmat_matrix_t* hmatrix);
+  int (*truncate)(hmat_matrix_t* hmatrix);
+  int (*vector_reorder)(void* vec_b, const hmat_cluster_tree_t* rows_ct, int rows, const hmat_cluster_tree_t* cols_ct,
+                        int cols);
+  int (*vector_restore)(void* vec_b, const hmat_cluster_tree_t* rows_ct, int rows, const hmat_cluster_tree_t* cols_ct,
+                        int cols);
+  int (*gemm)(char trans_a, char trans_b, const void* alpha, hmat_matrix_t* hmatrix, hmat_matrix_t* hmatrix_b,
+              const void* beta, hmat_matrix_t* hmatrix_c);
+  int (*axpy)(void* a, hmat_matrix_t* x, hmat_matrix_t* hmatrix_y);
+  int (*trsm)(char side, char uplo, char transa, char diag, int m, int n, void* alpha, hmat_matrix_t* A,
+              int is_b_hmat, void* B);
+  /* y <- alpha op(H) x + beta y, x and y column-major in client numbering, nrhs columns
+   * (reference c_wrapping.hpp:233-252).  x and y are host memory. */
+  int (*gemv)(char trans_a, void* alpha, hmat_matrix_t* hmatrix, void* vec_b, void* beta, void* vec_c, int nrhs);
+  int (*gemm_scalar)(char trans_a, void* alpha, hmat_matrix_t* hmatrix, void* vec_b, void* beta, void* vec_c,
+                     int nrhs);
+  int (*full_gemm)(char trans_a, char trans_b, int mc, int nc, void* c, void* alpha, void* a, hmat_matrix_t* hmat_b,
+                   void* beta);
+  int (*gemm_dense)(char trans_b, char trans_x, char side, const void* alpha, hmat_matrix_t* holder, void* vec_x,
+                    const void* beta, void* vec_y, int nrhs);
+  int (*add_identity)(hmat_matrix_t* hmatrix, void* alpha);
+  int (*init)(void);
+  int (*finalize)(void);
+  int (*get_info)(hmat_matrix_t* hmatrix, hmat_info_t* info);
+  int (*get_profile)(hmat_matrix_t* hmatrix, hmat_profile_t* profile);
+  int (*get_ratio)(hmat_matrix_t* hmatrix, hmat_FPCompressionRatio_t* ratio);
+  int (*FPcompress)(hmat_matrix_t* hmatrix);
+  int (*FPdecompress)(hmat_matrix_t* hmatrix);
+  hmat_fp_settings_t (*GetFPCompressionSettings)(hmat_matrix_t* hmatrix);
+  int (*SetFPCompressionSettings)(hmat_matrix_t* hmatrix, hmat_fp_settings_t settings);
+  int (*SetFPCompressionSettingsParams)(hmat_matrix_t* hmatrix, float epsilonFP, int nb_blocs,
+                                        hmat_FPcompress_t compressor, bool compressFull, bool compressRk);
+  int (*dump_info)(hmat_matrix_t* hmatrix, char* prefix);
+  int (*get_cluster_trees)(hmat_matrix_t* hmatrix, const hmat_cluster_tree_t** rows, const hmat_cluster_tree_t** cols);
+  int (*set_cluster_trees)(hmat_matrix_t* hmatrix, const hmat_cluster_tree_t* rows, const hmat_cluster_tree_t* cols);
+  int (*extract_diagonal)(hmat_matrix_t* holder, void* diag, int size);
+  int (*solve_lower_triangular)(hmat_matrix_t* hmatrix, int transpose, void* b, int nrhs);
+  int (*solve_lower_triangular_dense)(hmat_matrix_t* hmatrix, int transpose, void* b, int nrhs);
+  int (*get_block)(struct hmat_get_values_context_t* ctx);
+  int (*get_values)(struct hmat_get_values_context_t* ctx);
+  int (*walk)(hmat_matrix_t* hmatrix, hmat_procedure_t* proc);
+  int (*apply_on_leaf)(hmat_matrix_t* hmatrix, const hmat_leaf_procedure_t* proc);
+  hmat_value_t value_type;
+  void* internal;
+  hmat_matrix_t* (*read_struct)(hmat_iostream readfunc, void* user_data);
+  void (*write_struct)(hmat_matrix_t* matrix, hmat_iostream writefunc, void* user_data);
+  void (*read_data)(hmat_matrix_t* matrix, hmat_iostream readfunc, void* user_data);
+  void (*write_data)(hmat_matrix_t* matrix, hmat_iostream writefunc, void* user_data);
+  void (*set_progressbar)(hmat_matrix_t* matrix, hmat_progress_t* progress);
+  int (*extract_diagonal_block)(hmat_matrix_t* holder, int components, void* diag);
+} hmat_interface_t;
+
+/* Fills the table for one value type (reference: c_default_interface.cpp:242-252). */
+void hmat_init_default_interface(hmat_interface_t* i, hmat_value_t type);
+
+typedef struct {
+  int compressionMinLeafSize;
+  double coarseningEpsilon;
+  int maxLeafSize;
+  int coarsening;
+  int validateNullRowCol;
+  int validateCompression;
+  int validateRecompression;
+  int dumpTrace;
+  int validationReRun;
+  int validationDump;
+  double validationErrorThreshold;
+} hmat_settings_t;
+/* Global settings (reference: c_default_interface.cpp:254-288).  Of these the engine
+ * uses maxLeafSize (default leaf size of clustering algorithms without max_dof) and
+ * compressionMinLeafSize: admissible blocks with max(rows, cols) below it are compressed
+ * by a dense SVD, as AssemblyFunction::assemble does (assembly.cpp:59-64). */
+void hmat_get_parameters(hmat_settings_t* settings);
+int hmat_set_parameters(hmat_settings_t* settings);
+const char* hmat_get_version(void);
+
+/* ======================================================================================
+ * B200 extensions (no counterpart in the reference's C API).
+ * ====================================================================================== */
+
+/* Interaction kernels evaluated on the device:
+ *   HMAT_B200_LAPLACE_REG    K = 1 / (4 pi (r + delta))
+ *   HMAT_B200_EXP_COV        K = exp(-r / ell) + nugget * [row == col]
+ *   HMAT_B200_HELMHOLTZ_REG  K = exp(i k r) / (4 pi (r + delta))   (complex types only) */
+typedef enum { HMAT_B200_LAPLACE_REG = 0, HMAT_B200_EXP_COV = 1, HMAT_B200_HELMHOLTZ_REG = 2 } hmat_b200_kernel_kind_t;
+
+typedef struct {
+  hmat_b200_kernel_kind_t kind;
+  double delta;
+  double ell;
+  double nugget;
+  double wavenumber;
+} hmat_b200_kernel_t;
+
+/* Assembly descriptor for hmat_assemble_context_t.assembly: kernel + the points it is
+ * evaluated on (client numbering, point-major xyz, copied).  NULL on bad input. */
+void* hmat_b200_create_assembly(const hmat_b200_kernel_t* kernel, const double* coord, int n_points);
+void hmat_b200_delete_assembly(void* assembly);
+
+/* gemv on device buffers (x, y column-major, client numbering, leading dimension = the
+ * vector length), enqueued on `stream` (a cudaStream_t, NULL for the engine's own) and
+ * not synchronised.  Same maths and return convention as hmat_interface_t.gemv. */
+int hmat_b200_gemv_device(hmat_matrix_t* hmatrix, char trans, const void* alpha, const void* x_dev,
+                          const void* beta, void* y_dev, int nrhs, void* stream);
+
+/* Leaf table: `n` leaves in the reference's depth-first order, 6 ints each: row offset,
+ * rows, col offset, cols (cluster numbering), type (0 full, 1 rk), rank (-1 for full). */
+int hmat_b200_leaf_count(hmat_matrix_t* hmatrix);
+int hmat_b200_leaf_table(hmat_matrix_t* hmatrix, int* out);
+/* Payload of leaf `leaf` copied to host memory `out` (full: m x n column-major; rk: A
+ * (m x k) then B (n x k)); returns the number of scalars, or -1. */
+long long hmat_b200_leaf_payload(hmat_matrix_t* hmatrix, int leaf, void* out);
+
+/* Device views of the assembled leaves: the full-leaf and Rk arenas and, per leaf, the
+ * element offset of its payload in its arena (-1 for empty).  Pointers stay valid until
+ * the matrix is destroyed or re-assembled. */
+int hmat_b200_leaf_arenas(hmat_matrix_t* hmatrix, void** full_arena, long long* full_elems, void** rk_arena,
+                          long long* rk_elems, long long* leaf_offsets);
+
+/* Leaf-factor gradients of L(H) for a loss whose gradient w.r.t. y = H x is `r`
+ * (device buffers, client numbering, nrhs columns): accumulates (beta = 0 clears first)
+ *   dF += r_I x_J^T              per full leaf
+ *   dA += r_I (B^T x_J)^T        dB += x_J (A^T r_I)^T     per Rk leaf (A B^T)
+ * into `grad_full` / `grad_rk`, laid out like the arenas.  The gradient w.r.t. x is
+ * gemv('T') of r.  Real types only. */
+int hmat_b200_leaf_gradients(hmat_matrix_t* hmatrix, const void* x_dev, const void* r_dev, int nrhs,
+                             void* grad_full, void* grad_rk, int accumulate, void* stream);
+
+/* One eager product y = op(H) x on device buffers (1 to 16 right-hand sides), timed per
+ * phase with CUDA events: ms3 = device ms of [gather, z-phase, y-phase], bytes3 = their
+ * algorithmic bytes (x read and x_rm written; the B (A for 'T') factors; full leaves,
+ * A (B) factors and the y write).  Synchronous. */
+int hmat_b200_gemv_profile(hmat_matrix_t* hmatrix, char trans, const void* x_dev, void* y_dev, int nrhs, double* ms3,
+                           double* bytes3);
+
+/* Device time of the last phases on this matrix, milliseconds: [0] full assembly,
+ * [1] ACA, [2] truncation (+ compaction), [3] last gemv. */
+int hmat_b200_phase_times(hmat_matrix_t* hmatrix, double* out4);
+
+/* Last error message of the calling thread ("" if none). */
+const char* hmat_b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HMAT_B200_H */

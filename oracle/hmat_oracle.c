@@ -26,13 +26,18 @@ typedef struct {
   void* data;
 } oracle_leaf;
 
-struct oracle_hmat {
-  int n, leaf_size, is_complex;
-  double eta;
-  double* pts; /* client numbering, point-major */
-  int* perm;   /* internal -> client */
+typedef struct {
+  int leaf_size;
+  int* perm; /* internal -> client */
   oracle_node* nodes;
   int nnodes, cap_nodes;
+} oracle_tree;
+
+struct oracle_hmat {
+  int n, is_complex;
+  double eta;
+  double* pts; /* client numbering, point-major */
+  oracle_tree rt, ct; /* row and column cluster trees (same points) */
   oracle_leaf* leaves;
   int nleaves, cap_leaves;
   int nr_block_clusters;
@@ -42,7 +47,7 @@ struct oracle_hmat {
 /* Cluster tree: median bisection (clustering.cpp:108-152,257-301,488-565).             */
 /* ------------------------------------------------------------------------------------ */
 
-static int new_node(oracle_hmat* h, int offset, int size) {
+static int new_node(oracle_tree* h, int offset, int size) {
   if (h->nnodes == h->cap_nodes) {
     h->cap_nodes = h->cap_nodes ? 2 * h->cap_nodes : 64;
     h->nodes = (oracle_node*)realloc(h->nodes, sizeof(oracle_node) * h->cap_nodes);
@@ -56,11 +61,11 @@ static int new_node(oracle_hmat* h, int offset, int size) {
 }
 
 /* AxisAlignedBoundingBox(const ClusterData&) (cluster_tree.cpp:212-230) */
-static void compute_bbox(const oracle_hmat* h, int offset, int size, double* bb) {
+static void compute_bbox(const oracle_tree* h, const double* pts, int offset, int size, double* bb) {
   const int* idx = h->perm + offset;
-  for (int d = 0; d < 3; ++d) bb[d] = bb[d + 3] = h->pts[3 * (size_t)idx[0] + d];
+  for (int d = 0; d < 3; ++d) bb[d] = bb[d + 3] = pts[3 * (size_t)idx[0] + d];
   for (int i = 1; i < size; ++i) {
-    const double* p = h->pts + 3 * (size_t)idx[i];
+    const double* p = pts + 3 * (size_t)idx[i];
     for (int d = 0; d < 3; ++d) {
       double v = p[d];
       bb[d] = v < bb[d] ? v : bb[d];           /* std::min(bb, v) */
@@ -110,13 +115,13 @@ static void stable_sort_axis(int* idx, int n, const double* pts, int dim, int* t
   memcpy(idx, tmp, sizeof(int) * n);
 }
 
-static void divide_recursive(oracle_hmat* h, int node, int currentAxis, int* tmp) {
+static void divide_recursive(oracle_tree* h, const double* pts, int node, int currentAxis, int* tmp) {
   int offset = h->nodes[node].offset, size = h->nodes[node].size;
   if (size <= h->leaf_size) return;
   double bb[6];
-  compute_bbox(h, offset, size, bb);
+  compute_bbox(h, pts, offset, size, bb);
   int dim = largest_dimension(bb, currentAxis);
-  stable_sort_axis(h->perm + offset, size, h->pts, dim, tmp);
+  stable_sort_axis(h->perm + offset, size, pts, dim, tmp);
   int middle = size / 2; /* size * i / divider with divider 2 */
   int c0 = -1, c1;
   if (middle > 0) c0 = new_node(h, offset, middle);
@@ -125,7 +130,7 @@ static void divide_recursive(oracle_hmat* h, int node, int currentAxis, int* tmp
   if (c0 >= 0) h->nodes[node].child[k++] = c0;
   h->nodes[node].child[k++] = c1;
   h->nodes[node].nchild = k;
-  for (int c = 0; c < k; ++c) divide_recursive(h, h->nodes[node].child[c], dim, tmp);
+  for (int c = 0; c < k; ++c) divide_recursive(h, pts, h->nodes[node].child[c], dim, tmp);
 }
 
 /* ------------------------------------------------------------------------------------ */
@@ -160,18 +165,18 @@ static void add_leaf(oracle_hmat* h, int rn, int cn, int type) {
     h->leaves = (oracle_leaf*)realloc(h->leaves, sizeof(oracle_leaf) * h->cap_leaves);
   }
   oracle_leaf* L = &h->leaves[h->nleaves++];
-  L->row_off = h->nodes[rn].offset;
-  L->m = h->nodes[rn].size;
-  L->col_off = h->nodes[cn].offset;
-  L->n = h->nodes[cn].size;
+  L->row_off = h->rt.nodes[rn].offset;
+  L->m = h->rt.nodes[rn].size;
+  L->col_off = h->ct.nodes[cn].offset;
+  L->n = h->ct.nodes[cn].size;
   L->type = type;
   L->rank = type == 0 ? -1 : 0;
   L->data = NULL;
 }
 
 static void build_block(oracle_hmat* h, int rn, int cn) {
-  const oracle_node* R = &h->nodes[rn];
-  const oracle_node* C = &h->nodes[cn];
+  const oracle_node* R = &h->rt.nodes[rn];
+  const oracle_node* C = &h->ct.nodes[cn];
   h->nr_block_clusters++;
   if (R->size == 0 || C->size == 0) return; /* isVoid */
   double dr = bb_diameter(R->bb), dc = bb_diameter(C->bb);
@@ -190,42 +195,54 @@ static void build_block(oracle_hmat* h, int rn, int cn) {
   int nc = colsLeaf ? 1 : C->nchild;
   for (int j = 0; j < nc; ++j)
     for (int i = 0; i < nr; ++i) {
-      int rc = rowsLeaf ? rn : h->nodes[rn].child[i];
-      int cc = colsLeaf ? cn : h->nodes[cn].child[j];
+      int rc = rowsLeaf ? rn : R->child[i];
+      int cc = colsLeaf ? cn : C->child[j];
       build_block(h, rc, cc);
     }
 }
 
-oracle_hmat* oracle_create(const double* pts, int n, int leaf_size, double eta) {
+static void build_tree(oracle_tree* t, const double* pts, int n, int leaf_size) {
+  t->leaf_size = leaf_size;
+  t->perm = (int*)malloc(sizeof(int) * (size_t)n);
+  for (int i = 0; i < n; ++i) t->perm[i] = i;
+  int* tmp = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  int root = new_node(t, 0, n);
+  divide_recursive(t, pts, root, -1, tmp);
+  free(tmp);
+  for (int i = 0; i < t->nnodes; ++i)
+    if (t->nodes[i].size > 0) compute_bbox(t, pts, t->nodes[i].offset, t->nodes[i].size, t->nodes[i].bb);
+}
+
+oracle_hmat* oracle_create2(const double* pts, int n, int leaf_rows, int leaf_cols, double eta) {
   oracle_hmat* h = (oracle_hmat*)calloc(1, sizeof(oracle_hmat));
   h->n = n;
-  h->leaf_size = leaf_size;
   h->eta = eta;
   h->pts = (double*)malloc(sizeof(double) * 3 * (size_t)n);
   memcpy(h->pts, pts, sizeof(double) * 3 * (size_t)n);
-  h->perm = (int*)malloc(sizeof(int) * (size_t)n);
-  for (int i = 0; i < n; ++i) h->perm[i] = i;
-  int* tmp = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
-  int root = new_node(h, 0, n);
-  divide_recursive(h, root, -1, tmp);
-  free(tmp);
-  for (int i = 0; i < h->nnodes; ++i)
-    if (h->nodes[i].size > 0) compute_bbox(h, h->nodes[i].offset, h->nodes[i].size, h->nodes[i].bb);
-  build_block(h, root, root);
+  build_tree(&h->rt, h->pts, n, leaf_rows);
+  build_tree(&h->ct, h->pts, n, leaf_cols);
+  build_block(h, 0, 0);
   return h;
+}
+
+oracle_hmat* oracle_create(const double* pts, int n, int leaf_size, double eta) {
+  return oracle_create2(pts, n, leaf_size, leaf_size, eta);
 }
 
 void oracle_destroy(oracle_hmat* h) {
   if (!h) return;
   for (int i = 0; i < h->nleaves; ++i) free(h->leaves[i].data);
   free(h->leaves);
-  free(h->nodes);
-  free(h->perm);
+  free(h->rt.nodes);
+  free(h->rt.perm);
+  free(h->ct.nodes);
+  free(h->ct.perm);
   free(h->pts);
   free(h);
 }
 
-void oracle_perm(const oracle_hmat* h, int* out) { memcpy(out, h->perm, sizeof(int) * (size_t)h->n); }
+void oracle_perm(const oracle_hmat* h, int* out) { memcpy(out, h->rt.perm, sizeof(int) * (size_t)h->n); }
+void oracle_perm_cols(const oracle_hmat* h, int* out) { memcpy(out, h->ct.perm, sizeof(int) * (size_t)h->n); }
 
 int oracle_num_leaves(const oracle_hmat* h) { return h->nleaves; }
 
@@ -241,14 +258,14 @@ void oracle_leaves(const oracle_hmat* h, int* out) {
   }
 }
 
-int oracle_num_nodes(const oracle_hmat* h) { return h->nnodes; }
+int oracle_num_nodes(const oracle_hmat* h) { return h->rt.nnodes; }
 
 void oracle_nodes(const oracle_hmat* h, int* out) {
-  for (int i = 0; i < h->nnodes; ++i) {
-    out[4 * i + 0] = h->nodes[i].offset;
-    out[4 * i + 1] = h->nodes[i].size;
-    out[4 * i + 2] = h->nodes[i].child[0];
-    out[4 * i + 3] = h->nodes[i].child[1];
+  for (int i = 0; i < h->rt.nnodes; ++i) {
+    out[4 * i + 0] = h->rt.nodes[i].offset;
+    out[4 * i + 1] = h->rt.nodes[i].size;
+    out[4 * i + 2] = h->rt.nodes[i].child[0];
+    out[4 * i + 3] = h->rt.nodes[i].child[1];
   }
 }
 
@@ -320,6 +337,11 @@ void oracle_kernel_eval(const oracle_hmat* h, const oracle_kernel* k, int row, i
   }
 }
 
+static double complex complex_recip(double complex z) {
+  double d = creal(z) * creal(z) + cimag(z) * cimag(z);
+  return CMPLX(creal(z) / d, -cimag(z) / d);
+}
+
 /* ---- instantiate the leaf algorithms for double ---- */
 #define SC double
 #define FN(x) x##_r
@@ -327,6 +349,7 @@ void oracle_kernel_eval(const oracle_hmat* h, const oracle_kernel* k, int row, i
 #define CONJ(x) (x)
 #define REALP(x) (x)
 #define IAMAX_KEY(x) fabs(x)
+#define RECIP(x) (1.0 / (x))
 #define SC_EVAL(h, k, r, c) real_eval(h, k, r, c)
 #include "oracle_leaf.inc"
 #undef SC
@@ -335,6 +358,7 @@ void oracle_kernel_eval(const oracle_hmat* h, const oracle_kernel* k, int row, i
 #undef CONJ
 #undef REALP
 #undef IAMAX_KEY
+#undef RECIP
 #undef SC_EVAL
 
 /* ---- and for double complex ---- */
@@ -344,6 +368,7 @@ void oracle_kernel_eval(const oracle_hmat* h, const oracle_kernel* k, int row, i
 #define CONJ(x) conj(x)
 #define REALP(x) creal(x)
 #define IAMAX_KEY(x) (fabs(creal(x)) + fabs(cimag(x)))
+#define RECIP(x) complex_recip(x)
 #define SC_EVAL(h, k, r, c) complex_eval(h, k, r, c)
 #include "oracle_leaf.inc"
 #undef SC
@@ -352,16 +377,21 @@ void oracle_kernel_eval(const oracle_hmat* h, const oracle_kernel* k, int row, i
 #undef CONJ
 #undef REALP
 #undef IAMAX_KEY
+#undef RECIP
 #undef SC_EVAL
 
-int oracle_assemble(oracle_hmat* h, const oracle_kernel* k, double epsilon, int is_complex) {
+int oracle_assemble2(oracle_hmat* h, const oracle_kernel* k, double epsilon, int is_complex, int min_leaf) {
   if (is_complex != (k->kind == 2)) return 1;
   h->is_complex = is_complex;
   for (int i = 0; i < h->nleaves; ++i) {
-    if (is_complex) assemble_leaf_c(h, k, &h->leaves[i], epsilon);
-    else assemble_leaf_r(h, k, &h->leaves[i], epsilon);
+    if (is_complex) assemble_leaf_c(h, k, &h->leaves[i], epsilon, min_leaf);
+    else assemble_leaf_r(h, k, &h->leaves[i], epsilon, min_leaf);
   }
   return 0;
+}
+
+int oracle_assemble(oracle_hmat* h, const oracle_kernel* k, double epsilon, int is_complex) {
+  return oracle_assemble2(h, k, epsilon, is_complex, 0);
 }
 
 long long oracle_leaf_payload_size(const oracle_hmat* h, int i) {
@@ -380,12 +410,14 @@ void oracle_leaf_payload(const oracle_hmat* h, int i, double* out) {
 int oracle_gemv(const oracle_hmat* h, char trans, int nrhs, const double* x, double* y) {
   const int N = h->n;
   const size_t w = h->is_complex ? 2 : 1;
+  const int* pin = trans == 'N' ? h->ct.perm : h->rt.perm;
+  const int* pout = trans == 'N' ? h->rt.perm : h->ct.perm;
   double* xi = (double*)malloc(sizeof(double) * w * (size_t)N * nrhs);
   double* yi = (double*)calloc(w * (size_t)N * nrhs, sizeof(double));
   for (int r = 0; r < nrhs; ++r)
     for (int i = 0; i < N; ++i)
       for (size_t c = 0; c < w; ++c)
-        xi[w * ((size_t)r * N + i) + c] = x[w * ((size_t)r * N + h->perm[i]) + c];
+        xi[w * ((size_t)r * N + i) + c] = x[w * ((size_t)r * N + pin[i]) + c];
   for (int l = 0; l < h->nleaves; ++l) {
     if (h->is_complex)
       gemv_leaf_c(&h->leaves[l], trans, nrhs, (const double complex*)xi, (double complex*)yi, N);
@@ -395,7 +427,7 @@ int oracle_gemv(const oracle_hmat* h, char trans, int nrhs, const double* x, dou
   for (int r = 0; r < nrhs; ++r)
     for (int i = 0; i < N; ++i)
       for (size_t c = 0; c < w; ++c)
-        y[w * ((size_t)r * N + h->perm[i]) + c] = yi[w * ((size_t)r * N + i) + c];
+        y[w * ((size_t)r * N + pout[i]) + c] = yi[w * ((size_t)r * N + i) + c];
   free(xi);
   free(yi);
   return 0;

@@ -35,10 +35,14 @@ typedef struct {
 /* Builds the cluster tree on n points (point-major xyz) with leaves of at most
  * `leaf_size` points, and the block tree with the standard admissibility `eta`. */
 oracle_hmat* oracle_create(const double* pts, int n, int leaf_size, double eta);
+/* Same with separate row and column trees (same points, different leaf sizes). */
+oracle_hmat* oracle_create2(const double* pts, int n, int leaf_rows, int leaf_cols, double eta);
 void oracle_destroy(oracle_hmat* h);
 
-/* Internal -> client permutation (n ints), as hmat_cluster_get_indices returns it. */
+/* Internal -> client permutation (n ints) of the row (column) tree, as
+ * hmat_cluster_get_indices returns it. */
 void oracle_perm(const oracle_hmat* h, int* out);
+void oracle_perm_cols(const oracle_hmat* h, int* out);
 int oracle_num_leaves(const oracle_hmat* h);
 /* 6 ints per leaf: row offset, row size, col offset, col size, type (0 full, 1 rk), rank
  * (-1 for full leaves).  Leaves come in the reference's depth-first order. */
@@ -55,6 +59,9 @@ void oracle_info(const oracle_hmat* h, long long* out);
  * `epsilon` for admissible ones.  is_complex selects the double complex path (kernel 2).
  * Returns 0 on success. */
 int oracle_assemble(oracle_hmat* h, const oracle_kernel* k, double epsilon, int is_complex);
+/* Same, compressing admissible blocks with max(m, n) < min_leaf by a dense SVD (the
+ * reference's compressionMinLeafSize setting, assembly.cpp:59-64). */
+int oracle_assemble2(oracle_hmat* h, const oracle_kernel* k, double epsilon, int is_complex, int min_leaf);
 
 /* Payload size in scalars of leaf `i` (m*n for full, k*(m+n) for rk) and a copy of it:
  * full leaves column-major m x n; rk leaves A (m x k) then B (n x k), column-major.

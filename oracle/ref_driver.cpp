@@ -193,8 +193,12 @@ int run(const Params& p, hmat_value_t vt) {
   hmat_clustering_algorithm_t* median = hmat_create_clustering_median();
   hmat_clustering_algorithm_t* algo = hmat_create_clustering_max_dof(median, (int)p.num("leaf", 64));
   hmat_cluster_tree_t* ct = hmat_create_cluster_tree(pts.data(), 3, n, algo);
+  // optional second tree for the columns (same points, another leaf size)
+  const int leaf_cols = (int)p.num("leaf_cols", 0);
+  hmat_clustering_algorithm_t* algo_c = leaf_cols > 0 ? hmat_create_clustering_max_dof(median, leaf_cols) : nullptr;
+  hmat_cluster_tree_t* cct = algo_c ? hmat_create_cluster_tree(pts.data(), 3, n, algo_c) : ct;
   hmat_admissibility_t* adm = hmat_create_admissibility_standard(p.num("eta", 2.0));
-  hmat_matrix_t* M = hi.create_empty_hmatrix_admissibility(ct, ct, 0, adm);
+  hmat_matrix_t* M = hi.create_empty_hmatrix_admissibility(ct, cct, 0, adm);
   const double eps = p.num("eps", 1e-4);
   hi.set_low_rank_epsilon(M, eps);
   double t_build = now_s() - t0;
@@ -226,6 +230,7 @@ int run(const Params& p, hmat_value_t vt) {
   // Cluster permutation (internal -> client).
   const int* perm = hmat_cluster_get_indices(ct);
   write_file(out + ".perm", perm, sizeof(int) * (size_t)n);
+  write_file(out + ".permc", hmat_cluster_get_indices(cct), sizeof(int) * (size_t)n);
 
   // Leaves.
   hmat::HMatInterface<T>* hm = (hmat::HMatInterface<T>*)M;
@@ -244,6 +249,7 @@ int run(const Params& p, hmat_value_t vt) {
   const int nrhs = (int)p.num("nrhs", 1);
   const std::string trans = p.get("trans", "N");
   const int reps = (int)p.num("gemv_reps", 1);
+  const int warm = (int)p.num("gemv_warmup", 0);
   double t_gemv_first = 0, t_gemv_mean = 0;
   if (!p.get("x").empty()) {
     std::vector<char> xb = read_file(p.get("x"));
@@ -253,14 +259,16 @@ int run(const Params& p, hmat_value_t vt) {
     }
     std::vector<T> x((size_t)n * nrhs), y((size_t)n * nrhs);
     T alpha = T(1), beta = T(0);
-    for (int rep = 0; rep <= reps; ++rep) {
+    // the first call is timed on its own, then `warm` untimed calls, then `reps` timed ones
+    for (int rep = 0; rep <= warm + reps; ++rep) {
       memcpy(x.data(), xb.data(), xb.size());
       std::fill(y.begin(), y.end(), T(0));
       t0 = now_s();
       rc = hi.gemv(trans[0], &alpha, M, x.data(), &beta, y.data(), nrhs);
       double dt = now_s() - t0;
       if (rc) { fprintf(stderr, "gemv failed\n"); return 4; }
-      if (rep == 0) t_gemv_first = dt; else t_gemv_mean += dt / reps;
+      if (rep == 0) t_gemv_first = dt;
+      else if (rep > warm) t_gemv_mean += dt / reps;
     }
     write_file(out + ".y", y.data(), y.size() * sizeof(T));
   }
@@ -280,6 +288,8 @@ int run(const Params& p, hmat_value_t vt) {
 
   hi.destroy(M);
   hmat_delete_cluster_tree(ct);
+  if (cct != ct) hmat_delete_cluster_tree(cct);
+  if (algo_c) hmat_delete_clustering(algo_c);
   hmat_delete_admissibility(adm);
   hmat_delete_compression(ctx.compression);
   hmat_delete_clustering(algo);

@@ -1,0 +1,38 @@
+"""Inputs of the golden fixtures: seeded point clouds, kernels, tree parameters and
+right-hand sides (shared by make_golden.py and the tests that replay the cases)."""
+import importlib.util
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+
+spec = importlib.util.spec_from_file_location("workloads", os.path.join(ROOT, "hmat-oss_b200", "workloads.py"))
+wl = importlib.util.module_from_spec(spec)
+spec.loader.exec_module(wl)
+
+# name -> (points builder, kernel kwargs, tree/compression kwargs, nrhs, rhs seed, scalar, dump payload)
+CASES = {
+    "cfg0_laplace": (lambda: wl.cylinder(80, 100), dict(kind=0, delta=0.01), dict(leaf=64, eta=2.0, eps=1e-4), 1, 0,
+                     "D", False),
+    "cube_expcov": (lambda: wl.cube(800, 11), dict(kind=1, ell=0.3, nugget=1e-6), dict(leaf=32, eta=2.0, eps=1e-6), 3,
+                    12, "D", False),
+    "cube_expcov_payload": (lambda: wl.cube(300, 21), dict(kind=1, ell=0.2, nugget=1e-6),
+                            dict(leaf=16, eta=2.0, eps=1e-5), 1, 22, "D", True),
+    "helmholtz_small": (lambda: wl.cylinder(30, 40), dict(kind=2, delta=0.01, wavenumber=wl.helmholtz_wavenumber(1200)),
+                        dict(leaf=32, eta=3.0, eps=1e-4), 2, 13, "Z", False),
+    "helmholtz_payload": (lambda: wl.cylinder(15, 20), dict(kind=2, delta=0.01, wavenumber=wl.helmholtz_wavenumber(300)),
+                          dict(leaf=16, eta=3.0, eps=1e-4), 1, 23, "Z", True),
+    "tall_partial": (lambda: wl.cube(6000, 5), dict(kind=1, ell=0.3, nugget=1e-6),
+                     dict(leaf=2048, leaf_cols=16, eta=2.0, eps=1e-5), 1, 3, "D", False),
+    "svd_small": (lambda: wl.cylinder(40, 50), dict(kind=0, delta=0.01), dict(leaf=32, eta=2.0, eps=1e-4, min_leaf=100),
+                  2, 14, "D", False),
+}
+
+
+
+
+def inputs(name):
+    build, kern, tree, nrhs, seed, scalar, dump = CASES[name]
+    pts = build()
+    x = wl.rhs(len(pts), nrhs, seed, complex_=scalar in ("Z", "C"))
+    return pts, x

@@ -1,0 +1,138 @@
+"""Parity of the B200 engine (CUDA path, through the C ABI) with the reference library's
+outputs (golden fixtures) and with the oracle, on the GPU.
+
+FP64 engines (D, Z) must reproduce the reference's partition exactly, its ranks and leaf
+approximations (up to rare pivot-tie flips, which must stay within the compression
+epsilon of the exact block) and its products to 1e-12 relative.  Mixed-precision
+engines (S, C: FP32 bulk, FP64 truncation) are checked against the FP64 results within
+the compression epsilon.
+"""
+import numpy as np
+import pytest
+from cases import CASES, inputs
+from conftest import golden, rel
+
+pytestmark = pytest.mark.gpu
+
+VT = {"D": 1, "Z": 3}
+# Complex cases on the symmetric cylinder meet exact pivot ties (see test_oracle_golden).
+GEMV_TOL = {"helmholtz_small": 2e-6, "helmholtz_payload": 2e-6}
+
+
+def build_engine(hb, name, value_type=None, **over):
+    _, kern, tree, nrhs, seed, scalar, dump = CASES[name]
+    pts, x = inputs(name)
+    hb.set_parameters(compressionMinLeafSize=tree.get("min_leaf", 0))
+    k = hb.kernel(kern["kind"], delta=kern.get("delta", 0.01), ell=kern.get("ell", 0.3),
+                  nugget=kern.get("nugget", 0.0), wavenumber=kern.get("wavenumber", 0.0))
+    vt = VT[scalar] if value_type is None else value_type
+    h = hb.HMatrix(pts, k, value_type=vt, leaf_size=tree["leaf"], leaf_size_cols=tree.get("leaf_cols"),
+                   eta=tree["eta"], epsilon=tree["eps"], **over)
+    return h, pts, x, kern, tree
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fp64_engine_matches_reference(hb, name):
+    g = golden(name)
+    h, pts, x, kern, tree = build_engine(hb, name)
+    try:
+        T = h.leaf_table()
+        assert np.array_equal(h.perm(), g["perm"])
+        assert np.array_equal(h.perm(cols=True), g["perm_cols"])
+        assert np.array_equal(T[:, :5], g["leaves"][:, :5])
+        rk = g["leaves"][:, 4] == 1
+        mism = int((T[rk, 5] != g["leaves"][rk, 5]).sum())
+        assert mism <= max(1, rk.sum() // 100), f"{mism} rank mismatches"
+        tol = GEMV_TOL.get(name, 1e-12)
+        assert rel(h.gemv(x, "N"), g["y"]) < tol
+        assert rel(h.gemv(x, "T"), g["y_T"]) < tol
+        if "y_C" in g:
+            assert rel(h.gemv(x, "C"), g["y_C"]) < tol
+    finally:
+        h.close()
+
+
+@pytest.mark.parametrize("name", [n for n in sorted(CASES) if CASES[n][6]])
+def test_fp64_engine_rk_factors_match_reference(hb, oracle, name):
+    g = golden(name)
+    h, pts, x, kern, tree = build_engine(hb, name)
+    try:
+        T = h.leaf_table()
+        perm = h.perm()
+        pay = g["rk_payload"]
+        off = flips = nrk = 0
+        for i, (r0, m, c0, n, t, k) in enumerate(g["leaves"]):
+            if t != 1 or k <= 0:
+                continue
+            nrk += 1
+            A = pay[off:off + k * m].reshape(k, m).T
+            B = pay[off + k * m:off + k * (m + n)].reshape(k, n).T
+            off += k * (m + n)
+            Mr = A @ B.T
+            Me = h.leaf_block(i)
+            if rel(Me, Mr) < 1e-11:
+                continue
+            flips += 1
+            ex = oracle.kernel_matrix(pts[perm[r0:r0 + m]], pts[perm[c0:c0 + n]], **kern)
+            assert rel(Me, ex) < 10 * tree["eps"], (i, rel(Me, ex))
+        assert flips <= max(1, nrk // 100)
+        # full leaves are plain kernel entries: exact agreement with the FP64 formula
+        for i in np.nonzero(T[:, 4] == 0)[0][:50]:
+            r0, m, c0, n, t, k = T[i]
+            ex = oracle.kernel_matrix(pts[perm[r0:r0 + m]], pts[perm[c0:c0 + n]], **kern,
+                                      ids=(perm[r0:r0 + m], perm[c0:c0 + n]))
+            assert rel(h.leaf_block(i), ex) < 1e-14
+    finally:
+        h.close()
+
+
+@pytest.mark.parametrize("name", ["cfg0_laplace", "cube_expcov", "helmholtz_small"])
+def test_engine_matches_oracle(hb, oracle, name):
+    """Same inputs through the engine and the oracle: ranks and products."""
+    h, pts, x, kern, tree = build_engine(hb, name)
+    try:
+        o = oracle.OracleHMatrix(pts, leaf=tree["leaf"], eta=tree["eta"])
+        o.assemble(eps=tree["eps"], **kern)
+        tol = GEMV_TOL.get(name, 1e-12)
+        assert rel(h.gemv(x, "N"), o.gemv(x, "N")) < tol
+        assert rel(h.gemv(x, "T"), o.gemv(x, "T")) < tol
+    finally:
+        h.close()
+
+
+@pytest.mark.parametrize("name,vt", [("cfg0_laplace", 0), ("cube_expcov", 0), ("helmholtz_small", 2)])
+def test_mixed_precision_within_epsilon(hb, oracle, name, vt):
+    """FP32 bulk + FP64 truncation against the FP64 dense product: the error stays at
+    the compression epsilon level (not above the FP64 H-matrix's own error by more than
+    the FP32 rounding floor)."""
+    h64, pts, x, kern, tree = build_engine(hb, name)
+    h32, _, _, _, _ = build_engine(hb, name, value_type=vt)
+    try:
+        dense = oracle.dense_product(pts, x, **kern)
+        e64 = rel(h64.gemv(x), dense)
+        e32 = rel(h32.gemv(x.astype(np.complex64 if vt == 2 else np.float32)).astype(dense.dtype), dense)
+        assert e64 < 10 * tree["eps"]
+        assert e32 < max(2 * e64, 20 * tree["eps"]) + 1e-5, (e32, e64)
+        T64, T32 = h64.leaf_table(), h32.leaf_table()
+        assert np.array_equal(T64[:, :5], T32[:, :5])
+    finally:
+        h64.close()
+        h32.close()
+
+
+def test_gemv_alpha_beta_and_multi_rhs(hb, oracle):
+    h, pts, x, kern, tree = build_engine(hb, "cube_expcov")
+    try:
+        rng = np.random.default_rng(5)
+        X = np.asfortranarray(rng.standard_normal((len(pts), 21)))
+        Y0 = np.asfortranarray(rng.standard_normal((len(pts), 21)))
+        o = oracle.OracleHMatrix(pts, leaf=tree["leaf"], eta=tree["eta"])
+        o.assemble(eps=tree["eps"], **kern)
+        ref = 0.5 * o.gemv(X) - 2.0 * Y0
+        got = h.gemv(X, alpha=0.5, beta=-2.0, y=Y0)
+        assert rel(got, ref) < 1e-12
+        # one right-hand side at a time gives the same columns
+        for q in (0, 7, 20):
+            assert rel(h.gemv(X[:, q]), o.gemv(X[:, q])) < 1e-12
+    finally:
+        h.close()
