@@ -208,8 +208,11 @@ def main():
     def time_gemv(h, dtype):
         xd = torch.from_numpy(np.ascontiguousarray(x_host.T)).to(device="cuda", dtype=dtype)  # column-major N x r
         yd = torch.zeros_like(xd)
-        stream = torch.cuda.current_stream()
+        # an explicit stream: the engine launches on the stream it is given, and events
+        # recorded on that same stream bracket the timed region
+        stream = torch.cuda.Stream()
         sp = stream.cuda_stream
+        torch.cuda.synchronize()
         for _ in range(args.warmup):
             h.gemv_device(xd.data_ptr(), yd.data_ptr(), nrhs, stream=sp)
         torch.cuda.synchronize()

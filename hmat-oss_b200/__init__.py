@@ -288,7 +288,7 @@ class HMatrix:
         if y is None:
             y = np.zeros_like(x)
         else:
-            y = np.asfortranarray(y, dtype=self.dtype).copy()
+            y = np.array(y, dtype=self.dtype, order="F", copy=True)
         a = np.array([alpha], dtype=self.dtype)
         b = np.array([beta], dtype=self.dtype)
         _check(self.hi.gemv(trans.encode(), a.ctypes.data, self.m, x.ctypes.data, b.ctypes.data, y.ctypes.data,

@@ -8,7 +8,7 @@
 // i?amax rule (first index of the largest |x|, |Re|+|Im| for complex) and the
 // strict-minimum / strict-maximum first-index rules of the scalar loops, so the FP64
 // engine picks the reference's pivots.  Residual updates are per-element sequential in
-// the rank index with one FMA per term, like the axpy sequence they restate.
+// the rank index, each term rounded like the CPU axpy sequence they restate (see upd()).
 //
 // Vectors of a leaf live in its workspace slot (global memory, L1/L2 resident while the
 // CTA works on it); FP64 accumulators carry the Frobenius-norm estimate for every T.
@@ -46,7 +46,7 @@ struct Aca {
     __syncthreads();
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
       T v = entry(i, j);
-      for (int l = 0; l < k; ++l) v = fmadd(coef[l], B[(size_t)l * n + j], v);
+      for (int l = 0; l < k; ++l) v = upd(coef[l], B[(size_t)l * n + j], v);
       out[j] = v;
     }
     __syncthreads();
@@ -58,18 +58,18 @@ struct Aca {
     __syncthreads();
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
       T v = entry(i, j);
-      for (int l = 0; l < k; ++l) v = fmadd(coef[l], A[(size_t)l * m + i], v);
+      for (int l = 0; l < k; ++l) v = upd(coef[l], A[(size_t)l * m + i], v);
       out[i] = v;
     }
     __syncthreads();
   }
   __device__ void scale(T* v, int len, T s) {
-    for (int e = threadIdx.x; e < len; e += blockDim.x) v[e] = v[e] * s;
+    for (int e = threadIdx.x; e < len; e += blockDim.x) v[e] = mul_rn(v[e], s);
     __syncthreads();
   }
   // v += a * x
   __device__ void axpy(T a, const T* x, T* v, int len) {
-    for (int e = threadIdx.x; e < len; e += blockDim.x) v[e] = fmadd(a, x[e], v[e]);
+    for (int e = threadIdx.x; e < len; e += blockDim.x) v[e] = upd(a, x[e], v[e]);
     __syncthreads();
   }
   __device__ bool is_zero(const T* v, int len) {

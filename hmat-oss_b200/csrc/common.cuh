@@ -72,7 +72,13 @@ struct Traits<cdouble> {
 __device__ __host__ inline double abs2(float a) { return (double)a * (double)a; }
 __device__ __host__ inline double abs2(double a) { return a * a; }
 __device__ __host__ inline double abs2(cfloat a) { return (double)a.x * a.x + (double)a.y * a.y; }
-__device__ __host__ inline double abs2(cdouble a) { return a.x * a.x + a.y * a.y; }
+__device__ __host__ inline double abs2(cdouble a) {
+#ifdef __CUDA_ARCH__
+  return __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));  // no contraction: the host rounding
+#else
+  return a.x * a.x + a.y * a.y;
+#endif
+}
 
 // Ranking key of BLAS i?amax: |x| for real, |Re|+|Im| for complex (blas_overloads.hpp:159-180).
 __device__ inline double amax_key(float a) { return fabs((double)a); }
@@ -149,6 +155,7 @@ __device__ __host__ inline cdouble narrow<cdouble>(cdouble a) {
   return a;
 }
 
+#ifdef __CUDACC__  // device arithmetic (host translation units only need the types above)
 // acc + a * b with a single rounding per real multiply-add (the FMA form OpenBLAS axpy
 // kernels use on x86).
 __device__ inline float fmadd(float a, float b, float acc) { return fmaf(a, b, acc); }
@@ -160,17 +167,38 @@ __device__ inline cdouble fmadd(cdouble a, cdouble b, cdouble acc) {
   return cdouble{fma(-a.y, b.y, fma(a.x, b.x, acc.x)), fma(a.y, b.x, fma(a.x, b.y, acc.y))};
 }
 
-// 1 / z, as std::complex division computes it for the pivot scaling.
+// 1 / z for the pivot scaling: conj(z) / |z|^2, the textbook form the reference's
+// -ffast-math build evaluates, each operation rounded separately in FP64.
 __device__ inline float recip(float a) { return 1.0f / a; }
-__device__ inline double recip(double a) { return 1.0 / a; }
+__device__ inline double recip(double a) { return __ddiv_rn(1.0, a); }
 __device__ inline cfloat recip(cfloat a) {
   float d = a.x * a.x + a.y * a.y;
   return cfloat{a.x / d, -a.y / d};
 }
 __device__ inline cdouble recip(cdouble a) {
-  double d = a.x * a.x + a.y * a.y;
-  return cdouble{a.x / d, -a.y / d};
+  double d = __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));
+  return cdouble{__ddiv_rn(a.x, d), __ddiv_rn(-a.y, d)};
 }
+
+// Residual updates and scalings of ACA (v + a * x, v * s).  The FP64 engines round every
+// product and sum separately, as the reference's CPU arithmetic does (an FMA would round
+// once and change which of two tied pivot candidates wins); the FP32 engines use FMA.
+__device__ inline float upd(float a, float x, float v) { return fmaf(a, x, v); }
+__device__ inline cfloat upd(cfloat a, cfloat x, cfloat v) { return fmadd(a, x, v); }
+__device__ inline double upd(double a, double x, double v) { return __dadd_rn(v, __dmul_rn(a, x)); }
+__device__ inline cdouble upd(cdouble a, cdouble x, cdouble v) {
+  const double re = __dsub_rn(__dmul_rn(a.x, x.x), __dmul_rn(a.y, x.y));
+  const double im = __dadd_rn(__dmul_rn(a.x, x.y), __dmul_rn(a.y, x.x));
+  return cdouble{__dadd_rn(v.x, re), __dadd_rn(v.y, im)};
+}
+__device__ inline float mul_rn(float v, float s) { return v * s; }
+__device__ inline cfloat mul_rn(cfloat v, cfloat s) { return v * s; }
+__device__ inline double mul_rn(double v, double s) { return __dmul_rn(v, s); }
+__device__ inline cdouble mul_rn(cdouble v, cdouble s) {
+  return cdouble{__dsub_rn(__dmul_rn(v.x, s.x), __dmul_rn(v.y, s.y)),
+                 __dadd_rn(__dmul_rn(v.x, s.y), __dmul_rn(v.y, s.x))};
+}
+#endif  // __CUDACC__
 
 // ------------------------------------------------------------------------------------
 // Interaction kernels.  Entries are evaluated from cluster-ordered coordinates; the
@@ -199,7 +227,7 @@ struct Points {
 
 #define HB_FOUR_PI 12.566370614359172  // 4 * M_PI in double
 
-#ifdef __CUDACC__
+#ifdef __CUDACC__  // device arithmetic continues
 
 __device__ inline double dist_fp64(const Points& p, int i, int j) {
   double dx = __dsub_rn(p.rx[i], p.cx[j]);
