@@ -119,7 +119,8 @@ EXPORTED = [
     "hmat_create_compression_rrqr", "hmat_delete_compression", "hmat_default_progress",
     "hmat_assemble_context_init", "hmat_factorization_context_init", "hmat_solve_context_init",
     "hmat_init_default_interface", "hmat_get_parameters", "hmat_set_parameters", "hmat_get_version",
-    "hmat_b200_create_assembly", "hmat_b200_delete_assembly", "hmat_b200_gemv_device", "hmat_b200_leaf_count",
+    "hmat_b200_create_assembly", "hmat_b200_delete_assembly", "hmat_b200_gemv_device", "hmat_b200_gemv_device_noalloc",
+    "hmat_b200_leaf_count",
     "hmat_b200_leaf_table", "hmat_b200_leaf_payload", "hmat_b200_leaf_arenas", "hmat_b200_leaf_gradients",
     "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_last_error",
 ]
@@ -155,6 +156,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "hmat_b200_create_assembly": (_P, [C.POINTER(KernelDesc), _P, C.c_int]),
         "hmat_b200_delete_assembly": (None, [_P]),
         "hmat_b200_gemv_device": (C.c_int, [_P, C.c_char, _P, _P, _P, _P, C.c_int, _P]),
+        "hmat_b200_gemv_device_noalloc": (C.c_int, [_P, C.c_char, _P, _P, _P, _P, C.c_int, _P]),
         "hmat_b200_leaf_count": (C.c_int, [_P]),
         "hmat_b200_leaf_table": (C.c_int, [_P, _P]),
         "hmat_b200_leaf_payload": (C.c_longlong, [_P, C.c_int, _P]),
@@ -301,6 +303,14 @@ class HMatrix:
         _check(self.lib.hmat_b200_gemv_device(self.m, trans.encode(), a.ctypes.data, C.c_void_p(x_ptr),
                                               b.ctypes.data, C.c_void_p(y_ptr), nrhs, C.c_void_p(stream)),
                "hmat_b200_gemv_device")
+
+    def gemv_device_noalloc(self, x_ptr: int, y_ptr: int, nrhs: int, trans: str = "N", alpha=1.0, beta=0.0,
+                            stream=0) -> int:
+        """The allocation-free device gemv; returns the C return code (0 on success)."""
+        a = np.array([alpha], dtype=self.dtype)
+        b = np.array([beta], dtype=self.dtype)
+        return self.lib.hmat_b200_gemv_device_noalloc(self.m, trans.encode(), a.ctypes.data, C.c_void_p(x_ptr),
+                                                      b.ctypes.data, C.c_void_p(y_ptr), nrhs, C.c_void_p(stream))
 
     def info(self) -> dict:
         return self.hi.get_info(self.m).as_dict()

@@ -641,3 +641,9 @@ int hmat_b200_phase_times(hmat_matrix_t* m, double* out4) {
 const char* hmat_b200_last_error(void) { return g_last_error.c_str(); }
 
 }  // extern "C"
+
+// Internal helpers for the other translation units of the library (not exported).
+namespace hmatb200 {
+EngineBase* existing_engine(hmat_matrix_t* m) { return m ? m->engine.get() : nullptr; }
+int report_failure(const char* where, const std::string& msg) { return fail(where, msg); }
+}  // namespace hmatb200

@@ -273,6 +273,25 @@ class Engine : public EngineBase {
     bytes3[2] = (full + (trans == 'N' ? fa : fb)) * s + n_out * nrhs * s;
   }
 
+  size_t gemv_scratch_bytes() const override {
+    const size_t xr = (size_t)std::max(R_->n, C_->n) * 16 * sizeof(T);
+    const size_t z = (size_t)std::max(plan_.z_elems, 16LL) * sizeof(T);
+    return ((xr + 255) & ~(size_t)255) + z;
+  }
+
+  void gemv_device_with_scratch(char trans, const void* alpha, const void* x, const void* beta, void* y, int nrhs,
+                                cudaStream_t stream, void* scratch, size_t scratch_bytes) override {
+    check_gemv_args(trans, nrhs);
+    if (nrhs == 0) return;
+    if (gemv_scratch_bytes() > scratch_bytes) throw Error("scratch buffer too small for this matrix");
+    const size_t xr = (size_t)std::max(R_->n, C_->n) * 16 * sizeof(T);
+    T* x_rm = (T*)scratch;
+    T* z = (T*)((char*)scratch + ((xr + 255) & ~(size_t)255));
+    launch_gemv<T>(plan_, trans, nrhs, *(const T*)alpha, *(const T*)beta, (const T*)x, (T*)y, x_rm, z, z,
+                   stream ? stream : stream_);
+    HB_CUDA(cudaGetLastError());
+  }
+
   void retruncate(double eps) override {
     (void)eps;
     throw Error("re-truncation of an assembled matrix is not available yet");

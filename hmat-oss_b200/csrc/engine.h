@@ -42,6 +42,11 @@ class EngineBase {
   // One eager product on device buffers with events between its phases: device ms of
   // [gather, z-phase, y-phase] and their algorithmic bytes (nrhs <= 16).
   virtual void profile_gemv(char trans, const void* x, void* y, int nrhs, double* ms3, double* bytes3) = 0;
+  // Bytes of scratch one eager product needs (x in cluster order + the z buffer), and that
+  // product run eagerly with its scratch carved from `scratch` (no allocation, no graph).
+  virtual size_t gemv_scratch_bytes() const = 0;
+  virtual void gemv_device_with_scratch(char trans, const void* alpha, const void* x, const void* beta, void* y,
+                                        int nrhs, cudaStream_t stream, void* scratch, size_t scratch_bytes) = 0;
 
   bool assembled = false;
   std::vector<int> ranks;  // per leaf, -1 for full leaves

@@ -376,6 +376,26 @@ void hmat_b200_delete_assembly(void* assembly);
 int hmat_b200_gemv_device(hmat_matrix_t* hmatrix, char trans, const void* alpha, const void* x_dev,
                           const void* beta, void* y_dev, int nrhs, void* stream);
 
+/* hmat_b200_gemv_device for callers that cannot allocate device memory when they
+ * multiply (no counterpart in the reference's C API).  Callers inside a caching
+ * allocator or memory pool they do not control, inside callbacks where cudaMalloc /
+ * cudaFree would synchronise or deadlock, or in loops that forbid allocation after
+ * start-up can use it: it calls no cudaMalloc, cudaFree or other allocating routine and
+ * builds no CUDA graph.  Its scratch (x in cluster order and the per-leaf B^T x values) is
+ * one fixed 16 MiB device array compiled into the library: every GPU on which the
+ * library's device code is loaded holds it until the process exits.  Matrices whose
+ * product needs more scratch than that are rejected with a non-zero return and an
+ * error message (use hmat_b200_gemv_device for them).  The first call on each device
+ * looks up the array's device address (with that device current); make that first call
+ * before any stream capture.  Every call shares the one array, so calls that can overlap
+ * on the GPU (different streams, or different host threads, without ordering between
+ * them) race: order them on one stream.  The array keeps the previous call's contents;
+ * nothing in it needs to start at zero, since each product overwrites what it reads.
+ * Same arguments, maths and return convention as hmat_b200_gemv_device; `stream` NULL
+ * means the matrix's own stream. */
+int hmat_b200_gemv_device_noalloc(hmat_matrix_t* hmatrix, char trans, const void* alpha, const void* x_dev,
+                                  const void* beta, void* y_dev, int nrhs, void* stream);
+
 /* Leaf table: `n` leaves in the reference's depth-first order, 6 ints each: row offset,
  * rows, col offset, cols (cluster numbering), type (0 full, 1 rk), rank (-1 for full). */
 int hmat_b200_leaf_count(hmat_matrix_t* hmatrix);
