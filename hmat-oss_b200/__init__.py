@@ -121,7 +121,7 @@ EXPORTED = [
     "hmat_init_default_interface", "hmat_get_parameters", "hmat_set_parameters", "hmat_get_version",
     "hmat_b200_create_assembly", "hmat_b200_delete_assembly", "hmat_b200_gemv_device", "hmat_b200_gemv_device_noalloc",
     "hmat_b200_leaf_count",
-    "hmat_b200_leaf_table", "hmat_b200_leaf_payload", "hmat_b200_leaf_arenas", "hmat_b200_leaf_gradients",
+    "hmat_b200_leaf_table", "hmat_b200_leaf_payload", "hmat_b200_payload_layout", "hmat_b200_leaf_gradients",
     "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_last_error",
 ]
 
@@ -160,9 +160,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "hmat_b200_leaf_count": (C.c_int, [_P]),
         "hmat_b200_leaf_table": (C.c_int, [_P, _P]),
         "hmat_b200_leaf_payload": (C.c_longlong, [_P, C.c_int, _P]),
-        "hmat_b200_leaf_arenas": (C.c_int, [_P, C.POINTER(_P), C.POINTER(C.c_longlong), C.POINTER(_P),
-                                            C.POINTER(C.c_longlong), _P]),
-        "hmat_b200_leaf_gradients": (C.c_int, [_P, _P, _P, C.c_int, _P, _P, C.c_int, _P]),
+        "hmat_b200_payload_layout": (C.c_int, [_P, _P, C.POINTER(C.c_longlong)]),
+        "hmat_b200_leaf_gradients": (C.c_int, [_P, _P, _P, C.c_int, _P, C.c_int, _P]),
         "hmat_b200_phase_times": (C.c_int, [_P, _P]),
         "hmat_b200_gemv_profile": (C.c_int, [_P, C.c_char, _P, _P, C.c_int, _P, _P]),
         "hmat_b200_last_error": (C.c_char_p, []),
@@ -346,19 +345,18 @@ class HMatrix:
         B = p[k * m:].reshape(k, n).T
         return A @ B.T
 
-    def arenas(self):
+    def payload_layout(self):
+        """Canonical payload offsets per leaf and the total number of scalars."""
         n = self.lib.hmat_b200_leaf_count(self.m)
-        full, rk = C.c_void_p(), C.c_void_p()
-        fe, re = C.c_longlong(), C.c_longlong()
         offs = np.zeros(n, dtype=np.int64)
-        _check(self.lib.hmat_b200_leaf_arenas(self.m, C.byref(full), C.byref(fe), C.byref(rk), C.byref(re),
-                                              offs.ctypes.data), "hmat_b200_leaf_arenas")
-        return (full.value or 0, fe.value, rk.value or 0, re.value, offs)
+        tot = C.c_longlong()
+        _check(self.lib.hmat_b200_payload_layout(self.m, offs.ctypes.data, C.byref(tot)), "hmat_b200_payload_layout")
+        return offs, tot.value
 
-    def leaf_gradients(self, x_ptr, r_ptr, nrhs, gfull_ptr, grk_ptr, accumulate=False, stream=0):
+    def leaf_gradients(self, x_ptr, r_ptr, nrhs, grad_ptr, accumulate=False, stream=0):
         _check(self.lib.hmat_b200_leaf_gradients(self.m, C.c_void_p(x_ptr), C.c_void_p(r_ptr), nrhs,
-                                                 C.c_void_p(gfull_ptr), C.c_void_p(grk_ptr), int(accumulate),
-                                                 C.c_void_p(stream)), "hmat_b200_leaf_gradients")
+                                                 C.c_void_p(grad_ptr), int(accumulate), C.c_void_p(stream)),
+               "hmat_b200_leaf_gradients")
 
     def gemv_profile(self, x_ptr: int, y_ptr: int, nrhs: int, trans: str = "N"):
         ms = np.zeros(3)

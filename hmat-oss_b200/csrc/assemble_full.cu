@@ -7,16 +7,22 @@
 namespace hmatb200 {
 namespace {
 
+// Each leaf is stored as row panels (one per output block of its rows), each panel
+// column-major len x n.
 template <typename T>
 __global__ void __launch_bounds__(256) assemble_full_kernel(const FullLeafDesc* __restrict__ leaves, int nleaves,
-                                                            KernelParams kp, Points pts, T* __restrict__ arena) {
+                                                            const PanelDesc* __restrict__ panels, KernelParams kp,
+                                                            Points pts, T* __restrict__ arena) {
   for (int leaf = blockIdx.x; leaf < nleaves; leaf += gridDim.x) {
     const FullLeafDesc d = leaves[leaf];
-    T* F = arena + d.off;
-    const int mn = d.m * d.n;
-    for (int e = threadIdx.x; e < mn; e += blockDim.x) {
-      const int i = e % d.m, j = e / d.m;
-      F[e] = KernelEval<T>::eval(kp, pts, d.row_off + i, d.col_off + j);
+    for (int p = 0; p < d.npanel; ++p) {
+      const PanelDesc P = panels[d.panel_first + p];
+      T* F = arena + P.off;
+      const int mn = P.len * d.n;
+      for (int e = threadIdx.x; e < mn; e += blockDim.x) {
+        const int i = e % P.len, j = e / P.len;
+        F[e] = KernelEval<T>::eval(kp, pts, d.row_off + P.rs + i, d.col_off + j);
+      }
     }
   }
 }
@@ -24,16 +30,17 @@ __global__ void __launch_bounds__(256) assemble_full_kernel(const FullLeafDesc* 
 }  // namespace
 
 template <typename T>
-void launch_assemble_full(const FullLeafDesc* d_leaves, int nleaves, const KernelParams& kp, Points pts,
-                          T* arena, cudaStream_t s) {
+void launch_assemble_full(const FullLeafDesc* d_leaves, int nleaves, const PanelDesc* panels, const KernelParams& kp,
+                          Points pts, T* arena, cudaStream_t s) {
   if (nleaves <= 0) return;
   int grid = persistent_grid(8);
   if (grid > nleaves) grid = nleaves;
-  assemble_full_kernel<T><<<grid, 256, 0, s>>>(d_leaves, nleaves, kp, pts, arena);
+  assemble_full_kernel<T><<<grid, 256, 0, s>>>(d_leaves, nleaves, panels, kp, pts, arena);
 }
 
-#define HB_INST(T) \
-  template void launch_assemble_full<T>(const FullLeafDesc*, int, const KernelParams&, Points, T*, cudaStream_t);
+#define HB_INST(T)                                                                                      \
+  template void launch_assemble_full<T>(const FullLeafDesc*, int, const PanelDesc*, const KernelParams&, \
+                                        Points, T*, cudaStream_t);
 HB_INST(float)
 HB_INST(double)
 HB_INST(cfloat)

@@ -604,21 +604,20 @@ long long hmat_b200_leaf_payload(hmat_matrix_t* m, int leaf, void* out) {
   }
 }
 
-int hmat_b200_leaf_arenas(hmat_matrix_t* m, void** full, long long* full_elems, void** rk, long long* rk_elems,
-                          long long* offsets) {
-  HB_TRY("hmat_b200_leaf_arenas", {
+int hmat_b200_payload_layout(hmat_matrix_t* m, long long* offsets, long long* total) {
+  HB_TRY("hmat_b200_payload_layout", {
     if (!m) throw Error("null matrix");
     if (!engine_of(m).assembled) throw Error("matrix is not assembled");
-    m->engine->arenas(full, full_elems, rk, rk_elems, offsets);
+    m->engine->payload_layout(offsets, total);
   });
   return 0;
 }
 
-int hmat_b200_leaf_gradients(hmat_matrix_t* m, const void* x, const void* r, int nrhs, void* gfull, void* grk,
-                             int accumulate, void* stream) {
+int hmat_b200_leaf_gradients(hmat_matrix_t* m, const void* x, const void* r, int nrhs, void* grad, int accumulate,
+                             void* stream) {
   HB_TRY("hmat_b200_leaf_gradients", {
-    if (!m || !x || !r) throw Error("null argument");
-    engine_of(m).leaf_gradients(x, r, nrhs, gfull, grk, accumulate != 0, (cudaStream_t)stream);
+    if (!m || !x || !r || !grad) throw Error("null argument");
+    engine_of(m).leaf_gradients(x, r, nrhs, grad, accumulate != 0, (cudaStream_t)stream);
   });
   return 0;
 }

@@ -10,9 +10,9 @@
 #include "gemv_plan.h"
 #include "kernels.h"
 
-#define HB_CUDA(x)                                                                                  \
-  do {                                                                                              \
-    cudaError_t e_ = (x);                                                                           \
+#define HB_CUDA(x)                                                                                          \
+  do {                                                                                                      \
+    cudaError_t e_ = (x);                                                                                   \
     if (e_ != cudaSuccess) throw Error(std::string("CUDA error: ") + cudaGetErrorString(e_) + " in " #x); \
   } while (0)
 
@@ -66,18 +66,54 @@ int initial_kcap() {
   return k < 4 ? 4 : k;
 }
 
+// Output blocks of a cluster tree: its leaves in cluster order, cut into near-equal pieces
+// of at most 128 rows (the row capacity of a gemv task).
+struct Block {
+  int off, len;
+};
+std::vector<Block> output_blocks(const ClusterTree& t) {
+  std::vector<Block> b;
+  for (int nd : t.leaf_nodes) {
+    const int off = t.nodes[nd].offset, size = t.nodes[nd].size;
+    if (size == 0) continue;
+    const int nb = (size + 127) / 128, base = size / nb, rem = size % nb;
+    int o = off;
+    for (int i = 0; i < nb; ++i) {
+      const int len = base + (i < rem ? 1 : 0);
+      b.push_back(Block{o, len});
+      o += len;
+    }
+  }
+  return b;
+}
+// Blocks covering [off, off + len) (a union of blocks, since cluster ranges are).
+std::pair<int, int> block_range(const std::vector<Block>& b, const std::vector<int>& starts, int off, int len) {
+  int first = (int)(std::upper_bound(starts.begin(), starts.end(), off) - starts.begin()) - 1;
+  int last = first;
+  while (last < (int)b.size() && b[last].off < off + len) ++last;
+  return {first, last};
+}
+
 template <typename T>
 class Engine : public EngineBase {
-  struct SideBufs;
   struct Piece;
 
  public:
+  static constexpr int kPad = 16 / (int)sizeof(T) > 0 ? 16 / (int)sizeof(T) : 1;  // 16-byte alignment (elements)
+  static long long padded(long long e) { return (e + kPad - 1) / kPad * kPad; }
+
   Engine(const ClusterTree* rows, const ClusterTree* cols, const BlockTree* bt) : R_(rows), C_(cols), bt_(bt) {
     HB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     for (auto& e : ev_) HB_CUDA(cudaEventCreate(&e));
     ranks.assign(bt_->leaves.size(), -1);
     for (size_t i = 0; i < bt_->leaves.size(); ++i)
       if (bt_->leaves[i].type == 1) ranks[i] = 0;
+    rblocks_ = output_blocks(*R_);
+    cblocks_ = output_blocks(*C_);
+    for (auto& b : rblocks_) rstarts_.push_back(b.off);
+    for (auto& b : cblocks_) cstarts_.push_back(b.off);
+    err_.alloc(1);
+    HB_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
   }
   ~Engine() override {
     if (gexec_) cudaGraphExecDestroy(gexec_);
@@ -102,34 +138,59 @@ class Engine : public EngineBase {
     upload_points(a);
     const auto& L = bt_->leaves;
     const int nleaves = (int)L.size();
-    full_off_.assign(nleaves, -1);
-    rk_off_.assign(nleaves, -1);
+    leaf_off_.assign(nleaves, -1);
+    times_ms[0] = times_ms[1] = times_ms[2] = 0;
 
-    // ---- full leaves ----
+    // ---- layout of the full leaves (row panels) ----
     std::vector<FullLeafDesc> fd;
-    long long fel = 0;
+    std::vector<PanelDesc> fpanels;
+    long long pos = 0;
     for (int i = 0; i < nleaves; ++i) {
       if (L[i].type != 0 || L[i].m == 0 || L[i].n == 0) continue;
-      FullLeafDesc d{L[i].row_off, L[i].m, L[i].col_off, L[i].n, fel};
-      full_off_[i] = fel;
-      fel += pad32((long long)L[i].m * L[i].n);
+      FullLeafDesc d{L[i].row_off, L[i].m, L[i].col_off, L[i].n, (int)fpanels.size(), 0};
+      leaf_off_[i] = pos;
+      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
+      for (int b = br.first; b < br.second; ++b) {
+        fpanels.push_back(PanelDesc{rblocks_[b].off - L[i].row_off, rblocks_[b].len, pos});
+        pos += padded((long long)rblocks_[b].len * L[i].n);
+        d.npanel++;
+      }
       fd.push_back(d);
     }
-    full_arena_.alloc((size_t)std::max(fel, 1LL));
-    full_elems_ = fel;
+    const long long full_total = pad32(pos);
+
+    // ---- admissible leaves: ACA / SVD, truncation, compaction into pieces ----
+    assemble_rk(method, eps_aca, eps_trunc, svd_below);
+    long long rk_total = 0;
+    for (auto& pc : pieces_) rk_total += pad32(pc.elems);
+
+    // ---- final arena: full leaves, then the Rk pieces ----
+    arena_.alloc((size_t)(full_total + rk_total + 256));
+    arena_elems_ = full_total + rk_total;
     DevArray<FullLeafDesc> d_fd;
+    DevArray<PanelDesc> d_fp;
     d_fd.upload(fd, stream_);
+    d_fp.upload(fpanels, stream_);
     HB_CUDA(cudaEventRecord(ev_[0], stream_));
-    launch_assemble_full<T>(d_fd.p, (int)fd.size(), kp_, pts_, full_arena_.p, stream_);
+    launch_assemble_full<T>(d_fd.p, (int)fd.size(), d_fp.p, kp_, pts_, arena_.p, stream_);
     HB_CUDA(cudaGetLastError());
     HB_CUDA(cudaEventRecord(ev_[1], stream_));
+    long long base = full_total;
+    std::vector<long long> piece_base(pieces_.size());
+    for (size_t p = 0; p < pieces_.size(); ++p) {
+      piece_base[p] = base;
+      if (pieces_[p].elems)
+        HB_CUDA(cudaMemcpyAsync(arena_.p + base, pieces_[p].arena.p, pieces_[p].elems * sizeof(T),
+                                cudaMemcpyDeviceToDevice, stream_));
+      base += pad32(pieces_[p].elems);
+    }
+    for (int i = 0; i < nleaves; ++i)
+      if (L[i].type == 1 && piece_of_[i] >= 0) leaf_off_[i] += piece_base[piece_of_[i]];
     HB_CUDA(cudaStreamSynchronize(stream_));
     float ms = 0;
     HB_CUDA(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
     times_ms[0] = ms;
-
-    // ---- admissible leaves ----
-    assemble_rk(method, eps_aca, eps_trunc, svd_below);
+    pieces_.clear();
     build_plan();
     HB_CUDA(cudaStreamSynchronize(stream_));
     assembled = true;
@@ -141,9 +202,8 @@ class Engine : public EngineBase {
     check_gemv_args(trans, nrhs);
     if (nrhs == 0) return;
     const T a = *(const T*)alpha, b = *(const T*)beta;
-    x_rm_.ensure((size_t)std::max(R_->n, C_->n) * 16);
-    zbuf_.ensure((size_t)std::max(plan_.z_elems, 16LL));
-    GraphKey key{trans, nrhs, x, y};
+    xz_.ensure(xz_elems());
+    GraphKey key(trans, nrhs, x, y);
     memcpy(key.ab, &a, sizeof(T));
     memcpy(key.ab + sizeof(T), &b, sizeof(T));
     if (!gexec_ || memcmp(&key, &gkey_, sizeof(GraphKey)) != 0) {
@@ -153,7 +213,7 @@ class Engine : public EngineBase {
       }
       cudaGraph_t g;
       HB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-      launch_gemv<T>(plan_, trans, nrhs, a, b, (const T*)x, (T*)y, x_rm_.p, zbuf_.p, zbuf_.p, stream_);
+      launch_gemv<T>(plan_, trans, nrhs, a, b, (const T*)x, (T*)y, xz_.p, err_.p, stream_);
       cudaError_t launch_err = cudaGetLastError();
       HB_CUDA(cudaStreamEndCapture(stream_, &g));
       HB_CUDA(launch_err);
@@ -166,7 +226,6 @@ class Engine : public EngineBase {
     HB_CUDA(cudaEventRecord(ev_[6], s));
     HB_CUDA(cudaGraphLaunch(gexec_, s));
     HB_CUDA(cudaEventRecord(ev_[7], s));
-    gemv_timed_ = true;
   }
 
   void gemv_host(char trans, const void* alpha, const void* x, const void* beta, void* y, int nrhs) override {
@@ -183,6 +242,7 @@ class Engine : public EngineBase {
     HB_CUDA(cudaMemcpyAsync(y, stage_y_.p, n_out * nrhs * sizeof(T), cudaMemcpyDeviceToHost, stream_));
     HB_CUDA(cudaStreamSynchronize(stream_));
     HB_CUDA(cudaGetLastError());
+    check_err_flag();
     float ms = 0;
     if (cudaEventElapsedTime(&ms, ev_[6], ev_[7]) == cudaSuccess) times_ms[3] = ms;
   }
@@ -191,56 +251,68 @@ class Engine : public EngineBase {
   long long leaf_payload(int leaf, void* out) override {
     if (!assembled || leaf < 0 || leaf >= (int)bt_->leaves.size()) return -1;
     const LeafInfo& L = bt_->leaves[leaf];
-    long long cnt = 0;
-    const T* src = nullptr;
-    if (L.type == 0) {
-      if (full_off_[leaf] < 0) return 0;
-      cnt = (long long)L.m * L.n;
-      src = full_arena_.p + full_off_[leaf];
-    } else {
-      if (ranks[leaf] <= 0) return 0;
-      cnt = (long long)ranks[leaf] * (L.m + L.n);
-      src = rk_arena_.p + rk_off_[leaf];
+    if (leaf_off_[leaf] < 0) return 0;
+    const int k = ranks[leaf];
+    if (L.type == 1 && k <= 0) return 0;
+    auto br = block_range(rblocks_, rstarts_, L.row_off, L.m);
+    const int w = L.type == 0 ? L.n : k;  // columns of a row panel
+    long long span = 0;
+    for (int b = br.first; b < br.second; ++b) span += padded((long long)rblocks_[b].len * w);
+    const long long bt_off = span;
+    if (L.type == 1) span += (long long)k * L.n;
+    std::vector<T> h((size_t)span);
+    HB_CUDA(cudaMemcpy(h.data(), arena_.p + leaf_off_[leaf], span * sizeof(T), cudaMemcpyDeviceToHost));
+    T* o = (T*)out;
+    long long p = 0;
+    for (int b = br.first; b < br.second; ++b) {  // row panels -> column-major m x w
+      const int rs = rblocks_[b].off - L.row_off, len = rblocks_[b].len;
+      for (int j = 0; j < w; ++j)
+        for (int i = 0; i < len; ++i) o[(size_t)rs + i + (size_t)j * L.m] = h[p + i + (size_t)j * len];
+      p += padded((long long)len * w);
     }
-    HB_CUDA(cudaMemcpy(out, src, cnt * sizeof(T), cudaMemcpyDeviceToHost));
-    return cnt;
+    if (L.type == 0) return (long long)L.m * L.n;
+    T* Bo = o + (size_t)L.m * k;  // B^T (k x n) -> B (n x k)
+    for (int j = 0; j < L.n; ++j)
+      for (int l = 0; l < k; ++l) Bo[j + (size_t)l * L.n] = h[bt_off + l + (size_t)j * k];
+    return (long long)k * (L.m + L.n);
   }
 
-  void arenas(void** full, long long* full_elems, void** rk, long long* rk_elems, long long* offsets) override {
-    if (full) *full = full_arena_.p;
-    if (full_elems) *full_elems = full_elems_;
-    if (rk) *rk = rk_arena_.p;
-    if (rk_elems) *rk_elems = rk_elems_;
-    if (offsets)
-      for (size_t i = 0; i < bt_->leaves.size(); ++i)
-        offsets[i] = bt_->leaves[i].type == 0 ? full_off_[i] : rk_off_[i];
+  void payload_layout(long long* offsets, long long* total) override {
+    long long acc = 0;
+    const auto& L = bt_->leaves;
+    for (size_t i = 0; i < L.size(); ++i) {
+      if (offsets) offsets[i] = acc;
+      if (L[i].type == 0) acc += (long long)L[i].m * L[i].n;
+      else if (ranks[i] > 0) acc += (long long)ranks[i] * (L[i].m + L[i].n);
+    }
+    if (total) *total = acc;
   }
 
-  void leaf_gradients(const void* x, const void* r, int nrhs, void* gfull, void* grk, bool accumulate,
+  void leaf_gradients(const void* x, const void* r, int nrhs, void* grad, bool accumulate,
                       cudaStream_t user_stream) override {
     if (!assembled) throw Error("matrix is not assembled");
     if (Traits<T>::is_complex) throw Error("leaf gradients are implemented for real value types");
     if (nrhs < 1 || nrhs > 16) throw Error("leaf gradients take 1 to 16 right-hand sides");
-    const size_t nmax = (size_t)std::max(R_->n, C_->n);
-    x_rm_.ensure(nmax * 16);
-    r_rm_.ensure(nmax * 16);
-    zbuf_.ensure((size_t)std::max(plan_.z_elems, 16LL));
-    zbuf2_.ensure((size_t)std::max(plan_.z_elems, 16LL));
+    xz_.ensure(xz_elems());
+    rz_.ensure(xz_elems());
     cudaStream_t s = user_stream ? user_stream : stream_;
-    launch_leaf_gradients<T>(plan_, nrhs, (const T*)x, (const T*)r, x_rm_.p, r_rm_.p, zbuf_.p, zbuf2_.p, (T*)gfull,
-                             (T*)grk, accumulate, s);
+    launch_leaf_gradients<T>(plan_, nrhs, (const T*)x, (const T*)r, xz_.p, rz_.p, (T*)grad, (T*)grad, accumulate,
+                             err_.p, s);
     HB_CUDA(cudaGetLastError());
+  }
+
+  void retruncate(double eps) override {
+    (void)eps;
+    throw Error("re-truncation of an assembled matrix is not available yet");
   }
 
   void profile_gemv(char trans, const void* x, void* y, int nrhs, double* ms3, double* bytes3) override {
     check_gemv_args(trans, nrhs);
     if (nrhs < 1 || nrhs > 16) throw Error("profile_gemv takes 1 to 16 right-hand sides");
-    x_rm_.ensure((size_t)std::max(R_->n, C_->n) * 16);
-    zbuf_.ensure((size_t)std::max(plan_.z_elems, 16LL));
+    xz_.ensure(xz_elems());
     GemvTiming tm;
     for (int i = 0; i < 4; ++i) HB_CUDA(cudaEventCreate(&tm.ev[i]));
-    const T one_v = one<T>(), zero_v = zero<T>();
-    launch_gemv<T>(plan_, trans, nrhs, one_v, zero_v, (const T*)x, (T*)y, x_rm_.p, zbuf_.p, zbuf_.p, stream_, &tm);
+    launch_gemv<T>(plan_, trans, nrhs, one<T>(), zero<T>(), (const T*)x, (T*)y, xz_.p, err_.p, stream_, &tm);
     cudaError_t le = cudaGetLastError();
     cudaError_t se = cudaStreamSynchronize(stream_);
     float a = 0, b = 0, c = 0;
@@ -252,16 +324,15 @@ class Engine : public EngineBase {
     for (int i = 0; i < 4; ++i) cudaEventDestroy(tm.ev[i]);
     HB_CUDA(le);
     HB_CUDA(se);
+    check_err_flag();
     ms3[0] = a;
     ms3[1] = b;
     ms3[2] = c;
-    // algorithmic bytes: x read + x_rm write; B (A for 'T') factors; full leaves, A (B)
-    // factors and the y write
     const double s = sizeof(T);
     const auto& L = bt_->leaves;
     double full = 0, fa = 0, fb = 0;
     for (size_t i = 0; i < L.size(); ++i) {
-      if (L[i].type == 0 && full_off_[i] >= 0) full += (double)L[i].m * L[i].n;
+      if (L[i].type == 0 && leaf_off_[i] >= 0) full += (double)L[i].m * L[i].n;
       if (L[i].type == 1 && ranks[i] > 0) {
         fa += (double)L[i].m * ranks[i];
         fb += (double)L[i].n * ranks[i];
@@ -273,28 +344,19 @@ class Engine : public EngineBase {
     bytes3[2] = (full + (trans == 'N' ? fa : fb)) * s + n_out * nrhs * s;
   }
 
-  size_t gemv_scratch_bytes() const override {
-    const size_t xr = (size_t)std::max(R_->n, C_->n) * 16 * sizeof(T);
-    const size_t z = (size_t)std::max(plan_.z_elems, 16LL) * sizeof(T);
-    return ((xr + 255) & ~(size_t)255) + z;
-  }
+  size_t gemv_scratch_bytes() const override { return 256 + xz_elems() * sizeof(T); }
 
   void gemv_device_with_scratch(char trans, const void* alpha, const void* x, const void* beta, void* y, int nrhs,
                                 cudaStream_t stream, void* scratch, size_t scratch_bytes) override {
     check_gemv_args(trans, nrhs);
     if (nrhs == 0) return;
     if (gemv_scratch_bytes() > scratch_bytes) throw Error("scratch buffer too small for this matrix");
-    const size_t xr = (size_t)std::max(R_->n, C_->n) * 16 * sizeof(T);
-    T* x_rm = (T*)scratch;
-    T* z = (T*)((char*)scratch + ((xr + 255) & ~(size_t)255));
-    launch_gemv<T>(plan_, trans, nrhs, *(const T*)alpha, *(const T*)beta, (const T*)x, (T*)y, x_rm, z, z,
-                   stream ? stream : stream_);
+    int* err = (int*)scratch;
+    T* xz = (T*)((char*)scratch + 256);
+    cudaStream_t s = stream ? stream : stream_;
+    HB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    launch_gemv<T>(plan_, trans, nrhs, *(const T*)alpha, *(const T*)beta, (const T*)x, (T*)y, xz, err, s);
     HB_CUDA(cudaGetLastError());
-  }
-
-  void retruncate(double eps) override {
-    (void)eps;
-    throw Error("re-truncation of an assembled matrix is not available yet");
   }
 
  private:
@@ -314,10 +376,23 @@ class Engine : public EngineBase {
     }
   };
 
+  size_t xz_elems() const {
+    return (size_t)std::max(plan_.xz_rows, 1LL) * gemv_rhs_stride((int)sizeof(T), 16);
+  }
+
   void check_gemv_args(char trans, int nrhs) {
     if (!assembled) throw Error("matrix is not assembled");
     if (trans != 'N' && trans != 'T' && trans != 'C') throw Error("gemv: trans must be 'N', 'T' or 'C'");
     if (nrhs < 0) throw Error("gemv: negative number of right-hand sides");
+  }
+
+  void check_err_flag() {
+    int e = 0;
+    HB_CUDA(cudaMemcpy(&e, err_.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+      HB_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
+      throw Error("gemv: a shared-memory pipeline wait gave up (copy did not complete)");
+    }
   }
 
   void upload_points(const AssemblyDesc& a) {
@@ -346,10 +421,14 @@ class Engine : public EngineBase {
     int kcap;
     bool svd;
   };
+  struct Piece {
+    DevArray<T> arena;
+    long long elems = 0;
+  };
 
   // Runs ACA (or the dense-SVD fill) and the truncation on one batch of admissible
   // leaves; leaves that ran out of rank capacity are returned in `retry`, the others are
-  // compacted into a new piece.
+  // compacted (A as row panels, B transposed) into a new piece.
   void run_batch(const std::vector<RkJob>& jobs, double eps_aca, double eps_trunc, std::vector<RkJob>& retry) {
     const auto& L = bt_->leaves;
     const int nb = (int)jobs.size();
@@ -373,7 +452,6 @@ class Engine : public EngineBase {
       max_n = std::max(max_n, l.n);
       max_cap = std::max(max_cap, d.kcap);
     }
-    // cost-sorted orders (largest first) for the ACA and dense-fill groups
     std::vector<int> aca_order, svd_order;
     for (int b = 0; b < nb; ++b) (jobs[b].svd ? svd_order : aca_order).push_back(b);
     auto cost = [&](int b) { return (double)(desc[b].m + desc[b].n) * std::min(desc[b].m, desc[b].n); };
@@ -392,6 +470,7 @@ class Engine : public EngineBase {
     HB_CUDA(cudaMemsetAsync(d_status.p, 0, nb * sizeof(int), stream_));
     d_aca_order.upload(aca_order, stream_);
     d_svd_order.upload(svd_order, stream_);
+    HB_CUDA(cudaStreamSynchronize(stream_));
 
     HB_CUDA(cudaEventRecord(ev_[2], stream_));
     if (!aca_order.empty()) {
@@ -425,62 +504,83 @@ class Engine : public EngineBase {
         h_ranks[b] = 0;
         continue;
       }
-      if (h_status[b] != kLeafOk) throw Error("device compression failed on a leaf (status " +
-                                              std::to_string(h_status[b]) + ")");
+      if (h_status[b] != kLeafOk)
+        throw Error("device compression failed on a leaf (status " + std::to_string(h_status[b]) + ")");
       if (h_ranks[b] > 0) good.push_back(b);
       max_k = std::max(max_k, h_ranks[b]);
     }
     auto tcost = [&](int b) { return (double)(desc[b].m + desc[b].n) * h_ranks[b] * h_ranks[b]; };
     std::stable_sort(good.begin(), good.end(), [&](int x, int y) { return tcost(x) > tcost(y); });
 
+    typedef typename Traits<T>::wide W;
+    DevArray<W> d_scratch;
+    DevArray<int> d_good, d_svd_good;
+    long long slab = 0, grid = 0;
+    std::vector<int> svd_good;
+    if (!good.empty()) {
+      slab = truncate_slab_elems<T>(max_m, max_n, max_k);
+      const size_t budget = workspace_budget();
+      grid = std::min<long long>((long long)good.size(), persistent_grid(2));
+      grid = std::max(1LL, std::min<long long>(grid, (long long)(budget / (slab * sizeof(W)))));
+      d_scratch.alloc((size_t)(grid * slab));
+      for (int b : good)
+        if (jobs[b].svd) svd_good.push_back(b);
+      d_svd_good.upload(svd_good, stream_);
+      d_good.upload(good, stream_);
+      HB_CUDA(cudaStreamSynchronize(stream_));
+    }
     HB_CUDA(cudaEventRecord(ev_[4], stream_));
     if (!good.empty()) {
-      typedef typename Traits<T>::wide W;
-      const long long slab = truncate_slab_elems<T>(max_m, max_n, max_k);
-      const size_t budget = workspace_budget();
-      long long grid = std::min<long long>((long long)good.size(), persistent_grid(2));
-      grid = std::max(1LL, std::min<long long>(grid, (long long)(budget / (slab * sizeof(W)))));
-      DevArray<W> d_scratch;
-      d_scratch.alloc((size_t)(grid * slab));
-      DevArray<int> d_good;
-      if (!svd_order.empty()) {
+      if (!svd_good.empty()) {
         // SVD of the dense blocks at the compression epsilon, then the regular truncation
-        std::vector<int> svd_good;
-        for (int b : good)
-          if (jobs[b].svd) svd_good.push_back(b);
-        if (!svd_good.empty()) {
-          d_good.upload(svd_good, stream_);
-          HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
-          launch_truncate<T>(d_desc.p, d_good.p, (int)svd_good.size(), eps_aca, d_ws.p, d_ranks.p, d_status.p,
-                             d_counter.p, d_scratch.p, slab, (int)grid, stream_);
-          HB_CUDA(cudaGetLastError());
-        }
+        HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
+        launch_truncate<T>(d_desc.p, d_svd_good.p, (int)svd_good.size(), eps_aca, d_ws.p, d_ranks.p, d_status.p,
+                           d_counter.p, d_scratch.p, slab, (int)grid, stream_);
+        HB_CUDA(cudaGetLastError());
       }
-      d_good.upload(good, stream_);
       HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
       launch_truncate<T>(d_desc.p, d_good.p, (int)good.size(), eps_trunc, d_ws.p, d_ranks.p, d_status.p,
                          d_counter.p, d_scratch.p, slab, (int)grid, stream_);
       HB_CUDA(cudaGetLastError());
     }
-    // overflowed leaves must not be compacted
+    HB_CUDA(cudaEventRecord(ev_[5], stream_));
     HB_CUDA(cudaMemcpyAsync(h_ranks.data(), d_ranks.p, nb * sizeof(int), cudaMemcpyDeviceToHost, stream_));
     HB_CUDA(cudaMemcpyAsync(h_status.data(), d_status.p, nb * sizeof(int), cudaMemcpyDeviceToHost, stream_));
     HB_CUDA(cudaStreamSynchronize(stream_));
+    HB_CUDA(cudaEventElapsedTime(&ms, ev_[4], ev_[5]));
+    times_ms[2] += ms;
     for (int b = 0; b < nb; ++b)
       if (h_status[b] == kLeafAcaCapacity) h_ranks[b] = 0;
-    HB_CUDA(cudaMemcpyAsync(d_ranks.p, h_ranks.data(), nb * sizeof(int), cudaMemcpyHostToDevice, stream_));
-    std::vector<long long> dst(nb, 0);
+    // storage of each leaf in the new piece: A row panels, then B^T
+    std::vector<RkStoreDesc> store(nb);
+    std::vector<PanelDesc> panels;
+    std::vector<long long> loff(nb, -1);
     long long pe = 0;
     for (int b = 0; b < nb; ++b) {
-      dst[b] = pe;
-      if (h_ranks[b] > 0) pe += pad32((long long)h_ranks[b] * (desc[b].m + desc[b].n));
+      store[b] = RkStoreDesc{(int)panels.size(), 0, 0};
+      const int k = h_ranks[b];
+      if (k <= 0) continue;
+      const LeafInfo& l = L[jobs[b].leaf];
+      loff[b] = pe;
+      auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
+      for (int q = br.first; q < br.second; ++q) {
+        panels.push_back(PanelDesc{rblocks_[q].off - l.row_off, rblocks_[q].len, pe});
+        pe += padded((long long)rblocks_[q].len * k);
+        store[b].npanel++;
+      }
+      store[b].bt_off = pe;
+      pe += padded((long long)k * l.n);
     }
+    HB_CUDA(cudaMemcpyAsync(d_ranks.p, h_ranks.data(), nb * sizeof(int), cudaMemcpyHostToDevice, stream_));
     Piece piece;
-    piece.arena.alloc((size_t)std::max(pe, 1LL));
+    piece.arena.alloc((size_t)std::max(pe, 1LL) + 64);
     piece.elems = pe;
-    DevArray<long long> d_dst;
-    d_dst.upload(dst, stream_);
-    launch_compact<T>(d_desc.p, nb, d_ws.p, d_ranks.p, d_dst.p, piece.arena.p, stream_);
+    DevArray<RkStoreDesc> d_store;
+    DevArray<PanelDesc> d_panels;
+    d_store.upload(store, stream_);
+    d_panels.upload(panels, stream_);
+    HB_CUDA(cudaEventRecord(ev_[4], stream_));
+    launch_compact<T>(d_desc.p, nb, d_ws.p, d_ranks.p, d_store.p, d_panels.p, piece.arena.p, stream_);
     HB_CUDA(cudaGetLastError());
     HB_CUDA(cudaEventRecord(ev_[5], stream_));
     HB_CUDA(cudaStreamSynchronize(stream_));
@@ -492,8 +592,7 @@ class Engine : public EngineBase {
       const int leaf = jobs[b].leaf;
       ranks[leaf] = h_ranks[b];
       piece_of_[leaf] = h_ranks[b] > 0 ? pid : -1;
-      rk_off_[leaf] = h_ranks[b] > 0 ? dst[b] : -1;
-      if (h_status[b] == kLeafSvdNoConverge) svd_warnings_++;
+      leaf_off_[leaf] = loff[b];
     }
     pieces_.push_back(std::move(piece));
   }
@@ -502,14 +601,13 @@ class Engine : public EngineBase {
     (void)method;
     const auto& L = bt_->leaves;
     const int nleaves = (int)L.size();
-    times_ms[1] = times_ms[2] = 0;
     piece_of_.assign(nleaves, -1);
     pieces_.clear();
-    svd_warnings_ = 0;
     std::vector<RkJob> queue;
     const int k0 = initial_kcap();
     for (int i = 0; i < nleaves; ++i) {
       if (L[i].type != 1) continue;
+      ranks[i] = 0;
       RkJob j;
       j.leaf = i;
       j.svd = std::max(L[i].m, L[i].n) < svd_below;
@@ -535,160 +633,295 @@ class Engine : public EngineBase {
       }
       queue.swap(retry);
     }
-    // concatenate the pieces into one arena
-    std::vector<long long> base(pieces_.size(), 0);
-    long long tot = 0;
-    for (size_t p = 0; p < pieces_.size(); ++p) {
-      base[p] = tot;
-      tot += pad32(pieces_[p].elems);
-    }
-    rk_arena_.alloc((size_t)std::max(tot, 1LL));
-    rk_elems_ = tot;
-    for (size_t p = 0; p < pieces_.size(); ++p)
-      if (pieces_[p].elems)
-        HB_CUDA(cudaMemcpyAsync(rk_arena_.p + base[p], pieces_[p].arena.p, pieces_[p].elems * sizeof(T),
-                                cudaMemcpyDeviceToDevice, stream_));
-    for (int i = 0; i < nleaves; ++i)
-      if (L[i].type == 1 && piece_of_[i] >= 0) rk_off_[i] += base[piece_of_[i]];
-    HB_CUDA(cudaStreamSynchronize(stream_));
-    pieces_.clear();
   }
 
   // ------------------------------------------------------------------------------
-  void build_side(bool trans, const std::vector<GemvFullLeaf>& F, const std::vector<GemvRkLeaf>& K,
-                  long long zbase, SideBufs& sb, GemvSide& side) {
-    const ClusterTree& out = trans ? *C_ : *R_;
-    const int nb = (int)out.leaf_nodes.size();
-    std::vector<int> start(nb);
-    for (int b = 0; b < nb; ++b) start[b] = out.nodes[out.leaf_nodes[b]].offset;
-    std::vector<std::vector<GemvYEntry>> lists(nb);
-    auto add_range = [&](int type, int idx, int off, int len) {
-      int b = (int)(std::upper_bound(start.begin(), start.end(), off) - start.begin()) - 1;
-      for (; b < nb && start[b] < off + len; ++b) {
-        GemvYEntry e{type, idx, start[b] - off, 0};
-        lists[b].push_back(e);
-      }
-    };
-    for (int f = 0; f < (int)F.size(); ++f)
-      add_range(0, f, trans ? F[f].col_off : F[f].row_off, trans ? F[f].n : F[f].m);
-    for (int k = 0; k < (int)K.size(); ++k)
-      add_range(1, k, trans ? K[k].col_off : K[k].row_off, trans ? K[k].n : K[k].m);
-    std::vector<GemvYBlock> blocks;
-    std::vector<GemvYEntry> entries;
-    int maxlen = 1;
-    for (int b = 0; b < nb; ++b) {
-      const ClusterNode& nd = out.nodes[out.leaf_nodes[b]];
-      GemvYBlock blk{nd.offset, nd.size, (int)entries.size(), (int)lists[b].size()};
-      entries.insert(entries.end(), lists[b].begin(), lists[b].end());
-      blocks.push_back(blk);
-      maxlen = std::max(maxlen, nd.size);
+  // gemv schedule
+  struct SideBuf {
+    DevArray<GemvUnit> units;
+    DevArray<GemvTask> tasks[GemvSide::kMaxLaunch + 1];
+    DevArray<int> begin[GemvSide::kMaxLaunch + 1];
+    DevArray<GemvZred> zred;
+  };
+
+  static int rank_class(int k) { return k <= 16 ? 0 : (k <= 32 ? 1 : (k <= 64 ? 2 : 3)); }
+  static void class_shape(int c, int& ol, int& rpt) {
+    ol = c == 0 ? 16 : 32;
+    rpt = c <= 1 ? 1 : (c == 2 ? 2 : 4);
+  }
+
+  // Units of out(O rows) += P X for a column-major O x C block at `poff`, X rows from `xrow`.
+  void px_units(std::vector<GemvUnit>& u, long long poff, int O, int C, int xrow) {
+    for (int j0 = 0; j0 < C; j0 += 32) {
+      GemvUnit g;
+      g.poff = poff + (long long)j0 * O;
+      g.xrow = xrow + j0;
+      g.c = std::min(32, C - j0);
+      g.o0 = 0;
+      g.ow = O;
+      g.pel = O * g.c;
+      g.shift = (int)(g.poff % kPad);
+      if (g.shift) throw Error("gemv plan: misaligned panel piece");
+      u.push_back(g);
     }
-    // z items: long leaves are cut into chunks whose partials are summed afterwards
-    const int kChunk = 512;
-    std::vector<GemvZItem> items;
-    std::vector<int> multi, mfirst, mcount;
-    long long zpos = zbase;
-    for (int k = 0; k < (int)K.size(); ++k) {
-      const int len = trans ? K[k].m : K[k].n;
-      if (len <= kChunk) {
-        items.push_back(GemvZItem{k, 0, len, 0, K[k].zoff});
+  }
+  // Units of out[o_base + w] += sum_i P[i, w] X[i] for a column-major C x W block at `poff`.
+  void ptx_units(std::vector<GemvUnit>& u, long long poff, int C, int W, int o_base, int xrow) {
+    if (C > 128) throw Error("gemv plan: transposed inner extent above 128 (rank or block too large)");
+    for (int w0 = 0; w0 < W; w0 += 32) {
+      GemvUnit g;
+      g.poff = poff + (long long)w0 * C;
+      g.xrow = xrow;
+      g.c = C;
+      g.o0 = o_base + w0;
+      g.ow = std::min(32, W - w0);
+      g.pel = C * g.ow;
+      g.shift = (int)(g.poff % kPad);
+      u.push_back(g);
+    }
+  }
+
+  // Contiguous ranges of tasks of about equal bytes for a persistent grid.
+  std::vector<int> partition(const std::vector<GemvTask>& tasks, const std::vector<GemvUnit>& units, int omax,
+                             bool transposed) {
+    const int Rmax = sizeof(T) >= 16 ? 4 : 16;
+    const int RS16 = gemv_rhs_stride((int)sizeof(T), Rmax);
+    const size_t smem = stream_smem_bytes((int)sizeof(T), Rmax, RS16, omax, transposed);
+    int per_sm = (int)std::min<size_t>(8, (226 * 1024) / (smem + 1024));
+    per_sm = std::max(per_sm, 1);
+    const int G = std::max(1, std::min((int)tasks.size(), persistent_grid(per_sm)));
+    std::vector<double> cost(tasks.size());
+    double tot = 0;
+    for (size_t t = 0; t < tasks.size(); ++t) {
+      double c = 0;
+      for (int u = tasks[t].first_unit; u < tasks[t].first_unit + tasks[t].nunits; ++u)
+        c += (double)units[u].pel + (double)units[u].c * RS16 + 64;
+      cost[t] = c;
+      tot += c;
+    }
+    std::vector<int> begin(G + 1, (int)tasks.size());
+    begin[0] = 0;
+    double acc = 0;
+    int g = 1;
+    for (size_t t = 0; t < tasks.size() && g < G; ++t) {
+      acc += cost[t];
+      while (g < G && acc >= tot * g / G) begin[g++] = (int)t + 1;
+    }
+    for (; g < G; ++g) begin[g] = (int)tasks.size();
+    begin[G] = (int)tasks.size();
+    return begin;
+  }
+
+  void finish_launch(GemvLaunch& L, SideBuf& sb, int slot, std::vector<GemvTask>& tasks,
+                     const std::vector<GemvUnit>& units, int ol, int rpt, bool transposed, bool out_is_y) {
+    L.ntasks = (int)tasks.size();
+    L.ol = ol;
+    L.rpt = rpt;
+    L.transposed = transposed;
+    L.out_is_y = out_is_y;
+    if (tasks.empty()) return;
+    std::vector<int> begin = partition(tasks, units, ol * rpt, transposed);
+    L.ncta = (int)begin.size() - 1;
+    sb.tasks[slot].upload(tasks, stream_);
+    sb.begin[slot].upload(begin, stream_);
+    L.tasks = sb.tasks[slot].p;
+    L.cta_begin = sb.begin[slot].p;
+  }
+
+  // Builds one side: 'N' (trans = false) or 'T' / 'C'.
+  void build_side(bool trans, const std::vector<GemvRkLeaf>& K, const std::vector<int>& rk_leaf,
+                  long long& next_row, GemvSide& side, SideBuf& sb) {
+    const auto& L = bt_->leaves;
+    const std::vector<Block>& oblocks = trans ? cblocks_ : rblocks_;
+    const std::vector<int>& ostarts = trans ? cstarts_ : rstarts_;
+    std::vector<GemvUnit> units;
+    const int kMaxUnits = 64;  // a longer z task is cut into chunks summed afterwards
+
+    // ---- z-phase: one task per Rk leaf (or chunk), one launch per rank class ----
+    std::vector<GemvTask> zt[4];
+    std::vector<GemvZred> zred;
+    std::vector<GemvUnit> lu;
+    for (size_t t = 0; t < K.size(); ++t) {
+      const GemvRkLeaf& k = K[t];
+      const int leaf = rk_leaf[t];
+      const long long base = leaf_off_[leaf];
+      lu.clear();
+      if (!trans) {
+        // z = B^T x_J: B^T is k x n column-major after the A panels
+        px_units(lu, bt_offset(leaf), k.k, k.n, k.col_off);
       } else {
-        multi.push_back(k);
-        mfirst.push_back((int)items.size());
-        int cnt = 0;
-        for (int s = 0; s < len; s += kChunk, ++cnt) {
-          items.push_back(GemvZItem{k, s, std::min(kChunk, len - s), 0, zpos});
-          zpos += (long long)K[k].k * 16;
+        // z' = A^T x_I: each A panel (len x k) is a transposed piece
+        auto br = block_range(rblocks_, rstarts_, k.row_off, k.m);
+        long long p = base;
+        for (int b = br.first; b < br.second; ++b) {
+          ptx_units(lu, p, rblocks_[b].len, k.k, 0, rblocks_[b].off);
+          p += padded((long long)rblocks_[b].len * k.k);
         }
-        mcount.push_back(cnt);
+      }
+      if (k.k > 128) throw Error("gemv plan: ranks above 128 are not supported by the streamed kernels");
+      const int cls = rank_class(k.k);
+      const int zrow = trans ? k.zrow_t : k.zrow_n;
+      if ((int)lu.size() <= kMaxUnits) {
+        zt[cls].push_back(GemvTask{k.k, (int)units.size(), (int)lu.size(), zrow});
+        units.insert(units.end(), lu.begin(), lu.end());
+      } else {
+        const int nparts = ((int)lu.size() + kMaxUnits - 1) / kMaxUnits;
+        const int part_row = (int)next_row;
+        next_row += (long long)nparts * k.k;
+        for (int pidx = 0; pidx < nparts; ++pidx) {
+          const int u0 = pidx * kMaxUnits, u1 = std::min((int)lu.size(), u0 + kMaxUnits);
+          zt[cls].push_back(GemvTask{k.k, (int)units.size(), u1 - u0, part_row + pidx * k.k});
+          units.insert(units.end(), lu.begin() + u0, lu.begin() + u1);
+        }
+        zred.push_back(GemvZred{zrow, k.k, part_row, nparts});
       }
     }
-    plan_.z_elems = std::max(plan_.z_elems, zpos);
-    sb.blocks.upload(blocks, stream_);
-    sb.entries.upload(entries, stream_);
-    sb.items.upload(items, stream_);
-    sb.multi.upload(multi, stream_);
-    sb.mfirst.upload(mfirst, stream_);
-    sb.mcount.upload(mcount, stream_);
-    side.nblocks = nb;
-    side.blocks = sb.blocks.p;
-    side.entries = sb.entries.p;
-    side.nzitems = (int)items.size();
-    side.zitems = sb.items.p;
-    side.nmulti = (int)multi.size();
-    side.multi = sb.multi.p;
-    side.mfirst = sb.mfirst.p;
-    side.mcount = sb.mcount.p;
-    int gs = ((maxlen + 31) / 32) * 32;
-    side.GS = std::min(gs, 128);
+    // ---- y-phase: one task per output block ----
+    std::vector<std::vector<std::pair<int, int>>> per_block(oblocks.size());  // (leaf, 0 full / 1 rk index)
+    for (int i = 0; i < (int)L.size(); ++i) {
+      if (leaf_off_[i] < 0) continue;
+      if (L[i].type == 1 && ranks[i] <= 0) continue;
+      auto br = trans ? block_range(oblocks, ostarts, L[i].col_off, L[i].n)
+                      : block_range(oblocks, ostarts, L[i].row_off, L[i].m);
+      for (int b = br.first; b < br.second; ++b) per_block[b].push_back({i, 0});
+    }
+    std::vector<int> rk_index(L.size(), -1);
+    for (size_t t = 0; t < rk_leaf.size(); ++t) rk_index[rk_leaf[t]] = (int)t;
+    std::vector<GemvTask> yt;
+    int maxlen = 1;
+    for (size_t b = 0; b < oblocks.size(); ++b) {
+      const Block& ob = oblocks[b];
+      const int first = (int)units.size();
+      for (auto& pr : per_block[b]) {
+        const int i = pr.first;
+        const LeafInfo& l = L[i];
+        if (!trans) {
+          // row panel of leaf i for block b
+          const int w = l.type == 0 ? l.n : ranks[i];
+          const long long poff = row_panel_offset(i, ob.off, w);
+          const int xrow = l.type == 0 ? l.col_off : K[rk_index[i]].zrow_n;
+          px_units(units, poff, ob.len, w, xrow);
+        } else if (l.type == 0) {
+          // columns of block b in every row panel of full leaf i
+          auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
+          long long p = leaf_off_[i];
+          for (int q = br.first; q < br.second; ++q) {
+            const int len = rblocks_[q].len;
+            ptx_units(units, p + (long long)(ob.off - l.col_off) * len, len, ob.len, 0, rblocks_[q].off);
+            p += padded((long long)len * l.n);
+          }
+        } else {
+          const int k = ranks[i];
+          ptx_units(units, bt_offset(i) + (long long)(ob.off - l.col_off) * k, k, ob.len, 0,
+                    K[rk_index[i]].zrow_t);
+        }
+      }
+      yt.push_back(GemvTask{ob.len, first, (int)units.size() - first, ob.off});
+      maxlen = std::max(maxlen, ob.len);
+    }
+    // launches
+    side.nz = 0;
+    for (int c = 0; c < 4; ++c) {
+      if (zt[c].empty()) continue;
+      int ol, rpt;
+      class_shape(c, ol, rpt);
+      finish_launch(side.z[side.nz], sb, side.nz, zt[c], units, ol, rpt, trans, false);
+      side.nz++;
+    }
+    const int rpt = maxlen <= 32 ? 1 : (maxlen <= 64 ? 2 : 4);
+    finish_launch(side.y, sb, GemvSide::kMaxLaunch, yt, units, 32, rpt, trans, true);
+    sb.units.upload(units, stream_);
+    side.units = sb.units.p;
+    sb.zred.upload(zred, stream_);
+    side.nzred = (int)zred.size();
+    side.zred = sb.zred.p;
+  }
+
+  long long bt_offset(int leaf) const {
+    const LeafInfo& l = bt_->leaves[leaf];
+    auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
+    long long p = leaf_off_[leaf];
+    for (int b = br.first; b < br.second; ++b) p += padded((long long)rblocks_[b].len * ranks[leaf]);
+    return p;
+  }
+  long long row_panel_offset(int leaf, int block_off, int w) const {
+    const LeafInfo& l = bt_->leaves[leaf];
+    auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
+    long long p = leaf_off_[leaf];
+    for (int b = br.first; b < br.second; ++b) {
+      if (rblocks_[b].off == block_off) return p;
+      p += padded((long long)rblocks_[b].len * w);
+    }
+    throw Error("gemv plan: block outside the leaf");
   }
 
   void build_plan() {
     const auto& L = bt_->leaves;
     std::vector<GemvFullLeaf> F;
     std::vector<GemvRkLeaf> K;
-    long long zoff = 0;
-    for (size_t i = 0; i < L.size(); ++i) {
-      if (L[i].type == 0 && full_off_[i] >= 0) {
-        F.push_back(GemvFullLeaf{L[i].row_off, L[i].m, L[i].col_off, L[i].n, full_off_[i]});
-      } else if (L[i].type == 1 && ranks[i] > 0) {
-        GemvRkLeaf k{L[i].row_off, L[i].m, L[i].col_off, L[i].n, ranks[i], 0, rk_off_[i], zoff};
-        zoff += (long long)ranks[i] * 16;
-        K.push_back(k);
-      }
-    }
+    std::vector<int> rk_leaf;
+    long long goff = 0;
     plan_ = GemvPlan();
     plan_.n_rows = R_->n;
     plan_.n_cols = C_->n;
+    plan_.n_in_max = std::max(R_->n, C_->n);
+    long long next_row = plan_.n_in_max;
+    for (size_t i = 0; i < L.size(); ++i) {
+      if (L[i].type == 0 && leaf_off_[i] >= 0) {
+        F.push_back(GemvFullLeaf{L[i].row_off, L[i].m, L[i].col_off, L[i].n, goff});
+        goff += (long long)L[i].m * L[i].n;
+      } else if (L[i].type == 1 && ranks[i] > 0) {
+        GemvRkLeaf k{L[i].row_off, L[i].m, L[i].col_off, L[i].n, ranks[i], 0, goff, 0, 0};
+        goff += (long long)ranks[i] * (L[i].m + L[i].n);
+        k.zrow_n = (int)next_row;
+        next_row += ranks[i];
+        K.push_back(k);
+        rk_leaf.push_back((int)i);
+      }
+    }
+    for (auto& k : K) {
+      k.zrow_t = (int)next_row;
+      next_row += k.k;
+    }
     plan_.perm_rows = d_perm_rows_.p;
     plan_.perm_cols = d_perm_cols_.p;
+    plan_.arena = arena_.p;
     g_full_.upload(F, stream_);
     g_rk_.upload(K, stream_);
     plan_.full = g_full_.p;
     plan_.rk = g_rk_.p;
     plan_.nfull = (int)F.size();
     plan_.nrk = (int)K.size();
-    plan_.full_arena = full_arena_.p;
-    plan_.rk_arena = rk_arena_.p;
-    plan_.z_elems = zoff;
-    build_side(false, F, K, zoff, side_n_, plan_.side_n);
-    build_side(true, F, K, zoff, side_t_, plan_.side_t);
+    build_side(false, K, rk_leaf, next_row, plan_.side[0], side_buf_[0]);
+    build_side(true, K, rk_leaf, next_row, plan_.side[1], side_buf_[1]);
+    plan_.xz_rows = next_row;
+    if (next_row >= (1LL << 31)) throw Error("gemv plan: z buffer too large");
   }
-
-  struct Piece {
-    DevArray<T> arena;
-    long long elems = 0;
-  };
-  struct SideBufs {
-    DevArray<GemvYBlock> blocks;
-    DevArray<GemvYEntry> entries;
-    DevArray<GemvZItem> items;
-    DevArray<int> multi, mfirst, mcount;
-  };
 
   const ClusterTree* R_;
   const ClusterTree* C_;
   const BlockTree* bt_;
+  std::vector<Block> rblocks_, cblocks_;
+  std::vector<int> rstarts_, cstarts_;
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev_[8];
   KernelParams kp_{};
   Points pts_{};
   DevArray<double> d_pts_;
   DevArray<int> d_perm_rows_, d_perm_cols_;
-  std::vector<long long> full_off_, rk_off_;
+  std::vector<long long> leaf_off_;
   std::vector<int> piece_of_;
   std::vector<Piece> pieces_;
-  DevArray<T> full_arena_, rk_arena_;
-  long long full_elems_ = 0, rk_elems_ = 0;
-  int svd_warnings_ = 0;
+  DevArray<T> arena_;
+  long long arena_elems_ = 0;
   DevArray<GemvFullLeaf> g_full_;
   DevArray<GemvRkLeaf> g_rk_;
-  SideBufs side_n_, side_t_;
+  SideBuf side_buf_[2];
   GemvPlan plan_;
-  DevArray<T> x_rm_, r_rm_, zbuf_, zbuf2_, stage_x_, stage_y_;
+  DevArray<T> xz_, rz_, stage_x_, stage_y_;
+  DevArray<int> err_;
   cudaGraphExec_t gexec_ = nullptr;
   GraphKey gkey_;
-  bool gemv_timed_ = false;
 };
 
 }  // namespace

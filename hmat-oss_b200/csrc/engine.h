@@ -34,9 +34,9 @@ class EngineBase {
                            cudaStream_t user_stream) = 0;
   virtual void gemv_host(char trans, const void* alpha, const void* x, const void* beta, void* y, int nrhs) = 0;
   virtual long long leaf_payload(int leaf, void* out) = 0;
-  virtual void arenas(void** full, long long* full_elems, void** rk, long long* rk_elems,
-                      long long* offsets) = 0;
-  virtual void leaf_gradients(const void* x, const void* r, int nrhs, void* gfull, void* grk, bool accumulate,
+  // Canonical payload layout (leaf order; full: m x n, Rk: A m x k then B n x k, column-major).
+  virtual void payload_layout(long long* offsets, long long* total) = 0;
+  virtual void leaf_gradients(const void* x, const void* r, int nrhs, void* grad, bool accumulate,
                               cudaStream_t user_stream) = 0;
   virtual void retruncate(double eps) = 0;
   // One eager product on device buffers with events between its phases: device ms of

@@ -1,57 +1,64 @@
-// Batched H-matrix-vector product over all leaves, as three launches on device-resident
-// schedules (captured together in a CUDA graph by the engine):
+// Batched H-matrix-vector product over all leaves (sm_100a).
 //
-//   gather   x_rm[i][q] = x[perm[i] + q N]            client -> cluster order, row-major
-//   z-phase  z_L = B_L^T x_J (or A_L^T x_I for 'T')     per Rk leaf, long leaves in chunks
-//   y-phase  y_I = beta y_I + alpha (sum_F F x_J + sum_Rk A_L[I] z_L)
-//                                                       one CTA per row-cluster leaf, so every
-//                                                       row of y has exactly one writer; the
-//                                                       result is scattered to client order.
+// Restates HMatrix<T>::gemv (h_matrix.cpp:792-857) with its leaf products
+// (ScalarArray::gemm, scalar_array.cpp:413-443; RkMatrix::gemv, rk_matrix.cpp:156-206) and the
+// reorderVector / restoreVectorOrder permutations of the C wrapper (h_matrix.cpp:75-141,
+// c_wrapping.hpp:233-252), as a few launches over device-resident schedules (gemv_plan.h):
 //
-// This restates HMatrix<T>::gemv (h_matrix.cpp:792-857) with its leaf products
-// (ScalarArray::gemm, scalar_array.cpp:413-443; RkMatrix::gemv, rk_matrix.cpp:156-206) and
-// the reorderVector / restoreVectorOrder permutations of the C wrapper
-// (h_matrix.cpp:75-141, c_wrapping.hpp:233-252).  Summation over the leaves of a row block
-// is deterministic (fixed group order), so repeated products are bitwise identical.
+//   gather   xz[i][q] = x[perm[i] + q ld]           client -> cluster order, row-major
+//   z-phase  z_L = B_L^T x_J ('N') / A_L^T x_I ('T')  one task per Rk leaf (chunks for long ones)
+//   z-reduce sums the chunk partials of long leaves
+//   y-phase  y_I = beta y_I + alpha sum (F x | A z)   one task per output block; the result is
+//                                                     scattered straight to client order
+//
+// Every task streams its units (contiguous pieces of the leaf arena and of the xz buffer)
+// through a shared-memory pipeline filled by TMA bulk copies (cp.async.bulk, completion on
+// an mbarrier), on a persistent grid where each CTA owns a contiguous range of tasks of
+// about equal bytes.  Each thread accumulates up to 4 output rows x R right-hand sides in
+// registers; inner-dimension slices (warps, and lanes when the output is narrow) are summed
+// at the end of each task in a fixed order, so repeated products are bitwise identical.
 #include "gemv_plan.h"
 #include "kernels.h"
 
 namespace hmatb200 {
 namespace {
 
-constexpr int kZThreads = 128;
-constexpr int kYThreads = 128;
+constexpr int kThreads = 128;
+constexpr int kWarps = kThreads / 32;
+constexpr int kPieceCols = 32;         // inner extent of a non-transposed unit
+constexpr int kPieceElems = 128 * 32;  // P capacity of a stage (elements)
+constexpr int kMaxInner = 128;         // inner extent of a transposed unit
+constexpr long long kWaitLimit = 1LL << 26;
 
-template <typename T, int Q>
-struct Vec {
-  T v[Q];
-};
+// ---------------------------------------------------------------------------------
+// TMA bulk copy + mbarrier helpers
+__device__ inline uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Loads Q consecutive elements (Q * sizeof(T) bytes, aligned to that size or 16 B).
-template <typename T, int Q>
-__device__ inline void load_vec(const T* p, T (&out)[Q]) {
-  constexpr int bytes = Q * (int)sizeof(T);
-  if constexpr (bytes % 16 == 0) {
-    const uint4* s = reinterpret_cast<const uint4*>(p);
-    uint4* d = reinterpret_cast<uint4*>(out);
-#pragma unroll
-    for (int c = 0; c < bytes / 16; ++c) d[c] = __ldg(s + c);
-  } else if constexpr (bytes % 8 == 0) {
-    const uint2* s = reinterpret_cast<const uint2*>(p);
-    uint2* d = reinterpret_cast<uint2*>(out);
-#pragma unroll
-    for (int c = 0; c < bytes / 8; ++c) d[c] = __ldg(s + c);
-  } else {
-#pragma unroll
-    for (int c = 0; c < Q; ++c) out[c] = p[c];
-  }
+__device__ inline void mbar_init(uint64_t* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ inline void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ inline void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ inline void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ inline bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
 }
 
-template <typename T, bool CONJ>
-__device__ inline T maybe_conj(T a) {
-  if constexpr (CONJ) return conjg(a);
-  else return a;
-}
+__device__ inline uint32_t round16(uint64_t b) { return (uint32_t)((b + 15) & ~15ull); }
 
 __device__ inline float shfl_xor(float v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
 __device__ inline double shfl_xor(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
@@ -62,275 +69,313 @@ __device__ inline cdouble shfl_xor(cdouble v, int m) {
   return cdouble{__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m)};
 }
 
-// ---------------------------------------------------------------------------------
-template <typename T, int R>
-__global__ void gather_kernel(const T* __restrict__ x, int N, int ldx, int q0, int r, const int* __restrict__ perm,
-                              T* __restrict__ x_rm) {
-  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (long long)N * R) return;
-  const int i = (int)(e / R), q = (int)(e % R);
-  x_rm[e] = (q0 + q < r) ? x[(size_t)perm[i] + (size_t)(q0 + q) * ldx] : zero<T>();
-}
-
-// ---------------------------------------------------------------------------------
-// z-phase.  Warp w takes rank columns l = w, w + 4, ...; lanes are RG row groups x QG
-// right-hand-side groups of Q values each; partial sums meet through xor shuffles.
-template <typename T, int R, bool TRANS, bool CONJ>
-__global__ void __launch_bounds__(kZThreads) zphase_kernel(const GemvRkLeaf* __restrict__ rk,
-                                                           const GemvZItem* __restrict__ items,
-                                                           const T* __restrict__ arena,
-                                                           const T* __restrict__ x_rm, T* __restrict__ zout) {
-  constexpr int Q = R >= 4 ? 4 : R;
-  constexpr int QG = R / Q;
-  constexpr int RG = 32 / QG;
-  const GemvZItem it = items[blockIdx.x];
-  const GemvRkLeaf L = rk[it.leaf];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kZThreads / 32;
-  const int rg = lane / QG, qg = lane % QG;
-  const T* P;
-  int ld, base;
-  if constexpr (!TRANS) {
-    P = arena + L.off + (size_t)L.m * L.k;  // B, n x k
-    ld = L.n;
-    base = L.col_off;
+// Loads Q consecutive elements from shared memory (vectorised when aligned).
+template <typename T, int Q>
+__device__ inline void lds_vec(const T* p, T (&out)[Q]) {
+  constexpr int bytes = Q * (int)sizeof(T);
+  if constexpr (bytes % 16 == 0) {
+    const uint4* s = reinterpret_cast<const uint4*>(p);
+    uint4* d = reinterpret_cast<uint4*>(out);
+#pragma unroll
+    for (int c = 0; c < bytes / 16; ++c) d[c] = s[c];
+  } else if constexpr (bytes % 8 == 0) {
+    const uint2* s = reinterpret_cast<const uint2*>(p);
+    uint2* d = reinterpret_cast<uint2*>(out);
+#pragma unroll
+    for (int c = 0; c < bytes / 8; ++c) d[c] = s[c];
   } else {
-    P = arena + L.off;  // A, m x k
-    ld = L.m;
-    base = L.row_off;
-  }
-  T* dst = zout + it.dst_off;
-  for (int l = warp; l < L.k; l += nw) {
-    T acc[Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) acc[q] = zero<T>();
-    const T* col = P + (size_t)l * ld;
-    for (int j = it.start + rg; j < it.start + it.len; j += RG) {
-      const T p = maybe_conj<T, CONJ>(col[j]);
-      T xv[Q];
-      load_vec<T, Q>(x_rm + (size_t)(base + j) * R + qg * Q, xv);
-#pragma unroll
-      for (int q = 0; q < Q; ++q) acc[q] = fmadd(p, xv[q], acc[q]);
-    }
-#pragma unroll
-    for (int msk = QG; msk < 32; msk <<= 1)
-#pragma unroll
-      for (int q = 0; q < Q; ++q) acc[q] = acc[q] + shfl_xor(acc[q], msk);
-    if (rg == 0) {
-#pragma unroll
-      for (int q = 0; q < Q; ++q) dst[(size_t)l * R + qg * Q + q] = acc[q];
-    }
+    for (int c = 0; c < Q; ++c) out[c] = p[c];
   }
 }
 
-// Sums the chunk partials of long leaves in item order.
-template <typename T, int R>
-__global__ void zred_kernel(const GemvRkLeaf* __restrict__ rk, const int* __restrict__ multi,
-                            const int* __restrict__ mfirst, const int* __restrict__ mcount,
-                            const GemvZItem* __restrict__ items, T* __restrict__ z) {
-  const int leaf = multi[blockIdx.x];
-  const GemvRkLeaf L = rk[leaf];
-  const int cnt = mcount[blockIdx.x], first = mfirst[blockIdx.x];
-  for (int e = threadIdx.x; e < L.k * R; e += blockDim.x) {
+template <typename T>
+constexpr int rs_of(int R) {
+  return R * (int)sizeof(T) >= 16 ? R : (16 / (int)sizeof(T));
+}
+template <typename T>
+constexpr int nstage_of() {
+  return sizeof(T) >= 16 ? 2 : 3;
+}
+
+// ---------------------------------------------------------------------------------
+template <typename T, int R, int RS>
+__global__ void gather_kernel(const T* __restrict__ x, int N, int ldx, int q0, int r, const int* __restrict__ perm,
+                              T* __restrict__ xz) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)N * RS) return;
+  const int i = (int)(e / RS), q = (int)(e % RS);
+  xz[e] = (q < R && q0 + q < r) ? x[(size_t)perm[i] + (size_t)(q0 + q) * ldx] : zero<T>();
+}
+
+// ---------------------------------------------------------------------------------
+// The streamed task kernel.  OL output lanes x (32 / OL) inner slices per warp, RPT rows per
+// lane (output rows <= OL * RPT), R right-hand sides (xz row stride RS).
+template <typename T, int R, int RS, int OL, int RPT, bool TRANSP, int NSTAGE>
+__global__ void __launch_bounds__(kThreads) stream_kernel(const GemvTask* __restrict__ tasks,
+                                                          const int* __restrict__ cta_begin,
+                                                          const GemvUnit* __restrict__ units,
+                                                          const T* __restrict__ arena, T* xz, int conj,
+                                                          int out_is_y, const int* __restrict__ perm_out,
+                                                          T* __restrict__ y, int ldy, int q0, int r, T alpha,
+                                                          T beta, int* err) {
+  constexpr int LS = 32 / OL;
+  constexpr int OMAX = OL * RPT;
+  constexpr int XCAP = (TRANSP ? kMaxInner : kPieceCols) * RS;
+  constexpr int PCAP = kPieceElems + 2 * OMAX + 16;  // slack: alignment shift, masked lanes reading past a piece
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T* Ps = reinterpret_cast<T*>(smem_raw);
+  T* Xs = Ps + (size_t)NSTAGE * PCAP;
+  T* red = Xs + (size_t)NSTAGE * XCAP;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(red + (size_t)kWarps * OMAX * R);
+
+  const int t0 = cta_begin[blockIdx.x], t1 = cta_begin[blockIdx.x + 1];
+  if (t0 >= t1) return;
+  const int u_begin = tasks[t0].first_unit;
+  const int u_end = tasks[t1 - 1].first_unit + tasks[t1 - 1].nunits;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ol = lane % OL, ls = lane / OL;
+
+  if (tid == 0) {
+    for (int s = 0; s < NSTAGE; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  // producer: thread 0 arms a stage's barrier and issues the unit's two bulk copies
+  auto issue = [&](int u) {
+    const int s = (u - u_begin) % NSTAGE;
+    const GemvUnit U = units[u];
+    // the copy starts at the 16-byte boundary at or below the piece (TMA alignment rule)
+    const uint32_t pbytes = round16((uint64_t)(U.pel + U.shift) * sizeof(T));
+    const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(T);
+    mbar_expect_tx(&bars[s], pbytes + xbytes);
+    bulk_g2s(Ps + (size_t)s * PCAP, arena + (U.poff - U.shift), pbytes, &bars[s]);
+    bulk_g2s(Xs + (size_t)s * XCAP, xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
+  };
+  if (tid == 0)
+    for (int u = u_begin; u < u_end && u < u_begin + NSTAGE; ++u) issue(u);
+
+  int u = u_begin;
+  for (int t = t0; t < t1; ++t) {
+    const GemvTask task = tasks[t];
+    T acc[RPT][R];
+#pragma unroll
+    for (int a = 0; a < RPT; ++a)
+#pragma unroll
+      for (int q = 0; q < R; ++q) acc[a][q] = zero<T>();
+
+    for (int k = 0; k < task.nunits; ++k, ++u) {
+      const int s = (u - u_begin) % NSTAGE;
+      const uint32_t parity = (uint32_t)(((u - u_begin) / NSTAGE) & 1);
+      long long spins = 0;
+      while (!mbar_try_wait(&bars[s], parity)) {
+        if (++spins > kWaitLimit) {
+          if (tid == 0) atomicExch(err, 1);
+          return;  // a copy that never lands: stop this CTA, the host sees the error flag
+        }
+      }
+      const GemvUnit U = units[u];
+      const T* P = Ps + (size_t)s * PCAP + U.shift;
+      const T* X = Xs + (size_t)s * XCAP;
+      const int c = U.c;
+      if constexpr (!TRANSP) {
+        // P is O x c column-major: out[o] += sum_j P[o, j] X[j]
+        const int O = task.O;
+#pragma unroll 2
+        for (int j = warp * LS + ls; j < c; j += kWarps * LS) {
+          T xv[R];
+          lds_vec<T, R>(X + (size_t)j * RS, xv);
+#pragma unroll
+          for (int a = 0; a < RPT; ++a) {
+            const T p = P[ol + a * OL + (size_t)j * O];
+#pragma unroll
+            for (int q = 0; q < R; ++q) acc[a][q] = fmadd(p, xv[q], acc[a][q]);
+          }
+        }
+      } else {
+        // P is c x ow column-major, covering outputs [o0, o0 + ow):
+        // out[o] += sum_j op(P[j, o - o0]) X[j]
+        const int o0 = U.o0, ow = U.ow;
+        for (int j = warp * LS + ls; j < c; j += kWarps * LS) {
+          T xv[R];
+          lds_vec<T, R>(X + (size_t)j * RS, xv);
+#pragma unroll
+          for (int a = 0; a < RPT; ++a) {
+            const int oo = ol + a * OL - o0;
+            if (oo >= 0 && oo < ow) {
+              T p = P[j + (size_t)oo * c];
+              if (conj) p = conjg(p);
+#pragma unroll
+              for (int q = 0; q < R; ++q) acc[a][q] = fmadd(p, xv[q], acc[a][q]);
+            }
+          }
+        }
+      }
+      __syncthreads();  // stage s is free again
+      if (tid == 0 && u + NSTAGE < u_end) issue(u + NSTAGE);
+    }
+
+    // ---- epilogue: lane slices, then warps, in a fixed order ----
+#pragma unroll
+    for (int m = OL; m < 32; m <<= 1)
+#pragma unroll
+      for (int a = 0; a < RPT; ++a)
+#pragma unroll
+        for (int q = 0; q < R; ++q) acc[a][q] = acc[a][q] + shfl_xor(acc[a][q], m);
+    if (ls == 0) {
+#pragma unroll
+      for (int a = 0; a < RPT; ++a)
+#pragma unroll
+        for (int q = 0; q < R; ++q) red[((size_t)warp * OMAX + ol + a * OL) * R + q] = acc[a][q];
+    }
+    __syncthreads();
+    for (int e = tid; e < task.O * R; e += kThreads) {
+      const int o = e / R, q = e % R;
+      T v = red[(size_t)o * R + q];
+#pragma unroll
+      for (int w = 1; w < kWarps; ++w) v = v + red[((size_t)w * OMAX + o) * R + q];
+      if (out_is_y) {
+        if (q0 + q < r) {
+          T* yp = y + (size_t)perm_out[task.out_row + o] + (size_t)(q0 + q) * ldy;
+          T outv = alpha * v;
+          if (!is_zero_val(beta)) outv = fmadd(beta, *yp, outv);
+          *yp = outv;
+        }
+      } else {
+        xz[(size_t)(task.out_row + o) * RS + q] = v;
+      }
+    }
+    if constexpr (RS > R) {
+      if (!out_is_y)
+        for (int e = tid; e < task.O * (RS - R); e += kThreads)
+          xz[(size_t)(task.out_row + e / (RS - R)) * RS + R + e % (RS - R)] = zero<T>();
+    }
+    __syncthreads();
+  }
+}
+
+// Sums the chunk partials of long leaves: xz[final + l] = sum_p xz[part + p k + l].
+template <typename T, int RS>
+__global__ void zred_kernel(const GemvZred* __restrict__ zr, T* xz) {
+  const GemvZred d = zr[blockIdx.x];
+  for (int e = threadIdx.x; e < d.k * RS; e += blockDim.x) {
     T s = zero<T>();
-    for (int c = 0; c < cnt; ++c) s = s + z[items[first + c].dst_off + e];
-    z[L.zoff + e] = s;
+    for (int p = 0; p < d.nparts; ++p) s = s + xz[((size_t)d.part_row + (size_t)p * d.k) * RS + e];
+    xz[(size_t)d.final_row * RS + e] = s;
   }
 }
 
 // ---------------------------------------------------------------------------------
-// y-phase.  The CTA owns rows [blk.off, blk.off + blk.len) of the output; its threads form
-// NG = blockDim / GS groups of GS threads (one output row per thread) that take the
-// block's entries round-robin.  Group partials are summed in group order at the end.
-template <typename T, int R, bool TRANS, bool CONJ>
-__global__ void __launch_bounds__(kYThreads) yphase_kernel(
-    const GemvYBlock* __restrict__ blocks, const GemvYEntry* __restrict__ entries,
-    const GemvFullLeaf* __restrict__ full, const GemvRkLeaf* __restrict__ rk, const T* __restrict__ full_arena,
-    const T* __restrict__ rk_arena, const T* __restrict__ x_rm, const T* __restrict__ z, int GS,
-    const int* __restrict__ perm_out, T* __restrict__ y, int ldy, int q0, int r, T alpha, T beta) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* red = reinterpret_cast<T*>(smem_raw);
-  const GemvYBlock blk = blocks[blockIdx.x];
-  const int NG = kYThreads / GS;
-  const int g = threadIdx.x / GS;
-  for (int r0 = 0; r0 < blk.len; r0 += GS) {
-    const int i = r0 + (threadIdx.x % GS);
-    const bool active = g < NG && i < blk.len;
-    T acc[R];
-#pragma unroll
-    for (int q = 0; q < R; ++q) acc[q] = zero<T>();
-    if (active) {
-      for (int e = blk.first + g; e < blk.first + blk.count; e += NG) {
-        const GemvYEntry en = entries[e];
-        if (en.type == 0) {
-          const GemvFullLeaf F = full[en.leaf];
-          const T* Fp = full_arena + F.off;
-          if constexpr (!TRANS) {
-            // rows of F are the block rows: y_i += sum_j F[i, j] x_j
-            const T* col = Fp + en.sub + i;
-            const T* xr = x_rm + (size_t)F.col_off * R;
-            for (int j = 0; j < F.n; ++j) {
-              const T f = col[(size_t)j * F.m];
-              T xv[R];
-              load_vec<T, R>(xr + (size_t)j * R, xv);
-#pragma unroll
-              for (int q = 0; q < R; ++q) acc[q] = fmadd(f, xv[q], acc[q]);
-            }
-          } else {
-            // columns of F are the block rows: y_j += sum_i op(F[i, j]) x_i
-            const T* col = Fp + (size_t)(en.sub + i) * F.m;
-            const T* xr = x_rm + (size_t)F.row_off * R;
-            for (int ii = 0; ii < F.m; ++ii) {
-              const T f = maybe_conj<T, CONJ>(col[ii]);
-              T xv[R];
-              load_vec<T, R>(xr + (size_t)ii * R, xv);
-#pragma unroll
-              for (int q = 0; q < R; ++q) acc[q] = fmadd(f, xv[q], acc[q]);
-            }
-          }
-        } else {
-          const GemvRkLeaf L = rk[en.leaf];
-          const T* P;
-          int ld;
-          if constexpr (!TRANS) {
-            P = rk_arena + L.off;  // A
-            ld = L.m;
-          } else {
-            P = rk_arena + L.off + (size_t)L.m * L.k;  // B
-            ld = L.n;
-          }
-          const T* zl = z + L.zoff;
-          const T* row = P + en.sub + i;
-          for (int l = 0; l < L.k; ++l) {
-            const T p = maybe_conj<T, CONJ>(row[(size_t)l * ld]);
-            T zv[R];
-            load_vec<T, R>(zl + (size_t)l * R, zv);
-#pragma unroll
-            for (int q = 0; q < R; ++q) acc[q] = fmadd(p, zv[q], acc[q]);
-          }
-        }
-      }
-    }
-    // cross-group sum (group order), then scale and scatter to client order
-    if (NG > 1) {
-      __syncthreads();
-      if (active) {
-#pragma unroll
-        for (int q = 0; q < R; ++q) red[((size_t)g * GS + (threadIdx.x % GS)) * R + q] = acc[q];
-      }
-      __syncthreads();
-      if (g == 0 && active) {
-        for (int gg = 1; gg < NG; ++gg)
-#pragma unroll
-          for (int q = 0; q < R; ++q) acc[q] = acc[q] + red[((size_t)gg * GS + threadIdx.x) * R + q];
-      }
-    }
-    if (g == 0 && active) {
-      const size_t dst = (size_t)perm_out[blk.off + i];
-#pragma unroll
-      for (int q = 0; q < R; ++q) {
-        if (q0 + q < r) {
-          T* yp = y + dst + (size_t)(q0 + q) * ldy;
-          T v = alpha * acc[q];
-          if (!is_zero_val(beta)) v = fmadd(beta, *yp, v);
-          *yp = v;
-        }
-      }
-    }
+template <typename T, int R, int RS, int OL, int RPT, bool TRANSP>
+void launch_stream_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, int conj,
+                     const int* perm_out, T* y, int ldy, int q0, int r, T alpha, T beta, int* err, cudaStream_t s) {
+  constexpr int NSTAGE = nstage_of<T>();
+  auto kern = stream_kernel<T, R, RS, OL, RPT, TRANSP, NSTAGE>;
+  const size_t smem = stream_smem_bytes(sizeof(T), R, RS, OL * RPT, TRANSP);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
   }
+  kern<<<L.ncta, kThreads, smem, s>>>(L.tasks, L.cta_begin, units, arena, xz, conj, L.out_is_y ? 1 : 0, perm_out, y,
+                                       ldy, q0, r, alpha, beta, err);
 }
 
-template <typename T, int R, bool TRANS, bool CONJ>
-void run_tile(const GemvPlan& p, const GemvSide& side, int nrhs, int q0, T alpha, T beta, const T* x, T* y, T* x_rm,
-              T* zpart, T* z, cudaStream_t s, const GemvTiming* tm) {
+template <typename T, int R, int RS, bool TRANSP>
+void launch_stream(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, int conj, const int* perm_out,
+                   T* y, int ldy, int q0, int r, T alpha, T beta, int* err, cudaStream_t s) {
+  if (L.ntasks <= 0) return;
+  if (L.ol == 16)
+    launch_stream_t<T, R, RS, 16, 1, TRANSP>(L, units, arena, xz, conj, perm_out, y, ldy, q0, r, alpha, beta, err, s);
+  else if (L.rpt == 1)
+    launch_stream_t<T, R, RS, 32, 1, TRANSP>(L, units, arena, xz, conj, perm_out, y, ldy, q0, r, alpha, beta, err, s);
+  else if (L.rpt == 2)
+    launch_stream_t<T, R, RS, 32, 2, TRANSP>(L, units, arena, xz, conj, perm_out, y, ldy, q0, r, alpha, beta, err, s);
+  else
+    launch_stream_t<T, R, RS, 32, 4, TRANSP>(L, units, arena, xz, conj, perm_out, y, ldy, q0, r, alpha, beta, err, s);
+}
+
+template <typename T, int R, bool TRANSP>
+void run_tile(const GemvPlan& p, int nrhs, int q0, T alpha, T beta, const T* x, T* y, T* xz, int conj, int* err,
+              cudaStream_t s, const GemvTiming* tm) {
+  constexpr int RS = rs_of<T>(R);
+  const GemvSide& side = p.side[TRANSP ? 1 : 0];
+  const int n_in = TRANSP ? p.n_rows : p.n_cols;
+  const int* perm_in = TRANSP ? p.perm_rows : p.perm_cols;
+  const int* perm_out = TRANSP ? p.perm_cols : p.perm_rows;
+  const int ld_in = n_in, ld_out = TRANSP ? p.n_cols : p.n_rows;
+  const T* arena = (const T*)p.arena;
   if (tm) cudaEventRecord(tm->ev[0], s);
-  const int n_in = TRANS ? p.n_rows : p.n_cols;
-  const int* perm_in = TRANS ? p.perm_rows : p.perm_cols;
-  const int* perm_out = TRANS ? p.perm_cols : p.perm_rows;
-  const int ld_in = n_in, ld_out = TRANS ? p.n_cols : p.n_rows;
-  long long tot = (long long)n_in * R;
-  gather_kernel<T, R><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(x, n_in, ld_in, q0, nrhs, perm_in, x_rm);
+  const long long tot = (long long)n_in * RS;
+  gather_kernel<T, R, RS><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(x, n_in, ld_in, q0, nrhs, perm_in, xz);
   if (tm) cudaEventRecord(tm->ev[1], s);
-  if (side.nzitems > 0) {
-    // single-item leaves write z directly; chunked leaves write partials
-    // single-item leaves write their z in place; chunks of long leaves write partials
-    // further down the same buffer, summed by zred
-    zphase_kernel<T, R, TRANS, CONJ><<<side.nzitems, kZThreads, 0, s>>>(p.rk, side.zitems,
-                                                                        (const T*)p.rk_arena, x_rm, z);
-    if (side.nmulti > 0)
-      zred_kernel<T, R><<<side.nmulti, 128, 0, s>>>(p.rk, side.multi, side.mfirst, side.mcount, side.zitems, z);
-  }
+  for (int c = 0; c < side.nz; ++c)
+    launch_stream<T, R, RS, TRANSP>(side.z[c], side.units, arena, xz, conj, nullptr, nullptr, 0, 0, 0, alpha, beta,
+                                    err, s);
+  if (side.nzred > 0) zred_kernel<T, RS><<<side.nzred, 128, 0, s>>>(side.zred, xz);
   if (tm) cudaEventRecord(tm->ev[2], s);
-  if (side.nblocks > 0) {
-    size_t smem = (size_t)kYThreads * R * sizeof(T);
-    yphase_kernel<T, R, TRANS, CONJ><<<side.nblocks, kYThreads, smem, s>>>(
-        side.blocks, side.entries, p.full, p.rk, (const T*)p.full_arena, (const T*)p.rk_arena, x_rm, z, side.GS,
-        perm_out, y, ld_out, q0, nrhs, alpha, beta);
-  }
+  launch_stream<T, R, RS, TRANSP>(side.y, side.units, arena, xz, conj, perm_out, y, ld_out, q0, nrhs, alpha, beta,
+                                  err, s);
   if (tm) cudaEventRecord(tm->ev[3], s);
 }
 
-template <typename T, bool TRANS, bool CONJ>
-void run_all(const GemvPlan& p, int nrhs, T alpha, T beta, const T* x, T* y, T* x_rm, T* zpart, T* z,
+template <typename T, bool TRANSP>
+void run_all(const GemvPlan& p, int nrhs, T alpha, T beta, const T* x, T* y, T* xz, int conj, int* err,
              cudaStream_t s, const GemvTiming* tm) {
-  const GemvSide& side = TRANS ? p.side_t : p.side_n;
-  for (int q0 = 0; q0 < nrhs; q0 += 16) {
+  // complex double keeps tiles of at most 4 right-hand sides (shared-memory budget)
+  constexpr int maxR = sizeof(T) >= 16 ? 4 : 16;
+  for (int q0 = 0; q0 < nrhs; q0 += maxR) {
     const int rem = nrhs - q0;
-    if (rem > 8) run_tile<T, 16, TRANS, CONJ>(p, side, nrhs, q0, alpha, beta, x, y, x_rm, zpart, z, s, tm);
-    else if (rem > 4) run_tile<T, 8, TRANS, CONJ>(p, side, nrhs, q0, alpha, beta, x, y, x_rm, zpart, z, s, tm);
-    else if (rem > 2) run_tile<T, 4, TRANS, CONJ>(p, side, nrhs, q0, alpha, beta, x, y, x_rm, zpart, z, s, tm);
-    else if (rem == 2) run_tile<T, 2, TRANS, CONJ>(p, side, nrhs, q0, alpha, beta, x, y, x_rm, zpart, z, s, tm);
-    else run_tile<T, 1, TRANS, CONJ>(p, side, nrhs, q0, alpha, beta, x, y, x_rm, zpart, z, s, tm);
+    if (maxR == 16 && rem > 8) run_tile<T, (maxR >= 16 ? 16 : 4), TRANSP>(p, nrhs, q0, alpha, beta, x, y, xz, conj, err, s, tm);
+    else if (maxR == 16 && rem > 4) run_tile<T, (maxR >= 16 ? 8 : 4), TRANSP>(p, nrhs, q0, alpha, beta, x, y, xz, conj, err, s, tm);
+    else if (rem > 1) run_tile<T, 4, TRANSP>(p, nrhs, q0, alpha, beta, x, y, xz, conj, err, s, tm);
+    else run_tile<T, 1, TRANSP>(p, nrhs, q0, alpha, beta, x, y, xz, conj, err, s, tm);
   }
 }
 
 // ---------------------------------------------------------------------------------
-// Leaf-factor gradients (adjoint of y = H x with respect to the stored leaves).
-template <typename T, int R>
-__global__ void grad_full_kernel(const GemvFullLeaf* __restrict__ full, int nfull, const T* __restrict__ x_rm,
-                                 const T* __restrict__ r_rm, T* __restrict__ g, bool accumulate) {
+// Leaf-factor gradients (adjoint of y = H x with respect to the stored leaves), written in
+// the canonical layout (full: m x n, Rk: A m x k then B n x k, column-major).
+template <typename T, int RS>
+__global__ void grad_full_kernel(const GemvFullLeaf* __restrict__ full, int nfull, const T* __restrict__ xs,
+                                 const T* __restrict__ rs, int R, T* __restrict__ g, bool accumulate) {
   for (int f = blockIdx.x; f < nfull; f += gridDim.x) {
     const GemvFullLeaf F = full[f];
-    T* dF = g + F.off;
+    T* dF = g + F.goff;
     for (int e = threadIdx.x; e < F.m * F.n; e += blockDim.x) {
       const int i = e % F.m, j = e / F.m;
-      T rv[R], xv[R];
-      load_vec<T, R>(r_rm + (size_t)(F.row_off + i) * R, rv);
-      load_vec<T, R>(x_rm + (size_t)(F.col_off + j) * R, xv);
+      const T* rv = rs + (size_t)(F.row_off + i) * RS;
+      const T* xv = xs + (size_t)(F.col_off + j) * RS;
       T acc = accumulate ? dF[e] : zero<T>();
-#pragma unroll
       for (int q = 0; q < R; ++q) acc = fmadd(rv[q], xv[q], acc);
       dF[e] = acc;
     }
   }
 }
 
-template <typename T, int R>
-__global__ void grad_rk_kernel(const GemvRkLeaf* __restrict__ rk, int nrk, const T* __restrict__ x_rm,
-                               const T* __restrict__ r_rm, const T* __restrict__ zx, const T* __restrict__ zr,
-                               T* __restrict__ g, bool accumulate) {
+template <typename T, int RS>
+__global__ void grad_rk_kernel(const GemvRkLeaf* __restrict__ rk, int nrk, const T* __restrict__ xs,
+                               const T* __restrict__ rs, int R, T* __restrict__ g, bool accumulate) {
   for (int t = blockIdx.x; t < nrk; t += gridDim.x) {
     const GemvRkLeaf L = rk[t];
-    T* dA = g + L.off;
+    T* dA = g + L.goff;
     T* dB = dA + (size_t)L.m * L.k;
-    // dA[i, l] = sum_q r[i, q] z[l, q],  z = B^T x
+    // dA[i, l] = sum_q r[i, q] z[l, q],  z = B^T x  (rows zrow_n of the x buffer)
     for (int e = threadIdx.x; e < L.m * L.k; e += blockDim.x) {
       const int i = e % L.m, l = e / L.m;
-      T rv[R], zv[R];
-      load_vec<T, R>(r_rm + (size_t)(L.row_off + i) * R, rv);
-      load_vec<T, R>(zx + L.zoff + (size_t)l * R, zv);
+      const T* rv = rs + (size_t)(L.row_off + i) * RS;
+      const T* zv = xs + (size_t)(L.zrow_n + l) * RS;
       T acc = accumulate ? dA[e] : zero<T>();
-#pragma unroll
       for (int q = 0; q < R; ++q) acc = fmadd(rv[q], zv[q], acc);
       dA[e] = acc;
     }
-    // dB[j, l] = sum_q x[j, q] w[l, q],  w = A^T r
+    // dB[j, l] = sum_q x[j, q] w[l, q],  w = A^T r  (rows zrow_t of the r buffer)
     for (int e = threadIdx.x; e < L.n * L.k; e += blockDim.x) {
       const int j = e % L.n, l = e / L.n;
-      T xv[R], wv[R];
-      load_vec<T, R>(x_rm + (size_t)(L.col_off + j) * R, xv);
-      load_vec<T, R>(zr + L.zoff + (size_t)l * R, wv);
+      const T* xv = xs + (size_t)(L.col_off + j) * RS;
+      const T* wv = rs + (size_t)(L.zrow_t + l) * RS;
       T acc = accumulate ? dB[e] : zero<T>();
-#pragma unroll
       for (int q = 0; q < R; ++q) acc = fmadd(xv[q], wv[q], acc);
       dB[e] = acc;
     }
@@ -338,57 +383,68 @@ __global__ void grad_rk_kernel(const GemvRkLeaf* __restrict__ rk, int nrk, const
 }
 
 template <typename T, int R>
-void grads_tile(const GemvPlan& p, int nrhs, const T* x, const T* r, T* x_rm, T* r_rm, T* zx, T* zr, T* gfull,
-                T* grk, bool accumulate, cudaStream_t s) {
-  long long tot = (long long)p.n_cols * R;
-  gather_kernel<T, R><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(x, p.n_cols, p.n_cols, 0, nrhs, p.perm_cols,
-                                                                     x_rm);
-  tot = (long long)p.n_rows * R;
-  gather_kernel<T, R><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(r, p.n_rows, p.n_rows, 0, nrhs, p.perm_rows,
-                                                                     r_rm);
-  const GemvSide& sn = p.side_n;
-  const GemvSide& st = p.side_t;
-  if (sn.nzitems > 0) {
-    zphase_kernel<T, R, false, false><<<sn.nzitems, kZThreads, 0, s>>>(p.rk, sn.zitems, (const T*)p.rk_arena, x_rm,
-                                                                       zx);
-    if (sn.nmulti > 0) zred_kernel<T, R><<<sn.nmulti, 128, 0, s>>>(p.rk, sn.multi, sn.mfirst, sn.mcount, sn.zitems, zx);
-  }
-  if (st.nzitems > 0) {
-    zphase_kernel<T, R, true, false><<<st.nzitems, kZThreads, 0, s>>>(p.rk, st.zitems, (const T*)p.rk_arena, r_rm,
-                                                                      zr);
-    if (st.nmulti > 0) zred_kernel<T, R><<<st.nmulti, 128, 0, s>>>(p.rk, st.multi, st.mfirst, st.mcount, st.zitems, zr);
-  }
+void grads_tile(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* rz, T* gfull, T* grk, bool accumulate,
+                int* err, cudaStream_t s) {
+  constexpr int RS = rs_of<T>(R);
+  const T* arena = (const T*)p.arena;
+  // x in cluster order (columns) and z = B^T x
+  long long tot = (long long)p.n_cols * RS;
+  gather_kernel<T, R, RS><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(x, p.n_cols, p.n_cols, 0, nrhs, p.perm_cols,
+                                                                         xz);
+  const GemvSide& sn = p.side[0];
+  for (int c = 0; c < sn.nz; ++c)
+    launch_stream<T, R, RS, false>(sn.z[c], sn.units, arena, xz, 0, nullptr, nullptr, 0, 0, 0, one<T>(), zero<T>(),
+                                   err, s);
+  if (sn.nzred > 0) zred_kernel<T, RS><<<sn.nzred, 128, 0, s>>>(sn.zred, xz);
+  // r in cluster order (rows) and w = A^T r
+  tot = (long long)p.n_rows * RS;
+  gather_kernel<T, R, RS><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(r, p.n_rows, p.n_rows, 0, nrhs, p.perm_rows,
+                                                                         rz);
+  const GemvSide& st = p.side[1];
+  for (int c = 0; c < st.nz; ++c)
+    launch_stream<T, R, RS, true>(st.z[c], st.units, arena, rz, 0, nullptr, nullptr, 0, 0, 0, one<T>(), zero<T>(),
+                                  err, s);
+  if (st.nzred > 0) zred_kernel<T, RS><<<st.nzred, 128, 0, s>>>(st.zred, rz);
   const int grid = persistent_grid(4);
   if (p.nfull > 0 && gfull)
-    grad_full_kernel<T, R><<<grid, 256, 0, s>>>(p.full, p.nfull, x_rm, r_rm, gfull, accumulate);
-  if (p.nrk > 0 && grk) grad_rk_kernel<T, R><<<grid, 256, 0, s>>>(p.rk, p.nrk, x_rm, r_rm, zx, zr, grk, accumulate);
+    grad_full_kernel<T, RS><<<grid, 256, 0, s>>>(p.full, p.nfull, xz, rz, nrhs, gfull, accumulate);
+  if (p.nrk > 0 && grk) grad_rk_kernel<T, RS><<<grid, 256, 0, s>>>(p.rk, p.nrk, xz, rz, nrhs, grk, accumulate);
 }
 
 }  // namespace
 
+size_t stream_smem_bytes(int elem_bytes, int R, int RS, int omax, bool transposed) {
+  const int nstage = elem_bytes >= 16 ? 2 : 3;
+  const size_t xcap = (size_t)(transposed ? kMaxInner : kPieceCols) * RS;
+  const size_t pcap = (size_t)kPieceElems + 2 * omax + 16;
+  return (size_t)nstage * (pcap + xcap) * elem_bytes + (size_t)kWarps * omax * R * elem_bytes + nstage * 8 + 16;
+}
+
+int gemv_rhs_stride(int elem_bytes, int R) { return R * elem_bytes >= 16 ? R : 16 / elem_bytes; }
+
 template <typename T>
-void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, T* x_rm, T* r_rm, T* zx, T* zr,
-                           T* gfull, T* grk, bool accumulate, cudaStream_t s) {
-  if (nrhs > 8) grads_tile<T, 16>(p, nrhs, x, r, x_rm, r_rm, zx, zr, gfull, grk, accumulate, s);
-  else if (nrhs > 4) grads_tile<T, 8>(p, nrhs, x, r, x_rm, r_rm, zx, zr, gfull, grk, accumulate, s);
-  else if (nrhs > 2) grads_tile<T, 4>(p, nrhs, x, r, x_rm, r_rm, zx, zr, gfull, grk, accumulate, s);
-  else if (nrhs == 2) grads_tile<T, 2>(p, nrhs, x, r, x_rm, r_rm, zx, zr, gfull, grk, accumulate, s);
-  else grads_tile<T, 1>(p, nrhs, x, r, x_rm, r_rm, zx, zr, gfull, grk, accumulate, s);
+void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* rz, T* gfull, T* grk,
+                           bool accumulate, int* err, cudaStream_t s) {
+  constexpr bool big = sizeof(T) < 16;
+  if (big && nrhs > 8) grads_tile<T, big ? 16 : 4>(p, nrhs, x, r, xz, rz, gfull, grk, accumulate, err, s);
+  else if (big && nrhs > 4) grads_tile<T, big ? 8 : 4>(p, nrhs, x, r, xz, rz, gfull, grk, accumulate, err, s);
+  else if (nrhs > 1) grads_tile<T, 4>(p, nrhs, x, r, xz, rz, gfull, grk, accumulate, err, s);
+  else grads_tile<T, 1>(p, nrhs, x, r, xz, rz, gfull, grk, accumulate, err, s);
 }
 
 template <typename T>
-void launch_gemv(const GemvPlan& p, char trans, int nrhs, T alpha, T beta, const T* x_client, T* y_client,
-                 T* x_rm, T* zpart, T* z, cudaStream_t s, const GemvTiming* tm) {
-  if (trans == 'N') run_all<T, false, false>(p, nrhs, alpha, beta, x_client, y_client, x_rm, zpart, z, s, tm);
-  else if (trans == 'T' || !Traits<T>::is_complex)
-    run_all<T, true, false>(p, nrhs, alpha, beta, x_client, y_client, x_rm, zpart, z, s, tm);
-  else run_all<T, true, true>(p, nrhs, alpha, beta, x_client, y_client, x_rm, zpart, z, s, tm);
+void launch_gemv(const GemvPlan& p, char trans, int nrhs, T alpha, T beta, const T* x_client, T* y_client, T* xz,
+                 int* err, cudaStream_t s, const GemvTiming* tm) {
+  if (trans == 'N') run_all<T, false>(p, nrhs, alpha, beta, x_client, y_client, xz, 0, err, s, tm);
+  else
+    run_all<T, true>(p, nrhs, alpha, beta, x_client, y_client, xz, (trans == 'C' && Traits<T>::is_complex) ? 1 : 0,
+                     err, s, tm);
 }
 
-#define HB_INST(T)                                                                                          \
-  template void launch_gemv<T>(const GemvPlan&, char, int, T, T, const T*, T*, T*, T*, T*, cudaStream_t,         \
+#define HB_INST(T)                                                                                            \
+  template void launch_gemv<T>(const GemvPlan&, char, int, T, T, const T*, T*, T*, int*, cudaStream_t,         \
                                const GemvTiming*);                                                             \
-  template void launch_leaf_gradients<T>(const GemvPlan&, int, const T*, const T*, T*, T*, T*, T*, T*, T*, bool, \
+  template void launch_leaf_gradients<T>(const GemvPlan&, int, const T*, const T*, T*, T*, T*, T*, bool, int*, \
                                          cudaStream_t);
 HB_INST(float)
 HB_INST(double)

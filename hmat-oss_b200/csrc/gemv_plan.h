@@ -1,69 +1,93 @@
 // Device-resident schedule of the batched H-matrix-vector product (built on the host by
 // the engine from the leaf list, consumed by gemv.cu).
+//
+// Leaf storage is panelised so that every product term is one contiguous chunk:
+//  * a full leaf F (m x n) is stored as row panels, one per output block of its rows,
+//    each panel column-major (len x n);
+//  * an Rk leaf stores A as row panels (len x k, column-major) and B transposed,
+//    B^T column-major (k x n), i.e. each row of B contiguous.
+// An output block is a leaf of the output cluster tree, cut into pieces of at most 128 rows.
+//
+// A product is a list of tasks; a task is one output (an output block of y, or the z = B^T x
+// slot of an Rk leaf) accumulated from a list of units; a unit is out += op(P) X for one
+// contiguous piece P of the leaf arena and one contiguous piece X of the xz buffer (x in
+// cluster order, row-major, followed by the z rows).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 namespace hmatb200 {
 
-struct GemvFullLeaf {
-  int row_off, m, col_off, n;
-  long long off;  // element offset in the full arena (column-major m x n)
+struct GemvUnit {
+  long long poff;  // element offset of the piece P in the arena (16-byte aligned)
+  int xrow;        // first row of the X piece in the xz buffer
+  int c;           // inner extent (rows of X)
+  int o0, ow;      // transposed units: output rows [o0, o0 + ow) this piece covers
+  int pel;         // elements of the piece P (O x c, or c x ow when transposed)
+  int shift;       // elements between the 16-byte aligned copy start and the piece
 };
 
-struct GemvRkLeaf {
-  int row_off, m, col_off, n, k, pad;
-  long long off;   // element offset of A (m x k), B (n x k) follows
-  long long zoff;  // element offset of this leaf's z (k x 16 slots) in the z buffer
+struct GemvTask {
+  int O;           // output rows
+  int first_unit;  // units [first_unit, first_unit + nunits) in order
+  int nunits;
+  int out_row;     // y: first output row (cluster order); z: first xz row of the slot
 };
 
-// A chunk [start, start + len) of the rows of B ('N') or A ('T') of one Rk leaf.
-struct GemvZItem {
-  int leaf, start, len, pad;
-  long long dst_off;  // where its k x R partial goes in the z buffer
+// One launch: tasks of one shape class, each CTA of a persistent grid takes a contiguous
+// range [cta_begin[b], cta_begin[b + 1]) of tasks.
+struct GemvLaunch {
+  int ntasks = 0;
+  int ncta = 0;
+  const GemvTask* tasks = nullptr;
+  const int* cta_begin = nullptr;
+  int rpt = 1;          // rows per lane: output rows <= 32 * rpt
+  int ol = 32;          // output lanes (16 or 32)
+  bool transposed = false;
+  bool out_is_y = false;
 };
 
-// One output block: rows [off, off + len) of y in cluster order, fed by `count` entries.
-struct GemvYBlock {
-  int off, len, first, count;
-};
-struct GemvYEntry {
-  int type;  // 0 full leaf, 1 rk leaf
-  int leaf;  // index in the full or rk table
-  int sub;   // offset of the block inside the leaf's rows ('N') or cols ('T')
-  int pad;
+// A long leaf whose z is computed in several chunks: the chunks' partial slots
+// (nparts consecutive slots of k rows from part_row) are summed into final_row.
+struct GemvZred {
+  int final_row, k, part_row, nparts;
 };
 
 struct GemvSide {
-  int nzitems = 0;
-  const GemvZItem* zitems = nullptr;
-  int nmulti = 0;  // leaves split into several items
-  const int* multi = nullptr;
-  const int* mfirst = nullptr;
-  const int* mcount = nullptr;
-  int nblocks = 0;
-  const GemvYBlock* blocks = nullptr;
-  const GemvYEntry* entries = nullptr;
-  int GS = 64;  // threads per row group in the y-phase
+  static const int kMaxLaunch = 8;
+  int nz = 0;  // z-phase launches (one per rank class)
+  GemvLaunch z[kMaxLaunch];
+  int nzred = 0;
+  const GemvZred* zred = nullptr;
+  GemvLaunch y;
+  const GemvUnit* units = nullptr;
 };
 
-// Optional per-phase timing of one eager product: events recorded before the gather and
-// after the gather, z-phase (+ reduction) and y-phase.
+struct GemvFullLeaf {
+  int row_off, m, col_off, n;
+  long long goff;  // canonical offset (gradients, payload): column-major m x n
+};
+struct GemvRkLeaf {
+  int row_off, m, col_off, n, k, pad;
+  long long goff;   // canonical offset: A (m x k) then B (n x k), column-major
+  int zrow_n, zrow_t;  // xz rows of z = B^T x ('N') and z' = A^T x ('T' / 'C')
+};
+
 struct GemvTiming {
   cudaEvent_t ev[4];
 };
 
 struct GemvPlan {
   int n_rows = 0, n_cols = 0;
-  const int* perm_rows = nullptr;  // internal -> client, rows
+  int n_in_max = 0;      // rows of the x part of the xz buffer
+  long long xz_rows = 0; // total rows of the xz buffer (x part + z slots + partial slots)
+  const int* perm_rows = nullptr;  // internal -> client
   const int* perm_cols = nullptr;
+  const void* arena = nullptr;
   int nfull = 0, nrk = 0;
   const GemvFullLeaf* full = nullptr;
   const GemvRkLeaf* rk = nullptr;
-  const void* full_arena = nullptr;
-  const void* rk_arena = nullptr;
-  GemvSide side_n, side_t;
-  long long z_elems = 0;
+  GemvSide side[2];                       // [0] 'N', [1] 'T' / 'C'
 };
 
 }  // namespace hmatb200

@@ -21,16 +21,29 @@ struct RkLeafDesc {
 // aRef (m), bRef (n).
 inline long long rk_slot_elems(int m, int n, int kcap) { return (long long)(m + n) * (kcap + 1); }
 
-// One dense (non-admissible) leaf.
+// A row panel of a leaf in the arena: rows [rs, rs + len) of the leaf (relative), stored
+// column-major at `off` (len x n for full leaves, len x k for the A factor of Rk leaves).
+struct PanelDesc {
+  int rs, len;
+  long long off;
+};
+
+// One dense (non-admissible) leaf and its row panels.
 struct FullLeafDesc {
   int row_off, m, col_off, n;
-  long long off;  // element offset in the full-leaf arena (column-major m x n)
+  int panel_first, npanel;
+};
+
+// Where the truncated factors of an Rk leaf go: A as row panels, B transposed (k x n).
+struct RkStoreDesc {
+  int panel_first, npanel;
+  long long bt_off;
 };
 
 // ---- assembly ----
 template <typename T>
-void launch_assemble_full(const FullLeafDesc* d_leaves, int nleaves, const KernelParams& kp, Points pts,
-                          T* arena, cudaStream_t s);
+void launch_assemble_full(const FullLeafDesc* d_leaves, int nleaves, const PanelDesc* panels, const KernelParams& kp,
+                          Points pts, T* arena, cudaStream_t s);
 
 // ACA+ (compression.cpp:553-724), delegating to partial ACA when n * 100 < m.  Leaves are
 // taken in `order` from a device work counter that must be zero at launch.
@@ -55,26 +68,33 @@ void launch_truncate(const RkLeafDesc* d_leaves, const int* d_order, int nleaves
 template <typename T>
 long long truncate_slab_elems(int max_m, int max_n, int max_k);
 
-// Copies the truncated factors of each leaf from its workspace slot into the compact
-// Rk arena at dst_off[leaf] (A then B, column-major).
+// Copies the truncated factors of each leaf from its workspace slot into the arena:
+// A as row panels, B transposed.
 template <typename T>
 void launch_compact(const RkLeafDesc* d_leaves, int nleaves, const T* ws, const int* ranks,
-                    const long long* dst_off, T* arena, cudaStream_t s);
+                    const RkStoreDesc* store, const PanelDesc* panels, T* arena, cudaStream_t s);
 
 // ---- gemv ----
 }  // namespace hmatb200
 #include "gemv_plan.h"
 namespace hmatb200 {
+// y = alpha op(H) x + beta y on device buffers (client numbering); `xz` is the scratch
+// buffer of plan.xz_rows rows of gemv_rhs_stride(sizeof(T), 16) scalars; `err` is set when
+// a pipeline wait gives up.
 template <typename T>
-void launch_gemv(const GemvPlan& p, char trans, int nrhs, T alpha, T beta, const T* x_client, T* y_client,
-                 T* x_rm, T* zpart, T* z, cudaStream_t s, const GemvTiming* timing = nullptr);
+void launch_gemv(const GemvPlan& p, char trans, int nrhs, T alpha, T beta, const T* x_client, T* y_client, T* xz,
+                 int* err, cudaStream_t s, const GemvTiming* timing = nullptr);
+// Row stride (scalars) of the xz buffer for R right-hand sides.
+int gemv_rhs_stride(int elem_bytes, int R);
+// Dynamic shared memory of one streamed-task CTA.
+size_t stream_smem_bytes(int elem_bytes, int R, int RS, int omax, bool transposed);
 
 // Leaf-factor gradients of y = H x for the output gradient r (real types; x, r device,
 // client numbering, nrhs <= 16): dF = r_I x_J^T, dA = r_I (B^T x_J)^T, dB = x_J (A^T r_I)^T,
 // written (or added) into gradient arenas laid out like the leaf arenas.
 template <typename T>
-void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, T* x_rm, T* r_rm, T* zx, T* zr,
-                           T* gfull, T* grk, bool accumulate, cudaStream_t s);
+void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* rz, T* gfull, T* grk,
+                           bool accumulate, int* err, cudaStream_t s);
 
 // Grid size of a persistent launch: a multiple of the SM count.
 int persistent_grid(int blocks_per_sm);

@@ -254,20 +254,32 @@ __global__ void __launch_bounds__(kTruncThreads) truncate_kernel(const RkLeafDes
   }
 }
 
+// Writes A as row panels (len x k column-major each) and B transposed (k x n column-major).
 template <typename T>
 __global__ void compact_kernel(const RkLeafDesc* __restrict__ leaves, int nleaves, const T* __restrict__ ws,
-                               const int* __restrict__ ranks, const long long* __restrict__ dst_off, T* arena) {
+                               const int* __restrict__ ranks, const RkStoreDesc* __restrict__ store,
+                               const PanelDesc* __restrict__ panels, T* arena) {
   const int leaf = blockIdx.x;
   if (leaf >= nleaves) return;
   const RkLeafDesc d = leaves[leaf];
   const int k = ranks[leaf];
   if (k <= 0) return;
+  const RkStoreDesc st = store[leaf];
   const T* A = ws + d.ws_off;
   const T* B = A + (size_t)d.m * d.kcap;
-  T* dst = arena + dst_off[leaf];
-  const size_t na = (size_t)d.m * k, nb = (size_t)d.n * k;
-  for (size_t e = threadIdx.x; e < na; e += blockDim.x) dst[e] = A[e];
-  for (size_t e = threadIdx.x; e < nb; e += blockDim.x) dst[na + e] = B[e];
+  for (int p = 0; p < st.npanel; ++p) {
+    const PanelDesc P = panels[st.panel_first + p];
+    T* dst = arena + P.off;
+    for (int e = threadIdx.x; e < P.len * k; e += blockDim.x) {
+      const int i = e % P.len, l = e / P.len;
+      dst[e] = A[(size_t)l * d.m + P.rs + i];
+    }
+  }
+  T* bt = arena + st.bt_off;
+  for (int e = threadIdx.x; e < d.n * k; e += blockDim.x) {
+    const int l = e % k, j = e / k;
+    bt[e] = B[(size_t)l * d.n + j];
+  }
 }
 
 }  // namespace
@@ -291,17 +303,17 @@ void launch_truncate(const RkLeafDesc* d_leaves, const int* d_order, int nleaves
 
 template <typename T>
 void launch_compact(const RkLeafDesc* d_leaves, int nleaves, const T* ws, const int* ranks,
-                    const long long* dst_off, T* arena, cudaStream_t s) {
+                    const RkStoreDesc* store, const PanelDesc* panels, T* arena, cudaStream_t s) {
   if (nleaves <= 0) return;
-  compact_kernel<T><<<nleaves, 256, 0, s>>>(d_leaves, nleaves, ws, ranks, dst_off, arena);
+  compact_kernel<T><<<nleaves, 256, 0, s>>>(d_leaves, nleaves, ws, ranks, store, panels, arena);
 }
 
 #define HB_INST(T)                                                                                         \
   template long long truncate_slab_elems<T>(int, int, int);                                               \
   template void launch_truncate<T>(const RkLeafDesc*, const int*, int, double, T*, int*, int*, int*,     \
                                    typename Traits<T>::wide*, long long, int, cudaStream_t);               \
-  template void launch_compact<T>(const RkLeafDesc*, int, const T*, const int*, const long long*, T*,    \
-                                  cudaStream_t);
+  template void launch_compact<T>(const RkLeafDesc*, int, const T*, const int*, const RkStoreDesc*,        \
+                                  const PanelDesc*, T*, cudaStream_t);
 HB_INST(float)
 HB_INST(double)
 HB_INST(cfloat)

@@ -404,20 +404,20 @@ int hmat_b200_leaf_table(hmat_matrix_t* hmatrix, int* out);
  * (m x k) then B (n x k)); returns the number of scalars, or -1. */
 long long hmat_b200_leaf_payload(hmat_matrix_t* hmatrix, int leaf, void* out);
 
-/* Device views of the assembled leaves: the full-leaf and Rk arenas and, per leaf, the
- * element offset of its payload in its arena (-1 for empty).  Pointers stay valid until
- * the matrix is destroyed or re-assembled. */
-int hmat_b200_leaf_arenas(hmat_matrix_t* hmatrix, void** full_arena, long long* full_elems, void** rk_arena,
-                          long long* rk_elems, long long* leaf_offsets);
+/* Canonical payload layout of the assembled leaves: leaves in leaf-table order, each full
+ * leaf as F (m x n), each Rk leaf as A (m x k) then B (n x k), column-major, rank-0 leaves
+ * empty.  offsets[leaf] (leaf_count entries, may be NULL) and the total number of scalars.
+ * (The device storage itself is internal: row panels and B transposed.) */
+int hmat_b200_payload_layout(hmat_matrix_t* hmatrix, long long* offsets, long long* total);
 
-/* Leaf-factor gradients of L(H) for a loss whose gradient w.r.t. y = H x is `r`
- * (device buffers, client numbering, nrhs columns): accumulates (beta = 0 clears first)
- *   dF += r_I x_J^T              per full leaf
- *   dA += r_I (B^T x_J)^T        dB += x_J (A^T r_I)^T     per Rk leaf (A B^T)
- * into `grad_full` / `grad_rk`, laid out like the arenas.  The gradient w.r.t. x is
- * gemv('T') of r.  Real types only. */
-int hmat_b200_leaf_gradients(hmat_matrix_t* hmatrix, const void* x_dev, const void* r_dev, int nrhs,
-                             void* grad_full, void* grad_rk, int accumulate, void* stream);
+/* Leaf-factor gradients of y = H x for an output gradient `r` (device buffers, client
+ * numbering, 1 to 16 columns), written into `grad` (device, canonical payload layout),
+ * added to its contents when `accumulate` is non-zero:
+ *   dF = r_I x_J^T                                         per full leaf F
+ *   dA = r_I (B^T x_J)^T,  dB = x_J (A^T r_I)^T             per Rk leaf A B^T
+ * The gradient with respect to x is gemv('T') of r.  Real value types only. */
+int hmat_b200_leaf_gradients(hmat_matrix_t* hmatrix, const void* x_dev, const void* r_dev, int nrhs, void* grad,
+                             int accumulate, void* stream);
 
 /* One eager product y = op(H) x on device buffers (1 to 16 right-hand sides), timed per
  * phase with CUDA events: ms3 = device ms of [gather, z-phase, y-phase], bytes3 = their
