@@ -642,6 +642,7 @@ class Engine : public EngineBase {
     DevArray<GemvTask> tasks[GemvSide::kMaxLaunch + 1];
     DevArray<int> begin[GemvSide::kMaxLaunch + 1];
     DevArray<GemvZred> zred;
+    DevArray<int2> yrows;
   };
 
   static int rank_class(int k) { return k <= 16 ? 0 : (k <= 32 ? 1 : (k <= 64 ? 2 : 3)); }
@@ -650,13 +651,27 @@ class Engine : public EngineBase {
     rpt = c <= 1 ? 1 : (c == 2 ? 2 : 4);
   }
 
-  // Units of out(O rows) += P X for a column-major O x C block at `poff`, X rows from `xrow`.
-  void px_units(std::vector<GemvUnit>& u, long long poff, int O, int C, int xrow) {
-    for (int j0 = 0; j0 < C; j0 += 32) {
+  // Columns per unit of a warp-level launch: the piece (O x cols) and its X rows fit one
+  // pipeline stage at the widest right-hand-side tile.
+  static int warp_unit_cols(int O) {
+    const int Rmax = sizeof(T) >= 16 ? 4 : 16;
+    const int xrow_bytes = gemv_rhs_stride((int)sizeof(T), Rmax) * (int)sizeof(T);
+    // pieces start 16-byte aligned when cols * O * sizeof(T) is a multiple of 16
+    const int g = sizeof(T) >= 16 ? 1 : 16 / (int)sizeof(T);
+    int cols = std::min(kWarpXBytes / xrow_bytes, kWarpPieceBytes / (O * (int)sizeof(T)));
+    cols -= cols % g;
+    if (cols < g) throw Error("gemv plan: output too tall for a warp-level unit");
+    return cols;
+  }
+
+  // Units of out(O rows) += P X for a column-major O x C block at `poff`, X rows from `xrow`,
+  // `cols` columns per unit.
+  void px_units(std::vector<GemvUnit>& u, long long poff, int O, int C, int xrow, int cols = 32) {
+    for (int j0 = 0; j0 < C; j0 += cols) {
       GemvUnit g;
       g.poff = poff + (long long)j0 * O;
       g.xrow = xrow + j0;
-      g.c = std::min(32, C - j0);
+      g.c = std::min(cols, C - j0);
       g.o0 = 0;
       g.ow = O;
       g.pel = O * g.c;
@@ -681,15 +696,21 @@ class Engine : public EngineBase {
     }
   }
 
-  // Contiguous ranges of tasks of about equal bytes for a persistent grid.
+  // Contiguous ranges of tasks of about equal bytes for a persistent grid: one range per
+  // CTA, or per warp for warp-level launches.  Returns the range starts; *ncta is the grid.
   std::vector<int> partition(const std::vector<GemvTask>& tasks, const std::vector<GemvUnit>& units, int omax,
-                             bool transposed) {
+                             bool transposed, bool warp_level, int* ncta) {
     const int Rmax = sizeof(T) >= 16 ? 4 : 16;
     const int RS16 = gemv_rhs_stride((int)sizeof(T), Rmax);
-    const size_t smem = stream_smem_bytes((int)sizeof(T), Rmax, RS16, omax, transposed);
+    const size_t smem = warp_level ? warp_stream_smem_bytes((int)sizeof(T))
+                                   : stream_smem_bytes((int)sizeof(T), Rmax, RS16, omax, transposed);
     int per_sm = (int)std::min<size_t>(8, (226 * 1024) / (smem + 1024));
     per_sm = std::max(per_sm, 1);
-    const int G = std::max(1, std::min((int)tasks.size(), persistent_grid(per_sm)));
+    const int wpc = warp_level ? warp_stream_warps_per_cta() : 1;
+    const int nt = (int)tasks.size();
+    const int cta = std::max(1, std::min((nt + wpc - 1) / wpc, persistent_grid(per_sm)));
+    *ncta = cta;
+    const int G = cta * wpc;
     std::vector<double> cost(tasks.size());
     double tot = 0;
     for (size_t t = 0; t < tasks.size(); ++t) {
@@ -712,16 +733,44 @@ class Engine : public EngineBase {
     return begin;
   }
 
+  // Warp-level shape of an 'N' launch for tasks of at most omax rows: the column-slice
+  // window up to 32 rows, half-warp row groups up to 64, lanes over rows up to 128.
+  static void warp_shape(GemvLaunch& L, int omax) {
+    L.warp_level = true;
+    L.ol = 32;
+    L.map = omax <= 32 ? 2 : (omax <= 64 ? 1 : 0);
+    L.rpt = omax <= 32 ? 1 : 4;
+  }
+
   void finish_launch(GemvLaunch& L, SideBuf& sb, int slot, std::vector<GemvTask>& tasks,
                      const std::vector<GemvUnit>& units, int ol, int rpt, bool transposed, bool out_is_y) {
     L.ntasks = (int)tasks.size();
-    L.ol = ol;
-    L.rpt = rpt;
+    if (!L.warp_level) {
+      L.ol = ol;
+      L.rpt = rpt;
+    }
     L.transposed = transposed;
     L.out_is_y = out_is_y;
     if (tasks.empty()) return;
-    std::vector<int> begin = partition(tasks, units, ol * rpt, transposed);
-    L.ncta = (int)begin.size() - 1;
+    // the kernel walks units sequentially across the tasks of a CTA
+    for (size_t t = 1; t < tasks.size(); ++t)
+      if (tasks[t].first_unit != tasks[t - 1].first_unit + tasks[t - 1].nunits)
+        throw Error("gemv plan: units of a launch are not contiguous");
+    const int omax = L.warp_level ? (L.map == 2 ? 32 : (L.map == 1 ? 64 : 128)) : ol * rpt;
+    for (auto& t : tasks)
+      if (t.O > omax) throw Error("gemv plan: task taller than its launch shape");
+    if (L.warp_level) {
+      // every unit of the launch must fit one stage of the per-warp pipeline
+      const int Rmax = sizeof(T) >= 16 ? 4 : 16;
+      const long long xrow_bytes = (long long)gemv_rhs_stride((int)sizeof(T), Rmax) * sizeof(T);
+      for (auto& t : tasks)
+        for (int u = t.first_unit; u < t.first_unit + t.nunits; ++u) {
+          const GemvUnit& g = units[u];
+          if ((long long)g.pel * sizeof(T) > kWarpPieceBytes || g.shift != 0 || g.c * xrow_bytes > kWarpXBytes)
+            throw Error("gemv plan: unit above the warp-level stage capacity");
+        }
+    }
+    std::vector<int> begin = partition(tasks, units, omax, transposed, L.warp_level, &L.ncta);
     sb.tasks[slot].upload(tasks, stream_);
     sb.begin[slot].upload(begin, stream_);
     L.tasks = sb.tasks[slot].p;
@@ -739,6 +788,7 @@ class Engine : public EngineBase {
 
     // ---- z-phase: one task per Rk leaf (or chunk), one launch per rank class ----
     std::vector<GemvTask> zt[4];
+    std::vector<GemvUnit> zunits[4];
     std::vector<GemvZred> zred;
     std::vector<GemvUnit> lu;
     for (size_t t = 0; t < K.size(); ++t) {
@@ -748,7 +798,7 @@ class Engine : public EngineBase {
       lu.clear();
       if (!trans) {
         // z = B^T x_J: B^T is k x n column-major after the A panels
-        px_units(lu, bt_offset(leaf), k.k, k.n, k.col_off);
+        px_units(lu, bt_offset(leaf), k.k, k.n, k.col_off, warp_unit_cols(k.k));
       } else {
         // z' = A^T x_I: each A panel (len x k) is a transposed piece
         auto br = block_range(rblocks_, rstarts_, k.row_off, k.m);
@@ -759,22 +809,30 @@ class Engine : public EngineBase {
         }
       }
       if (k.k > 128) throw Error("gemv plan: ranks above 128 are not supported by the streamed kernels");
-      const int cls = rank_class(k.k);
+      // 'N' launches take every rank up to 32 in one column-slice window launch
+      const int cls = trans ? rank_class(k.k) : std::max(1, rank_class(k.k));
       const int zrow = trans ? k.zrow_t : k.zrow_n;
+      // units of one launch must be contiguous in task order: collect them per class
+      std::vector<GemvUnit>& cu = zunits[cls];
       if ((int)lu.size() <= kMaxUnits) {
-        zt[cls].push_back(GemvTask{k.k, (int)units.size(), (int)lu.size(), zrow});
-        units.insert(units.end(), lu.begin(), lu.end());
+        zt[cls].push_back(GemvTask{k.k, (int)cu.size(), (int)lu.size(), zrow});
+        cu.insert(cu.end(), lu.begin(), lu.end());
       } else {
         const int nparts = ((int)lu.size() + kMaxUnits - 1) / kMaxUnits;
         const int part_row = (int)next_row;
         next_row += (long long)nparts * k.k;
         for (int pidx = 0; pidx < nparts; ++pidx) {
           const int u0 = pidx * kMaxUnits, u1 = std::min((int)lu.size(), u0 + kMaxUnits);
-          zt[cls].push_back(GemvTask{k.k, (int)units.size(), u1 - u0, part_row + pidx * k.k});
-          units.insert(units.end(), lu.begin() + u0, lu.begin() + u1);
+          zt[cls].push_back(GemvTask{k.k, (int)cu.size(), u1 - u0, part_row + pidx * k.k});
+          cu.insert(cu.end(), lu.begin() + u0, lu.begin() + u1);
         }
         zred.push_back(GemvZred{zrow, k.k, part_row, nparts});
       }
+    }
+    for (int c = 0; c < 4; ++c) {
+      const int shift = (int)units.size();
+      for (auto& t : zt[c]) t.first_unit += shift;
+      units.insert(units.end(), zunits[c].begin(), zunits[c].end());
     }
     // ---- y-phase: one task per output block ----
     std::vector<std::vector<std::pair<int, int>>> per_block(oblocks.size());  // (leaf, 0 full / 1 rk index)
@@ -789,6 +847,11 @@ class Engine : public EngineBase {
     for (size_t t = 0; t < rk_leaf.size(); ++t) rk_index[rk_leaf[t]] = (int)t;
     std::vector<GemvTask> yt;
     int maxlen = 1;
+    // 'N': each output block is cut into chunks of at most kYChunkUnits units whose partial
+    // rows go to xz; a final pass sums them into y (client order)
+    const int kYChunkUnits = 16;
+    std::vector<int2> yrows;
+    if (!trans) yrows.assign(R_->n, int2{0, 0});
     for (size_t b = 0; b < oblocks.size(); ++b) {
       const Block& ob = oblocks[b];
       const int first = (int)units.size();
@@ -800,7 +863,7 @@ class Engine : public EngineBase {
           const int w = l.type == 0 ? l.n : ranks[i];
           const long long poff = row_panel_offset(i, ob.off, w);
           const int xrow = l.type == 0 ? l.col_off : K[rk_index[i]].zrow_n;
-          px_units(units, poff, ob.len, w, xrow);
+          px_units(units, poff, ob.len, w, xrow, warp_unit_cols(ob.len));
         } else if (l.type == 0) {
           // columns of block b in every row panel of full leaf i
           auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
@@ -816,25 +879,46 @@ class Engine : public EngineBase {
                     K[rk_index[i]].zrow_t);
         }
       }
-      yt.push_back(GemvTask{ob.len, first, (int)units.size() - first, ob.off});
       maxlen = std::max(maxlen, ob.len);
+      const int nu = (int)units.size() - first;
+      if (trans) {
+        yt.push_back(GemvTask{ob.len, first, nu, ob.off});
+        continue;
+      }
+      const int nparts = (nu + kYChunkUnits - 1) / kYChunkUnits;
+      const int part_row = (int)next_row;
+      next_row += (long long)nparts * ob.len;
+      for (int pidx = 0; pidx < nparts; ++pidx) {
+        const int u0 = pidx * kYChunkUnits, u1 = std::min(nu, u0 + kYChunkUnits);
+        yt.push_back(GemvTask{ob.len, first + u0, u1 - u0, part_row + pidx * ob.len});
+      }
+      for (int l = 0; l < ob.len; ++l) yrows[R_->perm[ob.off + l]] = int2{part_row + l, (nparts << 8) | ob.len};
     }
     // launches
     side.nz = 0;
+    static const int kClassMax[4] = {16, 32, 64, 128};
     for (int c = 0; c < 4; ++c) {
       if (zt[c].empty()) continue;
       int ol, rpt;
       class_shape(c, ol, rpt);
-      finish_launch(side.z[side.nz], sb, side.nz, zt[c], units, ol, rpt, trans, false);
+      GemvLaunch& L = side.z[side.nz];
+      L = GemvLaunch();
+      if (!trans) warp_shape(L, kClassMax[c]);
+      finish_launch(L, sb, side.nz, zt[c], units, ol, rpt, trans, false);
       side.nz++;
     }
     const int rpt = maxlen <= 32 ? 1 : (maxlen <= 64 ? 2 : 4);
+    side.y = GemvLaunch();
+    if (!trans) warp_shape(side.y, maxlen);
     finish_launch(side.y, sb, GemvSide::kMaxLaunch, yt, units, 32, rpt, trans, true);
     sb.units.upload(units, stream_);
     side.units = sb.units.p;
     sb.zred.upload(zred, stream_);
     side.nzred = (int)zred.size();
     side.zred = sb.zred.p;
+    sb.yrows.upload(yrows, stream_);
+    side.nyrows = (int)yrows.size();
+    side.yrows = sb.yrows.p;
   }
 
   long long bt_offset(int leaf) const {

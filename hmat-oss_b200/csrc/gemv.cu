@@ -17,10 +17,13 @@
 // about equal bytes.  Each thread accumulates up to 4 output rows x R right-hand sides in
 // registers; inner-dimension slices (warps, and lanes when the output is narrow) are summed
 // at the end of each task in a fixed order, so repeated products are bitwise identical.
+#include <type_traits>
+
 #include "gemv_plan.h"
 #include "kernels.h"
 
 namespace hmatb200 {
+size_t warp_stream_smem_bytes(int elem_bytes);
 namespace {
 
 constexpr int kThreads = 128;
@@ -67,6 +70,14 @@ __device__ inline cfloat shfl_xor(cfloat v, int m) {
 }
 __device__ inline cdouble shfl_xor(cdouble v, int m) {
   return cdouble{__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m)};
+}
+__device__ inline float shfl_idx(float v, int l) { return __shfl_sync(0xffffffffu, v, l); }
+__device__ inline double shfl_idx(double v, int l) { return __shfl_sync(0xffffffffu, v, l); }
+__device__ inline cfloat shfl_idx(cfloat v, int l) {
+  return cfloat{__shfl_sync(0xffffffffu, v.x, l), __shfl_sync(0xffffffffu, v.y, l)};
+}
+__device__ inline cdouble shfl_idx(cdouble v, int l) {
+  return cdouble{__shfl_sync(0xffffffffu, v.x, l), __shfl_sync(0xffffffffu, v.y, l)};
 }
 
 // Loads Q consecutive elements from shared memory (vectorised when aligned).
@@ -255,6 +266,259 @@ __global__ void __launch_bounds__(kThreads) stream_kernel(const GemvTask* __rest
   }
 }
 
+// ---------------------------------------------------------------------------------
+// Warp-level streamed tasks (the 'N' products).  Every warp owns a contiguous range of whole
+// tasks and runs its own two-stage TMA pipeline: lane 0 copies the unit descriptor into the
+// stage and issues the unit's two bulk copies (P piece, X rows), completion on the stage's
+// mbarrier, so warps never wait for one another.  Lane maps (output rows O of the task):
+//   MODE 2 (O <= 32): the warp is a window of floor(32 / O) column slices x O rows, lane =
+//          slice * O + row; P is read as one contiguous run per step (no bank conflicts);
+//          the slices are summed through shared memory at the end of the task.
+//   MODE 1 (O <= 16 * A2): two column slices (half-warps) x 16 rows, A2 rows per lane
+//          (row, row + 16, ...); slices summed with one shuffle.
+//   MODE 0 (O <= 32 * A2): lanes over rows, A2 rows per lane, one slice.
+// Row groups above O are skipped warp-uniformly.  Every lane keeps all R right-hand sides
+// of its rows; float sums use the paired FMA (fma.rn.f32x2: two IEEE fmaf per
+// instruction).  Summation orders are fixed, so repeated products are bitwise identical.
+constexpr int kWarpCTA = 4;
+constexpr int kWarpStages = 2;
+constexpr int kWarpStageBytes = kWarpPieceBytes + kWarpXBytes;
+
+// R accumulators of one output row, and one X row as the FMAs consume it.
+template <typename T, int R, bool PAIR = std::is_same<T, float>::value && (R % 2 == 0)>
+struct RowOps {
+  using XV = T[R];
+  using AV = T[R];
+  __device__ static void load(const T* p, XV& x) { lds_vec<T, R>(p, x); }
+  __device__ static void zero_(AV& a) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) a[q] = zero<T>();
+  }
+  __device__ static void fma(T p, const XV& x, AV& a) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) a[q] = fmadd(p, x[q], a[q]);
+  }
+  __device__ static T get(const AV& a, int q) { return a[q]; }
+};
+template <int R>
+struct RowOps<float, R, true> {
+  static constexpr int N = R / 2;
+  using XV = unsigned long long[N];
+  using AV = unsigned long long[N];
+  __device__ static void load(const float* p, XV& x) {
+    if constexpr (R % 4 == 0) {
+      const uint4* s = reinterpret_cast<const uint4*>(p);
+#pragma unroll
+      for (int c = 0; c < R / 4; ++c) {
+        const uint4 v = s[c];
+        x[2 * c] = ((unsigned long long)v.y << 32) | v.x;
+        x[2 * c + 1] = ((unsigned long long)v.w << 32) | v.z;
+      }
+    } else {
+      const unsigned long long* s = reinterpret_cast<const unsigned long long*>(p);
+#pragma unroll
+      for (int c = 0; c < N; ++c) x[c] = s[c];
+    }
+  }
+  __device__ static void zero_(AV& a) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) a[i] = 0ull;  // the bits of (+0.0f, +0.0f)
+  }
+  __device__ static void fma(float p, const XV& x, AV& a) {
+    unsigned long long pp;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(pp) : "f"(p));
+#pragma unroll
+    for (int i = 0; i < N; ++i) asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(a[i]) : "l"(pp), "l"(x[i]));
+  }
+  __device__ static float get(const AV& a, int q) {
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a[q / 2]));
+    return (q & 1) ? hi : lo;
+  }
+};
+
+// Blocks per SM the register budget allows: more accumulator bytes, fewer resident warps.
+template <typename T, int R, int A2>
+constexpr int warp_min_blocks() {
+  return A2 * R * (int)sizeof(T) <= 256 ? 4 : 2;
+}
+
+template <typename T, int R, int RS, int MODE, int A2>
+__global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
+    warp_stream_kernel(const GemvTask* __restrict__ tasks, const int* __restrict__ warp_begin,
+                       const GemvUnit* __restrict__ units, const T* __restrict__ arena, T* xz, int* err) {
+  using Ops = RowOps<T, R>;
+  constexpr int OL = MODE == 0 ? 32 : 16;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char* wbase = smem_raw + (size_t)warp * kWarpStages * kWarpStageBytes;
+  GemvUnit* uslot =
+      reinterpret_cast<GemvUnit*>(smem_raw + (size_t)kWarpCTA * kWarpStages * kWarpStageBytes) + warp * kWarpStages;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWarpCTA * kWarpStages *
+                                                               (kWarpStageBytes + sizeof(GemvUnit))) +
+                   warp * kWarpStages;
+  const int gw = blockIdx.x * kWarpCTA + warp;
+  const int t0 = warp_begin[gw], t1 = warp_begin[gw + 1];
+  if (t0 >= t1) return;
+  const int u_begin = tasks[t0].first_unit;
+  const int u_end = tasks[t1 - 1].first_unit + tasks[t1 - 1].nunits;
+
+  if (lane == 0) {
+    for (int s = 0; s < kWarpStages; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  // lane 0: descriptor into the stage, then the unit's two bulk copies.  The descriptor of
+  // the next unit to issue is loaded one issue ahead, off the critical path.
+  GemvUnit nxt;
+  auto issue = [&](int u, const GemvUnit& U) {
+    const int s = (u - u_begin) % kWarpStages;
+    uslot[s] = U;
+    const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(T));
+    const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(T);
+    unsigned char* st = wbase + (size_t)s * kWarpStageBytes;
+    mbar_expect_tx(&bars[s], pbytes + xbytes);
+    bulk_g2s(st, arena + U.poff, pbytes, &bars[s]);
+    bulk_g2s(st + kWarpPieceBytes, xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
+  };
+  auto issue_next = [&](int v) {  // nxt holds units[v]
+    issue(v, nxt);
+    if (v + 1 < u_end) nxt = units[v + 1];
+  };
+  if (lane == 0) {
+    int v = u_begin;
+    for (; v < u_end && v < u_begin + kWarpStages; ++v) issue(v, units[v]);
+    if (v < u_end) nxt = units[v];
+  }
+
+  int u = u_begin;
+  GemvTask task_next = tasks[t0];
+  for (int t = t0; t < t1; ++t) {
+    const GemvTask task = task_next;
+    if (t + 1 < t1) task_next = tasks[t + 1];
+    const int O = task.O;
+    int row0, js, SL;
+    if constexpr (MODE == 2) {
+      // exact for lane < 32 and O <= 32: the quotients are at least 1/64 away from integers
+      const float inv = __frcp_rn((float)O);
+      SL = (int)(32.5f * inv);
+      js = (int)(((float)lane + 0.5f) * inv);
+      row0 = lane - js * O;
+    } else if constexpr (MODE == 1) {
+      SL = 2;
+      row0 = lane & 15;
+      js = lane >> 4;
+    } else {
+      SL = 1;
+      row0 = lane;
+      js = 0;
+    }
+    typename Ops::AV acc[A2];
+#pragma unroll
+    for (int a = 0; a < A2; ++a) Ops::zero_(acc[a]);
+
+    for (int kk = 0; kk < task.nunits; ++kk, ++u) {
+      const int s = (u - u_begin) % kWarpStages;
+      const uint32_t parity = (uint32_t)(((u - u_begin) / kWarpStages) & 1);
+      long long spins = 0;
+      while (!mbar_try_wait(&bars[s], parity)) {
+        if (++spins > kWaitLimit) {
+          if (lane == 0) atomicExch(err, 1);
+          return;
+        }
+      }
+      const int c = uslot[s].c;
+      const T* P = reinterpret_cast<const T*>(wbase + (size_t)s * kWarpStageBytes);
+      const T* X = reinterpret_cast<const T*>(wbase + (size_t)s * kWarpStageBytes + kWarpPieceBytes);
+      if constexpr (MODE == 2) {
+        if (js < SL) {
+#pragma unroll 4
+          for (int j = js; j < c; j += SL) {
+            typename Ops::XV xv;
+            Ops::load(X + (size_t)j * RS, xv);
+            Ops::fma(P[(size_t)j * O + row0], xv, acc[0]);
+          }
+        }
+      } else {
+#pragma unroll 2
+        for (int j = js; j < c; j += SL) {
+          typename Ops::XV xv;
+          Ops::load(X + (size_t)j * RS, xv);
+          const T* pc = P + (size_t)j * O + row0;
+#pragma unroll
+          for (int a = 0; a < A2; ++a)
+            if (a * OL < O) Ops::fma(pc[a * OL], xv, acc[a]);
+        }
+      }
+      __syncwarp();  // every lane is done with stage s
+      if (lane == 0 && u + kWarpStages < u_end) issue_next(u + kWarpStages);
+    }
+
+    // ---- epilogue: the task's rows go to xz[out_row + l], zero-padded to RS ----
+    T* out = xz + (size_t)task.out_row * RS;
+    if constexpr (MODE == 2) {
+      // slices summed in slice order into the lanes of slice 0 (lane = row)
+      T tot[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) tot[q] = Ops::get(acc[0], q);
+      for (int k = 1; k < SL; ++k) {
+        const int src = (lane + k * O) & 31;
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const T v = shfl_idx(Ops::get(acc[0], q), src);
+          tot[q] = tot[q] + v;
+        }
+      }
+      if (lane < O) {
+        T* row = out + (size_t)lane * RS;
+#pragma unroll
+        for (int q = 0; q < R; ++q) row[q] = tot[q];
+#pragma unroll
+        for (int q = R; q < RS; ++q) row[q] = zero<T>();
+      }
+    } else {
+#pragma unroll
+      for (int a = 0; a < A2; ++a) {
+        if (a * OL < O) {
+          const int l = row0 + a * OL;
+          T* row = out + (size_t)l * RS;
+#pragma unroll
+          for (int q = 0; q < R; ++q) {
+            T v = Ops::get(acc[a], q);
+            if constexpr (MODE == 1) v = v + shfl_xor(v, 16);
+            // MODE 1: half-warp js writes half js of the right-hand sides
+            const bool mine = MODE == 0 || (js == 0 ? q < (R + 1) / 2 : q >= (R + 1) / 2);
+            if (l < O && mine) row[q] = v;
+          }
+          if (l < O && js == 0)
+#pragma unroll
+            for (int q = R; q < RS; ++q) row[q] = zero<T>();
+        }
+      }
+    }
+  }
+}
+
+// y in client order from the partial rows of the 'N' y tasks:
+// y[i, q0 + q] = alpha * sum_p xz[pos + p * O, q] + beta * y[i, q0 + q], rows i of the client
+// order (consecutive threads write consecutive rows of one column of y).
+template <typename T, int R, int RS>
+__global__ void yfinal_kernel(const int2* __restrict__ rows, int n, const T* __restrict__ xz, T* __restrict__ y,
+                              int ldy, int q0, int r, T alpha, T beta) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)n * R) return;
+  const int i = (int)(e % n), q = (int)(e / n);
+  if (q0 + q >= r) return;
+  const int2 d = rows[i];
+  const int O = d.y & 255, np = d.y >> 8;
+  T v = zero<T>();
+  for (int p = 0; p < np; ++p) v = v + xz[((size_t)d.x + (size_t)p * O) * RS + q];
+  T* yp = y + (size_t)i + (size_t)(q0 + q) * ldy;
+  T outv = alpha * v;
+  if (!is_zero_val(beta)) outv = fmadd(beta, *yp, outv);
+  *yp = outv;
+}
+
 // Sums the chunk partials of long leaves: xz[final + l] = sum_p xz[part + p k + l].
 template <typename T, int RS>
 __global__ void zred_kernel(const GemvZred* __restrict__ zr, T* xz) {
@@ -282,10 +546,31 @@ void launch_stream_t(const GemvLaunch& L, const GemvUnit* units, const T* arena,
                                        ldy, q0, r, alpha, beta, err);
 }
 
+template <typename T, int R, int RS, int MODE, int A2>
+void launch_warp_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, int* err, cudaStream_t s) {
+  auto kern = warp_stream_kernel<T, R, RS, MODE, A2>;
+  const size_t smem = warp_stream_smem_bytes((int)sizeof(T));
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  kern<<<L.ncta, kWarpCTA * 32, smem, s>>>(L.tasks, L.cta_begin, units, arena, xz, err);
+}
+
 template <typename T, int R, int RS, bool TRANSP>
 void launch_stream(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, int conj, const int* perm_out,
                    T* y, int ldy, int q0, int r, T alpha, T beta, int* err, cudaStream_t s) {
   if (L.ntasks <= 0) return;
+  if (L.warp_level) {
+    if (L.map == 2)
+      launch_warp_t<T, R, RS, 2, 1>(L, units, arena, xz, err, s);
+    else if (L.map == 1)
+      launch_warp_t<T, R, RS, 1, 4>(L, units, arena, xz, err, s);
+    else
+      launch_warp_t<T, R, RS, 0, 4>(L, units, arena, xz, err, s);
+    return;
+  }
   if (L.ol == 16)
     launch_stream_t<T, R, RS, 16, 1, TRANSP>(L, units, arena, xz, conj, perm_out, y, ldy, q0, r, alpha, beta, err, s);
   else if (L.rpt == 1)
@@ -317,6 +602,11 @@ void run_tile(const GemvPlan& p, int nrhs, int q0, T alpha, T beta, const T* x, 
   if (tm) cudaEventRecord(tm->ev[2], s);
   launch_stream<T, R, RS, TRANSP>(side.y, side.units, arena, xz, conj, perm_out, y, ld_out, q0, nrhs, alpha, beta,
                                   err, s);
+  if (side.y.warp_level) {
+    const long long ty = (long long)side.nyrows * R;
+    yfinal_kernel<T, R, RS><<<(unsigned)((ty + 255) / 256), 256, 0, s>>>(side.yrows, side.nyrows, xz, y, ld_out, q0,
+                                                                         nrhs, alpha, beta);
+  }
   if (tm) cudaEventRecord(tm->ev[3], s);
 }
 
@@ -421,6 +711,12 @@ size_t stream_smem_bytes(int elem_bytes, int R, int RS, int omax, bool transpose
 }
 
 int gemv_rhs_stride(int elem_bytes, int R) { return R * elem_bytes >= 16 ? R : 16 / elem_bytes; }
+
+size_t warp_stream_smem_bytes(int elem_bytes) {
+  (void)elem_bytes;
+  return (size_t)kWarpCTA * kWarpStages * (kWarpStageBytes + sizeof(GemvUnit) + sizeof(uint64_t));
+}
+int warp_stream_warps_per_cta() { return kWarpCTA; }
 
 template <typename T>
 void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* rz, T* gfull, T* grk,

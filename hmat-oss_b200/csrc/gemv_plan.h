@@ -40,12 +40,21 @@ struct GemvLaunch {
   int ntasks = 0;
   int ncta = 0;
   const GemvTask* tasks = nullptr;
-  const int* cta_begin = nullptr;
+  const int* cta_begin = nullptr;  // warp-level launches: one range per warp (ncta * 4 + 1 entries)
   int rpt = 1;          // rows per lane: output rows <= 32 * rpt
   int ol = 32;          // output lanes (16 or 32)
   bool transposed = false;
   bool out_is_y = false;
+  // Warp-level launches ('N' products): each warp owns whole tasks and pipelines its own
+  // units.  map 2: column-slice window over tasks of at most 32 rows; map 1: half-warp row
+  // groups (at most 64 rows); map 0: lanes over rows (at most 128 rows).
+  bool warp_level = false;
+  int map = 0;
 };
+
+// Per-stage capacities of the warp-level pipeline (bytes): one P piece and its X rows.
+constexpr int kWarpPieceBytes = 4096;
+constexpr int kWarpXBytes = 2048;
 
 // A long leaf whose z is computed in several chunks: the chunks' partial slots
 // (nparts consecutive slots of k rows from part_row) are summed into final_row.
@@ -61,6 +70,10 @@ struct GemvSide {
   const GemvZred* zred = nullptr;
   GemvLaunch y;
   const GemvUnit* units = nullptr;
+  // Warp-level y launches write partial rows (chunks of the output blocks) into xz; the
+  // final pass reads, per client row i, yrows[i] = {xz row of part 0, nparts << 8 | O}.
+  int nyrows = 0;
+  const int2* yrows = nullptr;
 };
 
 struct GemvFullLeaf {

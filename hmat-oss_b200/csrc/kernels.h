@@ -86,8 +86,10 @@ void launch_gemv(const GemvPlan& p, char trans, int nrhs, T alpha, T beta, const
                  int* err, cudaStream_t s, const GemvTiming* timing = nullptr);
 // Row stride (scalars) of the xz buffer for R right-hand sides.
 int gemv_rhs_stride(int elem_bytes, int R);
-// Dynamic shared memory of one streamed-task CTA.
+// Dynamic shared memory of one streamed-task CTA, and of one warp-level CTA (and its warps).
 size_t stream_smem_bytes(int elem_bytes, int R, int RS, int omax, bool transposed);
+size_t warp_stream_smem_bytes(int elem_bytes);
+int warp_stream_warps_per_cta();
 
 // Leaf-factor gradients of y = H x for the output gradient r (real types; x, r device,
 // client numbering, nrhs <= 16): dF = r_I x_J^T, dA = r_I (B^T x_J)^T, dB = x_J (A^T r_I)^T,
