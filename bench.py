@@ -165,6 +165,131 @@ def reference_arm(args, rank, world):
     return 0
 
 
+def _time_device(fn, steps, warmup, stream):
+    """Mean device ms of fn(stream) over `steps` calls after `warmup`, CUDA events on `stream`."""
+    import torch
+    for _ in range(warmup):
+        fn(stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def supplementary(args):
+    """One JSON line for a configuration other than the headline one (cfg0: plain FP64
+    cylinder 8,000; cfg2: uneven batch of 64 covariance matrices; cfg3: complex Helmholtz
+    cylinder 200,000; cfg4: adjoint of 1/2 ||H x - b||^2 on a 50,000-point cube)."""
+    import torch
+    hb, wl = package(), workloads()
+    name = args.workload
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    out = {"workload": name, "supplementary": True, "data": "synthetic", "steps": args.steps, "warmup": args.warmup}
+
+    def make(c, vt):
+        hb.set_parameters(compressionMinLeafSize=0)
+        k = hb.kernel(c["kind"], delta=c.get("delta", 0.01), ell=c.get("ell", 0.3), nugget=c.get("nugget", 0.0),
+                      wavenumber=c.get("wavenumber", 0.0))
+        t0 = time.time()
+        h = hb.HMatrix(c["points"], k, value_type=vt, leaf_size=c["leaf"], eta=c["eta"], epsilon=c["eps"])
+        torch.cuda.synchronize()
+        return h, time.time() - t0
+
+    def gemv_ms(h, x_host, dtype, trans="N"):
+        xd = torch.from_numpy(np.ascontiguousarray(x_host.T)).to("cuda", dtype)
+        yd = torch.zeros_like(xd)
+        nr = x_host.shape[1]
+        ms = _time_device(lambda s: h.gemv_device(xd.data_ptr(), yd.data_ptr(), nr, trans=trans,
+                                                  stream=s.cuda_stream), args.steps, args.warmup, stream)
+        return ms, yd.T.cpu().numpy()
+
+    def asm_ms(h):
+        t = h.phase_times()
+        return t["full_ms"] + t["aca_ms"] + t["truncate_ms"], t
+
+    if name in ("cfg0", "cfg3"):
+        c = wl.config(name)
+        cplx = c["complex"]
+        x = wl.rhs(len(c["points"]), c["nrhs"], c["seed"], complex_=cplx)
+        res = {}
+        for label, vt, dt in ((("C", 2, torch.complex64), ("Z", 3, torch.complex128)) if cplx else
+                              (("S", 0, torch.float32), ("D", 1, torch.float64))):
+            h, wall = make(c, vt)
+            a_ms, parts = asm_ms(h)
+            ms, y = gemv_ms(h, x, dt)
+            T = h.leaf_table()
+            nrk = int(((T[:, 4] == 1)).sum())
+            res[label] = {"assembly_device_ms": a_ms, "assembly_wall_s": wall, "phase_ms": parts,
+                          "gemv_ms": ms, "gemv_gbs": h.gemv_bytes(c["nrhs"]) / (ms * 1e-3) / 1e9,
+                          "rk_leaves": nrk, "aca_leaves_per_s": nrk / ((parts["aca_ms"] + parts["truncate_ms"]) * 1e-3),
+                          "y": y}
+            h.close()
+        lo, hi = ("C", "Z") if cplx else ("S", "D")
+        err = float(np.linalg.norm(res[lo]["y"] - res[hi]["y"]) / np.linalg.norm(res[hi]["y"]))
+        for v in res.values():
+            v.pop("y")
+        out.update({"metric": "H-gemv GB/s; ACA+ leaves/s", "nrhs": c["nrhs"], "n": len(c["points"]),
+                    "results": res, "mixed_rel_err_vs_fp64_hmatrix": err,
+                    "gemv_speedup_mixed_vs_fp64": res[hi]["gemv_ms"] / res[lo]["gemv_ms"]})
+    elif name == "cfg2":
+        batch = wl.batch_config(64, seed=0)
+        res = {}
+        for label, vt in (("S", 0), ("D", 1)):
+            dev_ms = wall = 0.0
+            leaves = rk = dof = 0
+            for c in batch:
+                h, w = make(c, vt)
+                a_ms, _ = asm_ms(h)
+                T = h.leaf_table()
+                dev_ms += a_ms
+                wall += w
+                leaves += len(T)
+                rk += int((T[:, 4] == 1).sum())
+                dof += len(c["points"])
+                h.close()
+            res[label] = {"matrices": len(batch), "dof": dof, "leaves": leaves, "rk_leaves": rk,
+                          "assembly_device_ms_total": dev_ms, "assembly_wall_s_total": wall,
+                          "aca_leaves_per_s_device": rk / (dev_ms * 1e-3),
+                          "matrices_per_s_device": len(batch) / (dev_ms * 1e-3)}
+        out.update({"metric": "ACA+ leaves/s over the batch (device assembly time)", "results": res})
+    elif name == "cfg4":
+        c = wl.config(name)
+        n = len(c["points"])
+        x = wl.rhs(n, 1, c["seed"])
+        b = wl.rhs(n, 1, c["seed"] + 1)
+        h, wall = make(c, 0)
+        xd = torch.from_numpy(np.ascontiguousarray(x.T)).to("cuda", torch.float32)
+        bd = torch.from_numpy(np.ascontiguousarray(b.T)).to("cuda", torch.float32)
+        rd = torch.zeros_like(xd)
+        dx = torch.zeros_like(xd)
+        offs, total = h.payload_layout()
+        g = torch.zeros(total, device="cuda", dtype=torch.float32)
+        one = 1.0
+
+        def backward(s):
+            # r = H x - b, dx = H^T r, leaf gradients
+            rd.copy_(bd)
+            h.gemv_device(xd.data_ptr(), rd.data_ptr(), 1, alpha=one, beta=-1.0, stream=s.cuda_stream)
+            h.gemv_device(rd.data_ptr(), dx.data_ptr(), 1, trans="T", stream=s.cuda_stream)
+            h.leaf_gradients(xd.data_ptr(), rd.data_ptr(), 1, g.data_ptr(), accumulate=False, stream=s.cuda_stream)
+
+        with torch.cuda.stream(stream):
+            ms = _time_device(backward, args.steps, args.warmup, stream)
+        fwd = h.gemv_bytes(1)
+        payload = total * 4
+        out.update({"metric": "adjoint GB/s (forward bytes + written leaf gradients)", "n": n,
+                    "backward_ms": ms, "bytes": fwd + payload,
+                    "gbs": (fwd + payload) / (ms * 1e-3) / 1e9, "assembly_device_ms": asm_ms(h)[0]})
+        h.close()
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -173,6 +298,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"],
+                    help="cfg1 is the headline line; the others print supplementary lines")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -180,6 +307,12 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return reference_arm(args, rank, world)
+    if args.workload != "cfg1":
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            return supplementary(args)
+        return 0
 
     import torch
     torch.cuda.set_device(local)
@@ -297,8 +430,7 @@ def main():
 
     if rank == 0:
         asm32 = pt32["full_ms"] + pt32["aca_ms"] + pt32["truncate_ms"]
-        rkT = T32[(T32[:, 4] == 1) & (T32[:, 5] > 0)]
-        launches = args.steps * (3 + int((rkT[:, 3] > 512).any()))  # gather, z-phase, [z-reduce], y-phase
+        launches = args.steps * h32.gemv_launches(nrhs)  # gather, z-phase classes, [z-reduce], y-phase, final
         line = {
             "metric": METRIC, "value": world * bytes32 / (ms32 * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True,

@@ -122,7 +122,7 @@ EXPORTED = [
     "hmat_b200_create_assembly", "hmat_b200_delete_assembly", "hmat_b200_gemv_device", "hmat_b200_gemv_device_noalloc",
     "hmat_b200_leaf_count",
     "hmat_b200_leaf_table", "hmat_b200_leaf_payload", "hmat_b200_payload_layout", "hmat_b200_leaf_gradients",
-    "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_last_error",
+    "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_gemv_launches", "hmat_b200_last_error",
 ]
 
 
@@ -164,6 +164,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "hmat_b200_leaf_gradients": (C.c_int, [_P, _P, _P, C.c_int, _P, C.c_int, _P]),
         "hmat_b200_phase_times": (C.c_int, [_P, _P]),
         "hmat_b200_gemv_profile": (C.c_int, [_P, C.c_char, _P, _P, C.c_int, _P, _P]),
+        "hmat_b200_gemv_launches": (C.c_int, [_P, C.c_char, C.c_int]),
         "hmat_b200_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():
@@ -365,6 +366,13 @@ class HMatrix:
                                                ms.ctypes.data, by.ctypes.data), "hmat_b200_gemv_profile")
         return {"ms": dict(zip(("gather", "zphase", "yphase"), ms)),
                 "bytes": dict(zip(("gather", "zphase", "yphase"), by))}
+
+    def gemv_launches(self, nrhs: int, trans: str = "N") -> int:
+        """Kernel launches one product with nrhs right-hand sides makes."""
+        n = self.lib.hmat_b200_gemv_launches(self.m, trans.encode(), nrhs)
+        if n < 0:
+            raise HMatError("hmat_b200_gemv_launches failed: " + self.lib.hmat_b200_last_error().decode())
+        return n
 
     def phase_times(self) -> dict:
         out = np.zeros(4, dtype=np.float64)

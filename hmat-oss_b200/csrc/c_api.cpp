@@ -631,6 +631,16 @@ int hmat_b200_gemv_profile(hmat_matrix_t* m, char trans, const void* x_dev, void
   return 0;
 }
 
+int hmat_b200_gemv_launches(hmat_matrix_t* m, char trans, int nrhs) {
+  try {
+    if (!m || nrhs < 1) throw Error("bad argument");
+    return engine_of(m).gemv_launches(trans, nrhs);
+  } catch (const std::exception& e) {
+    fail("hmat_b200_gemv_launches", e.what());
+    return -1;
+  }
+}
+
 int hmat_b200_phase_times(hmat_matrix_t* m, double* out4) {
   if (!m || !out4) return fail("hmat_b200_phase_times", "null argument");
   for (int i = 0; i < 4; ++i) out4[i] = m->engine ? m->engine->times_ms[i] : 0.0;

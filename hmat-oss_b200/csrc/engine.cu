@@ -5,6 +5,7 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <type_traits>
 
 #include "engine.h"
 #include "gemv_plan.h"
@@ -345,6 +346,10 @@ class Engine : public EngineBase {
   }
 
   size_t gemv_scratch_bytes() const override { return 256 + xz_elems() * sizeof(T); }
+  int gemv_launches(char trans, int nrhs) const override {
+    if (!assembled) throw Error("matrix not assembled");
+    return gemv_launch_count(plan_, trans, nrhs, (int)sizeof(T));
+  }
 
   void gemv_device_with_scratch(char trans, const void* alpha, const void* x, const void* beta, void* y, int nrhs,
                                 cudaStream_t stream, void* scratch, size_t scratch_bytes) override {
@@ -734,12 +739,19 @@ class Engine : public EngineBase {
   }
 
   // Warp-level shape of an 'N' launch for tasks of at most omax rows: the column-slice
-  // window up to 32 rows, half-warp row groups up to 64, lanes over rows up to 128.
+  // window (2 rows per lane) up to 32 rows, half-warp row groups up to 64, lanes over rows
+  // up to 128 (4 rows per lane).
   static void warp_shape(GemvLaunch& L, int omax) {
     L.warp_level = true;
     L.ol = 32;
+    if (std::is_same<T, float>::value) {
+      // FP32: tensor-core tiles of 16 rows (map 3, rpt = row tiles held per warp)
+      L.map = 3;
+      L.rpt = omax <= 32 ? 2 : (omax <= 64 ? 4 : 8);
+      return;
+    }
     L.map = omax <= 32 ? 2 : (omax <= 64 ? 1 : 0);
-    L.rpt = omax <= 32 ? 1 : 4;
+    L.rpt = omax <= 32 ? 2 : 4;
   }
 
   void finish_launch(GemvLaunch& L, SideBuf& sb, int slot, std::vector<GemvTask>& tasks,
@@ -756,7 +768,8 @@ class Engine : public EngineBase {
     for (size_t t = 1; t < tasks.size(); ++t)
       if (tasks[t].first_unit != tasks[t - 1].first_unit + tasks[t - 1].nunits)
         throw Error("gemv plan: units of a launch are not contiguous");
-    const int omax = L.warp_level ? (L.map == 2 ? 32 : (L.map == 1 ? 64 : 128)) : ol * rpt;
+    const int omax = L.warp_level ? (L.map == 3 ? 16 * L.rpt : (L.map == 2 ? 32 : (L.map == 1 ? 64 : 128)))
+                                  : ol * rpt;
     for (auto& t : tasks)
       if (t.O > omax) throw Error("gemv plan: task taller than its launch shape");
     if (L.warp_level) {

@@ -45,6 +45,8 @@ class EngineBase {
   // Bytes of scratch one eager product needs (x in cluster order + the z buffer), and that
   // product run eagerly with its scratch carved from `scratch` (no allocation, no graph).
   virtual size_t gemv_scratch_bytes() const = 0;
+  // Kernel launches of one product (gather, z-phase classes, z-reduce, y-phase, final pass).
+  virtual int gemv_launches(char trans, int nrhs) const = 0;
   virtual void gemv_device_with_scratch(char trans, const void* alpha, const void* x, const void* beta, void* y,
                                         int nrhs, cudaStream_t stream, void* scratch, size_t scratch_bytes) = 0;
 

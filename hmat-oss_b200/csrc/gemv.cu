@@ -71,14 +71,6 @@ __device__ inline cfloat shfl_xor(cfloat v, int m) {
 __device__ inline cdouble shfl_xor(cdouble v, int m) {
   return cdouble{__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m)};
 }
-__device__ inline float shfl_idx(float v, int l) { return __shfl_sync(0xffffffffu, v, l); }
-__device__ inline double shfl_idx(double v, int l) { return __shfl_sync(0xffffffffu, v, l); }
-__device__ inline cfloat shfl_idx(cfloat v, int l) {
-  return cfloat{__shfl_sync(0xffffffffu, v.x, l), __shfl_sync(0xffffffffu, v.y, l)};
-}
-__device__ inline cdouble shfl_idx(cdouble v, int l) {
-  return cdouble{__shfl_sync(0xffffffffu, v.x, l), __shfl_sync(0xffffffffu, v.y, l)};
-}
 
 // Loads Q consecutive elements from shared memory (vectorised when aligned).
 template <typename T, int Q>
@@ -307,12 +299,12 @@ struct RowOps<float, R, true> {
   using AV = unsigned long long[N];
   __device__ static void load(const float* p, XV& x) {
     if constexpr (R % 4 == 0) {
-      const uint4* s = reinterpret_cast<const uint4*>(p);
+      const ulonglong2* s = reinterpret_cast<const ulonglong2*>(p);
 #pragma unroll
       for (int c = 0; c < R / 4; ++c) {
-        const uint4 v = s[c];
-        x[2 * c] = ((unsigned long long)v.y << 32) | v.x;
-        x[2 * c + 1] = ((unsigned long long)v.w << 32) | v.z;
+        const ulonglong2 v = s[c];
+        x[2 * c] = v.x;
+        x[2 * c + 1] = v.y;
       }
     } else {
       const unsigned long long* s = reinterpret_cast<const unsigned long long*>(p);
@@ -336,6 +328,25 @@ struct RowOps<float, R, true> {
     return (q & 1) ? hi : lo;
   }
 };
+
+// One unit of a warp task: lane's rows row0 + a * stride (a < NA) of the columns
+// j = js, js + SL, ... < c, all R right-hand sides.
+// O is the column stride of the piece.  With `active` >= 0 only the first `active` row
+// groups are computed (a guarded loop).
+template <typename T, int R, int RS, int NA, int A2>
+__device__ __forceinline__ void rows_loop(const T* P, const T* X, int c, int js, int SL, int O, int row0, int stride,
+                                          typename RowOps<T, R>::AV (&acc)[A2], int active = -1) {
+  using Ops = RowOps<T, R>;
+#pragma unroll 2
+  for (int j = js; j < c; j += SL) {
+    typename Ops::XV xv;
+    Ops::load(X + (size_t)j * RS, xv);
+    const T* pc = P + (size_t)j * O + row0;
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+      if (active < 0 || a < active) Ops::fma(pc[a * stride], xv, acc[a]);
+  }
+}
 
 // Blocks per SM the register budget allows: more accumulator bytes, fewer resident warps.
 template <typename T, int R, int A2>
@@ -397,13 +408,16 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
     const GemvTask task = task_next;
     if (t + 1 < t1) task_next = tasks[t + 1];
     const int O = task.O;
-    int row0, js, SL;
+    int row0, js, SL, Og = O;
+    float inv = 1.f;
     if constexpr (MODE == 2) {
-      // exact for lane < 32 and O <= 32: the quotients are at least 1/64 away from integers
-      const float inv = __frcp_rn((float)O);
+      // window: Og = ceil(O / A2) lanes per column, SL = floor(32 / Og) columns per step;
+      // exact for lane < 32 and Og <= 32 (the quotients are at least 1/64 from integers)
+      Og = (O + A2 - 1) / A2;
+      inv = __frcp_rn((float)Og);
       SL = (int)(32.5f * inv);
       js = (int)(((float)lane + 0.5f) * inv);
-      row0 = lane - js * O;
+      row0 = lane - js * Og;
     } else if constexpr (MODE == 1) {
       SL = 2;
       row0 = lane & 15;
@@ -413,12 +427,15 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
       row0 = lane;
       js = 0;
     }
+    // row groups holding rows of this task (warp-uniform)
+    const int na = MODE == 2 ? A2 : min(A2, (O + OL - 1) / OL);
     typename Ops::AV acc[A2];
 #pragma unroll
     for (int a = 0; a < A2; ++a) Ops::zero_(acc[a]);
 
+    int s = 0;
     for (int kk = 0; kk < task.nunits; ++kk, ++u) {
-      const int s = (u - u_begin) % kWarpStages;
+      s = (u - u_begin) % kWarpStages;
       const uint32_t parity = (uint32_t)(((u - u_begin) / kWarpStages) & 1);
       long long spins = 0;
       while (!mbar_try_wait(&bars[s], parity)) {
@@ -430,52 +447,51 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
       const int c = uslot[s].c;
       const T* P = reinterpret_cast<const T*>(wbase + (size_t)s * kWarpStageBytes);
       const T* X = reinterpret_cast<const T*>(wbase + (size_t)s * kWarpStageBytes + kWarpPieceBytes);
+      // Rows of a lane past O read the next column (or, in the last column, the first
+      // elements of the X rows of the same stage); they are never written.
       if constexpr (MODE == 2) {
-        if (js < SL) {
-#pragma unroll 4
-          for (int j = js; j < c; j += SL) {
-            typename Ops::XV xv;
-            Ops::load(X + (size_t)j * RS, xv);
-            Ops::fma(P[(size_t)j * O + row0], xv, acc[0]);
-          }
-        }
+        if (js < SL) rows_loop<T, R, RS, A2, A2>(P, X, c, js, SL, O, row0, Og, acc);
       } else {
-#pragma unroll 2
-        for (int j = js; j < c; j += SL) {
-          typename Ops::XV xv;
-          Ops::load(X + (size_t)j * RS, xv);
-          const T* pc = P + (size_t)j * O + row0;
-#pragma unroll
-          for (int a = 0; a < A2; ++a)
-            if (a * OL < O) Ops::fma(pc[a * OL], xv, acc[a]);
-        }
+        rows_loop<T, R, RS, A2, A2>(P, X, c, js, SL, O, row0, OL, acc, na);
       }
       __syncwarp();  // every lane is done with stage s
-      if (lane == 0 && u + kWarpStages < u_end) issue_next(u + kWarpStages);
+      // the last unit's stage stays free until the epilogue has used it as scratch
+      if (lane == 0 && kk + 1 < task.nunits && u + kWarpStages < u_end) issue_next(u + kWarpStages);
     }
 
     // ---- epilogue: the task's rows go to xz[out_row + l], zero-padded to RS ----
     T* out = xz + (size_t)task.out_row * RS;
     if constexpr (MODE == 2) {
-      // slices summed in slice order into the lanes of slice 0 (lane = row)
-      T tot[R];
+      // slices summed in slice order through the stage just consumed, QC right-hand sides
+      // per round: lane's partial of (its row a, q) at sc[(lane * A2 + a) * QC + q - q0]
+      constexpr int QC0 = kWarpPieceBytes / (32 * A2 * (int)sizeof(T));
+      constexpr int QC = QC0 < R ? QC0 : R;
+      static_assert(QC >= 1 && (R % QC) == 0, "reduction chunk");
+      T* sc = reinterpret_cast<T*>(wbase + (size_t)s * kWarpStageBytes);
+      if (task.nunits > 0) {
 #pragma unroll
-      for (int q = 0; q < R; ++q) tot[q] = Ops::get(acc[0], q);
-      for (int k = 1; k < SL; ++k) {
-        const int src = (lane + k * O) & 31;
+        for (int qc0 = 0; qc0 < R; qc0 += QC) {
+          if (js < SL)
 #pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const T v = shfl_idx(Ops::get(acc[0], q), src);
-          tot[q] = tot[q] + v;
+            for (int a = 0; a < A2; ++a)
+#pragma unroll
+              for (int qq = 0; qq < QC; ++qq) sc[(lane * A2 + a) * QC + qq] = Ops::get(acc[a], qc0 + qq);
+          __syncwarp();
+          for (int e = lane; e < O * QC; e += 32) {
+            const int row = e / QC, qq = e % QC;
+            const int a = (int)(((float)row + 0.5f) * inv);  // row < 128, Og <= 32: exact
+            const int l = row - a * Og;
+            T v = sc[(l * A2 + a) * QC + qq];
+            for (int k = 1; k < SL; ++k) v = v + sc[((k * Og + l) * A2 + a) * QC + qq];
+            out[(size_t)row * RS + qc0 + qq] = v;
+          }
+          __syncwarp();
         }
+      } else {
+        for (int e = lane; e < O * R; e += 32) out[(size_t)(e / R) * RS + e % R] = zero<T>();
       }
-      if (lane < O) {
-        T* row = out + (size_t)lane * RS;
-#pragma unroll
-        for (int q = 0; q < R; ++q) row[q] = tot[q];
-#pragma unroll
-        for (int q = R; q < RS; ++q) row[q] = zero<T>();
-      }
+      if constexpr (RS > R)
+        for (int e = lane; e < O * (RS - R); e += 32) out[(size_t)(e / (RS - R)) * RS + R + e % (RS - R)] = zero<T>();
     } else {
 #pragma unroll
       for (int a = 0; a < A2; ++a) {
@@ -496,27 +512,196 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
         }
       }
     }
+    if (task.nunits > 0 && lane == 0 && (u - 1) + kWarpStages < u_end) {
+      // the scratch writes (generic proxy) are ordered before the copy that reuses the stage
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue_next(u - 1 + kWarpStages);
+    }
+  }
+}
+
+// Warp-level streamed tasks on the tensor cores (FP32 'N' products).  Same per-warp TMA
+// pipeline as warp_stream_kernel; the product of a unit is a sequence of warp MMAs
+// (mma.sync m16n8k8, TF32 operands, FP32 accumulators) over 16-row tiles of the piece P and
+// 8-column tiles of the right-hand sides.  FP32 accuracy is kept with the three-term split
+// a = a_hi + a_lo (a_hi = a rounded to TF32): P X ~ P_lo X_hi + P_hi X_lo + P_hi X_hi, the
+// P_lo X_lo term (2^-22 relative) dropped.  Operands are read from the stage in fragment
+// order (rows g, g + 8 and columns t, t + 4 of each tile, g = lane / 4, t = lane % 4);
+// rows at or past O are computed and never written, columns past the piece are zeros.
+__device__ __forceinline__ void tf32_split(float v, uint32_t& hi, uint32_t& lo) {
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(v));
+  lo = __float_as_uint(v - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <int R, int RS, int MT>
+__global__ void __launch_bounds__(kWarpCTA * 32, 4)
+    mma_stream_kernel(const GemvTask* __restrict__ tasks, const int* __restrict__ warp_begin,
+                      const GemvUnit* __restrict__ units, const float* __restrict__ arena, float* xz, int* err) {
+  constexpr int NT = (R + 7) / 8;  // 8-column tiles of the right-hand sides
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, tg = lane & 3;
+  unsigned char* wbase = smem_raw + (size_t)warp * kWarpStages * kWarpStageBytes;
+  GemvUnit* uslot =
+      reinterpret_cast<GemvUnit*>(smem_raw + (size_t)kWarpCTA * kWarpStages * kWarpStageBytes) + warp * kWarpStages;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWarpCTA * kWarpStages *
+                                                               (kWarpStageBytes + sizeof(GemvUnit))) +
+                   warp * kWarpStages;
+  const int gw = blockIdx.x * kWarpCTA + warp;
+  const int t0 = warp_begin[gw], t1 = warp_begin[gw + 1];
+  if (t0 >= t1) return;
+  const int u_begin = tasks[t0].first_unit;
+  const int u_end = tasks[t1 - 1].first_unit + tasks[t1 - 1].nunits;
+
+  if (lane == 0) {
+    for (int s = 0; s < kWarpStages; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  GemvUnit nxt;
+  auto issue = [&](int u, const GemvUnit& U) {
+    const int s = (u - u_begin) % kWarpStages;
+    uslot[s] = U;
+    const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(float));
+    const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(float);
+    unsigned char* st = wbase + (size_t)s * kWarpStageBytes;
+    mbar_expect_tx(&bars[s], pbytes + xbytes);
+    bulk_g2s(st, arena + U.poff, pbytes, &bars[s]);
+    bulk_g2s(st + kWarpPieceBytes, xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
+  };
+  auto issue_next = [&](int v) {
+    issue(v, nxt);
+    if (v + 1 < u_end) nxt = units[v + 1];
+  };
+  if (lane == 0) {
+    int v = u_begin;
+    for (; v < u_end && v < u_begin + kWarpStages; ++v) issue(v, units[v]);
+    if (v < u_end) nxt = units[v];
+  }
+
+  int u = u_begin;
+  GemvTask task_next = tasks[t0];
+  for (int t = t0; t < t1; ++t) {
+    const GemvTask task = task_next;
+    if (t + 1 < t1) task_next = tasks[t + 1];
+    const int O = task.O;
+    const int mtn = (O + 15) >> 4;  // row tiles holding rows of this task (warp-uniform)
+    float acc[MT][NT][4];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[mt][nt][e] = 0.f;
+
+    for (int kk = 0; kk < task.nunits; ++kk, ++u) {
+      const int s = (u - u_begin) % kWarpStages;
+      const uint32_t parity = (uint32_t)(((u - u_begin) / kWarpStages) & 1);
+      long long spins = 0;
+      while (!mbar_try_wait(&bars[s], parity)) {
+        if (++spins > kWaitLimit) {
+          if (lane == 0) atomicExch(err, 1);
+          return;
+        }
+      }
+      const int c = uslot[s].c;
+      const float* P = reinterpret_cast<const float*>(wbase + (size_t)s * kWarpStageBytes);
+      const float* X = reinterpret_cast<const float*>(wbase + (size_t)s * kWarpStageBytes + kWarpPieceBytes);
+      for (int k0 = 0; k0 < c; k0 += 8) {
+        const int ka = k0 + tg, kb = k0 + tg + 4;
+        const bool va = ka < c, vb = kb < c;
+        uint32_t bh[NT][2], bl[NT][2];
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+          const int n = nt * 8 + g;
+          const bool vn = n < R;
+          tf32_split((va && vn) ? X[ka * RS + n] : 0.f, bh[nt][0], bl[nt][0]);
+          tf32_split((vb && vn) ? X[kb * RS + n] : 0.f, bh[nt][1], bl[nt][1]);
+        }
+        const float* pa = P + ka * O + g;
+        const float* pb = P + kb * O + g;
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+          if (mt < mtn) {
+            uint32_t ah[4], al[4];
+            tf32_split(va ? pa[mt * 16] : 0.f, ah[0], al[0]);
+            tf32_split(va ? pa[mt * 16 + 8] : 0.f, ah[1], al[1]);
+            tf32_split(vb ? pb[mt * 16] : 0.f, ah[2], al[2]);
+            tf32_split(vb ? pb[mt * 16 + 8] : 0.f, ah[3], al[3]);
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) {
+              // the tensor core's FP32 sums are not rounded to nearest: each 8-column step
+              // goes to a fresh fragment, added to the running sum with FP32 adds
+              float d[4] = {0.f, 0.f, 0.f, 0.f};
+              mma_tf32(d, al, bh[nt][0], bh[nt][1]);
+              mma_tf32(d, ah, bl[nt][0], bl[nt][1]);
+              mma_tf32(d, ah, bh[nt][0], bh[nt][1]);
+#pragma unroll
+              for (int e = 0; e < 4; ++e) acc[mt][nt][e] += d[e];
+            }
+          }
+        }
+      }
+      __syncwarp();  // every lane is done with stage s
+      if (lane == 0 && u + kWarpStages < u_end) issue_next(u + kWarpStages);
+    }
+
+    // ---- epilogue: rows mt * 16 + g (+ 8), columns nt * 8 + 2 t (+ 1); columns past R
+    // hold exact zeros (their X columns were zeros), which pads the row to RS ----
+    float* out = xz + (size_t)task.out_row * RS;
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+      if (mt < mtn) {
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+          const int n = nt * 8 + 2 * tg;
+          const int m0 = mt * 16 + g, m1 = m0 + 8;
+          if (n < RS) {
+            if (m0 < O) *reinterpret_cast<float2*>(out + (size_t)m0 * RS + n) = make_float2(acc[mt][nt][0], acc[mt][nt][1]);
+            if (m1 < O) *reinterpret_cast<float2*>(out + (size_t)m1 * RS + n) = make_float2(acc[mt][nt][2], acc[mt][nt][3]);
+          }
+        }
+      }
+    }
   }
 }
 
 // y in client order from the partial rows of the 'N' y tasks:
-// y[i, q0 + q] = alpha * sum_p xz[pos + p * O, q] + beta * y[i, q0 + q], rows i of the client
-// order (consecutive threads write consecutive rows of one column of y).
+// y[i, q0 + q] = alpha * sum_p xz[pos + p * O, q] + beta * y[i, q0 + q].  A CTA takes 32
+// client rows: the partial rows are read along q (contiguous), transposed through shared
+// memory, and y is written along i (contiguous in each column of y).
+constexpr int kFinalRows = 32;
 template <typename T, int R, int RS>
-__global__ void yfinal_kernel(const int2* __restrict__ rows, int n, const T* __restrict__ xz, T* __restrict__ y,
-                              int ldy, int q0, int r, T alpha, T beta) {
-  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (long long)n * R) return;
-  const int i = (int)(e % n), q = (int)(e / n);
-  if (q0 + q >= r) return;
-  const int2 d = rows[i];
-  const int O = d.y & 255, np = d.y >> 8;
-  T v = zero<T>();
-  for (int p = 0; p < np; ++p) v = v + xz[((size_t)d.x + (size_t)p * O) * RS + q];
-  T* yp = y + (size_t)i + (size_t)(q0 + q) * ldy;
-  T outv = alpha * v;
-  if (!is_zero_val(beta)) outv = fmadd(beta, *yp, outv);
-  *yp = outv;
+__global__ void __launch_bounds__(256) yfinal_kernel(const int2* __restrict__ rows, int n, const T* __restrict__ xz,
+                                                     T* __restrict__ y, int ldy, int q0, int r, T alpha, T beta) {
+  __shared__ T tile[R][kFinalRows + 1];
+  const int i0 = blockIdx.x * kFinalRows;
+  for (int e = threadIdx.x; e < kFinalRows * R; e += blockDim.x) {
+    const int il = e / R, q = e % R, i = i0 + il;
+    T v = zero<T>();
+    if (i < n) {
+      const int2 d = rows[i];
+      const int O = d.y & 255, np = d.y >> 8;
+      for (int p = 0; p < np; ++p) v = v + xz[((size_t)d.x + (size_t)p * O) * RS + q];
+    }
+    tile[q][il] = v;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < kFinalRows * R; e += blockDim.x) {
+    const int q = e / kFinalRows, il = e % kFinalRows, i = i0 + il;
+    if (i < n && q0 + q < r) {
+      T* yp = y + (size_t)i + (size_t)(q0 + q) * ldy;
+      T outv = alpha * tile[q][il];
+      if (!is_zero_val(beta)) outv = fmadd(beta, *yp, outv);
+      *yp = outv;
+    }
+  }
 }
 
 // Sums the chunk partials of long leaves: xz[final + l] = sum_p xz[part + p k + l].
@@ -558,13 +743,37 @@ void launch_warp_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T
   kern<<<L.ncta, kWarpCTA * 32, smem, s>>>(L.tasks, L.cta_begin, units, arena, xz, err);
 }
 
+template <int R, int RS, int MT>
+void launch_mma_t(const GemvLaunch& L, const GemvUnit* units, const float* arena, float* xz, int* err,
+                  cudaStream_t s) {
+  auto kern = mma_stream_kernel<R, RS, MT>;
+  const size_t smem = warp_stream_smem_bytes((int)sizeof(float));
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  kern<<<L.ncta, kWarpCTA * 32, smem, s>>>(L.tasks, L.cta_begin, units, arena, xz, err);
+}
+
 template <typename T, int R, int RS, bool TRANSP>
 void launch_stream(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, int conj, const int* perm_out,
                    T* y, int ldy, int q0, int r, T alpha, T beta, int* err, cudaStream_t s) {
   if (L.ntasks <= 0) return;
   if (L.warp_level) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (L.map == 3) {
+        if (L.rpt <= 2)
+          launch_mma_t<R, RS, 2>(L, units, arena, xz, err, s);
+        else if (L.rpt <= 4)
+          launch_mma_t<R, RS, 4>(L, units, arena, xz, err, s);
+        else
+          launch_mma_t<R, RS, 8>(L, units, arena, xz, err, s);
+        return;
+      }
+    }
     if (L.map == 2)
-      launch_warp_t<T, R, RS, 2, 1>(L, units, arena, xz, err, s);
+      launch_warp_t<T, R, RS, 2, 2>(L, units, arena, xz, err, s);
     else if (L.map == 1)
       launch_warp_t<T, R, RS, 1, 4>(L, units, arena, xz, err, s);
     else
@@ -603,9 +812,8 @@ void run_tile(const GemvPlan& p, int nrhs, int q0, T alpha, T beta, const T* x, 
   launch_stream<T, R, RS, TRANSP>(side.y, side.units, arena, xz, conj, perm_out, y, ld_out, q0, nrhs, alpha, beta,
                                   err, s);
   if (side.y.warp_level) {
-    const long long ty = (long long)side.nyrows * R;
-    yfinal_kernel<T, R, RS><<<(unsigned)((ty + 255) / 256), 256, 0, s>>>(side.yrows, side.nyrows, xz, y, ld_out, q0,
-                                                                         nrhs, alpha, beta);
+    const unsigned nb = (unsigned)((side.nyrows + kFinalRows - 1) / kFinalRows);
+    yfinal_kernel<T, R, RS><<<nb, 256, 0, s>>>(side.yrows, side.nyrows, xz, y, ld_out, q0, nrhs, alpha, beta);
   }
   if (tm) cudaEventRecord(tm->ev[3], s);
 }
@@ -717,6 +925,17 @@ size_t warp_stream_smem_bytes(int elem_bytes) {
   return (size_t)kWarpCTA * kWarpStages * (kWarpStageBytes + sizeof(GemvUnit) + sizeof(uint64_t));
 }
 int warp_stream_warps_per_cta() { return kWarpCTA; }
+
+int gemv_launch_count(const GemvPlan& p, char trans, int nrhs, int elem_bytes) {
+  const GemvSide& side = p.side[(trans == 'N' || trans == 'n') ? 0 : 1];
+  int per_tile = 1;  // gather
+  for (int c = 0; c < side.nz; ++c) per_tile += side.z[c].ntasks > 0;
+  per_tile += side.nzred > 0;
+  per_tile += side.y.ntasks > 0;
+  per_tile += side.y.warp_level;  // final pass
+  const int maxR = elem_bytes >= 16 ? 4 : 16;
+  return per_tile * ((nrhs + maxR - 1) / maxR);
+}
 
 template <typename T>
 void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* rz, T* gfull, T* grk,

@@ -46,8 +46,9 @@ struct GemvLaunch {
   bool transposed = false;
   bool out_is_y = false;
   // Warp-level launches ('N' products): each warp owns whole tasks and pipelines its own
-  // units.  map 2: column-slice window over tasks of at most 32 rows; map 1: half-warp row
-  // groups (at most 64 rows); map 0: lanes over rows (at most 128 rows).
+  // units.  map 3 (FP32): tensor-core tiles, at most 16 * rpt rows; map 2: column-slice
+  // window over tasks of at most 32 rows (rpt rows per lane); map 1: half-warp row groups
+  // (at most 64 rows); map 0: lanes over rows (at most 128).
   bool warp_level = false;
   int map = 0;
 };

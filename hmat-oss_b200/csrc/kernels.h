@@ -86,6 +86,8 @@ void launch_gemv(const GemvPlan& p, char trans, int nrhs, T alpha, T beta, const
                  int* err, cudaStream_t s, const GemvTiming* timing = nullptr);
 // Row stride (scalars) of the xz buffer for R right-hand sides.
 int gemv_rhs_stride(int elem_bytes, int R);
+// Kernel launches of one product with nrhs right-hand sides.
+int gemv_launch_count(const GemvPlan& p, char trans, int nrhs, int elem_bytes);
 // Dynamic shared memory of one streamed-task CTA, and of one warp-level CTA (and its warps).
 size_t stream_smem_bytes(int elem_bytes, int R, int RS, int omax, bool transposed);
 size_t warp_stream_smem_bytes(int elem_bytes);

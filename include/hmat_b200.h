@@ -426,6 +426,11 @@ int hmat_b200_leaf_gradients(hmat_matrix_t* hmatrix, const void* x_dev, const vo
 int hmat_b200_gemv_profile(hmat_matrix_t* hmatrix, char trans, const void* x_dev, void* y_dev, int nrhs, double* ms3,
                            double* bytes3);
 
+/* Number of kernel launches one product with nrhs right-hand sides makes (gather, the
+ * z-phase launches, z-reduce, y-phase, final pass; per tile of right-hand sides), or -1
+ * (with hmat_b200_last_error set) on error.  No counterpart in the reference. */
+int hmat_b200_gemv_launches(hmat_matrix_t* hmatrix, char trans, int nrhs);
+
 /* Device time of the last phases on this matrix, milliseconds: [0] full assembly,
  * [1] ACA, [2] truncation (+ compaction), [3] last gemv. */
 int hmat_b200_phase_times(hmat_matrix_t* hmatrix, double* out4);
