@@ -524,19 +524,68 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
 // pipeline as warp_stream_kernel; the product of a unit is a sequence of warp MMAs
 // (mma.sync m16n8k8, TF32 operands, FP32 accumulators) over 16-row tiles of the piece P and
 // 8-column tiles of the right-hand sides.  FP32 accuracy is kept with the three-term split
-// a = a_hi + a_lo (a_hi = a rounded to TF32): P X ~ P_lo X_hi + P_hi X_lo + P_hi X_hi, the
-// P_lo X_lo term (2^-22 relative) dropped.  Operands are read from the stage in fragment
+// a = a_hi + a_lo (a_hi = a truncated to TF32): P X ~ P_lo X_hi + P_hi X_lo + P_hi X_hi, the
+// P_lo X_lo term (2^-20 relative at most) dropped.  Operands are read from the stage in fragment
 // order (rows g, g + 8 and columns t, t + 4 of each tile, g = lane / 4, t = lane % 4);
 // rows at or past O are computed and never written, columns past the piece are zeros.
+// a_hi = a with its low 13 mantissa bits cleared (a TF32 value), a_lo = a - a_hi (exact in
+// FP32; the MMA reads its leading 11 bits).
 __device__ __forceinline__ void tf32_split(float v, uint32_t& hi, uint32_t& lo) {
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(v));
+  hi = __float_as_uint(v) & 0xffffe000u;
   lo = __float_as_uint(v - __uint_as_float(hi));
 }
+// Not volatile: independent tiles' MMA chains may be interleaved by the scheduler.
 __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
+  asm(
       "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// One 8-column step k0 of a unit: B fragments from the X rows, then every row tile.  TAIL
+// masks the columns at or past c.
+template <int R, int RS, int MT, int NT, bool TAIL>
+__device__ __forceinline__ void mma_kstep(const float* P, const float* X, int k0, int c, int O, int g, int tg,
+                                          int mtn, float (&acc)[MT][NT][4]) {
+  const int ka = k0 + tg, kb = k0 + tg + 4;
+  const bool va = !TAIL || ka < c, vb = !TAIL || kb < c;
+  uint32_t bh[NT][2], bl[NT][2];
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    const int n = nt * 8 + g;
+    const bool vn = (R % 8 == 0) || n < R;
+    tf32_split((va && vn) ? X[ka * RS + n] : 0.f, bh[nt][0], bl[nt][0]);
+    tf32_split((vb && vn) ? X[kb * RS + n] : 0.f, bh[nt][1], bl[nt][1]);
+  }
+  const float* pa = P + ka * O + g;
+  const float* pb = P + kb * O + g;
+#pragma unroll
+  for (int mt = 0; mt < MT; ++mt) {
+    if (mt < mtn) {
+      uint32_t ah[4], al[4];
+      tf32_split(va ? pa[mt * 16] : 0.f, ah[0], al[0]);
+      tf32_split(va ? pa[mt * 16 + 8] : 0.f, ah[1], al[1]);
+      tf32_split(vb ? pb[mt * 16] : 0.f, ah[2], al[2]);
+      tf32_split(vb ? pb[mt * 16 + 8] : 0.f, ah[3], al[3]);
+      // the tensor core's FP32 sums are not rounded to nearest: each 8-column step goes to
+      // fresh fragments, added to the running sums with FP32 adds
+      float d[NT][4];
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) d[nt][e] = 0.f;
+        mma_tf32(d[nt], al, bh[nt][0], bh[nt][1]);
+      }
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) mma_tf32(d[nt], ah, bl[nt][0], bl[nt][1]);
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) mma_tf32(d[nt], ah, bh[nt][0], bh[nt][1]);
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[mt][nt][e] += d[nt][e];
+    }
+  }
 }
 
 template <int R, int RS, int MT>
@@ -613,41 +662,9 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 4)
       const int c = uslot[s].c;
       const float* P = reinterpret_cast<const float*>(wbase + (size_t)s * kWarpStageBytes);
       const float* X = reinterpret_cast<const float*>(wbase + (size_t)s * kWarpStageBytes + kWarpPieceBytes);
-      for (int k0 = 0; k0 < c; k0 += 8) {
-        const int ka = k0 + tg, kb = k0 + tg + 4;
-        const bool va = ka < c, vb = kb < c;
-        uint32_t bh[NT][2], bl[NT][2];
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt) {
-          const int n = nt * 8 + g;
-          const bool vn = n < R;
-          tf32_split((va && vn) ? X[ka * RS + n] : 0.f, bh[nt][0], bl[nt][0]);
-          tf32_split((vb && vn) ? X[kb * RS + n] : 0.f, bh[nt][1], bl[nt][1]);
-        }
-        const float* pa = P + ka * O + g;
-        const float* pb = P + kb * O + g;
-#pragma unroll
-        for (int mt = 0; mt < MT; ++mt) {
-          if (mt < mtn) {
-            uint32_t ah[4], al[4];
-            tf32_split(va ? pa[mt * 16] : 0.f, ah[0], al[0]);
-            tf32_split(va ? pa[mt * 16 + 8] : 0.f, ah[1], al[1]);
-            tf32_split(vb ? pb[mt * 16] : 0.f, ah[2], al[2]);
-            tf32_split(vb ? pb[mt * 16 + 8] : 0.f, ah[3], al[3]);
-#pragma unroll
-            for (int nt = 0; nt < NT; ++nt) {
-              // the tensor core's FP32 sums are not rounded to nearest: each 8-column step
-              // goes to a fresh fragment, added to the running sum with FP32 adds
-              float d[4] = {0.f, 0.f, 0.f, 0.f};
-              mma_tf32(d, al, bh[nt][0], bh[nt][1]);
-              mma_tf32(d, ah, bl[nt][0], bl[nt][1]);
-              mma_tf32(d, ah, bh[nt][0], bh[nt][1]);
-#pragma unroll
-              for (int e = 0; e < 4; ++e) acc[mt][nt][e] += d[e];
-            }
-          }
-        }
-      }
+      int k0 = 0;
+      for (; k0 + 8 <= c; k0 += 8) mma_kstep<R, RS, MT, NT, false>(P, X, k0, c, O, g, tg, mtn, acc);
+      if (k0 < c) mma_kstep<R, RS, MT, NT, true>(P, X, k0, c, O, g, tg, mtn, acc);
       __syncwarp();  // every lane is done with stage s
       if (lane == 0 && u + kWarpStages < u_end) issue_next(u + kWarpStages);
     }
