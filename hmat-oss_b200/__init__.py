@@ -367,6 +367,16 @@ class HMatrix:
         return {"ms": dict(zip(("gather", "zphase", "yphase"), ms)),
                 "bytes": dict(zip(("gather", "zphase", "yphase"), by))}
 
+    def set_low_rank_epsilon(self, eps: float) -> None:
+        self.hi.fn("set_low_rank_epsilon")(self.m, eps)
+
+    def truncate(self, eps: float | None = None) -> None:
+        """Re-truncates every Rk leaf at the low-rank epsilon (set first when `eps` is given),
+        through the C table's truncate."""
+        if eps is not None:
+            self.set_low_rank_epsilon(eps)
+        _check(self.hi.fn("truncate")(self.m), "truncate")
+
     def gemv_launches(self, nrhs: int, trans: str = "N") -> int:
         """Kernel launches one product with nrhs right-hand sides makes."""
         n = self.lib.hmat_b200_gemv_launches(self.m, trans.encode(), nrhs)

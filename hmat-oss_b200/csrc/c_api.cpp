@@ -276,7 +276,17 @@ int u_solve_systems(hmat_matrix_t*, void*, int) { return unsupported("solve_syst
 int u_solve_dense(hmat_matrix_t*, void*, int) { return unsupported("solve_dense"); }
 int u_transpose(hmat_matrix_t*) { return unsupported("transpose"); }
 int u_scale(void*, hmat_matrix_t*) { return unsupported("scale"); }
-int u_truncate(hmat_matrix_t*) { return unsupported("truncate"); }
+// HMatInterface::truncate (hmat_cpp_interface.cpp:225-229 -> HMatrix::truncate,
+// h_matrix.cpp:2107-2123): every Rk leaf re-truncated at the matrix's low-rank epsilon.
+int c_truncate(hmat_matrix_t* m) {
+  HB_TRY("truncate", {
+    if (!m) throw Error("null argument");
+    EngineBase* e = m->engine.get();
+    if (!e || !e->assembled) throw Error("truncate needs an assembled matrix");
+    e->retruncate(m->low_rank_eps);
+  });
+  return 0;
+}
 int u_gemm(char, char, const void*, hmat_matrix_t*, hmat_matrix_t*, const void*, hmat_matrix_t*) {
   return unsupported("gemm");
 }
@@ -344,7 +354,7 @@ void fill_table(hmat_interface_t* i) {
   i->solve_dense = u_solve_dense;
   i->transpose = u_transpose;
   i->scale = u_scale;
-  i->truncate = u_truncate;
+  i->truncate = c_truncate;
   i->vector_reorder = vector_reorder_t<T>;
   i->vector_restore = vector_restore_t<T>;
   i->gemm = u_gemm;

@@ -159,6 +159,7 @@ class Engine : public EngineBase {
       fd.push_back(d);
     }
     const long long full_total = pad32(pos);
+    full_total_ = full_total;
 
     // ---- admissible leaves: ACA / SVD, truncation, compaction into pieces ----
     assemble_rk(method, eps_aca, eps_trunc, svd_below);
@@ -302,9 +303,72 @@ class Engine : public EngineBase {
     HB_CUDA(cudaGetLastError());
   }
 
+  // HMatrix::truncate (h_matrix.cpp:2107-2123): every Rk leaf re-truncated at eps with the
+  // assembly's truncation kernels, then the arena and the gemv schedule rebuilt.
   void retruncate(double eps) override {
-    (void)eps;
-    throw Error("re-truncation of an assembled matrix is not available yet");
+    if (!assembled) throw Error("matrix not assembled");
+    const auto& L = bt_->leaves;
+    const int nleaves = (int)L.size();
+    double saved[4];
+    for (int i = 0; i < 4; ++i) saved[i] = times_ms[i];
+    std::vector<RkJob> queue;
+    for (int i = 0; i < nleaves; ++i)
+      if (L[i].type == 1 && ranks[i] > 0) {
+        RkJob j;
+        j.leaf = i;
+        j.kcap = ranks[i];
+        j.svd = false;
+        queue.push_back(j);
+      }
+    piece_of_.assign(nleaves, -1);
+    pieces_.clear();
+    const size_t budget = workspace_budget();
+    size_t pos = 0;
+    while (pos < queue.size()) {
+      std::vector<RkJob> batch, retry;
+      size_t bytes = 0;
+      while (pos < queue.size()) {
+        const LeafInfo& l = L[queue[pos].leaf];
+        size_t b = (size_t)pad32(rk_slot_elems(l.m, l.n, queue[pos].kcap)) * sizeof(T) + l.m + l.n;
+        if (!batch.empty() && bytes + b > budget) break;
+        bytes += b;
+        batch.push_back(queue[pos++]);
+      }
+      run_batch(batch, eps, eps, retry, arena_.p);
+      if (!retry.empty()) throw Error("re-truncation: unexpected capacity retry");
+    }
+    // new arena: the full leaves unchanged, then the re-truncated pieces
+    long long rk_total = 0;
+    for (auto& pc : pieces_) rk_total += pad32(pc.elems);
+    DevArray<T> na;
+    na.alloc((size_t)(full_total_ + rk_total + 256));
+    if (full_total_) HB_CUDA(cudaMemcpyAsync(na.p, arena_.p, full_total_ * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
+    long long base = full_total_;
+    std::vector<long long> piece_base(pieces_.size());
+    for (size_t p = 0; p < pieces_.size(); ++p) {
+      piece_base[p] = base;
+      if (pieces_[p].elems)
+        HB_CUDA(cudaMemcpyAsync(na.p + base, pieces_[p].arena.p, pieces_[p].elems * sizeof(T),
+                                cudaMemcpyDeviceToDevice, stream_));
+      base += pad32(pieces_[p].elems);
+    }
+    for (int i = 0; i < nleaves; ++i)
+      if (L[i].type == 1) leaf_off_[i] = piece_of_[i] >= 0 ? leaf_off_[i] + piece_base[piece_of_[i]] : -1;
+    HB_CUDA(cudaStreamSynchronize(stream_));
+    arena_.release();
+    arena_.p = na.p;
+    arena_.n = na.n;
+    na.p = nullptr;
+    na.n = 0;
+    arena_elems_ = full_total_ + rk_total;
+    pieces_.clear();
+    if (gexec_) {
+      cudaGraphExecDestroy(gexec_);
+      gexec_ = nullptr;
+    }
+    build_plan();
+    HB_CUDA(cudaStreamSynchronize(stream_));
+    for (int i = 0; i < 4; ++i) times_ms[i] = saved[i];
   }
 
   void profile_gemv(char trans, const void* x, void* y, int nrhs, double* ms3, double* bytes3) override {
@@ -434,7 +498,10 @@ class Engine : public EngineBase {
   // Runs ACA (or the dense-SVD fill) and the truncation on one batch of admissible
   // leaves; leaves that ran out of rank capacity are returned in `retry`, the others are
   // compacted (A as row panels, B transposed) into a new piece.
-  void run_batch(const std::vector<RkJob>& jobs, double eps_aca, double eps_trunc, std::vector<RkJob>& retry) {
+  // With `src` set, the leaves are already assembled: their factors are unpacked from the
+  // arena `src` (rank = kcap) instead of being computed, then truncated at eps_trunc.
+  void run_batch(const std::vector<RkJob>& jobs, double eps_aca, double eps_trunc, std::vector<RkJob>& retry,
+                 const T* src = nullptr) {
     const auto& L = bt_->leaves;
     const int nb = (int)jobs.size();
     std::vector<RkLeafDesc> desc(nb);
@@ -477,6 +544,36 @@ class Engine : public EngineBase {
     d_svd_order.upload(svd_order, stream_);
     HB_CUDA(cudaStreamSynchronize(stream_));
 
+    if (src) {
+      // rank = kcap: the stored factors, unpacked from their panels
+      std::vector<int> k0(nb);
+      std::vector<RkStoreDesc> ostore(nb);
+      std::vector<PanelDesc> opanels;
+      for (int b = 0; b < nb; ++b) {
+        const int leaf = jobs[b].leaf;
+        const LeafInfo& l = L[leaf];
+        k0[b] = jobs[b].kcap;
+        ostore[b] = RkStoreDesc{(int)opanels.size(), 0, 0};
+        long long p = leaf_off_[leaf];
+        auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
+        for (int q = br.first; q < br.second; ++q) {
+          opanels.push_back(PanelDesc{rblocks_[q].off - l.row_off, rblocks_[q].len, p});
+          p += padded((long long)rblocks_[q].len * k0[b]);
+          ostore[b].npanel++;
+        }
+        ostore[b].bt_off = p;
+      }
+      aca_order.clear();
+      svd_order.clear();
+      d_ranks.upload(k0, stream_);
+      DevArray<RkStoreDesc> d_ostore;
+      DevArray<PanelDesc> d_opanels;
+      d_ostore.upload(ostore, stream_);
+      d_opanels.upload(opanels, stream_);
+      launch_unpack<T>(d_desc.p, nb, d_ranks.p, d_ostore.p, d_opanels.p, src, d_ws.p, stream_);
+      HB_CUDA(cudaGetLastError());
+      HB_CUDA(cudaStreamSynchronize(stream_));
+    }
     HB_CUDA(cudaEventRecord(ev_[2], stream_));
     if (!aca_order.empty()) {
       HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
@@ -519,19 +616,39 @@ class Engine : public EngineBase {
 
     typedef typename Traits<T>::wide W;
     DevArray<W> d_scratch;
-    DevArray<int> d_good, d_svd_good;
+    DevArray<int> d_good, d_svd_good, d_small;
+    int wgrid = 0;
     long long slab = 0, grid = 0;
-    std::vector<int> svd_good;
+    std::vector<int> svd_good, small, large;
     if (!good.empty()) {
-      slab = truncate_slab_elems<T>(max_m, max_n, max_k);
-      const size_t budget = workspace_budget();
-      grid = std::min<long long>((long long)good.size(), persistent_grid(2));
-      grid = std::max(1LL, std::min<long long>(grid, (long long)(budget / (slab * sizeof(W)))));
-      d_scratch.alloc((size_t)(grid * slab));
+      // small leaves go to the warp-per-leaf kernel, the rest to the CTA-per-leaf kernel
+      int big_m = 1, big_n = 1, big_k = 1;
+      for (int b : good) {
+        if (truncate_warp_eligible<T>(desc[b].m, desc[b].n, h_ranks[b])) {
+          small.push_back(b);
+        } else {
+          large.push_back(b);
+          big_m = std::max(big_m, desc[b].m);
+          big_n = std::max(big_n, desc[b].n);
+          big_k = std::max(big_k, h_ranks[b]);
+        }
+      }
       for (int b : good)
         if (jobs[b].svd) svd_good.push_back(b);
+      if (!svd_good.empty()) {
+        big_m = max_m;
+        big_n = max_n;
+        big_k = max_k;
+      }
+      slab = truncate_slab_elems<T>(big_m, big_n, big_k);
+      const size_t budget = workspace_budget();
+      grid = std::min<long long>((long long)std::max(large.size(), svd_good.size()), persistent_grid(2));
+      grid = std::max(1LL, std::min<long long>(grid, (long long)(budget / (slab * sizeof(W)))));
+      if (!large.empty() || !svd_good.empty()) d_scratch.alloc((size_t)(grid * slab));
+      if (!small.empty()) wgrid = truncate_warp_grid<T>((int)small.size());
       d_svd_good.upload(svd_good, stream_);
-      d_good.upload(good, stream_);
+      d_good.upload(large, stream_);
+      d_small.upload(small, stream_);
       HB_CUDA(cudaStreamSynchronize(stream_));
     }
     HB_CUDA(cudaEventRecord(ev_[4], stream_));
@@ -543,10 +660,18 @@ class Engine : public EngineBase {
                            d_counter.p, d_scratch.p, slab, (int)grid, stream_);
         HB_CUDA(cudaGetLastError());
       }
-      HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
-      launch_truncate<T>(d_desc.p, d_good.p, (int)good.size(), eps_trunc, d_ws.p, d_ranks.p, d_status.p,
-                         d_counter.p, d_scratch.p, slab, (int)grid, stream_);
-      HB_CUDA(cudaGetLastError());
+      if (!large.empty()) {
+        HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
+        launch_truncate<T>(d_desc.p, d_good.p, (int)large.size(), eps_trunc, d_ws.p, d_ranks.p, d_status.p,
+                           d_counter.p, d_scratch.p, slab, (int)grid, stream_);
+        HB_CUDA(cudaGetLastError());
+      }
+      if (!small.empty()) {
+        HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
+        launch_truncate_warp<T>(d_desc.p, d_small.p, (int)small.size(), eps_trunc, d_ws.p, d_ranks.p, d_status.p,
+                                d_counter.p, wgrid, stream_);
+        HB_CUDA(cudaGetLastError());
+      }
     }
     HB_CUDA(cudaEventRecord(ev_[5], stream_));
     HB_CUDA(cudaMemcpyAsync(h_ranks.data(), d_ranks.p, nb * sizeof(int), cudaMemcpyDeviceToHost, stream_));
@@ -1011,6 +1136,7 @@ class Engine : public EngineBase {
   std::vector<Piece> pieces_;
   DevArray<T> arena_;
   long long arena_elems_ = 0;
+  long long full_total_ = 0;  // elements of the full-leaf region at the start of the arena
   DevArray<GemvFullLeaf> g_full_;
   DevArray<GemvRkLeaf> g_rk_;
   SideBuf side_buf_[2];

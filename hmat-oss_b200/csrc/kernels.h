@@ -70,6 +70,19 @@ long long truncate_slab_elems(int max_m, int max_n, int max_k);
 
 // Copies the truncated factors of each leaf from its workspace slot into the arena:
 // A as row panels, B transposed.
+// Arena panels of assembled Rk leaves back into workspace slots (inverse of launch_compact).
+template <typename T>
+void launch_unpack(const RkLeafDesc* d_leaves, int nleaves, const int* ranks, const RkStoreDesc* store,
+                   const PanelDesc* panels, const T* arena, T* ws, cudaStream_t s);
+
+// Warp-per-leaf truncation of small leaves (see truncate.cu) and its eligibility rule.
+template <typename T>
+bool truncate_warp_eligible(int m, int n, int k);
+template <typename T>
+int truncate_warp_grid(int nleaves);
+template <typename T>
+void launch_truncate_warp(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, double epsilon, T* ws,
+                          int* ranks, int* status, int* counter, int grid, cudaStream_t s);
 template <typename T>
 void launch_compact(const RkLeafDesc* d_leaves, int nleaves, const T* ws, const int* ranks,
                     const RkStoreDesc* store, const PanelDesc* panels, T* arena, cudaStream_t s);

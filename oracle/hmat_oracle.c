@@ -394,6 +394,14 @@ int oracle_assemble(oracle_hmat* h, const oracle_kernel* k, double epsilon, int 
   return oracle_assemble2(h, k, epsilon, is_complex, 0);
 }
 
+int oracle_retruncate(oracle_hmat* h, double epsilon) {
+  for (int i = 0; i < h->nleaves; ++i) {
+    if (h->is_complex) retruncate_leaf_c(&h->leaves[i], epsilon);
+    else retruncate_leaf_r(&h->leaves[i], epsilon);
+  }
+  return 0;
+}
+
 long long oracle_leaf_payload_size(const oracle_hmat* h, int i) {
   const oracle_leaf* L = &h->leaves[i];
   if (!L->data) return 0;

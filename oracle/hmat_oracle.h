@@ -66,6 +66,9 @@ int oracle_assemble2(oracle_hmat* h, const oracle_kernel* k, double epsilon, int
 /* Payload size in scalars of leaf `i` (m*n for full, k*(m+n) for rk) and a copy of it:
  * full leaves column-major m x n; rk leaves A (m x k) then B (n x k), column-major.
  * Complex payloads are interleaved (re, im) pairs. */
+/* Re-truncates every Rk leaf at `epsilon` (HMatrix::truncate, h_matrix.cpp:2107-2123). */
+int oracle_retruncate(oracle_hmat* h, double epsilon);
+
 long long oracle_leaf_payload_size(const oracle_hmat* h, int i);
 void oracle_leaf_payload(const oracle_hmat* h, int i, double* out);
 

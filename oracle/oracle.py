@@ -47,6 +47,7 @@ def lib():
         L.oracle_num_nodes.argtypes = [P]
         L.oracle_assemble.argtypes = [P, C.POINTER(Kernel), C.c_double, C.c_int]
         L.oracle_assemble2.argtypes = [P, C.POINTER(Kernel), C.c_double, C.c_int, C.c_int]
+        L.oracle_retruncate.argtypes = [P, C.c_double]
         L.oracle_leaf_payload_size.restype = C.c_longlong
         L.oracle_leaf_payload_size.argtypes = [P, C.c_int]
         L.oracle_leaf_payload.argtypes = [P, C.c_int, P]
@@ -94,6 +95,10 @@ class OracleHMatrix:
         self.is_complex = kind == 2
         rc = lib().oracle_assemble2(self.h, C.byref(self.kernel), eps, int(self.is_complex), min_leaf)
         assert rc == 0
+
+    def retruncate(self, eps):
+        """Re-truncates every Rk leaf at eps (HMatrix::truncate, h_matrix.cpp:2107-2123)."""
+        assert lib().oracle_retruncate(self.h, eps) == 0
 
     def payload(self, i):
         s = lib().oracle_leaf_payload_size(self.h, i)
@@ -165,7 +170,7 @@ def have_reference():
 
 def run_reference(points, kind, eps, leaf=64, eta=2.0, delta=0.01, ell=0.3, nugget=0.0, wavenumber=0.0, x=None,
                   nrhs=1, trans="N", scalar="D", dump_factors=False, gemv_reps=1, min_leaf=0, leaf_cols=0,
-                  gemv_warmup=0):
+                  gemv_warmup=0, retrunc=0.0):
     """Runs the reference library (oracle/_ref/ref_driver) and returns its outputs."""
     if not have_reference():
         raise FileNotFoundError(REF_DRIVER)
@@ -177,7 +182,7 @@ def run_reference(points, kind, eps, leaf=64, eta=2.0, delta=0.01, ell=0.3, nugg
                  f"nugget={nugget!r}", f"wavenumber={wavenumber!r}", f"leaf={leaf}", f"eta={eta!r}", f"eps={eps!r}",
                  f"nrhs={nrhs}", f"trans={trans}", f"scalar={scalar}", f"dump_factors={int(dump_factors)}",
                  f"gemv_reps={gemv_reps}", f"gemv_warmup={gemv_warmup}", f"min_leaf={min_leaf}",
-                 f"leaf_cols={leaf_cols}",
+                 f"leaf_cols={leaf_cols}", f"retrunc={retrunc!r}",
                  f"out={os.path.join(d, 'out')}"]
         dt = {"D": np.float64, "S": np.float32, "Z": np.complex128, "C": np.complex64}[scalar]
         if x is not None:

@@ -226,6 +226,16 @@ int run(const Params& p, hmat_value_t vt) {
     fprintf(stderr, "assemble_generic failed\n");
     return 3;
   }
+  // optional re-truncation of every Rk leaf at a new low-rank epsilon
+  // (hmat_interface_t.set_low_rank_epsilon, then .truncate)
+  const double retrunc = p.num("retrunc", 0.0);
+  if (retrunc > 0.0) {
+    hi.set_low_rank_epsilon(M, retrunc);
+    if (hi.truncate(M)) {
+      fprintf(stderr, "truncate failed\n");
+      return 4;
+    }
+  }
 
   // Cluster permutation (internal -> client).
   const int* perm = hmat_cluster_get_indices(ct);

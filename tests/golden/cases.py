@@ -26,6 +26,9 @@ CASES = {
                      dict(leaf=2048, leaf_cols=16, eta=2.0, eps=1e-5), 1, 3, "D", False),
     "svd_small": (lambda: wl.cylinder(40, 50), dict(kind=0, delta=0.01), dict(leaf=32, eta=2.0, eps=1e-4, min_leaf=100),
                   2, 14, "D", False),
+    # assembled at 1e-6, then set_low_rank_epsilon(1e-3) + truncate
+    "retrunc_expcov": (lambda: wl.cube(800, 31), dict(kind=1, ell=0.3, nugget=1e-6),
+                       dict(leaf=32, eta=2.0, eps=1e-6, retrunc=1e-3), 2, 32, "D", True),
 }
 
 
