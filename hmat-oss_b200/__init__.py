@@ -50,6 +50,13 @@ class AssembleContext(C.Structure):
                 ("progress", C.c_void_p)]
 
 
+class GetValuesContext(C.Structure):
+    """hmat_get_values_context_t (hmat.h:637-656)."""
+    _fields_ = [("matrix", C.c_void_p), ("values", C.c_void_p), ("row_offset", C.c_int), ("col_offset", C.c_int),
+                ("row_size", C.c_int), ("col_size", C.c_int), ("row_indices", C.POINTER(C.c_int)),
+                ("col_indices", C.POINTER(C.c_int)), ("renumber_rows", C.c_int, 1)]
+
+
 class Info(C.Structure):
     """hmat_info_t (reference: include/hmat/hmat.h:404-439)."""
     _fields_ = [("full_zeros", C.c_int), ("full_size", C.c_size_t), ("rk_size", C.c_size_t),
@@ -101,6 +108,9 @@ _PROTOS = {
     "vector_restore": C.CFUNCTYPE(C.c_int, _P, _P, C.c_int, _P, C.c_int),
     "truncate": C.CFUNCTYPE(C.c_int, _P),
     "gemm_dense": C.CFUNCTYPE(C.c_int, C.c_char, C.c_char, C.c_char, _P, _P, _P, _P, _P, C.c_int),
+    "gemm_scalar": C.CFUNCTYPE(C.c_int, C.c_char, _P, _P, _P, _P, _P, C.c_int),
+    "get_block": C.CFUNCTYPE(C.c_int, C.POINTER(GetValuesContext)),
+    "get_values": C.CFUNCTYPE(C.c_int, C.POINTER(GetValuesContext)),
     "solve_systems": C.CFUNCTYPE(C.c_int, _P, _P, C.c_int),
     "init": C.CFUNCTYPE(C.c_int),
     "finalize": C.CFUNCTYPE(C.c_int),
@@ -366,6 +376,52 @@ class HMatrix:
                                                ms.ctypes.data, by.ctypes.data), "hmat_b200_gemv_profile")
         return {"ms": dict(zip(("gather", "zphase", "yphase"), ms)),
                 "bytes": dict(zip(("gather", "zphase", "yphase"), by))}
+
+    def gemm_dense(self, trans_b: str, trans_x: str, side: str, alpha, x: np.ndarray, beta, y: np.ndarray) -> np.ndarray:
+        """op(Y) <- alpha op(B) op(X) + beta op(Y) (side 'L') or Y <- alpha op(X) op(B) + beta Y
+        (side 'R') in the internal numbering, through the C table's gemm_dense.  x and y are
+        column-major arrays whose shapes follow the flags; returns the new y."""
+        xf = np.array(x, dtype=self.dtype, order="F", copy=True)
+        yf = np.array(y, dtype=self.dtype, order="F", copy=True)
+        if yf.ndim != 2:
+            raise ValueError("y must be 2-D (n x nrhs for side 'L', nrhs x n for side 'R')")
+        nrhs = yf.shape[0] if side == "R" else yf.shape[1]
+        a = np.array([alpha], dtype=self.dtype)
+        b = np.array([beta], dtype=self.dtype)
+        _check(self.hi.fn("gemm_dense")(trans_b.encode(), trans_x.encode(), side.encode(), a.ctypes.data, self.m,
+                                        xf.ctypes.data, b.ctypes.data, yf.ctypes.data, int(nrhs)), "gemm_dense")
+        return yf
+
+    def gemm_scalar(self, x: np.ndarray, trans: str = "N", alpha=1.0, beta=0.0, y: np.ndarray | None = None):
+        """gemv in the internal numbering (the C table's gemm_scalar)."""
+        xf = np.asfortranarray(x, dtype=self.dtype)
+        nrhs = 1 if xf.ndim == 1 else xf.shape[1]
+        yf = np.zeros_like(xf) if y is None else np.array(y, dtype=self.dtype, order="F", copy=True)
+        a = np.array([alpha], dtype=self.dtype)
+        b = np.array([beta], dtype=self.dtype)
+        _check(self.hi.fn("gemm_scalar")(trans.encode(), a.ctypes.data, self.m, xf.ctypes.data, b.ctypes.data,
+                                         yf.ctypes.data, nrhs), "gemm_scalar")
+        return yf
+
+    def get_block(self, row_offset: int, row_size: int, col_offset: int, col_size: int, renumber_rows=False):
+        """Dense block (internal numbering) and its row / column numbering (get_block)."""
+        out = np.zeros((row_size, col_size), dtype=self.dtype, order="F")
+        ctx = GetValuesContext(self.m, out.ctypes.data, row_offset, col_offset, row_size, col_size, None, None,
+                               int(bool(renumber_rows)))
+        _check(self.hi.fn("get_block")(C.byref(ctx)), "get_block")
+        rows = np.ctypeslib.as_array(ctx.row_indices, shape=(row_size,)).copy() if row_size else np.zeros(0, int)
+        cols = np.ctypeslib.as_array(ctx.col_indices, shape=(col_size,)).copy() if col_size else np.zeros(0, int)
+        return out, rows, cols
+
+    def get_values(self, rows, cols) -> np.ndarray:
+        """Entries for rows x cols given in natural numbering 1..n (get_values)."""
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        c = np.ascontiguousarray(cols, dtype=np.int32)
+        out = np.zeros((len(r), len(c)), dtype=self.dtype, order="F")
+        ctx = GetValuesContext(self.m, out.ctypes.data, 0, 0, len(r), len(c),
+                               r.ctypes.data_as(C.POINTER(C.c_int)), c.ctypes.data_as(C.POINTER(C.c_int)), 0)
+        _check(self.hi.fn("get_values")(C.byref(ctx)), "get_values")
+        return out
 
     def set_low_rank_epsilon(self, eps: float) -> None:
         self.hi.fn("set_low_rank_epsilon")(self.m, eps)

@@ -1,6 +1,7 @@
 // C ABI of the B200 engine: the hmat-oss C entry points on the leaf-level path (same
 // names, argument meaning and 0 / non-zero return convention as c_default_interface.cpp
 // and c_wrapping.hpp) plus the hmat_b200_* extensions declared in include/hmat_b200.h.
+#include <algorithm>
 #include <complex>
 #include <cstdio>
 #include <cstring>
@@ -292,10 +293,228 @@ int u_gemm(char, char, const void*, hmat_matrix_t*, hmat_matrix_t*, const void*,
 }
 int u_axpy(void*, hmat_matrix_t*, hmat_matrix_t*) { return unsupported("axpy"); }
 int u_trsm(char, char, char, char, int, int, void*, hmat_matrix_t*, int, void*) { return unsupported("trsm"); }
-int u_gemm_scalar(char, void*, hmat_matrix_t*, void*, void*, void*, int) { return unsupported("gemm_scalar"); }
+
 int u_full_gemm(char, char, int, int, void*, void*, void*, hmat_matrix_t*, void*) { return unsupported("full_gemm"); }
-int u_gemm_dense(char, char, char, const void*, hmat_matrix_t*, void*, const void*, void*, int) {
-  return unsupported("gemm_dense");
+// ---- products and extraction in the H-matrix's internal (cluster) numbering ----
+// Host scalar type of each value type (layout-identical to the device types).
+template <int VT> struct HostScalar;
+template <> struct HostScalar<0> { typedef float type; };
+template <> struct HostScalar<1> { typedef double type; };
+template <> struct HostScalar<2> { typedef std::complex<float> type; };
+template <> struct HostScalar<3> { typedef std::complex<double> type; };
+inline float conj_s(float v) { return v; }
+inline double conj_s(double v) { return v; }
+template <typename R>
+std::complex<R> conj_s(std::complex<R> v) { return std::conj(v); }
+
+bool flag_trans(char t) { return t == 'T' || t == 'C'; }
+bool flag_conj(char t) { return t == 'C' || t == 'J'; }
+// switch_flag_trans / switch_flag_conj (c_wrapping.hpp:280-298)
+char switch_trans(char t) {
+  switch (t) {
+    case 'N': return 'T';
+    case 'T': return 'N';
+    case 'C': return 'J';
+    case 'J': return 'C';
+  }
+  throw Error(std::string("bad transposition flag '") + t + "'");
+}
+char switch_conj(char t) {
+  switch (t) {
+    case 'N': return 'J';
+    case 'T': return 'C';
+    case 'C': return 'T';
+    case 'J': return 'N';
+  }
+  throw Error(std::string("bad transposition flag '") + t + "'");
+}
+
+// op(Y) <- alpha op(B) op(X) + beta op(Y) with X, Y in internal numbering (gemm_dense,
+// c_wrapping.hpp:302-366, side 'L' after the side 'R' rewrite): the operands are brought
+// to client order, multiplied on the device, and returned.  Unlike the reference, X is not
+// left conjugated on return for the 'C' / 'J' flags.
+template <typename S>
+void internal_product(hmat_matrix_t* m, char tb, char tx, char ty, S alpha, S beta, const S* X, S* Y, int nrhs) {
+  if (tb != 'N' && tb != 'T' && tb != 'C') throw Error(std::string("bad transposition flag '") + tb + "'");
+  if (tx != 'N' && tx != 'T' && tx != 'C' && tx != 'J') throw Error(std::string("bad transposition flag '") + tx + "'");
+  const ClusterTree& rt = *m->rows_h->t;
+  const ClusterTree& ct = *m->cols_h->t;
+  const ClusterTree& in_t = !flag_trans(tb) ? ct : rt;
+  const ClusterTree& out_t = !flag_trans(tb) ? rt : ct;
+  const int nin = in_t.n, nout = out_t.n;
+  std::vector<S> xc((size_t)nin * nrhs), yc((size_t)nout * nrhs);
+  for (int q = 0; q < nrhs; ++q)
+    for (int i = 0; i < nin; ++i) {
+      S v = flag_trans(tx) ? X[q + (size_t)i * nrhs] : X[i + (size_t)q * nin];
+      if (flag_conj(tx)) v = conj_s(v);
+      xc[in_t.perm[i] + (size_t)q * nin] = v;
+    }
+  for (int q = 0; q < nrhs; ++q)
+    for (int i = 0; i < nout; ++i) {
+      S v = flag_trans(ty) ? Y[q + (size_t)i * nrhs] : Y[i + (size_t)q * nout];
+      if (flag_conj(ty)) v = conj_s(v);
+      yc[out_t.perm[i] + (size_t)q * nout] = v;
+    }
+  engine_of(m).gemv_host(tb, &alpha, xc.data(), &beta, yc.data(), nrhs);
+  for (int q = 0; q < nrhs; ++q)
+    for (int i = 0; i < nout; ++i) {
+      S v = yc[out_t.perm[i] + (size_t)q * nout];
+      if (flag_conj(ty)) v = conj_s(v);
+      if (flag_trans(ty)) Y[q + (size_t)i * nrhs] = v;
+      else Y[i + (size_t)q * nout] = v;
+    }
+}
+
+template <int VT>
+int gemm_dense_t(char trans_b, char trans_x, char side, const void* alpha, hmat_matrix_t* m, void* vec_x,
+                 const void* beta, void* vec_y, int nrhs) {
+  typedef typename HostScalar<VT>::type S;
+  HB_TRY("gemm_dense", {
+    if (!m || !alpha || !beta || (nrhs > 0 && (!vec_x || !vec_y))) throw Error("null argument");
+    if (m->vt != VT) throw Error("matrix value type does not match this interface");
+    S a = *(const S*)alpha, b = *(const S*)beta;
+    char ty = 'N';
+    if (side == 'R') {
+      // Y <- alpha X op(B) + beta Y  <=>  Y^T <- alpha op(B)^T X^T + beta Y^T (or ^H)
+      if (trans_b == 'C') {
+        trans_b = 'N';
+        trans_x = switch_conj(switch_trans(trans_x));
+        ty = 'C';
+        a = conj_s(a);
+        b = conj_s(b);
+      } else {
+        trans_b = switch_trans(trans_b);
+        trans_x = switch_trans(trans_x);
+        ty = 'T';
+      }
+    } else if (side != 'L') {
+      throw Error(std::string("bad side '") + side + "'");
+    }
+    if (nrhs > 0) internal_product<S>(m, trans_b, trans_x, ty, a, b, (const S*)vec_x, (S*)vec_y, nrhs);
+  });
+  return 0;
+}
+
+// gemm_scalar (c_wrapping.hpp:254-271): gemv in internal numbering.
+template <int VT>
+int gemm_scalar_t(char trans, void* alpha, hmat_matrix_t* m, void* x, void* beta, void* y, int nrhs) {
+  typedef typename HostScalar<VT>::type S;
+  HB_TRY("gemm_scalar", {
+    if (!m || !alpha || !beta || (nrhs > 0 && (!x || !y))) throw Error("null argument");
+    if (m->vt != VT) throw Error("matrix value type does not match this interface");
+    if (nrhs > 0) internal_product<S>(m, trans, 'N', 'N', *(const S*)alpha, *(const S*)beta, (const S*)x, (S*)y, nrhs);
+  });
+  return 0;
+}
+
+// Fills out[r, c] (query positions) for every leaf that meets the sorted row and column
+// queries (internal index, position), from the leaves' payloads.
+template <typename S>
+void fill_from_leaves(hmat_matrix_t* m, const std::vector<std::pair<int, int>>& rq,
+                      const std::vector<std::pair<int, int>>& cq, S* out, size_t ld) {
+  EngineBase& e = engine_of(m);
+  if (!e.assembled) throw Error("matrix not assembled");
+  const auto& L = m->bt.leaves;
+  std::vector<S> buf;
+  auto lo = [](const std::vector<std::pair<int, int>>& v, int x) {
+    return (size_t)(std::lower_bound(v.begin(), v.end(), std::make_pair(x, -1)) - v.begin());
+  };
+  for (size_t i = 0; i < L.size(); ++i) {
+    const LeafInfo& l = L[i];
+    const size_t r0 = lo(rq, l.row_off), r1 = lo(rq, l.row_off + l.m);
+    const size_t c0 = lo(cq, l.col_off), c1 = lo(cq, l.col_off + l.n);
+    if (r0 == r1 || c0 == c1) continue;
+    const int k = e.ranks[i];
+    if (l.type == 1 && k <= 0) continue;  // zero block
+    const size_t size = l.type == 0 ? (size_t)l.m * l.n : (size_t)k * (l.m + l.n);
+    buf.resize(std::max<size_t>(size, 1));
+    e.leaf_payload((int)i, buf.data());
+    for (size_t a = r0; a < r1; ++a)
+      for (size_t b = c0; b < c1; ++b) {
+        const int ri = rq[a].first - l.row_off, cj = cq[b].first - l.col_off;
+        S v;
+        if (l.type == 0) {
+          v = buf[ri + (size_t)l.m * cj];
+        } else {
+          v = S(0);
+          const S* A = buf.data();
+          const S* B = A + (size_t)l.m * k;
+          for (int t = 0; t < k; ++t) v += A[ri + (size_t)l.m * t] * B[cj + (size_t)l.n * t];
+        }
+        out[rq[a].second + ld * cq[b].second] = v;
+      }
+  }
+}
+
+// get_block (c_wrapping.hpp:833-868, uncompressed_block.hpp): the dense block of rows
+// [row_offset, +row_size) and columns [col_offset, +col_size) in internal numbering; the
+// numbering arrays point into the cluster trees' internal -> client permutations.
+template <int VT>
+int get_block_t(struct hmat_get_values_context_t* ctx) {
+  typedef typename HostScalar<VT>::type S;
+  HB_TRY("get_block", {
+    if (!ctx || !ctx->matrix || !ctx->values) throw Error("null argument");
+    hmat_matrix_t* m = ctx->matrix;
+    if (m->vt != VT) throw Error("matrix value type does not match this interface");
+    ClusterTree& rt = *m->rows_h->t;
+    ClusterTree& ct = *m->cols_h->t;
+    if (ctx->row_offset < 0 || ctx->row_size < 0 || ctx->row_offset + ctx->row_size > rt.n || ctx->col_offset < 0 ||
+        ctx->col_size < 0 || ctx->col_offset + ctx->col_size > ct.n)
+      throw Error("block outside the matrix");
+    const bool renumber = ctx->renumber_rows != 0;
+    if (renumber && (ctx->row_offset != 0 || ctx->row_size != rt.n)) throw Error("Cannot renumber");
+    std::vector<std::pair<int, int>> rq(ctx->row_size), cq(ctx->col_size);
+    for (int i = 0; i < ctx->row_size; ++i) rq[i] = {ctx->row_offset + i, i};
+    for (int j = 0; j < ctx->col_size; ++j) cq[j] = {ctx->col_offset + j, j};
+    S* out = (S*)ctx->values;
+    std::fill(out, out + (size_t)ctx->row_size * ctx->col_size, S(0));
+    fill_from_leaves<S>(m, rq, cq, out, (size_t)ctx->row_size);
+    if (renumber) {
+      // restoreVectorOrder on the rows: row i of the block moves to client row perm[i]
+      std::vector<S> tmp(ctx->row_size);
+      for (int j = 0; j < ctx->col_size; ++j) {
+        S* col = out + (size_t)j * ctx->row_size;
+        for (int i = 0; i < ctx->row_size; ++i) tmp[rt.perm[i]] = col[i];
+        std::copy(tmp.begin(), tmp.end(), col);
+      }
+    }
+    ctx->row_indices = rt.perm.data() + ctx->row_offset;
+    ctx->col_indices = ct.perm.data() + ctx->col_offset;
+  });
+  return 0;
+}
+
+// get_values (c_wrapping.hpp:871-890, uncompressed_values.hpp:82-95): entries for lists of
+// rows and columns in natural numbering (1 to n); values[i + row_size j].
+template <int VT>
+int get_values_t(struct hmat_get_values_context_t* ctx) {
+  typedef typename HostScalar<VT>::type S;
+  HB_TRY("get_values", {
+    if (!ctx || !ctx->matrix || !ctx->values || (ctx->row_size > 0 && !ctx->row_indices) ||
+        (ctx->col_size > 0 && !ctx->col_indices))
+      throw Error("null argument");
+    hmat_matrix_t* m = ctx->matrix;
+    if (m->vt != VT) throw Error("matrix value type does not match this interface");
+    const ClusterTree& rt = *m->rows_h->t;
+    const ClusterTree& ct = *m->cols_h->t;
+    std::vector<std::pair<int, int>> rq(ctx->row_size), cq(ctx->col_size);
+    for (int i = 0; i < ctx->row_size; ++i) {
+      const int q = ctx->row_indices[i];
+      if (q < 1 || q > rt.n) throw Error("row index outside 1..n");
+      rq[i] = {rt.rev[q - 1], i};
+    }
+    for (int j = 0; j < ctx->col_size; ++j) {
+      const int q = ctx->col_indices[j];
+      if (q < 1 || q > ct.n) throw Error("column index outside 1..n");
+      cq[j] = {ct.rev[q - 1], j};
+    }
+    std::sort(rq.begin(), rq.end());
+    std::sort(cq.begin(), cq.end());
+    S* out = (S*)ctx->values;
+    std::fill(out, out + (size_t)ctx->row_size * ctx->col_size, S(0));
+    fill_from_leaves<S>(m, rq, cq, out, (size_t)ctx->row_size);
+  });
+  return 0;
 }
 int u_add_identity(hmat_matrix_t*, void*) { return unsupported("add_identity"); }
 int u_get_profile(hmat_matrix_t*, hmat_profile_t*) { return unsupported("get_profile"); }
@@ -319,8 +538,7 @@ int u_set_cluster_trees(hmat_matrix_t*, const hmat_cluster_tree_t*, const hmat_c
 int u_extract_diagonal(hmat_matrix_t*, void*, int) { return unsupported("extract_diagonal"); }
 int u_solve_lower(hmat_matrix_t*, int, void*, int) { return unsupported("solve_lower_triangular"); }
 int u_solve_lower_dense(hmat_matrix_t*, int, void*, int) { return unsupported("solve_lower_triangular_dense"); }
-int u_get_block(struct hmat_get_values_context_t*) { return unsupported("get_block"); }
-int u_get_values(struct hmat_get_values_context_t*) { return unsupported("get_values"); }
+
 int u_walk(hmat_matrix_t*, hmat_procedure_t*) { return unsupported("walk"); }
 int u_apply_on_leaf(hmat_matrix_t*, const hmat_leaf_procedure_t*) { return unsupported("apply_on_leaf"); }
 hmat_matrix_t* u_read_struct(hmat_iostream, void*) {
@@ -361,9 +579,9 @@ void fill_table(hmat_interface_t* i) {
   i->axpy = u_axpy;
   i->trsm = u_trsm;
   i->gemv = gemv_t<VT>;
-  i->gemm_scalar = u_gemm_scalar;
+  i->gemm_scalar = gemm_scalar_t<VT>;
   i->full_gemm = u_full_gemm;
-  i->gemm_dense = u_gemm_dense;
+  i->gemm_dense = gemm_dense_t<VT>;
   i->add_identity = u_add_identity;
   i->init = init_fn;
   i->finalize = finalize_fn;
@@ -381,8 +599,8 @@ void fill_table(hmat_interface_t* i) {
   i->extract_diagonal = u_extract_diagonal;
   i->solve_lower_triangular = u_solve_lower;
   i->solve_lower_triangular_dense = u_solve_lower_dense;
-  i->get_block = u_get_block;
-  i->get_values = u_get_values;
+  i->get_block = get_block_t<VT>;
+  i->get_values = get_values_t<VT>;
   i->walk = u_walk;
   i->apply_on_leaf = u_apply_on_leaf;
   i->internal = nullptr;
