@@ -57,6 +57,10 @@ class GetValuesContext(C.Structure):
                 ("col_indices", C.POINTER(C.c_int)), ("renumber_rows", C.c_int, 1)]
 
 
+class ClusterInfo(C.Structure):
+    _fields_ = [("spatial_dimension", C.c_int), ("dimension", C.c_int), ("nr_tree_nodes", C.c_size_t)]
+
+
 class Info(C.Structure):
     """hmat_info_t (reference: include/hmat/hmat.h:404-439)."""
     _fields_ = [("full_zeros", C.c_int), ("full_size", C.c_size_t), ("rk_size", C.c_size_t),
@@ -96,6 +100,7 @@ class InterfaceTable(C.Structure):
 
 
 _P = C.c_void_p
+_IOSTREAM = C.CFUNCTYPE(None, C.c_void_p, C.c_size_t, C.c_void_p)
 _PROTOS = {
     "create_empty_hmatrix_admissibility": C.CFUNCTYPE(_P, _P, _P, C.c_int, _P),
     "own_cluster_trees": C.CFUNCTYPE(None, _P, C.c_int, C.c_int),
@@ -110,6 +115,11 @@ _PROTOS = {
     "gemm_dense": C.CFUNCTYPE(C.c_int, C.c_char, C.c_char, C.c_char, _P, _P, _P, _P, _P, C.c_int),
     "gemm_scalar": C.CFUNCTYPE(C.c_int, C.c_char, _P, _P, _P, _P, _P, C.c_int),
     "get_block": C.CFUNCTYPE(C.c_int, C.POINTER(GetValuesContext)),
+    "write_struct": C.CFUNCTYPE(None, _P, _IOSTREAM, _P),
+    "write_data": C.CFUNCTYPE(None, _P, _IOSTREAM, _P),
+    "read_struct": C.CFUNCTYPE(_P, _IOSTREAM, _P),
+    "read_data": C.CFUNCTYPE(None, _P, _IOSTREAM, _P),
+    "get_cluster_trees": C.CFUNCTYPE(C.c_int, _P, C.POINTER(_P), C.POINTER(_P)),
     "get_values": C.CFUNCTYPE(C.c_int, C.POINTER(GetValuesContext)),
     "solve_systems": C.CFUNCTYPE(C.c_int, _P, _P, C.c_int),
     "init": C.CFUNCTYPE(C.c_int),
@@ -133,6 +143,7 @@ EXPORTED = [
     "hmat_b200_leaf_count",
     "hmat_b200_leaf_table", "hmat_b200_leaf_payload", "hmat_b200_payload_layout", "hmat_b200_leaf_gradients",
     "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_gemv_launches", "hmat_b200_last_error",
+    "hmat_b200_clear_last_error",
 ]
 
 
@@ -176,6 +187,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "hmat_b200_gemv_profile": (C.c_int, [_P, C.c_char, _P, _P, C.c_int, _P, _P]),
         "hmat_b200_gemv_launches": (C.c_int, [_P, C.c_char, C.c_int]),
         "hmat_b200_last_error": (C.c_char_p, []),
+        "hmat_b200_clear_last_error": (None, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -326,8 +338,71 @@ class HMatrix:
         return self.hi.get_info(self.m).as_dict()
 
     def perm(self, cols: bool = False) -> np.ndarray:
-        p = self.lib.hmat_cluster_get_indices(self.tree_cols if (cols and self.tree_cols) else self.tree)
+        if getattr(self, "_borrowed_trees", None):  # a matrix read from a stream owns its trees
+            rt, ct = self._borrowed_trees
+            p = self.lib.hmat_cluster_get_indices(ct if cols else rt)
+        else:
+            p = self.lib.hmat_cluster_get_indices(self.tree_cols if (cols and self.tree_cols) else self.tree)
         return np.ctypeslib.as_array(p, shape=(self.n,)).copy()
+
+    # -- write_struct / write_data / read_struct / read_data --
+    def dump(self) -> tuple:
+        """(struct, data) streams of this matrix, through the C table's write_struct and
+        write_data."""
+        chunks = []
+        cb = _IOSTREAM(lambda buf, n, ud: chunks.append(C.string_at(buf, n)) if n else None)
+        self.lib.hmat_b200_clear_last_error()
+        self.hi.fn("write_struct")(self.m, cb, None)
+        st = b"".join(chunks)
+        chunks.clear()
+        self.hi.fn("write_data")(self.m, cb, None)
+        err = self.lib.hmat_b200_last_error()
+        if err:
+            raise HMatError(err.decode())
+        return st, b"".join(chunks)
+
+    @classmethod
+    def load(cls, value_type: int, struct_stream: bytes, data_stream: bytes) -> "HMatrix":
+        """A matrix read back with read_struct and read_data (no clustering, no assembly)."""
+        lib = load_library()
+        hi = HMatInterface(value_type)
+        short = []
+
+        def reader(data):
+            pos = [0]
+
+            def rd(buf, n, ud):
+                if n == 0:
+                    return
+                take = data[pos[0]:pos[0] + n]
+                pos[0] += n
+                if len(take) < n:  # past the end: zeros, reported after the call
+                    short.append(n)
+                    take = take + bytes(n - len(take))
+                C.memmove(buf, take, n)
+            return _IOSTREAM(rd)
+
+        lib.hmat_b200_clear_last_error()
+        rs, rdd = reader(struct_stream), reader(data_stream)
+        m = hi.fn("read_struct")(rs, None)
+        if not m:
+            raise HMatError("read_struct failed: " + lib.hmat_b200_last_error().decode())
+        hi.fn("read_data")(m, rdd, None)
+        err = lib.hmat_b200_last_error()
+        if err or short:
+            hi.destroy(m)
+            raise HMatError((err.decode() if err else "") + (" (stream too short)" if short else ""))
+        obj = cls.__new__(cls)
+        obj.lib, obj.hi, obj.m = lib, hi, m
+        obj.value_type, obj.dtype = value_type, DTYPES[value_type]
+        rt, ct = C.c_void_p(), C.c_void_p()
+        hi.fn("get_cluster_trees")(m, C.byref(rt), C.byref(ct))
+        obj._borrowed_trees = (rt.value, ct.value)
+        obj.tree = obj.tree_cols = None
+        info = ClusterInfo()
+        lib.hmat_cluster_get_info(rt, C.byref(info))
+        obj.n = int(info.dimension)
+        return obj
 
     def leaf_table(self) -> np.ndarray:
         n = self.lib.hmat_b200_leaf_count(self.m)

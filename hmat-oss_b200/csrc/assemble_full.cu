@@ -38,9 +38,40 @@ void launch_assemble_full(const FullLeafDesc* d_leaves, int nleaves, const Panel
   assemble_full_kernel<T><<<grid, 256, 0, s>>>(d_leaves, nleaves, panels, kp, pts, arena);
 }
 
+// Full leaves from their canonical payloads (m x n column-major at goff[leaf] in src) into
+// the arena's row panels, for loading a stored matrix.
+template <typename T>
+__global__ void full_from_canonical_kernel(const FullLeafDesc* __restrict__ leaves, const long long* __restrict__ goff,
+                                           int nleaves, const PanelDesc* __restrict__ panels,
+                                           const T* __restrict__ src, T* __restrict__ arena) {
+  for (int leaf = blockIdx.x; leaf < nleaves; leaf += gridDim.x) {
+    const FullLeafDesc d = leaves[leaf];
+    const T* F = src + goff[leaf];
+    for (int p = 0; p < d.npanel; ++p) {
+      const PanelDesc P = panels[d.panel_first + p];
+      T* dst = arena + P.off;
+      for (int e = threadIdx.x; e < P.len * d.n; e += blockDim.x) {
+        const int i = e % P.len, j = e / P.len;
+        dst[e] = F[(size_t)(P.rs + i) + (size_t)d.m * j];
+      }
+    }
+  }
+}
+
+template <typename T>
+void launch_full_from_canonical(const FullLeafDesc* d_leaves, const long long* goff, int nleaves,
+                                const PanelDesc* panels, const T* src, T* arena, cudaStream_t s) {
+  if (nleaves <= 0) return;
+  int grid = persistent_grid(8);
+  if (grid > nleaves) grid = nleaves;
+  full_from_canonical_kernel<T><<<grid, 256, 0, s>>>(d_leaves, goff, nleaves, panels, src, arena);
+}
+
 #define HB_INST(T)                                                                                      \
   template void launch_assemble_full<T>(const FullLeafDesc*, int, const PanelDesc*, const KernelParams&, \
-                                        Points, T*, cudaStream_t);
+                                        Points, T*, cudaStream_t);                                       \
+  template void launch_full_from_canonical<T>(const FullLeafDesc*, const long long*, int, const PanelDesc*, \
+                                              const T*, T*, cudaStream_t);
 HB_INST(float)
 HB_INST(double)
 HB_INST(cfloat)

@@ -541,13 +541,247 @@ int u_solve_lower_dense(hmat_matrix_t*, int, void*, int) { return unsupported("s
 
 int u_walk(hmat_matrix_t*, hmat_procedure_t*) { return unsupported("walk"); }
 int u_apply_on_leaf(hmat_matrix_t*, const hmat_leaf_procedure_t*) { return unsupported("apply_on_leaf"); }
-hmat_matrix_t* u_read_struct(hmat_iostream, void*) {
-  unsupported("read_struct");
-  return nullptr;
+// ---- write_struct / read_struct / write_data / read_data (c_wrapping.hpp:921-946) ----
+// This library's own stream format (native byte order), through the caller's hmat_iostream:
+//   struct: "HB2S", version, value type, rows tree, cols-tree flag (0: same as rows) [+ cols
+//           tree], leaf count, leaves (row node, col node, row offset, m, col offset, n, type),
+//           number of block clusters, low-rank epsilon
+//   tree:   n, points (3 n doubles, client numbering), permutation (internal -> client),
+//           node count, nodes (offset, size, children, child count, depth, bounding box),
+//           tree-leaf count, tree leaves
+//   data:   "HB2D", version, value type, leaf count, ranks (-1 for full leaves), scalar
+//           count, the canonical payload of every leaf (full m x n; Rk A m x k then B n x k;
+//           column-major, leaf order)
+// Both end with the mark "HB2E".
+// The reference's own format carries its internal node tree; streams are not exchangeable.
+const int kStreamVersion = 1;
+struct StreamOut {
+  hmat_iostream f;
+  void* ud;
+  template <typename X>
+  void val(X v) { f(&v, sizeof v, ud); }
+  void bytes(const void* p, size_t n) {
+    if (n) f(const_cast<void*>(p), n, ud);
+  }
+};
+struct StreamIn {
+  hmat_iostream f;
+  void* ud;
+  template <typename X>
+  X val() {
+    X v;
+    f(&v, sizeof v, ud);
+    return v;
+  }
+  void bytes(void* p, size_t n) {
+    if (n) f(p, n, ud);
+  }
+};
+void write_magic(StreamOut& o, char kind) {
+  const char mg[4] = {'H', 'B', '2', kind};
+  o.bytes(mg, 4);
+  o.val<int>(kStreamVersion);
 }
-void u_write_struct(hmat_matrix_t*, hmat_iostream, void*) { unsupported("write_struct"); }
-void u_read_data(hmat_matrix_t*, hmat_iostream, void*) { unsupported("read_data"); }
-void u_write_data(hmat_matrix_t*, hmat_iostream, void*) { unsupported("write_data"); }
+// Every stream ends with "HB2E": a stream cut short (or padded) is refused.
+void write_end(StreamOut& o) {
+  const char mg[4] = {'H', 'B', '2', 'E'};
+  o.bytes(mg, 4);
+}
+void read_end(StreamIn& in) {
+  char mg[4];
+  in.bytes(mg, 4);
+  if (mg[0] != 'H' || mg[1] != 'B' || mg[2] != '2' || mg[3] != 'E') throw Error("corrupt stream (no end mark)");
+}
+void read_magic(StreamIn& in, char kind) {
+  char mg[4];
+  in.bytes(mg, 4);
+  if (mg[0] != 'H' || mg[1] != 'B' || mg[2] != '2' || mg[3] != kind) throw Error("not a B200 engine stream");
+  if (in.val<int>() != kStreamVersion) throw Error("unsupported stream version");
+}
+void write_tree(StreamOut& o, const ClusterTree& t) {
+  o.val<int>(t.n);
+  o.bytes(t.pts.data(), t.pts.size() * sizeof(double));
+  o.bytes(t.perm.data(), t.perm.size() * sizeof(int));
+  o.val<int>((int)t.nodes.size());
+  for (const ClusterNode& c : t.nodes) {
+    o.val<int>(c.offset);
+    o.val<int>(c.size);
+    o.val<int>(c.child[0]);
+    o.val<int>(c.child[1]);
+    o.val<int>(c.nchild);
+    o.val<int>(c.depth);
+    o.bytes(c.bb, sizeof c.bb);
+  }
+  o.val<int>((int)t.leaf_nodes.size());
+  o.bytes(t.leaf_nodes.data(), t.leaf_nodes.size() * sizeof(int));
+}
+std::unique_ptr<ClusterTree> read_tree(StreamIn& in) {
+  auto t = std::make_unique<ClusterTree>();
+  t->n = in.val<int>();
+  if (t->n < 0) throw Error("corrupt stream (tree size)");
+  t->pts.resize((size_t)t->n * 3);
+  in.bytes(t->pts.data(), t->pts.size() * sizeof(double));
+  t->perm.resize(t->n);
+  in.bytes(t->perm.data(), t->perm.size() * sizeof(int));
+  t->rev.assign(t->n, -1);
+  for (int i = 0; i < t->n; ++i) {
+    if (t->perm[i] < 0 || t->perm[i] >= t->n || t->rev[t->perm[i]] != -1) throw Error("corrupt stream (permutation)");
+    t->rev[t->perm[i]] = i;
+  }
+  const int nn = in.val<int>();
+  if (nn < 0) throw Error("corrupt stream (node count)");
+  t->nodes.resize(nn);
+  for (ClusterNode& c : t->nodes) {
+    c.offset = in.val<int>();
+    c.size = in.val<int>();
+    c.child[0] = in.val<int>();
+    c.child[1] = in.val<int>();
+    c.nchild = in.val<int>();
+    c.depth = in.val<int>();
+    in.bytes(c.bb, sizeof c.bb);
+    if (c.offset < 0 || c.size < 0 || c.offset + c.size > t->n || c.child[0] >= nn || c.child[1] >= nn)
+      throw Error("corrupt stream (node)");
+  }
+  const int nl = in.val<int>();
+  if (nl < 0) throw Error("corrupt stream (tree leaves)");
+  t->leaf_nodes.resize(nl);
+  in.bytes(t->leaf_nodes.data(), (size_t)nl * sizeof(int));
+  return t;
+}
+
+void c_write_struct(hmat_matrix_t* m, hmat_iostream f, void* ud) {
+  try {
+    if (!m || !f) throw Error("null argument");
+    StreamOut o{f, ud};
+    write_magic(o, 'S');
+    o.val<int>(m->vt);
+    write_tree(o, *m->rows_h->t);
+    const bool same = m->cols_h == m->rows_h;
+    o.val<int>(same ? 0 : 1);
+    if (!same) write_tree(o, *m->cols_h->t);
+    o.val<int>((int)m->bt.leaves.size());
+    for (const LeafInfo& l : m->bt.leaves) {
+      const int v[7] = {l.row_node, l.col_node, l.row_off, l.m, l.col_off, l.n, l.type};
+      o.bytes(v, sizeof v);
+    }
+    o.val<int>(m->bt.nr_block_clusters);
+    o.val<double>(m->low_rank_eps);
+    write_end(o);
+  } catch (const std::exception& e) {
+    fail("write_struct", e.what());
+  }
+}
+
+template <int VT>
+hmat_matrix_t* c_read_struct(hmat_iostream f, void* ud) {
+  std::unique_ptr<hmat_matrix_t> m;
+  std::unique_ptr<hmat_cluster_tree_t> rt, ct;
+  try {
+    if (!f) throw Error("null argument");
+    StreamIn in{f, ud};
+    read_magic(in, 'S');
+    if (in.val<int>() != VT) throw Error("Type mismatch between the stream and this interface");
+    rt.reset(new hmat_cluster_tree_t());
+    rt->t = read_tree(in);
+    if (in.val<int>() != 0) {
+      ct.reset(new hmat_cluster_tree_t());
+      ct->t = read_tree(in);
+    }
+    m.reset(new hmat_matrix_t());
+    m->vt = VT;
+    const int nl = in.val<int>();
+    if (nl < 0) throw Error("corrupt stream (leaf count)");
+    const int nr = rt->t->n, nc = ct ? ct->t->n : nr;
+    m->bt.leaves.resize(nl);
+    for (LeafInfo& l : m->bt.leaves) {
+      int v[7];
+      in.bytes(v, sizeof v);
+      l.row_node = v[0];
+      l.col_node = v[1];
+      l.row_off = v[2];
+      l.m = v[3];
+      l.col_off = v[4];
+      l.n = v[5];
+      l.type = v[6];
+      if (l.row_off < 0 || l.m < 0 || l.row_off + l.m > nr || l.col_off < 0 || l.n < 0 || l.col_off + l.n > nc ||
+          (l.type != 0 && l.type != 1))
+        throw Error("corrupt stream (leaf)");
+    }
+    m->bt.nr_block_clusters = in.val<int>();
+    m->low_rank_eps = in.val<double>();
+    read_end(in);
+    m->rows_h = rt.release();
+    m->cols_h = ct ? ct.release() : m->rows_h;
+    m->own_rows = m->own_cols = true;
+    return m.release();
+  } catch (const std::exception& e) {
+    fail("read_struct", e.what());
+    return nullptr;
+  }
+}
+
+template <int VT>
+void c_write_data(hmat_matrix_t* m, hmat_iostream f, void* ud) {
+  typedef typename HostScalar<VT>::type S;
+  try {
+    if (!m || !f) throw Error("null argument");
+    if (m->vt != VT) throw Error("matrix value type does not match this interface");
+    EngineBase& e = engine_of(m);
+    if (!e.assembled) throw Error("write_data needs an assembled matrix");
+    const int nl = (int)m->bt.leaves.size();
+    long long total = 0;
+    e.payload_layout(nullptr, &total);
+    StreamOut o{f, ud};
+    write_magic(o, 'D');
+    o.val<int>(VT);
+    o.val<int>(nl);
+    o.bytes(e.ranks.data(), (size_t)nl * sizeof(int));
+    o.val<long long>(total);
+    std::vector<S> buf;
+    for (int i = 0; i < nl; ++i) {
+      const LeafInfo& l = m->bt.leaves[i];
+      const int k = e.ranks[i];
+      const size_t size = l.type == 0 ? (size_t)l.m * l.n : (k > 0 ? (size_t)k * (l.m + l.n) : 0);
+      if (!size) continue;
+      buf.resize(size);
+      e.leaf_payload(i, buf.data());
+      o.bytes(buf.data(), size * sizeof(S));
+    }
+    write_end(o);
+  } catch (const std::exception& ex) {
+    fail("write_data", ex.what());
+  }
+}
+
+template <int VT>
+void c_read_data(hmat_matrix_t* m, hmat_iostream f, void* ud) {
+  typedef typename HostScalar<VT>::type S;
+  try {
+    if (!m || !f) throw Error("null argument");
+    if (m->vt != VT) throw Error("matrix value type does not match this interface");
+    StreamIn in{f, ud};
+    read_magic(in, 'D');
+    if (in.val<int>() != VT) throw Error("Type mismatch between the stream and this interface");
+    const int nl = in.val<int>();
+    if (nl != (int)m->bt.leaves.size()) throw Error("stream and matrix have different leaves");
+    std::vector<int> rk(nl);
+    in.bytes(rk.data(), (size_t)nl * sizeof(int));
+    long long total = in.val<long long>();
+    long long want = 0;
+    for (int i = 0; i < nl; ++i) {
+      const LeafInfo& l = m->bt.leaves[i];
+      if (l.type == 0) want += (long long)l.m * l.n;
+      else if (rk[i] > 0) want += (long long)rk[i] * (l.m + l.n);
+    }
+    if (total != want) throw Error("corrupt stream (payload size)");
+    std::vector<S> payload((size_t)std::max(total, 1LL));
+    in.bytes(payload.data(), (size_t)total * sizeof(S));
+    read_end(in);
+    engine_of(m).load_leaves(rk.data(), payload.data());
+  } catch (const std::exception& e) {
+    fail("read_data", e.what());
+  }
+}
 void u_set_progressbar(hmat_matrix_t*, hmat_progress_t*) {}
 int u_extract_diagonal_block(hmat_matrix_t*, int, void*) { return unsupported("extract_diagonal_block"); }
 
@@ -604,10 +838,10 @@ void fill_table(hmat_interface_t* i) {
   i->walk = u_walk;
   i->apply_on_leaf = u_apply_on_leaf;
   i->internal = nullptr;
-  i->read_struct = u_read_struct;
-  i->write_struct = u_write_struct;
-  i->read_data = u_read_data;
-  i->write_data = u_write_data;
+  i->read_struct = c_read_struct<VT>;
+  i->write_struct = c_write_struct;
+  i->read_data = c_read_data<VT>;
+  i->write_data = c_write_data<VT>;
   i->set_progressbar = u_set_progressbar;
   i->extract_diagonal_block = u_extract_diagonal_block;
 }
@@ -876,6 +1110,7 @@ int hmat_b200_phase_times(hmat_matrix_t* m, double* out4) {
 }
 
 const char* hmat_b200_last_error(void) { return g_last_error.c_str(); }
+void hmat_b200_clear_last_error(void) { g_last_error.clear(); }
 
 }  // extern "C"
 

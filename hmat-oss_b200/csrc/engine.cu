@@ -303,6 +303,108 @@ class Engine : public EngineBase {
     HB_CUDA(cudaGetLastError());
   }
 
+  void load_leaves(const int* rk_in, const void* canonical) override {
+    const auto& L = bt_->leaves;
+    const int nleaves = (int)L.size();
+    for (int i = 0; i < nleaves; ++i) {
+      if (L[i].type == 0 && rk_in[i] != -1) throw Error("stored data: rank given for a full leaf");
+      if (L[i].type == 1 && (rk_in[i] < 0 || rk_in[i] > std::min(L[i].m, L[i].n)))
+        throw Error("stored data: rank out of range");
+    }
+    assembled = false;
+    if (gexec_) {
+      cudaGraphExecDestroy(gexec_);
+      gexec_ = nullptr;
+    }
+    ranks.assign(rk_in, rk_in + nleaves);
+    // the permutations the gemv gathers and scatters with (assemble uploads them with the
+    // points; a loaded matrix has no points)
+    d_perm_rows_.upload(R_->perm, stream_);
+    d_perm_cols_.upload(C_->perm, stream_);
+    std::vector<long long> goff(nleaves);
+    long long total = 0;
+    payload_layout(goff.data(), &total);
+    leaf_off_.assign(nleaves, -1);
+    // full leaves: row panels, as assemble lays them out
+    std::vector<FullLeafDesc> fd;
+    std::vector<long long> fgoff;
+    std::vector<PanelDesc> fpanels;
+    long long pos = 0;
+    for (int i = 0; i < nleaves; ++i) {
+      if (L[i].type != 0 || L[i].m == 0 || L[i].n == 0) continue;
+      FullLeafDesc d{L[i].row_off, L[i].m, L[i].col_off, L[i].n, (int)fpanels.size(), 0};
+      leaf_off_[i] = pos;
+      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
+      for (int b = br.first; b < br.second; ++b) {
+        fpanels.push_back(PanelDesc{rblocks_[b].off - L[i].row_off, rblocks_[b].len, pos});
+        pos += padded((long long)rblocks_[b].len * L[i].n);
+        d.npanel++;
+      }
+      fd.push_back(d);
+      fgoff.push_back(goff[i]);
+    }
+    full_total_ = pad32(pos);
+    // Rk leaves: A row panels then B^T, from the canonical A (m x k) and B (n x k)
+    std::vector<RkLeafDesc> rd;
+    std::vector<int> rk;
+    std::vector<RkStoreDesc> store;
+    std::vector<PanelDesc> panels;
+    long long pe = 0;
+    for (int i = 0; i < nleaves; ++i) {
+      const int k = ranks[i];
+      if (L[i].type != 1 || k <= 0) continue;
+      RkLeafDesc d;
+      d.row_off = L[i].row_off;
+      d.m = L[i].m;
+      d.col_off = L[i].col_off;
+      d.n = L[i].n;
+      d.ws_off = goff[i];
+      d.fl_off = 0;
+      d.kcap = k;
+      d.pad = 0;
+      rd.push_back(d);
+      rk.push_back(k);
+      RkStoreDesc st{(int)panels.size(), 0, 0};
+      leaf_off_[i] = full_total_ + pe;
+      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
+      for (int q = br.first; q < br.second; ++q) {
+        panels.push_back(PanelDesc{rblocks_[q].off - L[i].row_off, rblocks_[q].len, pe});
+        pe += padded((long long)rblocks_[q].len * k);
+        st.npanel++;
+      }
+      st.bt_off = pe;
+      pe += padded((long long)k * L[i].n);
+      store.push_back(st);
+    }
+    arena_.alloc((size_t)(full_total_ + pad32(pe) + 256));
+    arena_elems_ = full_total_ + pad32(pe);
+    DevArray<T> src;
+    src.alloc((size_t)std::max(total, 1LL));
+    if (total) HB_CUDA(cudaMemcpyAsync(src.p, canonical, total * sizeof(T), cudaMemcpyHostToDevice, stream_));
+    DevArray<FullLeafDesc> d_fd;
+    DevArray<long long> d_fgoff;
+    DevArray<PanelDesc> d_fp, d_panels;
+    DevArray<RkLeafDesc> d_rd;
+    DevArray<int> d_rk;
+    DevArray<RkStoreDesc> d_store;
+    d_fd.upload(fd, stream_);
+    d_fgoff.upload(fgoff, stream_);
+    d_fp.upload(fpanels, stream_);
+    d_rd.upload(rd, stream_);
+    d_rk.upload(rk, stream_);
+    d_store.upload(store, stream_);
+    d_panels.upload(panels, stream_);
+    launch_full_from_canonical<T>(d_fd.p, d_fgoff.p, (int)fd.size(), d_fp.p, src.p, arena_.p, stream_);
+    HB_CUDA(cudaGetLastError());
+    launch_compact<T>(d_rd.p, (int)rd.size(), src.p, d_rk.p, d_store.p, d_panels.p, arena_.p + full_total_, stream_);
+    HB_CUDA(cudaGetLastError());
+    HB_CUDA(cudaStreamSynchronize(stream_));
+    build_plan();
+    HB_CUDA(cudaStreamSynchronize(stream_));
+    for (int i = 0; i < 4; ++i) times_ms[i] = 0;
+    assembled = true;
+  }
+
   // HMatrix::truncate (h_matrix.cpp:2107-2123): every Rk leaf re-truncated at eps with the
   // assembly's truncation kernels, then the arena and the gemv schedule rebuilt.
   void retruncate(double eps) override {
@@ -1105,6 +1207,7 @@ class Engine : public EngineBase {
       k.zrow_t = (int)next_row;
       next_row += k.k;
     }
+    if (!d_perm_rows_.p || !d_perm_cols_.p) throw Error("gemv plan: cluster permutations are not on the device");
     plan_.perm_rows = d_perm_rows_.p;
     plan_.perm_cols = d_perm_cols_.p;
     plan_.arena = arena_.p;

@@ -39,6 +39,9 @@ class EngineBase {
   virtual void leaf_gradients(const void* x, const void* r, int nrhs, void* grad, bool accumulate,
                               cudaStream_t user_stream) = 0;
   virtual void retruncate(double eps) = 0;
+  // Loads stored leaves: ranks[i] (-1 for full leaves) and the canonical payload of every
+  // leaf (payload_layout order, host memory); the matrix is then assembled.
+  virtual void load_leaves(const int* ranks_in, const void* canonical) = 0;
   // One eager product on device buffers with events between its phases: device ms of
   // [gather, z-phase, y-phase] and their algorithmic bytes (nrhs <= 16).
   virtual void profile_gemv(char trans, const void* x, void* y, int nrhs, double* ms3, double* bytes3) = 0;

@@ -44,6 +44,10 @@ struct RkStoreDesc {
 template <typename T>
 void launch_assemble_full(const FullLeafDesc* d_leaves, int nleaves, const PanelDesc* panels, const KernelParams& kp,
                           Points pts, T* arena, cudaStream_t s);
+// Full leaves from canonical payloads (m x n column-major at goff[leaf]) into arena panels.
+template <typename T>
+void launch_full_from_canonical(const FullLeafDesc* d_leaves, const long long* goff, int nleaves,
+                                const PanelDesc* panels, const T* src, T* arena, cudaStream_t s);
 
 // ACA+ (compression.cpp:553-724), delegating to partial ACA when n * 100 < m.  Leaves are
 // taken in `order` from a device work counter that must be zero at launch.

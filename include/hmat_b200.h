@@ -437,6 +437,9 @@ int hmat_b200_phase_times(hmat_matrix_t* hmatrix, double* out4);
 
 /* Last error message of the calling thread ("" if none). */
 const char* hmat_b200_last_error(void);
+/* Clears the calling thread's last error (for the table entries that return no status,
+ * such as write_struct / read_data: clear, call, then read hmat_b200_last_error). */
+void hmat_b200_clear_last_error(void);
 
 #ifdef __cplusplus
 }
