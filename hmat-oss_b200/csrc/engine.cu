@@ -105,7 +105,9 @@ class Engine : public EngineBase {
 
   Engine(const ClusterTree* rows, const ClusterTree* cols, const BlockTree* bt) : R_(rows), C_(cols), bt_(bt) {
     HB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    HB_CUDA(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking));
     for (auto& e : ev_) HB_CUDA(cudaEventCreate(&e));
+    for (auto& e : fork_) HB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     ranks.assign(bt_->leaves.size(), -1);
     for (size_t i = 0; i < bt_->leaves.size(); ++i)
       if (bt_->leaves[i].type == 1) ranks[i] = 0;
@@ -119,6 +121,8 @@ class Engine : public EngineBase {
   ~Engine() override {
     if (gexec_) cudaGraphExecDestroy(gexec_);
     for (auto& e : ev_) cudaEventDestroy(e);
+    for (auto& e : fork_) cudaEventDestroy(e);
+    cudaStreamDestroy(stream2_);
     cudaStreamDestroy(stream_);
   }
 
@@ -639,7 +643,7 @@ class Engine : public EngineBase {
     DevArray<int> d_ranks, d_status, d_counter, d_aca_order, d_svd_order;
     d_ranks.alloc(nb);
     d_status.alloc(nb);
-    d_counter.alloc(1);
+    d_counter.alloc(2);
     HB_CUDA(cudaMemsetAsync(d_ranks.p, 0, nb * sizeof(int), stream_));
     HB_CUDA(cudaMemsetAsync(d_status.p, 0, nb * sizeof(int), stream_));
     d_aca_order.upload(aca_order, stream_);
@@ -762,18 +766,24 @@ class Engine : public EngineBase {
                            d_counter.p, d_scratch.p, slab, (int)grid, stream_);
         HB_CUDA(cudaGetLastError());
       }
+      // the two kernels hold disjoint leaves: the small ones run on a second stream beside
+      // the CTA-per-leaf kernel (each with its own work counter)
+      if (!small.empty()) {
+        HB_CUDA(cudaEventRecord(fork_[0], stream_));
+        HB_CUDA(cudaStreamWaitEvent(stream2_, fork_[0], 0));
+        HB_CUDA(cudaMemsetAsync(d_counter.p + 1, 0, sizeof(int), stream2_));
+        launch_truncate_warp<T>(d_desc.p, d_small.p, (int)small.size(), eps_trunc, d_ws.p, d_ranks.p, d_status.p,
+                                d_counter.p + 1, wgrid, stream2_);
+        HB_CUDA(cudaGetLastError());
+        HB_CUDA(cudaEventRecord(fork_[1], stream2_));
+      }
       if (!large.empty()) {
         HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
         launch_truncate<T>(d_desc.p, d_good.p, (int)large.size(), eps_trunc, d_ws.p, d_ranks.p, d_status.p,
                            d_counter.p, d_scratch.p, slab, (int)grid, stream_);
         HB_CUDA(cudaGetLastError());
       }
-      if (!small.empty()) {
-        HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
-        launch_truncate_warp<T>(d_desc.p, d_small.p, (int)small.size(), eps_trunc, d_ws.p, d_ranks.p, d_status.p,
-                                d_counter.p, wgrid, stream_);
-        HB_CUDA(cudaGetLastError());
-      }
+      if (!small.empty()) HB_CUDA(cudaStreamWaitEvent(stream_, fork_[1], 0));
     }
     HB_CUDA(cudaEventRecord(ev_[5], stream_));
     HB_CUDA(cudaMemcpyAsync(h_ranks.data(), d_ranks.p, nb * sizeof(int), cudaMemcpyDeviceToHost, stream_));
@@ -1229,7 +1239,9 @@ class Engine : public EngineBase {
   std::vector<Block> rblocks_, cblocks_;
   std::vector<int> rstarts_, cstarts_;
   cudaStream_t stream_ = nullptr;
+  cudaStream_t stream2_ = nullptr;  // runs the warp-per-leaf truncation beside the CTA kernel
   cudaEvent_t ev_[8];
+  cudaEvent_t fork_[2];
   KernelParams kp_{};
   Points pts_{};
   DevArray<double> d_pts_;

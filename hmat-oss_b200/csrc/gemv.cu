@@ -465,7 +465,8 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
       // slices summed in slice order through the stage just consumed, QC right-hand sides
       // per round: lane's partial of (its row a, q) at sc[(lane * A2 + a) * QC + q - q0]
       constexpr int QC0 = kWarpPieceBytes / (32 * A2 * (int)sizeof(T));
-      constexpr int QC = QC0 < R ? QC0 : R;
+      constexpr int QC1 = QC0 >= 16 ? 16 : (QC0 >= 8 ? 8 : (QC0 >= 4 ? 4 : (QC0 >= 2 ? 2 : 1)));  // power of two
+      constexpr int QC = QC1 < R ? QC1 : R;
       static_assert(QC >= 1 && (R % QC) == 0, "reduction chunk");
       T* sc = reinterpret_cast<T*>(wbase + (size_t)s * kWarpStageBytes);
       if (task.nunits > 0) {
@@ -663,6 +664,8 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 4)
       const float* P = reinterpret_cast<const float*>(wbase + (size_t)s * kWarpStageBytes);
       const float* X = reinterpret_cast<const float*>(wbase + (size_t)s * kWarpStageBytes + kWarpPieceBytes);
       int k0 = 0;
+      // two steps per iteration: their MMA chains are independent and overlap
+#pragma unroll 2
       for (; k0 + 8 <= c; k0 += 8) mma_kstep<R, RS, MT, NT, false>(P, X, k0, c, O, g, tg, mtn, acc);
       if (k0 < c) mma_kstep<R, RS, MT, NT, true>(P, X, k0, c, O, g, tg, mtn, acc);
       __syncwarp();  // every lane is done with stage s
