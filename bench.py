@@ -49,6 +49,17 @@ def workloads():
     return load_module("hmat_workloads", os.path.join(ROOT, "hmat-oss_b200", "workloads.py"))
 
 
+def measured_traffic(phase):
+    """DRAM bytes per launch of a gemv phase's kernel from the committed ncu capture of this
+    workload (profiles/traffic_cylinder100k_mixed.json), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic_cylinder100k_mixed.json")
+    try:
+        d = json.load(open(p))["phases"][phase]
+        return (d["dram_read_mb"] + d["dram_write_mb"]) * 1e6
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -442,7 +453,9 @@ def main():
                        "aca_leaves_per_s": n_rk / ((pt32["aca_ms"] + pt32["truncate_ms"]) * 1e-3),
                        "phase_ms": pt32},
             "roofline": {"bound": "hbm", "kernel": f"gemv {dom}", "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": measured_traffic(dom),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture "
+                                           "(profiles/traffic_cylinder100k_mixed.json)",
                          "phase_ms": ph_ms, "phase_bytes": ph_bytes,
                          "whole_gemv_frac": bytes32 / (ms32 * 1e-3) / 1e9 / peak},
             "mixed_vs_fp64": fp64,
