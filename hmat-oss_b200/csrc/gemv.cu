@@ -858,16 +858,19 @@ void run_all(const GemvPlan& p, int nrhs, T alpha, T beta, const T* x, T* y, T* 
 template <typename T, int RS>
 __global__ void grad_full_kernel(const GemvFullLeaf* __restrict__ full, int nfull, const T* __restrict__ xs,
                                  const T* __restrict__ rs, int R, T* __restrict__ g, bool accumulate) {
+  // warp per column j of a leaf, lanes over its rows: coalesced column writes, no division
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int f = blockIdx.x; f < nfull; f += gridDim.x) {
     const GemvFullLeaf F = full[f];
-    T* dF = g + F.goff;
-    for (int e = threadIdx.x; e < F.m * F.n; e += blockDim.x) {
-      const int i = e % F.m, j = e / F.m;
-      const T* rv = rs + (size_t)(F.row_off + i) * RS;
+    for (int j = warp; j < F.n; j += nw) {
       const T* xv = xs + (size_t)(F.col_off + j) * RS;
-      T acc = accumulate ? dF[e] : zero<T>();
-      for (int q = 0; q < R; ++q) acc = fmadd(rv[q], xv[q], acc);
-      dF[e] = acc;
+      T* dF = g + F.goff + (size_t)j * F.m;
+      for (int i = lane; i < F.m; i += 32) {
+        const T* rv = rs + (size_t)(F.row_off + i) * RS;
+        T acc = accumulate ? dF[i] : zero<T>();
+        for (int q = 0; q < R; ++q) acc = fmadd(rv[q], xv[q], acc);
+        dF[i] = acc;
+      }
     }
   }
 }
@@ -875,27 +878,33 @@ __global__ void grad_full_kernel(const GemvFullLeaf* __restrict__ full, int nful
 template <typename T, int RS>
 __global__ void grad_rk_kernel(const GemvRkLeaf* __restrict__ rk, int nrk, const T* __restrict__ xs,
                                const T* __restrict__ rs, int R, T* __restrict__ g, bool accumulate) {
+  // warp per factor column l, lanes over rows: coalesced column writes, no division
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int t = blockIdx.x; t < nrk; t += gridDim.x) {
     const GemvRkLeaf L = rk[t];
     T* dA = g + L.goff;
     T* dB = dA + (size_t)L.m * L.k;
     // dA[i, l] = sum_q r[i, q] z[l, q],  z = B^T x  (rows zrow_n of the x buffer)
-    for (int e = threadIdx.x; e < L.m * L.k; e += blockDim.x) {
-      const int i = e % L.m, l = e / L.m;
-      const T* rv = rs + (size_t)(L.row_off + i) * RS;
+    for (int l = warp; l < L.k; l += nw) {
       const T* zv = xs + (size_t)(L.zrow_n + l) * RS;
-      T acc = accumulate ? dA[e] : zero<T>();
-      for (int q = 0; q < R; ++q) acc = fmadd(rv[q], zv[q], acc);
-      dA[e] = acc;
+      T* col = dA + (size_t)l * L.m;
+      for (int i = lane; i < L.m; i += 32) {
+        const T* rv = rs + (size_t)(L.row_off + i) * RS;
+        T acc = accumulate ? col[i] : zero<T>();
+        for (int q = 0; q < R; ++q) acc = fmadd(rv[q], zv[q], acc);
+        col[i] = acc;
+      }
     }
     // dB[j, l] = sum_q x[j, q] w[l, q],  w = A^T r  (rows zrow_t of the r buffer)
-    for (int e = threadIdx.x; e < L.n * L.k; e += blockDim.x) {
-      const int j = e % L.n, l = e / L.n;
-      const T* xv = xs + (size_t)(L.col_off + j) * RS;
+    for (int l = warp; l < L.k; l += nw) {
       const T* wv = rs + (size_t)(L.zrow_t + l) * RS;
-      T acc = accumulate ? dB[e] : zero<T>();
-      for (int q = 0; q < R; ++q) acc = fmadd(xv[q], wv[q], acc);
-      dB[e] = acc;
+      T* col = dB + (size_t)l * L.n;
+      for (int j = lane; j < L.n; j += 32) {
+        const T* xv = xs + (size_t)(L.col_off + j) * RS;
+        T acc = accumulate ? col[j] : zero<T>();
+        for (int q = 0; q < R; ++q) acc = fmadd(xv[q], wv[q], acc);
+        col[j] = acc;
+      }
     }
   }
 }
