@@ -721,23 +721,78 @@ class Engine : public EngineBase {
     std::stable_sort(good.begin(), good.end(), [&](int x, int y) { return tcost(x) > tcost(y); });
 
     typedef typename Traits<T>::wide W;
-    DevArray<W> d_scratch;
-    DevArray<int> d_good, d_svd_good, d_small;
-    int wgrid = 0;
+    DevArray<W> d_scratch, d_tri, d_maps;
+    DevArray<int> d_good, d_svd_good;
+    DevArray<TsItem> d_ts_seg[3], d_ts_stack[3];
+    DevArray<TsCore> d_ts_core[3];
     long long slab = 0, grid = 0;
-    std::vector<int> svd_good, small, large;
+    std::vector<int> svd_good, large;
+    std::vector<TsItem> ts_seg[3], ts_stack[3];
+    std::vector<TsCore> ts_core[3];
+    bool any_ts = false;
     if (!good.empty()) {
-      // small leaves go to the warp-per-leaf kernel, the rest to the CTA-per-leaf kernel
+      // Leaves up to rank ts_kmax go to the tall-skinny phases (row segments of A and B
+      // reduced to triangles, stacks of triangles reduced again, core, apply); the others,
+      // and the dense-SVD jobs whose rank is only known on the device, to the CTA-per-leaf
+      // kernel.
       int big_m = 1, big_n = 1, big_k = 1;
+      long long tri_n = 0, map_n = 0;
+      const int kmax = ts_kmax<T>();
       for (int b : good) {
-        if (truncate_warp_eligible<T>(desc[b].m, desc[b].n, h_ranks[b])) {
-          small.push_back(b);
-        } else {
+        const int K = jobs[b].svd ? 0 : ts_bucket(h_ranks[b], kmax);
+        if (!K) {
           large.push_back(b);
           big_m = std::max(big_m, desc[b].m);
           big_n = std::max(big_n, desc[b].n);
           big_k = std::max(big_k, h_ranks[b]);
+          continue;
         }
+        const int q = K == 8 ? 0 : (K == 16 ? 1 : 2);
+        const RkLeafDesc& d = desc[b];
+        TsCore c{};
+        c.leaf = b;
+        c.k = h_ranks[b];
+        for (int side = 0; side < 2; ++side) {
+          const int len = side ? d.n : d.m;
+          const long long base = d.ws_off + (side ? (long long)d.m * d.kcap : 0);
+          const long long fin = tri_n, mo = map_n;
+          tri_n += (long long)K * K;
+          map_n += (long long)K * K;
+          (side ? c.rb : c.ra) = fin;
+          (side ? c.mb : c.ma) = mo;
+          const int p = (len + kTsSegRows - 1) / kTsSegRows;
+          long long stk = 0;
+          if (p > 1) {
+            stk = tri_n;
+            tri_n += (long long)p * K * K;
+          }
+          for (int sg = 0; sg < p; ++sg) {
+            TsItem it{};
+            it.src = base + (long long)sg * kTsSegRows;
+            it.rows = std::min(kTsSegRows, len - sg * kTsSegRows);
+            it.ld = len;
+            it.r_out = p == 1 ? fin : stk + (long long)sg * K;
+            it.ld_r = p == 1 ? K : p * K;
+            it.map = mo;
+            it.leaf = b;
+            it.k = c.k;
+            ts_seg[q].push_back(it);
+          }
+          if (p > 1) {
+            TsItem it{};
+            it.src = stk;
+            it.rows = p * K;
+            it.ld = p * K;
+            it.r_out = fin;
+            it.ld_r = K;
+            it.map = mo;
+            it.leaf = b;
+            it.k = c.k;
+            ts_stack[q].push_back(it);
+          }
+        }
+        ts_core[q].push_back(c);
+        any_ts = true;
       }
       for (int b : good)
         if (jobs[b].svd) svd_good.push_back(b);
@@ -746,15 +801,29 @@ class Engine : public EngineBase {
         big_n = max_n;
         big_k = max_k;
       }
-      slab = truncate_slab_elems<T>(big_m, big_n, big_k);
-      const size_t budget = workspace_budget();
-      grid = std::min<long long>((long long)std::max(large.size(), svd_good.size()), persistent_grid(2));
-      grid = std::max(1LL, std::min<long long>(grid, (long long)(budget / (slab * sizeof(W)))));
-      if (!large.empty() || !svd_good.empty()) d_scratch.alloc((size_t)(grid * slab));
-      if (!small.empty()) wgrid = truncate_warp_grid<T>((int)small.size());
+      if (!large.empty() || !svd_good.empty()) {
+        slab = truncate_slab_elems<T>(big_m, big_n, big_k);
+        const size_t budget = workspace_budget();
+        grid = std::min<long long>((long long)std::max(large.size(), svd_good.size()), persistent_grid(2));
+        grid = std::max(1LL, std::min<long long>(grid, (long long)(budget / (slab * sizeof(W)))));
+        d_scratch.alloc((size_t)(grid * slab));
+      }
+      if (any_ts) {
+        d_tri.alloc((size_t)tri_n);
+        d_maps.alloc((size_t)map_n);
+        for (int q = 0; q < 3; ++q) {
+          // longest segments first: the warps take items in order
+          std::stable_sort(ts_seg[q].begin(), ts_seg[q].end(),
+                           [](const TsItem& x, const TsItem& y) { return x.rows > y.rows; });
+          std::stable_sort(ts_stack[q].begin(), ts_stack[q].end(),
+                           [](const TsItem& x, const TsItem& y) { return x.rows > y.rows; });
+          d_ts_seg[q].upload(ts_seg[q], stream_);
+          d_ts_stack[q].upload(ts_stack[q], stream_);
+          d_ts_core[q].upload(ts_core[q], stream_);
+        }
+      }
       d_svd_good.upload(svd_good, stream_);
       d_good.upload(large, stream_);
-      d_small.upload(small, stream_);
       HB_CUDA(cudaStreamSynchronize(stream_));
     }
     HB_CUDA(cudaEventRecord(ev_[4], stream_));
@@ -766,15 +835,20 @@ class Engine : public EngineBase {
                            d_counter.p, d_scratch.p, slab, (int)grid, stream_);
         HB_CUDA(cudaGetLastError());
       }
-      // the two kernels hold disjoint leaves: the small ones run on a second stream beside
-      // the CTA-per-leaf kernel (each with its own work counter)
-      if (!small.empty()) {
+      // the tall-skinny phases hold leaves disjoint from the CTA kernel's: they run on a
+      // second stream beside it
+      if (any_ts) {
         HB_CUDA(cudaEventRecord(fork_[0], stream_));
         HB_CUDA(cudaStreamWaitEvent(stream2_, fork_[0], 0));
-        HB_CUDA(cudaMemsetAsync(d_counter.p + 1, 0, sizeof(int), stream2_));
-        launch_truncate_warp<T>(d_desc.p, d_small.p, (int)small.size(), eps_trunc, d_ws.p, d_ranks.p, d_status.p,
-                                d_counter.p + 1, wgrid, stream2_);
-        HB_CUDA(cudaGetLastError());
+        for (int q = 0; q < 3; ++q) {
+          const int K = 8 << q;
+          launch_tsqr<T>(K, d_ts_seg[q].p, (int)ts_seg[q].size(), d_ws.p, d_tri.p, false, stream2_);
+          launch_tsqr<T>(K, d_ts_stack[q].p, (int)ts_stack[q].size(), d_ws.p, d_tri.p, true, stream2_);
+          launch_tscore<T>(K, d_ts_core[q].p, (int)ts_core[q].size(), d_tri.p, d_maps.p, d_ranks.p, d_status.p,
+                           eps_trunc, stream2_);
+          launch_tsapply<T>(K, d_ts_seg[q].p, (int)ts_seg[q].size(), d_ws.p, d_maps.p, d_ranks.p, stream2_);
+          HB_CUDA(cudaGetLastError());
+        }
         HB_CUDA(cudaEventRecord(fork_[1], stream2_));
       }
       if (!large.empty()) {
@@ -783,7 +857,7 @@ class Engine : public EngineBase {
                            d_counter.p, d_scratch.p, slab, (int)grid, stream_);
         HB_CUDA(cudaGetLastError());
       }
-      if (!small.empty()) HB_CUDA(cudaStreamWaitEvent(stream_, fork_[1], 0));
+      if (any_ts) HB_CUDA(cudaStreamWaitEvent(stream_, fork_[1], 0));
     }
     HB_CUDA(cudaEventRecord(ev_[5], stream_));
     HB_CUDA(cudaMemcpyAsync(h_ranks.data(), d_ranks.p, nb * sizeof(int), cudaMemcpyDeviceToHost, stream_));
@@ -1239,7 +1313,7 @@ class Engine : public EngineBase {
   std::vector<Block> rblocks_, cblocks_;
   std::vector<int> rstarts_, cstarts_;
   cudaStream_t stream_ = nullptr;
-  cudaStream_t stream2_ = nullptr;  // runs the warp-per-leaf truncation beside the CTA kernel
+  cudaStream_t stream2_ = nullptr;  // runs the tall-skinny truncation beside the CTA kernel
   cudaEvent_t ev_[8];
   cudaEvent_t fork_[2];
   KernelParams kp_{};

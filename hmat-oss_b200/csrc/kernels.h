@@ -91,6 +91,41 @@ template <typename T>
 void launch_compact(const RkLeafDesc* d_leaves, int nleaves, const T* ws, const int* ranks,
                     const RkStoreDesc* store, const PanelDesc* panels, T* arena, cudaStream_t s);
 
+// Tall-skinny truncation (see truncate.cu): the triangular factors of A and B from row
+// segments, the core SVD, and the new factors as A and B times small maps.
+//
+// One row segment of a factor (or one stack of segment triangles), reduced to a K x K
+// triangle by the tsqr phase; the same list drives the apply phase.
+struct TsItem {
+  long long src;    // element offset of the segment's row 0, column 0 (ws, or the triangle buffer)
+  long long r_out;  // element offset (wide) of the output triangle in the triangle buffer
+  long long map;    // element offset (wide) of the factor's K x K map (apply phase)
+  int rows, ld;     // rows of the segment; leading dimension of the source
+  int ld_r;         // leading dimension of the output triangle
+  int leaf, k;      // leaf (rank written by the core phase) and its rank before truncation
+  int pad;
+};
+// One leaf of the core phase: its two K x K triangles and two K x K maps (ld K).
+struct TsCore {
+  long long ra, rb, ma, mb;
+  int leaf, k;
+};
+// Largest rank the tall-skinny path takes, and the rank bucket (8 or 16 real, 8 complex)
+// of rank k (0 when above).
+template <typename T>
+int ts_kmax();
+int ts_bucket(int k, int kmax);
+constexpr int kTsSegRows = 512;  // rows per segment
+template <typename T>
+void launch_tsqr(int K, const TsItem* items, int nitems, const T* ws, typename Traits<T>::wide* tri,
+                 bool from_tri, cudaStream_t s);
+template <typename T>
+void launch_tscore(int K, const TsCore* items, int nitems, const typename Traits<T>::wide* tri,
+                   typename Traits<T>::wide* maps, int* ranks, int* status, double eps, cudaStream_t s);
+template <typename T>
+void launch_tsapply(int K, const TsItem* items, int nitems, T* ws, const typename Traits<T>::wide* maps,
+                    const int* ranks, cudaStream_t s);
+
 // ---- gemv ----
 }  // namespace hmatb200
 #include "gemv_plan.h"

@@ -596,6 +596,376 @@ __global__ void unpack_kernel(const RkLeafDesc* __restrict__ leaves, int nleaves
   }
 }
 
+// ---------------------------------------------------------------------------------
+// Tall-skinny truncation (every Rk leaf of rank <= 16 real / 8 complex that is not a
+// dense-SVD job).
+//
+// Only the triangular factors of the two QRs are formed.  With A = Qa Ra, B = Qb Rb and the
+// core Ra Rb^T = U S V^H (one-sided Jacobi returns W = Ra Rb^T V = U S and V),
+//   A' = Qa U_k' S^1/2       = A (Rb^T V_k' S^-1/2)
+//   B' = Qb conj(V_k') S^1/2 = B (Ra^T conj(U_k') S^-1/2) = B (Ra^T conj(W_k') S^-3/2)
+// since Ra Rb^T V = U S and Rb Ra^T conj(U) = conj(V) S.  The new factors are A and B times
+// k x k' maps and no orthogonal factor is ever applied.  The product A' B'^T is the
+// reference's truncation (rk_matrix.cpp:490-585) up to rounding of order k u sigma_0, and
+// k' comes from the singular values of the same core (findK, scalar_array.cpp:97-115).
+//
+// The triangles come from a communication-avoiding Householder QR: one warp reduces a row
+// segment of a factor (kTsSegRows rows) chunk by chunk, [R; chunk] -> R, the chunk in
+// registers (lane l holds rows l, l + 32, ...) and column c of R in lane c; a factor with
+// several segments stacks the segment triangles and reduces the stack the same way.  The
+// phases (one launch per rank bucket, warp per item):
+//   tsqr (segments) -> tsqr (stacks) -> core (Jacobi, findK, maps) -> apply (A M, B M).
+constexpr int kTsWarps = 4;
+
+__device__ inline double ts_xor(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+__device__ inline cdouble ts_xor(cdouble v, int m) {
+  return cdouble{__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m)};
+}
+
+// Per-warp shared memory of the tsqr phase: the next chunk (raw source scalars, column
+// major, filled by cp.async while the current chunk is reduced), the partial dot products of
+// one Householder step (lane x column), their column sums, and R (row-major, padded).
+template <typename W, typename S, int K, int RPL>
+struct TsqrSmem {
+  S stage[K][32 * RPL];
+  W red[32][K + 1];
+  W sv[32];
+  W R[K][K + 1];
+};
+
+__device__ inline void ts_cp_async(void* dst, const void* src, int bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if (bytes == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+  else if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ inline void ts_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ inline void ts_cp_wait() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Issues the copies of rows [r0, r0 + 32 RPL) x columns [0, k) of an item into the stage;
+// each lane copies the rows it will read.
+template <typename W, typename S, int K, int RPL>
+__device__ __forceinline__ void ts_prefetch(TsqrSmem<W, S, K, RPL>& sm, const S* base, int ld, int rows, int k,
+                                            int r0, int lane) {
+#pragma unroll
+  for (int r = 0; r < RPL; ++r) {
+    const int row = r0 + r * 32 + lane;
+    if (row < rows)
+      for (int j = 0; j < k; ++j) ts_cp_async(&sm.stage[j][r * 32 + lane], base + (size_t)j * ld + row, sizeof(S));
+  }
+  ts_cp_commit();
+}
+
+// Householder step J of [R; chunk] -> R, then the steps after it (J is a compile-time
+// index so the chunk stays in registers).  The partial dot products of the chunk's column J
+// with the columns right of it are summed through shared memory: each lane stores its
+// partials, lane l adds up column J + 1 + (l mod 16) over half of the lanes, one exchange
+// joins the halves.
+template <typename W, typename S, int K, int RPL, int J>
+__device__ __forceinline__ void ts_house(W (&c)[RPL][K], TsqrSmem<W, S, K, RPL>& sm, int lane) {
+  if constexpr (J < K) {
+    constexpr int n = K - 1 - J;
+    double p2 = 0.0;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) p2 += abs2(c[r][J]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) p2 += __shfl_xor_sync(0xffffffffu, p2, off);
+    if (p2 != 0.0) {  // warp-uniform: the butterfly leaves the same sum in every lane
+      const W alpha = sm.R[J][J];
+      const double aa = sqrt_abs2(alpha);
+      const double nrm = sqrt(aa * aa + p2);
+      const W beta = scal(-nrm, phase_of(alpha, aa));
+      const W v0 = alpha - beta;
+      const double t = 2.0 / (p2 + abs2(v0));
+      W rnew[n > 0 ? n : 1];
+      if constexpr (n > 0) {
+#pragma unroll
+        for (int col = J + 1; col < K; ++col) {
+          W s = zero<W>();
+#pragma unroll
+          for (int r = 0; r < RPL; ++r) s = s + conjg(c[r][J]) * c[r][col];
+          sm.red[lane][col] = s;
+        }
+        __syncwarp();
+        if constexpr (n <= 16) {
+          const int q = lane & 15, h = lane >> 4;
+          W s = zero<W>();
+          if (q < n) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) s = s + sm.red[h * 16 + i][J + 1 + q];
+          }
+          s = s + ts_xor(s, 16);
+          if (h == 0 && q < n) sm.sv[q] = s;
+        } else {
+          W s = zero<W>();
+          if (lane < n) {
+#pragma unroll 8
+            for (int i = 0; i < 32; ++i) s = s + sm.red[i][J + 1 + lane];
+            sm.sv[lane] = s;
+          }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int col = J + 1; col < K; ++col) {
+          const W rjc = sm.R[J][col];
+          const W ts = scal(t, sm.sv[col - J - 1] + conjg(v0) * rjc);
+          rnew[col - J - 1] = rjc - ts * v0;
+#pragma unroll
+          for (int r = 0; r < RPL; ++r) c[r][col] = c[r][col] - ts * c[r][J];
+        }
+      }
+      __syncwarp();
+      if (lane == 0) {
+        sm.R[J][J] = beta;
+#pragma unroll
+        for (int col = J + 1; col < K; ++col) sm.R[J][col] = rnew[col - J - 1];
+      }
+      __syncwarp();
+    }
+    ts_house<W, S, K, RPL, J + 1>(c, sm, lane);
+  }
+}
+
+// R (K x K) of the rows of one item, written column-major with leading dimension ld_r.
+// A column whose part below the diagonal is already zero is left as it is (H_j = I, as
+// LAPACK's larfg does for real data).
+template <typename W, typename S, int K, int RPL, int NW>
+__global__ void __launch_bounds__(NW * 32) tsqr_kernel(const TsItem* __restrict__ items, int nitems, const S* src,
+                                                        W* tri) {
+  extern __shared__ __align__(16) unsigned char ts_smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  TsqrSmem<W, S, K, RPL>& sm = reinterpret_cast<TsqrSmem<W, S, K, RPL>*>(ts_smem)[warp];
+  constexpr int CH = 32 * RPL;
+  const int nwarps = gridDim.x * NW;
+  for (int it = blockIdx.x * NW + warp; it < nitems; it += nwarps) {
+    const TsItem d = items[it];
+    const int k = d.k;
+    const S* base = src + d.src;
+    __syncwarp();
+    for (int e = lane; e < K * (K + 1); e += 32) (&sm.R[0][0])[e] = zero<W>();
+    ts_prefetch(sm, base, d.ld, d.rows, k, 0, lane);
+    __syncwarp();
+    for (int r0 = 0; r0 < d.rows; r0 += CH) {
+      ts_cp_wait();  // each lane reads back only the elements it copied
+      W c[RPL][K];
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        const int row = r0 + r * 32 + lane;
+#pragma unroll
+        for (int j = 0; j < K; ++j) c[r][j] = (row < d.rows && j < k) ? widen(sm.stage[j][r * 32 + lane]) : zero<W>();
+      }
+      __syncwarp();  // the stage is read before the next copies overwrite it
+      if (r0 + CH < d.rows) ts_prefetch(sm, base, d.ld, d.rows, k, r0 + CH, lane);
+      ts_house<W, S, K, RPL, 0>(c, sm, lane);
+    }
+    __syncwarp();
+    W* out = tri + d.r_out;
+    for (int e = lane; e < K * K; e += 32) {
+      const int i = e % K, cc = e / K;
+      out[(size_t)cc * d.ld_r + i] = sm.R[i][cc];
+    }
+  }
+}
+
+// Core of one leaf: W = Ra Rb^T V by one-sided Jacobi (the circle schedule of the other
+// truncation kernels), k', and the two maps (K x K, rows >= k and columns >= k' zero).
+template <typename W, int K, int NW>
+__global__ void __launch_bounds__(NW * 32) tscore_kernel(const TsCore* __restrict__ items, int nitems,
+                                                          const W* __restrict__ tri, W* __restrict__ maps,
+                                                          int* ranks, int* status, double eps) {
+  __shared__ W s_ra[NW][K * K];
+  __shared__ W s_rb[NW][K * K];
+  __shared__ signed char s_partner[NW][K][32];
+  __shared__ int s_ord[NW][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  W* Ra = s_ra[warp];
+  W* Rb = s_rb[warp];
+  int* ord = s_ord[warp];
+  const int nwarps = gridDim.x * NW;
+  for (int it = blockIdx.x * NW + warp; it < nitems; it += nwarps) {
+    const TsCore d = items[it];
+    const int k = d.k;
+    __syncwarp();
+    for (int e = lane; e < K * K; e += 32) {
+      Ra[e] = tri[d.ra + e];
+      Rb[e] = tri[d.rb + e];
+    }
+    __syncwarp();
+    // lane j: column j of Ra Rb^T (rows < k), and of V = I
+    W w[K], v[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      W s = zero<W>();
+      if (lane < k && i < k)
+        for (int l = max(i, lane); l < k; ++l) s = s + Ra[i + l * K] * Rb[lane + l * K];
+      w[i] = s;
+      v[i] = (i == lane) ? one<W>() : zero<W>();
+    }
+    const int kk = (k + 1) & ~1;
+    if (lane < kk)
+      for (int round = 0; round < kk - 1; ++round) {
+        int partner = -1;
+        for (int pr = 0; pr < kk / 2; ++pr) {
+          const int a = pr == 0 ? 0 : 1 + (pr - 1 + round) % (kk - 1);
+          const int b = 1 + (kk - 2 - pr + round) % (kk - 1);
+          if (a == lane) partner = b;
+          if (b == lane) partner = a;
+        }
+        s_partner[warp][round][lane] = (signed char)partner;
+      }
+    __syncwarp();
+    bool conv = false;
+    for (int sweep = 0; sweep < kJacobiMaxSweeps && !conv; ++sweep) {
+      bool rot = false;
+      for (int round = 0; round < kk - 1; ++round) {
+        const int partner = lane < kk ? (int)s_partner[warp][round][lane] : -1;
+        const int src = partner < 0 ? lane : partner;
+        W pw[K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) pw[i] = wt_shfl(w[i], src);
+        const bool pair = partner >= 0 && lane < k && partner < k;
+        const bool is_p = lane < partner;
+        double n_own = 0.0, n_oth = 0.0;
+        W g_own = zero<W>();
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+          n_own += abs2(w[i]);
+          n_oth += abs2(pw[i]);
+          g_own = g_own + conjg(w[i]) * pw[i];
+        }
+        const W g_p = wt_shfl(g_own, src);
+        const double al = is_p ? n_own : n_oth, be = is_p ? n_oth : n_own;
+        const W g = is_p ? g_own : g_p;
+        const double ag = sqrt(abs2(g));
+        const bool do_rot = pair && !(ag == 0.0 || ag <= 1e-15 * sqrt(al * be));
+        rot |= do_rot;
+        double cs = 1.0, sn = 0.0;
+        W phc = one<W>();
+        if (do_rot) {
+          const W ph = scal(1.0 / ag, g);
+          const double zeta = (be - al) / (2.0 * ag);
+          const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          cs = 1.0 / sqrt(1.0 + tt * tt);
+          sn = cs * tt;
+          phc = conjg(ph);
+#pragma unroll
+          for (int i = 0; i < K; ++i) {
+            const W x = is_p ? w[i] : pw[i];
+            const W y = (is_p ? pw[i] : w[i]) * phc;
+            w[i] = is_p ? scal(cs, x) - scal(sn, y) : scal(sn, x) + scal(cs, y);
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < K; ++i) pw[i] = wt_shfl(v[i], src);
+        if (do_rot) {
+#pragma unroll
+          for (int i = 0; i < K; ++i) {
+            const W x = is_p ? v[i] : pw[i];
+            const W y = (is_p ? pw[i] : v[i]) * phc;
+            v[i] = is_p ? scal(cs, x) - scal(sn, y) : scal(sn, x) + scal(cs, y);
+          }
+        }
+      }
+      conv = !__any_sync(0xffffffffu, rot);
+    }
+    double sg = 0.0;
+#pragma unroll
+    for (int i = 0; i < K; ++i) sg += abs2(w[i]);
+    sg = sqrt(sg);
+    int rnk = 0;
+    for (int i = 0; i < k; ++i) {
+      const double si = __shfl_sync(0xffffffffu, sg, i);
+      rnk += (si > sg) || (si == sg && i < lane);
+    }
+    if (lane < k) ord[rnk] = lane;
+    __syncwarp();
+    int nk = 0;
+    {
+      const double thr = __shfl_sync(0xffffffffu, sg, ord[0]) * eps;
+      while (nk < k && !(__shfl_sync(0xffffffffu, sg, ord[nk]) <= thr)) nk++;
+    }
+    // Ma[:, c] = Rb^T V[:, o] / sqrt(s_o), Mb[:, c] = Ra^T conj(W[:, o]) / s_o^3/2 (lane = row)
+    for (int c = 0; c < K; ++c) {
+      W ma = zero<W>(), mb = zero<W>();
+      if (c < nk) {
+        const int o = ord[c];
+        const double so = __shfl_sync(0xffffffffu, sg, o);
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+          const W vl = wt_shfl(v[l], o), wl = wt_shfl(w[l], o);
+          if (lane < k && l <= lane) {
+            ma = ma + Rb[l + lane * K] * vl;
+            mb = mb + Ra[l + lane * K] * conjg(wl);
+          }
+        }
+        const double rs = 1.0 / sqrt(so);
+        ma = scal(rs, ma);
+        mb = scal(rs / so, mb);
+      }
+      if (lane < K) {
+        maps[d.ma + (size_t)c * K + lane] = ma;
+        maps[d.mb + (size_t)c * K + lane] = mb;
+      }
+    }
+    if (lane == 0) {
+      ranks[d.leaf] = nk;
+      if (!conv && status[d.leaf] == kLeafOk) status[d.leaf] = kLeafSvdNoConverge;
+    }
+  }
+}
+
+// New factor columns in place: rows of the segment times the K x K map, the first k'
+// columns written back narrowed.
+template <typename T, typename W, int K, int RPL>
+__global__ void __launch_bounds__(kTsWarps * 32) tsapply_kernel(const TsItem* __restrict__ items, int nitems,
+                                                                 T* ws, const W* __restrict__ maps,
+                                                                 const int* __restrict__ ranks) {
+  __shared__ W s_map[kTsWarps][K * K];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  W* M = s_map[warp];
+  const int nwarps = gridDim.x * kTsWarps;
+  for (int it = blockIdx.x * kTsWarps + warp; it < nitems; it += nwarps) {
+    const TsItem d = items[it];
+    const int k = d.k, nk = ranks[d.leaf];
+    if (nk <= 0) continue;
+    __syncwarp();
+    for (int e = lane; e < K * K; e += 32) M[e] = maps[d.map + e];
+    __syncwarp();
+    T* base = ws + d.src;
+    for (int r0 = 0; r0 < d.rows; r0 += 32 * RPL) {
+      W a[RPL][K];
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        const int row = r0 + r * 32 + lane;
+#pragma unroll
+        for (int l = 0; l < K; ++l)
+          a[r][l] = (row < d.rows && l < k) ? widen(base[(size_t)l * d.ld + row]) : zero<W>();
+      }
+#pragma unroll
+      for (int c = 0; c < K; ++c) {
+        if (c >= nk) break;
+        W o[RPL];
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) o[r] = zero<W>();
+#pragma unroll
+        for (int l = 0; l < K; ++l) {
+          const W mlc = M[l + c * K];
+#pragma unroll
+          for (int r = 0; r < RPL; ++r) o[r] = o[r] + a[r][l] * mlc;
+        }
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) {
+          const int row = r0 + r * 32 + lane;
+          if (row < d.rows) base[(size_t)c * d.ld + row] = narrow<T>(o[r]);
+        }
+      }
+    }
+  }
+}
+
 }  // namespace
 
 template <typename T>
@@ -659,6 +1029,119 @@ void launch_compact(const RkLeafDesc* d_leaves, int nleaves, const T* ws, const 
   compact_kernel<T><<<nleaves, 256, 0, s>>>(d_leaves, nleaves, ws, ranks, store, panels, arena);
 }
 
+template <typename T>
+int ts_kmax() {
+  return Traits<T>::is_complex ? 16 : 32;
+}
+int ts_bucket(int k, int kmax) {
+  if (k <= 0 || k > kmax) return 0;
+  return k <= 8 ? 8 : (k <= 16 ? 16 : 32);
+}
+
+// Grid of a warp-per-item launch: the resident CTAs of `kernel`, at most one warp per item.
+template <typename F>
+static int ts_grid(F kernel, int nitems, int warps = kTsWarps, size_t smem = 0) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, warps * 32, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const int need = (nitems + warps - 1) / warps;
+  const int g = persistent_grid(per_sm);
+  return g < need ? g : need;
+}
+
+// Rows per lane of a tsqr chunk and of an apply chunk: the chunk is RPL x K wide scalars
+// in each lane's registers.
+template <typename W, int K>
+struct TsShape {
+  static constexpr int words = sizeof(W) / 8;
+  // the chunk in registers: 64 doubles a lane
+  static constexpr int qr = 64 / (K * words) < 1 ? 1 : 64 / (K * words);
+  static constexpr int ap = 32 / (K * words) < 1 ? 1 : 32 / (K * words);
+  // warps per CTA of the core phase (its two triangles sit in shared memory)
+  static constexpr int core_warps = K * K * words * 16 * 4 <= 40 * 1024 ? 4 : 2;
+};
+
+template <typename W, typename S, int K>
+static void tsqr_run(const TsItem* items, int n, const S* src, W* tri, cudaStream_t s) {
+  constexpr int RPL = TsShape<W, K>::qr;
+  constexpr size_t per_warp = sizeof(TsqrSmem<W, S, K, RPL>);
+  constexpr int NW = per_warp * 4 <= 64 * 1024 ? 4 : 2;
+  constexpr size_t smem = per_warp * NW;
+  auto kern = tsqr_kernel<W, S, K, RPL, NW>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  kern<<<ts_grid(kern, n, NW, smem), NW * 32, smem, s>>>(items, n, src, tri);
+}
+
+template <typename T, int K>
+static void tsqr_k(const TsItem* items, int n, const T* ws, typename Traits<T>::wide* tri, bool from_tri,
+                   cudaStream_t s) {
+  typedef typename Traits<T>::wide W;
+  if (from_tri)
+    tsqr_run<W, W, K>(items, n, tri, tri, s);
+  else
+    tsqr_run<W, T, K>(items, n, ws, tri, s);
+}
+
+template <typename T>
+void launch_tsqr(int K, const TsItem* items, int nitems, const T* ws, typename Traits<T>::wide* tri,
+                 bool from_tri, cudaStream_t s) {
+  if (nitems <= 0) return;
+  if (K == 8)
+    tsqr_k<T, 8>(items, nitems, ws, tri, from_tri, s);
+  else if (K == 16)
+    tsqr_k<T, 16>(items, nitems, ws, tri, from_tri, s);
+  else if constexpr (!Traits<T>::is_complex) {
+    if (K == 32) tsqr_k<T, 32>(items, nitems, ws, tri, from_tri, s);
+  }
+}
+
+template <typename T, int K>
+static void tscore_k(const TsCore* items, int n, const typename Traits<T>::wide* tri,
+                     typename Traits<T>::wide* maps, int* ranks, int* status, double eps, cudaStream_t s) {
+  typedef typename Traits<T>::wide W;
+  constexpr int NW = TsShape<W, K>::core_warps;
+  auto kern = tscore_kernel<W, K, NW>;
+  kern<<<ts_grid(kern, n, NW), NW * 32, 0, s>>>(items, n, tri, maps, ranks, status, eps);
+}
+
+template <typename T>
+void launch_tscore(int K, const TsCore* items, int nitems, const typename Traits<T>::wide* tri,
+                   typename Traits<T>::wide* maps, int* ranks, int* status, double eps, cudaStream_t s) {
+  if (nitems <= 0) return;
+  if (K == 8)
+    tscore_k<T, 8>(items, nitems, tri, maps, ranks, status, eps, s);
+  else if (K == 16)
+    tscore_k<T, 16>(items, nitems, tri, maps, ranks, status, eps, s);
+  else if constexpr (!Traits<T>::is_complex) {
+    if (K == 32) tscore_k<T, 32>(items, nitems, tri, maps, ranks, status, eps, s);
+  }
+}
+
+template <typename T, int K>
+static void tsapply_k(const TsItem* items, int n, T* ws, const typename Traits<T>::wide* maps, const int* ranks,
+                      cudaStream_t s) {
+  typedef typename Traits<T>::wide W;
+  auto kern = tsapply_kernel<T, W, K, TsShape<W, K>::ap>;
+  kern<<<ts_grid(kern, n), kTsWarps * 32, 0, s>>>(items, n, ws, maps, ranks);
+}
+
+template <typename T>
+void launch_tsapply(int K, const TsItem* items, int nitems, T* ws, const typename Traits<T>::wide* maps,
+                    const int* ranks, cudaStream_t s) {
+  if (nitems <= 0) return;
+  if (K == 8)
+    tsapply_k<T, 8>(items, nitems, ws, maps, ranks, s);
+  else if (K == 16)
+    tsapply_k<T, 16>(items, nitems, ws, maps, ranks, s);
+  else if constexpr (!Traits<T>::is_complex) {
+    if (K == 32) tsapply_k<T, 32>(items, nitems, ws, maps, ranks, s);
+  }
+}
+
 #define HB_INST(T)                                                                                         \
   template long long truncate_slab_elems<T>(int, int, int);                                               \
   template void launch_truncate<T>(const RkLeafDesc*, const int*, int, double, T*, int*, int*, int*,     \
@@ -670,7 +1153,14 @@ void launch_compact(const RkLeafDesc* d_leaves, int nleaves, const T* ws, const 
                                  const T*, T*, cudaStream_t);                                             \
   template int truncate_warp_grid<T>(int);                                                                 \
   template void launch_truncate_warp<T>(const RkLeafDesc*, const int*, int, double, T*, int*, int*, int*,   \
-                                        int, cudaStream_t);
+                                        int, cudaStream_t);                                                \
+  template int ts_kmax<T>();                                                                               \
+  template void launch_tsqr<T>(int, const TsItem*, int, const T*, typename Traits<T>::wide*, bool,         \
+                               cudaStream_t);                                                              \
+  template void launch_tscore<T>(int, const TsCore*, int, const typename Traits<T>::wide*,                 \
+                                 typename Traits<T>::wide*, int*, int*, double, cudaStream_t);             \
+  template void launch_tsapply<T>(int, const TsItem*, int, T*, const typename Traits<T>::wide*, const int*, \
+                                  cudaStream_t);
 HB_INST(float)
 HB_INST(double)
 HB_INST(cfloat)
