@@ -770,64 +770,84 @@ __global__ void __launch_bounds__(NW * 32) tsqr_kernel(const TsItem* __restrict_
   }
 }
 
-// Core of one leaf: W = Ra Rb^T V by one-sided Jacobi (the circle schedule of the other
-// truncation kernels), k', and the two maps (K x K, rows >= k and columns >= k' zero).
+// Core of a leaf: W = Ra Rb^T V by one-sided Jacobi (the circle schedule of the other
+// truncation kernels), k', and the two maps (K x K, rows >= k and columns >= k' zero).  A
+// leaf takes K lanes (lane j of the group holds column j of W and of V), so a warp holds
+// 32 / K leaves; every shuffle is executed by the whole warp with width K, and a group whose
+// leaf has converged (or that has no leaf) computes along without rotating.
+__device__ inline double wt_shfl_w(double v, int src, int w) { return __shfl_sync(0xffffffffu, v, src, w); }
+__device__ inline cdouble wt_shfl_w(cdouble v, int src, int w) {
+  return cdouble{__shfl_sync(0xffffffffu, v.x, src, w), __shfl_sync(0xffffffffu, v.y, src, w)};
+}
+
 template <typename W, int K, int NW>
 __global__ void __launch_bounds__(NW * 32) tscore_kernel(const TsCore* __restrict__ items, int nitems,
                                                           const W* __restrict__ tri, W* __restrict__ maps,
                                                           int* ranks, int* status, double eps) {
-  __shared__ W s_ra[NW][K * K];
-  __shared__ W s_rb[NW][K * K];
+  constexpr int G = 32 / K;  // leaves per warp
+  __shared__ W s_ra[NW][G][K * K];
+  __shared__ W s_rb[NW][G][K * K];
   __shared__ signed char s_partner[NW][K][32];
   __shared__ int s_ord[NW][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  W* Ra = s_ra[warp];
-  W* Rb = s_rb[warp];
-  int* ord = s_ord[warp];
+  const int grp = lane / K, j = lane % K;  // leaf slot in the warp, column in the leaf
+  W* Ra = s_ra[warp][grp];
+  W* Rb = s_rb[warp][grp];
+  int* ord = s_ord[warp] + grp * K;
   const int nwarps = gridDim.x * NW;
-  for (int it = blockIdx.x * NW + warp; it < nitems; it += nwarps) {
-    const TsCore d = items[it];
-    const int k = d.k;
+  for (int base = (blockIdx.x * NW + warp) * G; base < nitems; base += nwarps * G) {
+    const int it = base + grp;
+    const bool live = it < nitems;
+    TsCore d{};
+    if (live) d = items[it];
+    const int k = live ? d.k : 0;
     __syncwarp();
-    for (int e = lane; e < K * K; e += 32) {
-      Ra[e] = tri[d.ra + e];
-      Rb[e] = tri[d.rb + e];
-    }
-    __syncwarp();
-    // lane j: column j of Ra Rb^T (rows < k), and of V = I
-    W w[K], v[K];
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-      W s = zero<W>();
-      if (lane < k && i < k)
-        for (int l = max(i, lane); l < k; ++l) s = s + Ra[i + l * K] * Rb[lane + l * K];
-      w[i] = s;
-      v[i] = (i == lane) ? one<W>() : zero<W>();
-    }
+    if (live)
+      for (int e = j; e < K * K; e += K) {
+        Ra[e] = tri[d.ra + e];
+        Rb[e] = tri[d.rb + e];
+      }
+    // the circle schedule of this leaf's rank (player 0 fixed, the others rotate)
     const int kk = (k + 1) & ~1;
-    if (lane < kk)
+    if (j < kk)
       for (int round = 0; round < kk - 1; ++round) {
         int partner = -1;
         for (int pr = 0; pr < kk / 2; ++pr) {
           const int a = pr == 0 ? 0 : 1 + (pr - 1 + round) % (kk - 1);
           const int b = 1 + (kk - 2 - pr + round) % (kk - 1);
-          if (a == lane) partner = b;
-          if (b == lane) partner = a;
+          if (a == j) partner = b;
+          if (b == j) partner = a;
         }
         s_partner[warp][round][lane] = (signed char)partner;
       }
     __syncwarp();
+    // column j of Ra Rb^T (rows < k), and of V = I
+    W w[K], v[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      W s = zero<W>();
+      if (j < k && i < k)
+        for (int l = max(i, j); l < k; ++l) s = s + Ra[i + l * K] * Rb[j + l * K];
+      w[i] = s;
+      v[i] = (i == j) ? one<W>() : zero<W>();
+    }
+    // rounds of the warp: the largest schedule among its leaves
+    int rounds = kk - 1;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) rounds = max(rounds, __shfl_xor_sync(0xffffffffu, rounds, off));
     bool conv = false;
-    for (int sweep = 0; sweep < kJacobiMaxSweeps && !conv; ++sweep) {
+    for (int sweep = 0; sweep < kJacobiMaxSweeps; ++sweep) {
       bool rot = false;
-      for (int round = 0; round < kk - 1; ++round) {
-        const int partner = lane < kk ? (int)s_partner[warp][round][lane] : -1;
-        const int src = partner < 0 ? lane : partner;
+      for (int round = 0; round < rounds; ++round) {
+        const int partner = (j < kk && round < kk - 1) ? (int)s_partner[warp][round][lane] : -1;
+        const int src = partner < 0 ? j : partner;
         W pw[K];
 #pragma unroll
-        for (int i = 0; i < K; ++i) pw[i] = wt_shfl(w[i], src);
-        const bool pair = partner >= 0 && lane < k && partner < k;
-        const bool is_p = lane < partner;
+        for (int i = 0; i < K; ++i) pw[i] = wt_shfl_w(w[i], src, K);
+        const bool pair = partner >= 0 && j < k && partner < k;
+        const bool is_p = j < partner;
+        // both lanes of a pair sum the same squares in the same order; <p, q> is formed on
+        // the p lane and sent to the q lane, so both rotate with identical coefficients
         double n_own = 0.0, n_oth = 0.0;
         W g_own = zero<W>();
 #pragma unroll
@@ -836,11 +856,11 @@ __global__ void __launch_bounds__(NW * 32) tscore_kernel(const TsCore* __restric
           n_oth += abs2(pw[i]);
           g_own = g_own + conjg(w[i]) * pw[i];
         }
-        const W g_p = wt_shfl(g_own, src);
+        const W g_p = wt_shfl_w(g_own, src, K);
         const double al = is_p ? n_own : n_oth, be = is_p ? n_oth : n_own;
         const W g = is_p ? g_own : g_p;
         const double ag = sqrt(abs2(g));
-        const bool do_rot = pair && !(ag == 0.0 || ag <= 1e-15 * sqrt(al * be));
+        const bool do_rot = pair && !conv && !(ag == 0.0 || ag <= 1e-15 * sqrt(al * be));
         rot |= do_rot;
         double cs = 1.0, sn = 0.0;
         W phc = one<W>();
@@ -859,7 +879,7 @@ __global__ void __launch_bounds__(NW * 32) tscore_kernel(const TsCore* __restric
           }
         }
 #pragma unroll
-        for (int i = 0; i < K; ++i) pw[i] = wt_shfl(v[i], src);
+        for (int i = 0; i < K; ++i) pw[i] = wt_shfl_w(v[i], src, K);
         if (do_rot) {
 #pragma unroll
           for (int i = 0; i < K; ++i) {
@@ -869,48 +889,60 @@ __global__ void __launch_bounds__(NW * 32) tscore_kernel(const TsCore* __restric
           }
         }
       }
-      conv = !__any_sync(0xffffffffu, rot);
+      // this leaf has converged when its group made no rotation in a whole sweep
+      const unsigned gmask = (K == 32 ? 0xffffffffu : ((1u << K) - 1u)) << (grp * K);
+      const unsigned any = __ballot_sync(0xffffffffu, rot);
+      if (!(any & gmask)) conv = true;
+      if (__all_sync(0xffffffffu, conv)) break;
     }
+    // singular values (column norms), descending order with ties by index
     double sg = 0.0;
 #pragma unroll
     for (int i = 0; i < K; ++i) sg += abs2(w[i]);
     sg = sqrt(sg);
     int rnk = 0;
-    for (int i = 0; i < k; ++i) {
-      const double si = __shfl_sync(0xffffffffu, sg, i);
-      rnk += (si > sg) || (si == sg && i < lane);
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+      const double si = __shfl_sync(0xffffffffu, sg, i, K);
+      if (i < k) rnk += (si > sg) || (si == sg && i < j);
     }
-    if (lane < k) ord[rnk] = lane;
+    if (j < k) ord[rnk] = j;
     __syncwarp();
     int nk = 0;
     {
-      const double thr = __shfl_sync(0xffffffffu, sg, ord[0]) * eps;
-      while (nk < k && !(__shfl_sync(0xffffffffu, sg, ord[nk]) <= thr)) nk++;
+      const double thr = __shfl_sync(0xffffffffu, sg, k > 0 ? ord[0] : j, K) * eps;
+      bool run = true;
+#pragma unroll
+      for (int i = 0; i < K; ++i) {
+        const double si = __shfl_sync(0xffffffffu, sg, i < k ? ord[i] : j, K);
+        run = run && i < k && !(si <= thr);
+        nk += run ? 1 : 0;
+      }
     }
     // Ma[:, c] = Rb^T V[:, o] / sqrt(s_o), Mb[:, c] = Ra^T conj(W[:, o]) / s_o^3/2 (lane = row)
     for (int c = 0; c < K; ++c) {
+      const int o = c < nk ? ord[c] : j;
+      const double so = __shfl_sync(0xffffffffu, sg, o, K);
       W ma = zero<W>(), mb = zero<W>();
-      if (c < nk) {
-        const int o = ord[c];
-        const double so = __shfl_sync(0xffffffffu, sg, o);
 #pragma unroll
-        for (int l = 0; l < K; ++l) {
-          const W vl = wt_shfl(v[l], o), wl = wt_shfl(w[l], o);
-          if (lane < k && l <= lane) {
-            ma = ma + Rb[l + lane * K] * vl;
-            mb = mb + Ra[l + lane * K] * conjg(wl);
-          }
+      for (int l = 0; l < K; ++l) {
+        const W vl = wt_shfl_w(v[l], o, K), wl = wt_shfl_w(w[l], o, K);
+        if (c < nk && j < k && l <= j) {
+          ma = ma + Rb[l + j * K] * vl;
+          mb = mb + Ra[l + j * K] * conjg(wl);
         }
+      }
+      if (c < nk) {
         const double rs = 1.0 / sqrt(so);
         ma = scal(rs, ma);
         mb = scal(rs / so, mb);
       }
-      if (lane < K) {
-        maps[d.ma + (size_t)c * K + lane] = ma;
-        maps[d.mb + (size_t)c * K + lane] = mb;
+      if (live) {
+        maps[d.ma + (size_t)c * K + j] = ma;
+        maps[d.mb + (size_t)c * K + j] = mb;
       }
     }
-    if (lane == 0) {
+    if (live && j == 0) {
       ranks[d.leaf] = nk;
       if (!conv && status[d.leaf] == kLeafOk) status[d.leaf] = kLeafSvdNoConverge;
     }
@@ -1057,8 +1089,8 @@ struct TsShape {
   // the chunk in registers: 64 doubles a lane
   static constexpr int qr = 64 / (K * words) < 1 ? 1 : 64 / (K * words);
   static constexpr int ap = 32 / (K * words) < 1 ? 1 : 32 / (K * words);
-  // warps per CTA of the core phase (its two triangles sit in shared memory)
-  static constexpr int core_warps = K * K * words * 16 * 4 <= 40 * 1024 ? 4 : 2;
+  // warps per CTA of the core phase (the triangles of its 32 / K leaves sit in shared memory)
+  static constexpr int core_warps = (32 / K) * K * K * words * 16 * 4 <= 40 * 1024 ? 4 : 2;
 };
 
 template <typename W, typename S, int K>
