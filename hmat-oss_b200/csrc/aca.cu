@@ -414,7 +414,15 @@ void launch_aca(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, con
                                              status, counter, kcap_max);
 }
 
+template <typename T>
+void preload_aca_kernels() {
+  cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, aca_kernel<T>);
+  cudaFuncGetAttributes(&a, dense_to_rk_kernel<T>);
+}
+
 #define HB_INST(T)                                                                                           \
+  template void preload_aca_kernels<T>();                                                                  \
   template void launch_aca<T>(const RkLeafDesc*, const int*, int, const KernelParams&, Points, double, T*, \
                               unsigned char*, int*, int*, int*, int, int, cudaStream_t);                    \
   template void launch_dense_to_rk<T>(const RkLeafDesc*, const int*, int, const KernelParams&, Points, T*, \

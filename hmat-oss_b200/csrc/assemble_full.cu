@@ -67,7 +67,15 @@ void launch_full_from_canonical(const FullLeafDesc* d_leaves, const long long* g
   full_from_canonical_kernel<T><<<grid, 256, 0, s>>>(d_leaves, goff, nleaves, panels, src, arena);
 }
 
+template <typename T>
+void preload_full_kernels() {
+  cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, assemble_full_kernel<T>);
+  cudaFuncGetAttributes(&a, full_from_canonical_kernel<T>);
+}
+
 #define HB_INST(T)                                                                                      \
+  template void preload_full_kernels<T>();                                                              \
   template void launch_assemble_full<T>(const FullLeafDesc*, int, const PanelDesc*, const KernelParams&, \
                                         Points, T*, cudaStream_t);                                       \
   template void launch_full_from_canonical<T>(const FullLeafDesc*, const long long*, int, const PanelDesc*, \

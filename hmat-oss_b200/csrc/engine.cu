@@ -117,6 +117,10 @@ class Engine : public EngineBase {
     for (auto& b : cblocks_) cstarts_.push_back(b.off);
     err_.alloc(1);
     HB_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
+    preload_full_kernels<T>();
+    preload_aca_kernels<T>();
+    preload_truncate_kernels<T>();
+    HB_CUDA(cudaGetLastError());
   }
   ~Engine() override {
     if (gexec_) cudaGraphExecDestroy(gexec_);

@@ -72,21 +72,13 @@ void launch_truncate(const RkLeafDesc* d_leaves, const int* d_order, int nleaves
 template <typename T>
 long long truncate_slab_elems(int max_m, int max_n, int max_k);
 
-// Copies the truncated factors of each leaf from its workspace slot into the arena:
-// A as row panels, B transposed.
 // Arena panels of assembled Rk leaves back into workspace slots (inverse of launch_compact).
 template <typename T>
 void launch_unpack(const RkLeafDesc* d_leaves, int nleaves, const int* ranks, const RkStoreDesc* store,
                    const PanelDesc* panels, const T* arena, T* ws, cudaStream_t s);
 
-// Warp-per-leaf truncation of small leaves (see truncate.cu) and its eligibility rule.
-template <typename T>
-bool truncate_warp_eligible(int m, int n, int k);
-template <typename T>
-int truncate_warp_grid(int nleaves);
-template <typename T>
-void launch_truncate_warp(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, double epsilon, T* ws,
-                          int* ranks, int* status, int* counter, int grid, cudaStream_t s);
+// Copies the truncated factors of each leaf from its workspace slot into the arena:
+// A as row panels, B transposed.
 template <typename T>
 void launch_compact(const RkLeafDesc* d_leaves, int nleaves, const T* ws, const int* ranks,
                     const RkStoreDesc* store, const PanelDesc* panels, T* arena, cudaStream_t s);
@@ -110,8 +102,8 @@ struct TsCore {
   long long ra, rb, ma, mb;
   int leaf, k;
 };
-// Largest rank the tall-skinny path takes, and the rank bucket (8 or 16 real, 8 complex)
-// of rank k (0 when above).
+// Largest rank the tall-skinny path takes (32 real, 16 complex), and the rank bucket
+// (8, 16 or 32) of rank k (0 when above the largest).
 template <typename T>
 int ts_kmax();
 int ts_bucket(int k, int kmax);
@@ -151,6 +143,14 @@ int warp_stream_warps_per_cta();
 template <typename T>
 void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* rz, T* gfull, T* grk,
                            bool accumulate, int* err, cudaStream_t s);
+
+// Load the assembly kernels of the storage type T ahead of the first assembly.
+template <typename T>
+void preload_aca_kernels();
+template <typename T>
+void preload_full_kernels();
+template <typename T>
+void preload_truncate_kernels();
 
 // Grid size of a persistent launch: a multiple of the SM count.
 int persistent_grid(int blocks_per_sm);

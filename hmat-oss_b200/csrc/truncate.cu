@@ -254,291 +254,6 @@ __global__ void __launch_bounds__(kTruncThreads) truncate_kernel(const RkLeafDes
   }
 }
 
-// ---------------------------------------------------------------------------------
-// Warp-per-leaf truncation for the common small leaves (rank <= 16 real / 8 complex,
-// m, n <= 128, working set within the warp's shared slab): the same Householder QR,
-// circle-schedule one-sided Jacobi, findK and back-transformation as truncate_kernel, run by
-// one warp with the Householder vectors in a per-warp shared-memory slab and the k x k core
-// in registers (lane j holds column j of the core and of V).  Many leaves are in flight per
-// SM and no block-wide barrier is taken.
-constexpr int kWtWarps = 2;                 // warps (leaves) per CTA
-constexpr int kWtSlabBytes = 24 * 1024;     // shared memory per warp
-constexpr int kWtMaxLen = 128;              // m, n <= 128
-
-template <typename W>
-__host__ __device__ constexpr int wt_kmax() {
-  return sizeof(W) == 8 ? 16 : 8;
-}
-__host__ __device__ inline long long wt_slab_need(long long m, long long n, long long k) {
-  // Wa, Wb, Ra, Rb, tau_a, tau_b, one output column
-  return (m + n) * k + 2 * k * k + 2 * k + (m > n ? m : n);
-}
-
-__device__ inline double wt_shfl(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
-__device__ inline cdouble wt_shfl(cdouble v, int src) {
-  return cdouble{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
-}
-template <typename W>
-__device__ inline W wt_allsum(W v) {
-  v = warp_sum(v);
-  return warp_bcast(v);
-}
-
-// Householder QR of X (len x k, ld = len) by one warp; same arithmetic as householder_qr.
-template <typename W>
-__device__ void warp_qr(W* X, int len, int k, W* tau, W* R) {
-  const int lane = threadIdx.x & 31;
-  for (int j = 0; j < k; ++j) {
-    W* x = X + (size_t)j * len;
-    double nrm2 = 0.0;
-    for (int i = j + lane; i < len; i += 32) nrm2 += abs2(x[i]);
-    nrm2 = wt_allsum(nrm2);
-    const double nrm = sqrt(nrm2);
-    const W alpha = x[j];
-    const double aa = sqrt_abs2(alpha);
-    W beta = scal(-nrm, phase_of(alpha, aa));
-    W t = zero<W>();
-    if (nrm > 0.0) {
-      W v0 = alpha - beta;
-      double vn2 = nrm2 - aa * aa + abs2(v0);
-      t = vn2 > 0.0 ? scal(2.0 / vn2, one<W>()) : zero<W>();
-      __syncwarp();
-      if (lane == 0) x[j] = v0;
-      __syncwarp();
-    } else {
-      beta = zero<W>();
-    }
-    if (lane == 0) {
-      tau[j] = t;
-      R[j + (size_t)j * k] = beta;
-      for (int i = j + 1; i < k; ++i) R[i + (size_t)j * k] = zero<W>();
-    }
-    // H_j applied to the columns right of j, two at a time (independent reductions)
-    int c = j + 1;
-    for (; c + 1 < k; c += 2) {
-      W* y0 = X + (size_t)c * len;
-      W* y1 = y0 + len;
-      W s0 = zero<W>(), s1 = zero<W>();
-      if (nrm > 0.0)
-        for (int i = j + lane; i < len; i += 32) {
-          const W cx = conjg(x[i]);
-          s0 = s0 + cx * y0[i];
-          s1 = s1 + cx * y1[i];
-        }
-      s0 = wt_allsum(s0);
-      s1 = wt_allsum(s1);
-      const W t0 = t * s0, t1 = t * s1;
-      if (nrm > 0.0)
-        for (int i = j + lane; i < len; i += 32) {
-          y0[i] = y0[i] - t0 * x[i];
-          y1[i] = y1[i] - t1 * x[i];
-        }
-      __syncwarp();
-      if (lane == 0) {
-        R[j + (size_t)c * k] = y0[j];
-        R[j + (size_t)(c + 1) * k] = y1[j];
-      }
-    }
-    if (c < k) {
-      W* y = X + (size_t)c * len;
-      W s0 = zero<W>();
-      if (nrm > 0.0)
-        for (int i = j + lane; i < len; i += 32) s0 = s0 + conjg(x[i]) * y[i];
-      s0 = wt_allsum(s0);
-      const W t0 = t * s0;
-      if (nrm > 0.0)
-        for (int i = j + lane; i < len; i += 32) y[i] = y[i] - t0 * x[i];
-      __syncwarp();
-      if (lane == 0) R[j + (size_t)c * k] = y[j];
-    }
-    __syncwarp();
-  }
-}
-
-// out = H_0 ... H_{k-1} y for one column y (len, in the slab; rows >= k start at zero),
-// written narrowed.
-template <typename T, typename W>
-__device__ void warp_apply_q_store(const W* X, int len, int k, const W* tau, W* y, T* out) {
-  const int lane = threadIdx.x & 31;
-  for (int h = k - 1; h >= 0; --h) {
-    const W* v = X + (size_t)h * len;
-    W s = zero<W>();
-    for (int i = h + lane; i < len; i += 32) s = s + conjg(v[i]) * y[i];
-    s = wt_allsum(s);
-    const W ts = tau[h] * s;
-    for (int i = h + lane; i < len; i += 32) y[i] = y[i] - ts * v[i];
-    __syncwarp();
-  }
-  for (int i = lane; i < len; i += 32) out[i] = narrow<T>(y[i]);
-  __syncwarp();
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kWtWarps * 32) truncate_warp_kernel(const RkLeafDesc* __restrict__ leaves,
-                                                                      const int* __restrict__ order, int nleaves,
-                                                                      double eps, T* ws, int* ranks, int* status,
-                                                                      int* counter) {
-  typedef typename Traits<T>::wide W;
-  constexpr int KM = wt_kmax<W>();
-  extern __shared__ __align__(16) unsigned char wt_smem[];
-  __shared__ int s_ord[kWtWarps][32];
-  __shared__ signed char s_partner[kWtWarps][32][32];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  W* const slab = reinterpret_cast<W*>(wt_smem + (size_t)warp * kWtSlabBytes);
-  int* ord = s_ord[warp];
-  for (;;) {
-    int item = 0;
-    if (lane == 0) item = atomicAdd(counter, 1);
-    item = __shfl_sync(0xffffffffu, item, 0);
-    if (item >= nleaves) break;
-    const int leaf = order[item];
-    const RkLeafDesc d = leaves[leaf];
-    const int m = d.m, n = d.n, k = ranks[leaf];
-    if (k <= 0) continue;
-    T* A = ws + d.ws_off;
-    T* B = A + (size_t)m * d.kcap;
-    W* Wa = slab;
-    W* Wb = Wa + (size_t)m * k;
-    W* Ra = Wb + (size_t)n * k;
-    W* Rb = Ra + (size_t)k * k;
-    W* tau_a = Rb + (size_t)k * k;
-    W* tau_b = tau_a + k;
-    W* ycol = tau_b + k;
-    for (int e = lane; e < m * k; e += 32) Wa[e] = widen(A[e]);
-    for (int e = lane; e < n * k; e += 32) Wb[e] = widen(B[e]);
-    __syncwarp();
-    warp_qr(Wa, m, k, tau_a, Ra);
-    warp_qr(Wb, n, k, tau_b, Rb);
-    __syncwarp();
-    // core Rm = Ra Rb^T: lane j holds column j (rows < k); V = I
-    W w[KM], v[KM];
-#pragma unroll
-    for (int i = 0; i < KM; ++i) {
-      W sacc = zero<W>();
-      if (lane < k && i < k)
-        for (int l = max(i, lane); l < k; ++l) sacc = sacc + Ra[i + (size_t)l * k] * Rb[lane + (size_t)l * k];
-      w[i] = sacc;
-      v[i] = (i == lane) ? one<W>() : zero<W>();
-    }
-    // one-sided Jacobi, circle schedule (player 0 fixed, the others rotate); the partner
-    // of every player in every round is tabulated once per leaf
-    const int kk = (k + 1) & ~1;
-    if (lane < kk)
-      for (int round = 0; round < kk - 1; ++round) {
-        int partner = -1;
-        for (int pr = 0; pr < kk / 2; ++pr) {
-          const int a = pr == 0 ? 0 : 1 + (pr - 1 + round) % (kk - 1);
-          const int b = 1 + (kk - 2 - pr + round) % (kk - 1);
-          if (a == lane) partner = b;
-          if (b == lane) partner = a;
-        }
-        s_partner[warp][round][lane] = (signed char)partner;
-      }
-    __syncwarp();
-    bool conv = false;
-    for (int sweep = 0; sweep < kJacobiMaxSweeps && !conv; ++sweep) {
-      bool rot = false;
-      for (int round = 0; round < kk - 1; ++round) {
-        const int partner = lane < kk ? (int)s_partner[warp][round][lane] : -1;
-        const int src = partner < 0 ? lane : partner;
-        W pw[KM];
-#pragma unroll
-        for (int i = 0; i < KM; ++i) pw[i] = wt_shfl(w[i], src);
-        const bool pair = partner >= 0 && lane < k && partner < k;
-        const bool is_p = lane < partner;
-        // both lanes of a pair sum the same squares in the same order; <p, q> is formed on
-        // the p lane and sent to the q lane, so both rotate with identical coefficients
-        double n_own = 0.0, n_oth = 0.0;
-        W g_own = zero<W>();
-#pragma unroll
-        for (int i = 0; i < KM; ++i) {
-          n_own += abs2(w[i]);
-          n_oth += abs2(pw[i]);
-          g_own = g_own + conjg(w[i]) * pw[i];
-        }
-        const W g_p = wt_shfl(g_own, src);
-        const double al = is_p ? n_own : n_oth, be = is_p ? n_oth : n_own;
-        const W g = is_p ? g_own : g_p;
-        const double ag = sqrt(abs2(g));
-        const bool do_rot = pair && !(ag == 0.0 || ag <= 1e-15 * sqrt(al * be));
-        rot |= do_rot;
-        double cs = 1.0, sn = 0.0;
-        W phc = one<W>();
-        if (do_rot) {
-          const W ph = scal(1.0 / ag, g);
-          const double zeta = (be - al) / (2.0 * ag);
-          const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-          cs = 1.0 / sqrt(1.0 + t * t);
-          sn = cs * t;
-          phc = conjg(ph);
-        }
-        if (do_rot) {
-#pragma unroll
-          for (int i = 0; i < KM; ++i) {
-            const W x = is_p ? w[i] : pw[i];
-            const W y = (is_p ? pw[i] : w[i]) * phc;
-            w[i] = is_p ? scal(cs, x) - scal(sn, y) : scal(sn, x) + scal(cs, y);
-          }
-        }
-#pragma unroll
-        for (int i = 0; i < KM; ++i) pw[i] = wt_shfl(v[i], src);
-        if (do_rot) {
-#pragma unroll
-          for (int i = 0; i < KM; ++i) {
-            const W x = is_p ? v[i] : pw[i];
-            const W y = (is_p ? pw[i] : v[i]) * phc;
-            v[i] = is_p ? scal(cs, x) - scal(sn, y) : scal(sn, x) + scal(cs, y);
-          }
-        }
-      }
-      conv = !__any_sync(0xffffffffu, rot);
-    }
-    // singular values (column norms), descending order with ties by index
-    double sg = 0.0;
-#pragma unroll
-    for (int i = 0; i < KM; ++i) sg += abs2(w[i]);
-    sg = sqrt(sg);
-    int rnk = 0;
-    for (int i = 0; i < k; ++i) {
-      const double si = __shfl_sync(0xffffffffu, sg, i);
-      rnk += (si > sg) || (si == sg && i < lane);
-    }
-    if (lane < k) ord[rnk] = lane;
-    __syncwarp();
-    int nk = 0;
-    {
-      const double thr = __shfl_sync(0xffffffffu, sg, ord[0]) * eps;
-      while (nk < k && !(__shfl_sync(0xffffffffu, sg, ord[nk]) <= thr)) nk++;
-    }
-    // A' = Qa [U_k' sqrt(S); 0], B' = Qb [conj(V_k') sqrt(S); 0], one column at a time
-    for (int c = 0; c < nk; ++c) {
-      const int o = ord[c];
-      const double sc = __shfl_sync(0xffffffffu, sg, o);
-      W ya = zero<W>(), yb = zero<W>();
-#pragma unroll
-      for (int i = 0; i < KM; ++i) {
-        const W wi = wt_shfl(w[i], o);
-        const W vi = wt_shfl(v[i], o);
-        if (lane == i && i < k) {
-          ya = sc > 0.0 ? scal(1.0 / sqrt(sc), wi) : zero<W>();
-          yb = scal(sqrt(sc), conjg(vi));
-        }
-      }
-      for (int i = lane; i < m; i += 32) ycol[i] = i < 32 ? ya : zero<W>();
-      __syncwarp();
-      warp_apply_q_store<T>(Wa, m, k, tau_a, ycol, A + (size_t)c * m);
-      for (int i = lane; i < n; i += 32) ycol[i] = i < 32 ? yb : zero<W>();
-      __syncwarp();
-      warp_apply_q_store<T>(Wb, n, k, tau_b, ycol, B + (size_t)c * n);
-    }
-    __syncwarp();
-    if (lane == 0) {
-      ranks[leaf] = nk;
-      if (!conv && status[leaf] == kLeafOk) status[leaf] = kLeafSvdNoConverge;
-    }
-  }
-}
-
 // Writes A as row panels (len x k column-major each) and B transposed (k x n column-major).
 template <typename T>
 __global__ void compact_kernel(const RkLeafDesc* __restrict__ leaves, int nleaves, const T* __restrict__ ws,
@@ -1025,36 +740,6 @@ void launch_unpack(const RkLeafDesc* d_leaves, int nleaves, const int* ranks, co
 }
 
 template <typename T>
-bool truncate_warp_eligible(int m, int n, int k) {
-  typedef typename Traits<T>::wide W;
-  return k <= wt_kmax<W>() && m <= kWtMaxLen && n <= kWtMaxLen &&
-         wt_slab_need(m, n, k) * (long long)sizeof(W) <= kWtSlabBytes;
-}
-
-template <typename T>
-int truncate_warp_grid(int nleaves) {
-  const int smem = kWtWarps * kWtSlabBytes;
-  const int per_sm = (226 * 1024) / (smem + 1024);
-  int grid = persistent_grid(per_sm < 1 ? 1 : per_sm);
-  const int need = (nleaves + kWtWarps - 1) / kWtWarps;
-  return grid > need ? need : grid;
-}
-
-template <typename T>
-void launch_truncate_warp(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, double epsilon, T* ws,
-                          int* ranks, int* status, int* counter, int grid, cudaStream_t s) {
-  if (nleaves <= 0) return;
-  const int smem = kWtWarps * kWtSlabBytes;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(truncate_warp_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    attr = true;
-  }
-  truncate_warp_kernel<T><<<grid, kWtWarps * 32, smem, s>>>(d_leaves, d_order, nleaves, epsilon, ws, ranks,
-                                                            status, counter);
-}
-
-template <typename T>
 void launch_compact(const RkLeafDesc* d_leaves, int nleaves, const T* ws, const int* ranks,
                     const RkStoreDesc* store, const PanelDesc* panels, T* arena, cudaStream_t s) {
   if (nleaves <= 0) return;
@@ -1105,6 +790,7 @@ static void tsqr_run(const TsItem* items, int n, const S* src, W* tri, cudaStrea
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = true;
   }
+  if (n <= 0) return;
   kern<<<ts_grid(kern, n, NW, smem), NW * 32, smem, s>>>(items, n, src, tri);
 }
 
@@ -1121,8 +807,7 @@ static void tsqr_k(const TsItem* items, int n, const T* ws, typename Traits<T>::
 template <typename T>
 void launch_tsqr(int K, const TsItem* items, int nitems, const T* ws, typename Traits<T>::wide* tri,
                  bool from_tri, cudaStream_t s) {
-  if (nitems <= 0) return;
-  if (K == 8)
+    if (K == 8)
     tsqr_k<T, 8>(items, nitems, ws, tri, from_tri, s);
   else if (K == 16)
     tsqr_k<T, 16>(items, nitems, ws, tri, from_tri, s);
@@ -1137,14 +822,18 @@ static void tscore_k(const TsCore* items, int n, const typename Traits<T>::wide*
   typedef typename Traits<T>::wide W;
   constexpr int NW = TsShape<W, K>::core_warps;
   auto kern = tscore_kernel<W, K, NW>;
+  if (n <= 0) {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, kern);
+    return;
+  }
   kern<<<ts_grid(kern, n, NW), NW * 32, 0, s>>>(items, n, tri, maps, ranks, status, eps);
 }
 
 template <typename T>
 void launch_tscore(int K, const TsCore* items, int nitems, const typename Traits<T>::wide* tri,
                    typename Traits<T>::wide* maps, int* ranks, int* status, double eps, cudaStream_t s) {
-  if (nitems <= 0) return;
-  if (K == 8)
+    if (K == 8)
     tscore_k<T, 8>(items, nitems, tri, maps, ranks, status, eps, s);
   else if (K == 16)
     tscore_k<T, 16>(items, nitems, tri, maps, ranks, status, eps, s);
@@ -1158,19 +847,41 @@ static void tsapply_k(const TsItem* items, int n, T* ws, const typename Traits<T
                       cudaStream_t s) {
   typedef typename Traits<T>::wide W;
   auto kern = tsapply_kernel<T, W, K, TsShape<W, K>::ap>;
+  if (n <= 0) {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, kern);
+    return;
+  }
   kern<<<ts_grid(kern, n), kTsWarps * 32, 0, s>>>(items, n, ws, maps, ranks);
 }
 
 template <typename T>
 void launch_tsapply(int K, const TsItem* items, int nitems, T* ws, const typename Traits<T>::wide* maps,
                     const int* ranks, cudaStream_t s) {
-  if (nitems <= 0) return;
-  if (K == 8)
+    if (K == 8)
     tsapply_k<T, 8>(items, nitems, ws, maps, ranks, s);
   else if (K == 16)
     tsapply_k<T, 16>(items, nitems, ws, maps, ranks, s);
   else if constexpr (!Traits<T>::is_complex) {
     if (K == 32) tsapply_k<T, 32>(items, nitems, ws, maps, ranks, s);
+  }
+}
+
+// Loads every truncation kernel of the storage type T (the CUDA runtime otherwise loads a
+// kernel at its first launch, inside the first assembly).
+template <typename T>
+void preload_truncate_kernels() {
+  typedef typename Traits<T>::wide W;
+  cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, truncate_kernel<T>);
+  cudaFuncGetAttributes(&a, compact_kernel<T>);
+  cudaFuncGetAttributes(&a, unpack_kernel<T>);
+  const int kmax = ts_kmax<T>();
+  for (int K = 8; K <= kmax; K *= 2) {
+    launch_tsqr<T>(K, nullptr, 0, nullptr, nullptr, false, 0);
+    launch_tsqr<T>(K, nullptr, 0, nullptr, nullptr, true, 0);
+    launch_tscore<T>(K, nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0.0, 0);
+    launch_tsapply<T>(K, nullptr, 0, nullptr, nullptr, nullptr, 0);
   }
 }
 
@@ -1180,12 +891,9 @@ void launch_tsapply(int K, const TsItem* items, int nitems, T* ws, const typenam
                                    typename Traits<T>::wide*, long long, int, cudaStream_t);               \
   template void launch_compact<T>(const RkLeafDesc*, int, const T*, const int*, const RkStoreDesc*,        \
                                   const PanelDesc*, T*, cudaStream_t);                                    \
-  template bool truncate_warp_eligible<T>(int, int, int);                                                  \
   template void launch_unpack<T>(const RkLeafDesc*, int, const int*, const RkStoreDesc*, const PanelDesc*,  \
                                  const T*, T*, cudaStream_t);                                             \
-  template int truncate_warp_grid<T>(int);                                                                 \
-  template void launch_truncate_warp<T>(const RkLeafDesc*, const int*, int, double, T*, int*, int*, int*,   \
-                                        int, cudaStream_t);                                                \
+  template void preload_truncate_kernels<T>();                                                            \
   template int ts_kmax<T>();                                                                               \
   template void launch_tsqr<T>(int, const TsItem*, int, const T*, typename Traits<T>::wide*, bool,         \
                                cudaStream_t);                                                              \
