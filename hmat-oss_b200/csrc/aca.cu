@@ -39,16 +39,46 @@ struct Aca {
 
   __device__ T entry(int i, int j) const { return KernelEval<T>::eval(kp, P, row_off + i, col_off + j); }
 
+  // out[e] = K(e) - sum_{l<k} coef[l] X[e, l] over len entries: each thread takes four
+  // entries at a time (blockDim apart) and issues their factor loads together; every entry
+  // is still updated in increasing l.
+  template <typename F>
+  __device__ void fill(F eval, const T* X, int len, int k, T* out) {
+    constexpr int E = 4;
+    const int nt = blockDim.x;
+    for (int e0 = threadIdx.x; e0 < len; e0 += E * nt) {
+      T v[E];
+#pragma unroll
+      for (int q = 0; q < E; ++q) v[q] = e0 + q * nt < len ? eval(e0 + q * nt) : zero<T>();
+      int l = 0;
+      for (; l + 4 <= k; l += 4) {
+        T x[4][E];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int q = 0; q < E; ++q)
+            x[u][q] = e0 + q * nt < len ? X[(size_t)(l + u) * len + e0 + q * nt] : zero<T>();
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int q = 0; q < E; ++q) v[q] = upd(coef[l + u], x[u][q], v[q]);
+      }
+      for (; l < k; ++l) {
+#pragma unroll
+        for (int q = 0; q < E; ++q)
+          if (e0 + q * nt < len) v[q] = upd(coef[l], X[(size_t)l * len + e0 + q * nt], v[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < E; ++q)
+        if (e0 + q * nt < len) out[e0 + q * nt] = v[q];
+    }
+  }
   // out[j] = K(i, j) - sum_{l<k} A[i, l] B[j, l]   (getRow + updateRow)
   __device__ void fill_row(int i, int k, T* out) {
     __syncthreads();
     for (int l = threadIdx.x; l < k; l += blockDim.x) coef[l] = -A[(size_t)l * m + i];
     __syncthreads();
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
-      T v = entry(i, j);
-      for (int l = 0; l < k; ++l) v = upd(coef[l], B[(size_t)l * n + j], v);
-      out[j] = v;
-    }
+    fill([&](int j) { return entry(i, j); }, B, n, k, out);
     __syncthreads();
   }
   // out[i] = K(i, j) - sum_{l<k} B[j, l] A[i, l]   (getCol + updateCol)
@@ -56,11 +86,7 @@ struct Aca {
     __syncthreads();
     for (int l = threadIdx.x; l < k; l += blockDim.x) coef[l] = -B[(size_t)l * n + j];
     __syncthreads();
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
-      T v = entry(i, j);
-      for (int l = 0; l < k; ++l) v = upd(coef[l], A[(size_t)l * m + i], v);
-      out[i] = v;
-    }
+    fill([&](int i) { return entry(i, j); }, A, m, k, out);
     __syncthreads();
   }
   __device__ void scale(T* v, int len, T s) {
@@ -342,6 +368,296 @@ __global__ void __launch_bounds__(kAcaThreads) aca_kernel(const RkLeafDesc* __re
   }
 }
 
+// ---------------------------------------------------------------------------------
+// Warp-per-leaf ACA+ for small leaves (m, n <= 64, the plus path): the control flow, pivot
+// rules and per-element arithmetic of Aca::plus, run by one warp without block barriers.
+// Lane l owns rows l and l + 32 of the new column and of the reference column, and columns
+// l and l + 32 of the new row and of the reference row; the factors grow in the warp's
+// shared memory (column-major, kAwLen rows a column) and go to the slot at the end.  The
+// free-row / free-column flags are 64-bit masks held by every lane.  Pivot searches keep
+// the first-index rules, and the FP64 Gram terms are summed per lane over rows lane,
+// lane + 32 and then by warp_sum, as in the CTA kernel, so both kernels build the same
+// factors.
+constexpr int kAwWarps = 4;
+constexpr int kAwLen = 64;
+
+__device__ inline float aw_shfl(float v, int s) { return __shfl_sync(0xffffffffu, v, s); }
+__device__ inline double aw_shfl(double v, int s) { return __shfl_sync(0xffffffffu, v, s); }
+__device__ inline cfloat aw_shfl(cfloat v, int s) {
+  return cfloat{__shfl_sync(0xffffffffu, v.x, s), __shfl_sync(0xffffffffu, v.y, s)};
+}
+__device__ inline cdouble aw_shfl(cdouble v, int s) {
+  return cdouble{__shfl_sync(0xffffffffu, v.x, s), __shfl_sync(0xffffffffu, v.y, s)};
+}
+__device__ inline unsigned long long aw_mask(int len) { return len >= 64 ? ~0ull : ((1ull << len) - 1ull); }
+
+template <typename T>
+struct AcaWarp {
+  typedef typename Traits<T>::wide W;
+  KernelParams kp;
+  Points P;
+  int row_off, m, col_off, n, kc;
+  T* sA;  // [kc][kAwLen]
+  T* sB;  // [kc][kAwLen]
+  unsigned long long rowFree, colFree;
+  int lane;
+
+  __device__ T entry(int i, int j) const { return KernelEval<T>::eval(kp, P, row_off + i, col_off + j); }
+  // element idx of a lane-distributed vector, in every lane
+  __device__ T get(const T (&v)[2], int idx) const {
+    const T mine = (idx >> 5) ? v[1] : v[0];
+    return aw_shfl(mine, idx & 31);
+  }
+  // out = K(i, :) - sum_{l<k} A[i, l] B[:, l]   (getRow + updateRow)
+  __device__ void fill_row(int i, int k, T (&out)[2]) const {
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int j = lane + 32 * r;
+      T v = zero<T>();
+      if (j < n) {
+        v = entry(i, j);
+        for (int l = 0; l < k; ++l) v = upd(-sA[l * kAwLen + i], sB[l * kAwLen + j], v);
+      }
+      out[r] = v;
+    }
+  }
+  // out = K(:, j) - sum_{l<k} B[j, l] A[:, l]   (getCol + updateCol)
+  __device__ void fill_col(int j, int k, T (&out)[2]) const {
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int i = lane + 32 * r;
+      T v = zero<T>();
+      if (i < m) {
+        v = entry(i, j);
+        for (int l = 0; l < k; ++l) v = upd(-sB[l * kAwLen + j], sA[l * kAwLen + i], v);
+      }
+      out[r] = v;
+    }
+  }
+  __device__ bool nonzero(const T (&v)[2], int len) const {
+    const bool nz = (lane < len && !is_zero_val(v[0])) || (lane + 32 < len && !is_zero_val(v[1]));
+    return __any_sync(0xffffffffu, nz);
+  }
+  __device__ int bcast_idx(KeyIdx b) const { return __shfl_sync(0xffffffffu, b.idx, 0); }
+  __device__ int iamax(const T (&v)[2], int len) const {
+    KeyIdx b{-1.0, -1};
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int e = lane + 32 * r;
+      if (e < len) {
+        const double kk = amax_key(v[r]);
+        if (kk > b.key) {
+          b.key = kk;
+          b.idx = e;
+        }
+      }
+    }
+    return bcast_idx(warp_arg<true>(b));
+  }
+  // first index of the strict minimum of |v|^2 over free entries (DBL_MAX start)
+  __device__ int argmin_free(const T (&v)[2], unsigned long long fr, int len) const {
+    KeyIdx b{DBL_MAX, -1};
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int e = lane + 32 * r;
+      if (e < len && ((fr >> e) & 1ull)) {
+        const double kk = abs2(v[r]);
+        if (kk < b.key) {
+          b.key = kk;
+          b.idx = e;
+        }
+      }
+    }
+    return bcast_idx(warp_arg<false>(b));
+  }
+  __device__ int find_col(T (&out)[2]) {
+    for (int j = 0; j < n; ++j) {
+      if ((colFree >> j) & 1ull) {
+        fill_col(j, 0, out);
+        colFree &= ~(1ull << j);
+        if (nonzero(out, m)) return j;
+      }
+    }
+    return -1;
+  }
+  __device__ int find_min_row(int k, const T (&ref)[2], T (&out)[2]) {
+    for (;;) {
+      const int i = argmin_free(ref, rowFree, m);
+      if (i < 0) return -1;
+      fill_row(i, k, out);
+      rowFree &= ~(1ull << i);
+      if (nonzero(out, n)) return i;
+    }
+  }
+  __device__ int find_min_col(int k, const T (&ref)[2], T (&out)[2]) {
+    for (;;) {
+      const int j = argmin_free(ref, colFree, n);
+      if (j < 0) return -1;
+      fill_col(j, k, out);
+      colFree &= ~(1ull << j);
+      if (nonzero(out, m)) return j;
+    }
+  }
+  // <x, y> over len entries of two stored columns: per-lane rows lane, lane + 32, then warp_sum
+  __device__ W dot(const T* x, const T* y, int len) const {
+    W acc = zero<W>();
+    for (int e = lane; e < len; e += 32) acc = acc + widen(conjg(x[e])) * widen(y[e]);
+    return warp_bcast(warp_sum(acc));
+  }
+  // Gram terms of the new pair (a_k, b_k), as Aca::update_estimate.
+  __device__ double update_estimate(int k, double& est) const {
+    const T* a = sA + k * kAwLen;
+    const T* b = sB + k * kAwLen;
+    double ne = 0.0;
+    for (int l = 0; l < k; ++l) {
+      const W da = dot(a, sA + l * kAwLen, m);
+      const W db = dot(b, sB + l * kAwLen, n);
+      ne += real_part(da * db);
+    }
+    const double na = real_part(dot(a, a, m)), nb = real_part(dot(b, b, n));
+    est += 2.0 * ne;
+    const double ab = na * nb;
+    est += ab;
+    return ab;
+  }
+  __device__ void store(T* col, const T (&v)[2], int len) const {
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+      if (lane + 32 * r < len) col[lane + 32 * r] = v[r];
+  }
+
+  __device__ int plus(double eps, bool* overflow) {
+    const int maxK = min(m, n);
+    rowFree = aw_mask(m);
+    colFree = aw_mask(n);
+    T aRef[2], bRef[2];
+    double est = 0.0;
+    int k = 0;
+    int j_ref = find_col(aRef);
+    if (j_ref < 0) return 0;
+    int i_ref = find_min_row(0, aRef, bRef);
+    if (i_ref < 0) return 0;
+    do {
+      if (k >= kc) {
+        *overflow = true;
+        break;
+      }
+      int i_star = iamax(aRef, m), j_star = iamax(bRef, n);
+      if (i_star < 0 || j_star < 0) break;  // no ordered entry (NaN data): stop, never index with -1
+      T aVec[2], bVec[2];
+      if (abs2(get(aRef, i_star)) > abs2(get(bRef, j_star))) {
+        fill_row(i_star, k, bVec);
+        j_star = iamax(bVec, n);
+        if (j_star < 0) break;
+        const T pivot = get(bVec, j_star);
+        fill_col(j_star, k, aVec);
+        if (!is_zero_val(pivot)) {
+          const T s = recip(pivot);
+          aVec[0] = mul_rn(aVec[0], s);
+          aVec[1] = mul_rn(aVec[1], s);
+        }
+      } else {
+        fill_col(j_star, k, aVec);
+        i_star = iamax(aVec, m);
+        if (i_star < 0) break;
+        const T pivot = get(aVec, i_star);
+        fill_row(i_star, k, bVec);
+        if (!is_zero_val(pivot)) {
+          const T s = recip(pivot);
+          bVec[0] = mul_rn(bVec[0], s);
+          bVec[1] = mul_rn(bVec[1], s);
+        }
+      }
+      store(sA + k * kAwLen, aVec, m);
+      store(sB + k * kAwLen, bVec, n);
+      __syncwarp();
+      rowFree &= ~(1ull << i_star);
+      colFree &= ~(1ull << j_star);
+      const double ab = update_estimate(k, est);
+      k++;
+      if (ab < eps * eps * est) break;
+
+      // aRef -= b_k[j_ref] a_k ; bRef -= a_k[i_ref] b_k
+      const T ca = -get(bVec, j_ref);
+      const T cb = -get(aVec, i_ref);
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        if (lane + 32 * r < m) aRef[r] = upd(ca, aVec[r], aRef[r]);
+        if (lane + 32 * r < n) bRef[r] = upd(cb, bVec[r], bRef[r]);
+      }
+      const bool needNewA = (j_star == j_ref) || !nonzero(aRef, m);
+      const bool needNewB = (i_star == i_ref) || !nonzero(bRef, n);
+      if (needNewA && needNewB) {
+        bool found = false;
+        while (!found) {
+          j_ref = find_col(aRef);
+          if (j_ref < 0) break;
+          fill_col(j_ref, k, aRef);
+          found = nonzero(aRef, m);
+        }
+        if (!found) break;
+        i_ref = find_min_row(k, aRef, bRef);
+        if (i_ref < 0) break;
+      } else if (needNewB) {
+        i_ref = find_min_row(k, aRef, bRef);
+        if (i_ref < 0) break;
+      } else if (needNewA) {
+        j_ref = find_min_col(k, bRef, aRef);
+        if (j_ref < 0) break;
+      }
+    } while (k < maxK);
+    return k;
+  }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kAwWarps * 32) aca_warp_kernel(const RkLeafDesc* __restrict__ leaves,
+                                                                 const int* __restrict__ order, int nleaves,
+                                                                 KernelParams kp, Points pts, double eps, T* ws,
+                                                                 int* ranks, int* status, int* counter, int kc) {
+  extern __shared__ __align__(16) unsigned char aw_smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* sA = reinterpret_cast<T*>(aw_smem) + (size_t)warp * 2 * kc * kAwLen;
+  T* sB = sA + (size_t)kc * kAwLen;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(counter, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= nleaves) break;
+    const int leaf = order[item];
+    const RkLeafDesc d = leaves[leaf];
+    AcaWarp<T> c;
+    c.kp = kp;
+    c.P = pts;
+    c.row_off = d.row_off;
+    c.m = d.m;
+    c.col_off = d.col_off;
+    c.n = d.n;
+    c.kc = min(d.kcap, kc);
+    c.sA = sA;
+    c.sB = sB;
+    c.lane = lane;
+    bool overflow = false;
+    __syncwarp();
+    const int k = c.plus(eps, &overflow);
+    __syncwarp();
+    T* A = ws + d.ws_off;
+    T* B = A + (size_t)d.m * d.kcap;
+    for (int l = 0; l < k; ++l) {
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int e = lane + 32 * r;
+        if (e < d.m) A[(size_t)l * d.m + e] = sA[l * kAwLen + e];
+        if (e < d.n) B[(size_t)l * d.n + e] = sB[l * kAwLen + e];
+      }
+    }
+    if (lane == 0) {
+      ranks[leaf] = k;
+      status[leaf] = overflow ? kLeafAcaCapacity : kLeafOk;
+    }
+  }
+}
+
 // Dense-SVD compression of small admissible blocks (doCompressionSVD, compression.cpp:241-251):
 // the block M is written into the slot as a trivially exact factorisation M = A B^T
 // (A = M, B = I when m >= n; A = I, B = M^T otherwise, rank min(m, n)), so the truncation
@@ -414,15 +730,51 @@ void launch_aca(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, con
                                              status, counter, kcap_max);
 }
 
+// Rank capacity of the warp-per-leaf kernel's shared factors (its slots are 2 x 64 x kc
+// scalars a warp).
+template <typename T>
+int aca_warp_cap() {
+  return sizeof(T) <= 4 ? 32 : (sizeof(T) <= 8 ? 24 : 16);
+}
+bool aca_warp_eligible(int m, int n) { return m <= kAwLen && n <= kAwLen && !(n * 100 < m); }
+
+template <typename T>
+void launch_aca_warp(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, const KernelParams& kp,
+                     Points pts, double epsilon, T* ws, int* ranks, int* status, int* counter, int kcap_max,
+                     cudaStream_t s) {
+  const int kc = kcap_max < aca_warp_cap<T>() ? kcap_max : aca_warp_cap<T>();
+  const size_t smem = (size_t)kAwWarps * 2 * kc * kAwLen * sizeof(T);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(aca_warp_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(kAwWarps * 2 * aca_warp_cap<T>() * kAwLen * sizeof(T)));
+    attr = true;
+  }
+  if (nleaves <= 0) return;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, aca_warp_kernel<T>, kAwWarps * 32, smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  int g = persistent_grid(per_sm);
+  const int need = (nleaves + kAwWarps - 1) / kAwWarps;
+  if (g > need) g = need;
+  aca_warp_kernel<T><<<g, kAwWarps * 32, smem, s>>>(d_leaves, d_order, nleaves, kp, pts, epsilon, ws, ranks,
+                                                    status, counter, kc);
+}
+
 template <typename T>
 void preload_aca_kernels() {
   cudaFuncAttributes a;
   cudaFuncGetAttributes(&a, aca_kernel<T>);
   cudaFuncGetAttributes(&a, dense_to_rk_kernel<T>);
+  launch_aca_warp<T>(nullptr, nullptr, 0, KernelParams{}, Points{}, 0.0, nullptr, nullptr, nullptr, nullptr, 1, 0);
 }
 
 #define HB_INST(T)                                                                                           \
   template void preload_aca_kernels<T>();                                                                  \
+  template void launch_aca_warp<T>(const RkLeafDesc*, const int*, int, const KernelParams&, Points, double, T*, \
+                                   int*, int*, int*, int, cudaStream_t);                                    \
   template void launch_aca<T>(const RkLeafDesc*, const int*, int, const KernelParams&, Points, double, T*, \
                               unsigned char*, int*, int*, int*, int, int, cudaStream_t);                    \
   template void launch_dense_to_rk<T>(const RkLeafDesc*, const int*, int, const KernelParams&, Points, T*, \

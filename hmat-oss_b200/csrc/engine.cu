@@ -599,6 +599,7 @@ class Engine : public EngineBase {
     int leaf;
     int kcap;
     bool svd;
+    bool cta = false;  // ACA on the CTA-per-leaf kernel (a retry after a capacity overflow)
   };
   struct Piece {
     DevArray<T> arena;
@@ -634,23 +635,33 @@ class Engine : public EngineBase {
       max_n = std::max(max_n, l.n);
       max_cap = std::max(max_cap, d.kcap);
     }
-    std::vector<int> aca_order, svd_order;
-    for (int b = 0; b < nb; ++b) (jobs[b].svd ? svd_order : aca_order).push_back(b);
+    // small leaves to the warp-per-leaf ACA kernel, the others to the CTA-per-leaf one
+    std::vector<int> aca_order, aw_order, svd_order;
+    for (int b = 0; b < nb; ++b) {
+      if (jobs[b].svd)
+        svd_order.push_back(b);
+      else if (!jobs[b].cta && aca_warp_eligible(desc[b].m, desc[b].n))
+        aw_order.push_back(b);
+      else
+        aca_order.push_back(b);
+    }
     auto cost = [&](int b) { return (double)(desc[b].m + desc[b].n) * std::min(desc[b].m, desc[b].n); };
     std::stable_sort(aca_order.begin(), aca_order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+    std::stable_sort(aw_order.begin(), aw_order.end(), [&](int x, int y) { return cost(x) > cost(y); });
     DevArray<RkLeafDesc> d_desc;
     d_desc.upload(desc, stream_);
     DevArray<T> d_ws;
     d_ws.alloc((size_t)ws);
     DevArray<unsigned char> d_flags;
     d_flags.alloc((size_t)std::max(fl, 1LL));
-    DevArray<int> d_ranks, d_status, d_counter, d_aca_order, d_svd_order;
+    DevArray<int> d_ranks, d_status, d_counter, d_aca_order, d_aw_order, d_svd_order;
     d_ranks.alloc(nb);
     d_status.alloc(nb);
     d_counter.alloc(2);
     HB_CUDA(cudaMemsetAsync(d_ranks.p, 0, nb * sizeof(int), stream_));
     HB_CUDA(cudaMemsetAsync(d_status.p, 0, nb * sizeof(int), stream_));
     d_aca_order.upload(aca_order, stream_);
+    d_aw_order.upload(aw_order, stream_);
     d_svd_order.upload(svd_order, stream_);
     HB_CUDA(cudaStreamSynchronize(stream_));
 
@@ -674,6 +685,7 @@ class Engine : public EngineBase {
         ostore[b].bt_off = p;
       }
       aca_order.clear();
+      aw_order.clear();
       svd_order.clear();
       d_ranks.upload(k0, stream_);
       DevArray<RkStoreDesc> d_ostore;
@@ -685,6 +697,16 @@ class Engine : public EngineBase {
       HB_CUDA(cudaStreamSynchronize(stream_));
     }
     HB_CUDA(cudaEventRecord(ev_[2], stream_));
+    if (!aw_order.empty()) {
+      // beside the CTA kernel, on the second stream with its own work counter
+      HB_CUDA(cudaEventRecord(fork_[0], stream_));
+      HB_CUDA(cudaStreamWaitEvent(stream2_, fork_[0], 0));
+      HB_CUDA(cudaMemsetAsync(d_counter.p + 1, 0, sizeof(int), stream2_));
+      launch_aca_warp<T>(d_desc.p, d_aw_order.p, (int)aw_order.size(), kp_, pts_, eps_aca, d_ws.p, d_ranks.p,
+                         d_status.p, d_counter.p + 1, max_cap, stream2_);
+      HB_CUDA(cudaGetLastError());
+      HB_CUDA(cudaEventRecord(fork_[1], stream2_));
+    }
     if (!aca_order.empty()) {
       HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
       launch_aca<T>(d_desc.p, d_aca_order.p, (int)aca_order.size(), kp_, pts_, eps_aca, d_ws.p, d_flags.p,
@@ -696,6 +718,7 @@ class Engine : public EngineBase {
                             d_status.p, stream_);
       HB_CUDA(cudaGetLastError());
     }
+    if (!aw_order.empty()) HB_CUDA(cudaStreamWaitEvent(stream_, fork_[1], 0));
     HB_CUDA(cudaEventRecord(ev_[3], stream_));
     std::vector<int> h_status(nb), h_ranks(nb);
     HB_CUDA(cudaMemcpyAsync(h_status.data(), d_status.p, nb * sizeof(int), cudaMemcpyDeviceToHost, stream_));
@@ -712,6 +735,7 @@ class Engine : public EngineBase {
         const LeafInfo& l = L[jobs[b].leaf];
         RkJob j = jobs[b];
         j.kcap = std::min(std::min(l.m, l.n), 2 * j.kcap);
+        j.cta = true;
         retry.push_back(j);
         h_ranks[b] = 0;
         continue;

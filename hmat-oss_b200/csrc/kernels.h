@@ -56,6 +56,16 @@ void launch_aca(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, con
                 double epsilon, T* ws, unsigned char* flags, int* ranks, int* status, int* counter, int kcap_max,
                 int grid, cudaStream_t s);
 
+// Warp-per-leaf ACA+ of the small leaves (m, n <= 64, not the partial-ACA delegate): same
+// pivots and factors as launch_aca, the factors growing in shared memory.  Its rank
+// capacity is min(slot capacity, 32 / 24 / 16 by scalar size); a leaf that needs more is
+// reported as out of capacity.  Separate work counter.
+bool aca_warp_eligible(int m, int n);
+template <typename T>
+void launch_aca_warp(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, const KernelParams& kp,
+                     Points pts, double epsilon, T* ws, int* ranks, int* status, int* counter, int kcap_max,
+                     cudaStream_t s);
+
 // Dense block written as an exact rank-min(m, n) factorisation, for the SVD compression
 // of small blocks (the truncation phase then performs the SVD).
 template <typename T>
