@@ -61,6 +61,14 @@ size_t workspace_budget() {
   return (size_t)mb << 20;
 }
 // Initial ACA rank capacity per leaf; leaves that reach it are rerun with twice as much.
+// The tensor-memory y-phase kernel (map 4) is opt-in: HMAT_B200_TC_Y=1.  With 16
+// right-hand sides each M=128, N=16, K=8 tf32 MMA costs about 90 cycles (measured), so the
+// three-term split caps it below the warp-level tensor-core kernel's rate.
+bool tc_y_enabled() {
+  const char* s = getenv("HMAT_B200_TC_Y");
+  return s && s[0] == '1';
+}
+
 int initial_kcap() {
   const char* s = getenv("HMAT_B200_ACA_KCAP");
   int k = s ? atoi(s) : 48;
@@ -1043,11 +1051,12 @@ class Engine : public EngineBase {
   // Contiguous ranges of tasks of about equal bytes for a persistent grid: one range per
   // CTA, or per warp for warp-level launches.  Returns the range starts; *ncta is the grid.
   std::vector<int> partition(const std::vector<GemvTask>& tasks, const std::vector<GemvUnit>& units, int omax,
-                             bool transposed, bool warp_level, int* ncta) {
+                             bool transposed, bool warp_level, int map, int* ncta) {
     const int Rmax = sizeof(T) >= 16 ? 4 : 16;
     const int RS16 = gemv_rhs_stride((int)sizeof(T), Rmax);
-    const size_t smem = warp_level ? warp_stream_smem_bytes((int)sizeof(T))
-                                   : stream_smem_bytes((int)sizeof(T), Rmax, RS16, omax, transposed);
+    const size_t smem = map == 4      ? umma_smem_bytes()
+                        : warp_level ? warp_stream_smem_bytes((int)sizeof(T))
+                                     : stream_smem_bytes((int)sizeof(T), Rmax, RS16, omax, transposed);
     int per_sm = (int)std::min<size_t>(8, (226 * 1024) / (smem + 1024));
     per_sm = std::max(per_sm, 1);
     const int wpc = warp_level ? warp_stream_warps_per_cta() : 1;
@@ -1107,8 +1116,9 @@ class Engine : public EngineBase {
     for (size_t t = 1; t < tasks.size(); ++t)
       if (tasks[t].first_unit != tasks[t - 1].first_unit + tasks[t - 1].nunits)
         throw Error("gemv plan: units of a launch are not contiguous");
-    const int omax = L.warp_level ? (L.map == 3 ? 16 * L.rpt : (L.map == 2 ? 32 : (L.map == 1 ? 64 : 128)))
-                                  : ol * rpt;
+    const int omax = L.map == 4       ? 128
+                     : L.warp_level ? (L.map == 3 ? 16 * L.rpt : (L.map == 2 ? 32 : (L.map == 1 ? 64 : 128)))
+                                    : ol * rpt;
     for (auto& t : tasks)
       if (t.O > omax) throw Error("gemv plan: task taller than its launch shape");
     if (L.warp_level) {
@@ -1122,7 +1132,16 @@ class Engine : public EngineBase {
             throw Error("gemv plan: unit above the warp-level stage capacity");
         }
     }
-    std::vector<int> begin = partition(tasks, units, omax, transposed, L.warp_level, &L.ncta);
+    if (L.map == 4) {
+      // every unit must fit one stage of the tensor-memory kernel
+      for (auto& t : tasks)
+        for (int u = t.first_unit; u < t.first_unit + t.nunits; ++u) {
+          const GemvUnit& g = units[u];
+          if ((long long)g.pel * 4 > kTcPieceBytes || g.c > kTcCols || g.shift != 0 || g.c * 16 * 4 > kTcXBytes)
+            throw Error("gemv plan: unit above the tensor-memory stage capacity");
+        }
+    }
+    std::vector<int> begin = partition(tasks, units, omax, transposed, L.warp_level, L.map, &L.ncta);
     sb.tasks[slot].upload(tasks, stream_);
     sb.begin[slot].upload(begin, stream_);
     L.tasks = sb.tasks[slot].p;
@@ -1137,6 +1156,8 @@ class Engine : public EngineBase {
     const std::vector<int>& ostarts = trans ? cstarts_ : rstarts_;
     std::vector<GemvUnit> units;
     const int kMaxUnits = 64;  // a longer z task is cut into chunks summed afterwards
+    // FP32 'N' y-phase on the tensor-memory kernel when HMAT_B200_TC_Y=1
+    const bool tc_y = !trans && std::is_same<T, float>::value && tc_y_enabled();
 
     // ---- z-phase: one task per Rk leaf (or chunk), one launch per rank class ----
     std::vector<GemvTask> zt[4];
@@ -1215,7 +1236,7 @@ class Engine : public EngineBase {
           const int w = l.type == 0 ? l.n : ranks[i];
           const long long poff = row_panel_offset(i, ob.off, w);
           const int xrow = l.type == 0 ? l.col_off : K[rk_index[i]].zrow_n;
-          px_units(units, poff, ob.len, w, xrow, warp_unit_cols(ob.len));
+          px_units(units, poff, ob.len, w, xrow, tc_y ? kTcCols : warp_unit_cols(ob.len));
         } else if (l.type == 0) {
           // columns of block b in every row panel of full leaf i
           auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
@@ -1261,7 +1282,10 @@ class Engine : public EngineBase {
     }
     const int rpt = maxlen <= 32 ? 1 : (maxlen <= 64 ? 2 : 4);
     side.y = GemvLaunch();
-    if (!trans) warp_shape(side.y, maxlen);
+    if (tc_y)
+      side.y.map = 4;
+    else if (!trans)
+      warp_shape(side.y, maxlen);
     finish_launch(side.y, sb, GemvSide::kMaxLaunch, yt, units, 32, rpt, trans, true);
     sb.units.upload(units, stream_);
     side.units = sb.units.p;

@@ -692,6 +692,233 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 4)
   }
 }
 
+// ---------------------------------------------------------------------------------
+// FP32 'N' product on the 5th-generation tensor cores (tcgen05.mma, accumulators in tensor
+// memory), one task at a time per CTA of 128 threads; thread t owns output row t.
+//
+// A unit out(O x 16) += P (O x c) X (c x 16), c <= kTcCols, is D = A B^T with A = P
+// (M = 128, K = c) and B = X^T (N = 16, K = c): TF32 operands in shared memory, K-major
+// without swizzle (8-row x 16-byte core matrices, 128 B between the two 4-column halves of a
+// k-step, 256 B between 8-row groups).  FP32 accuracy as in the warp-level kernel: the split
+// P X ~ P_lo X_hi + P_hi X_lo + P_hi X_hi, each 8-column step into its own accumulator
+// (tensor-memory columns 16 s) and the steps added in order to the running sums in registers
+// with FP32 round-to-nearest adds (the tensor core's own sums are not rounded to nearest).
+// Thread 0 streams the pieces through a ring of kTcStages stages (cp.async.bulk + mbarrier),
+// issues the MMAs and commits them to an mbarrier; all threads split the raw piece into the
+// hi / lo tiles and read the accumulators back (tcgen05.ld, one 32-lane quarter per warp).
+// Tile rows at or past O are not written: they hold what earlier units left and only reach
+// output rows that are never stored.  Every wait is bounded and sets `err` when it gives up.
+constexpr int kTcThreads = 128;
+constexpr int kTcStages = 4;
+constexpr int kTcSteps = kTcCols / 8;
+constexpr int kTcTileA = 128 * 8 * 4;  // one k-step of A: 4 KB
+constexpr int kTcTileB = 16 * 8 * 4;   // one k-step of B: 512 B
+constexpr int kTcStage = kTcPieceBytes + kTcXBytes;
+constexpr int kTcTmemCols = 16 * kTcSteps;  // a power of two >= 32
+constexpr uint32_t kTcIdesc = (1u << 4)     // D: F32
+                              | (2u << 7)   // A: TF32
+                              | (2u << 10)  // B: TF32
+                              | (2u << 17)  // N = 16
+                              | (8u << 24); // M = 128
+
+__device__ __forceinline__ uint32_t tc_kmaj(int r, int k) {
+  return (uint32_t)((r >> 3) * 256 + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4);
+}
+__device__ __forceinline__ uint64_t tc_desc(const void* p) {
+  const uint32_t a = smem_u32(p);
+  return (uint64_t)((a >> 4) & 0x3fff) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(256 >> 4) << 32) |
+         ((uint64_t)1 << 46);
+}
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(kTcIdesc), "r"(accumulate));
+}
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&f)[16]) {
+  uint32_t v[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) f[i] = __uint_as_float(v[i]);
+}
+__device__ __forceinline__ float4 tc_hi(float4 v, float4& lo) {
+  float4 h;
+  h.x = __uint_as_float(__float_as_uint(v.x) & 0xffffe000u);
+  h.y = __uint_as_float(__float_as_uint(v.y) & 0xffffe000u);
+  h.z = __uint_as_float(__float_as_uint(v.z) & 0xffffe000u);
+  h.w = __uint_as_float(__float_as_uint(v.w) & 0xffffe000u);
+  lo = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+  return h;
+}
+__device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity, int* err) {
+  long long spins = 0;
+  while (!mbar_try_wait(bar, parity)) {
+    if (++spins > kWaitLimit) {
+      atomicExch(err, 1);
+      return false;
+    }
+  }
+  return true;
+}
+
+template <int RS>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    umma_stream_kernel(const GemvTask* __restrict__ tasks, const int* __restrict__ cta_begin,
+                       const GemvUnit* __restrict__ units, const float* __restrict__ arena, float* xz, int* err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* ring = smem_raw;
+  unsigned char* tAh = ring + kTcStages * kTcStage;
+  unsigned char* tAl = tAh + kTcSteps * kTcTileA;
+  unsigned char* tBh = tAl + kTcSteps * kTcTileA;
+  unsigned char* tBl = tBh + kTcSteps * kTcTileB;
+  uint64_t* full = reinterpret_cast<uint64_t*>(tBl + kTcSteps * kTcTileB);
+  uint64_t* mmab = full + kTcStages;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mmab + 1);
+  GemvUnit* uslot = reinterpret_cast<GemvUnit*>(tslot + 4);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int t0 = cta_begin[blockIdx.x], t1 = cta_begin[blockIdx.x + 1];
+  if (t0 >= t1) return;
+  const int u_begin = tasks[t0].first_unit;
+  const int u_end = tasks[t1 - 1].first_unit + tasks[t1 - 1].nunits;
+  if (tid == 0) {
+    for (int s = 0; s < kTcStages; ++s) mbar_init(&full[s], 1);
+    mbar_init(mmab, 1);
+    mbar_fence_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(kTcTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  const uint32_t tlane = tmem + ((uint32_t)(warp * 32) << 16);
+
+  auto issue = [&](int v) {
+    const GemvUnit U = units[v];
+    const int s = (v - u_begin) % kTcStages;
+    uslot[s] = U;
+    const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(float));
+    const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(float);
+    unsigned char* st = ring + (size_t)s * kTcStage;
+    mbar_expect_tx(&full[s], pbytes + xbytes);
+    bulk_g2s(st, arena + U.poff, pbytes, &full[s]);
+    bulk_g2s(st + kTcPieceBytes, xz + (size_t)U.xrow * RS, xbytes, &full[s]);
+  };
+  if (tid == 0)
+    for (int v = u_begin; v < u_end && v < u_begin + kTcStages; ++v) issue(v);
+
+  uint32_t mma_parity = 0;
+  int u = u_begin;
+  for (int t = t0; t < t1; ++t) {
+    const GemvTask task = tasks[t];
+    const int O = task.O;
+    float acc[16];
+#pragma unroll
+    for (int n = 0; n < 16; ++n) acc[n] = 0.f;
+    for (int kk = 0; kk < task.nunits; ++kk, ++u) {
+      const int s = (u - u_begin) % kTcStages;
+      tc_wait(&full[s], (uint32_t)(((u - u_begin) / kTcStages) & 1), err);
+      const int c = uslot[s].c;
+      const float* P = reinterpret_cast<const float*>(ring + (size_t)s * kTcStage);
+      const float* X = reinterpret_cast<const float*>(ring + (size_t)s * kTcStage + kTcPieceBytes);
+      // A tiles: (row i, 4-column quad q), rows < O, columns past c as zeros
+      for (int it = tid; it < O * (kTcCols / 4); it += kTcThreads) {
+        const int i = it % O, q = it / O, k0 = 4 * q;
+        float4 v;
+        v.x = k0 < c ? P[(size_t)k0 * O + i] : 0.f;
+        v.y = k0 + 1 < c ? P[(size_t)(k0 + 1) * O + i] : 0.f;
+        v.z = k0 + 2 < c ? P[(size_t)(k0 + 2) * O + i] : 0.f;
+        v.w = k0 + 3 < c ? P[(size_t)(k0 + 3) * O + i] : 0.f;
+        float4 lo;
+        const float4 hi = tc_hi(v, lo);
+        const uint32_t off = (uint32_t)(q >> 1) * kTcTileA + tc_kmaj(i, (q & 1) * 4);
+        *reinterpret_cast<float4*>(tAh + off) = hi;
+        *reinterpret_cast<float4*>(tAl + off) = lo;
+      }
+      // B tiles: (right-hand side n, quad q), exactly one item a thread
+      {
+        const int n = tid & 15, q = tid >> 4, k0 = 4 * q;
+        float4 v;
+        v.x = (n < RS && k0 < c) ? X[(size_t)k0 * RS + n] : 0.f;
+        v.y = (n < RS && k0 + 1 < c) ? X[(size_t)(k0 + 1) * RS + n] : 0.f;
+        v.z = (n < RS && k0 + 2 < c) ? X[(size_t)(k0 + 2) * RS + n] : 0.f;
+        v.w = (n < RS && k0 + 3 < c) ? X[(size_t)(k0 + 3) * RS + n] : 0.f;
+        float4 lo;
+        const float4 hi = tc_hi(v, lo);
+        const uint32_t off = (uint32_t)(q >> 1) * kTcTileB + tc_kmaj(n, (q & 1) * 4);
+        *reinterpret_cast<float4*>(tBh + off) = hi;
+        *reinterpret_cast<float4*>(tBl + off) = lo;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();  // tiles written, stage s read
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int nsteps = (c + 7) >> 3;
+      if (tid == 0) {
+        for (int st = 0; st < nsteps; ++st) {
+          const uint64_t ah = tc_desc(tAh + st * kTcTileA), al = tc_desc(tAl + st * kTcTileA);
+          const uint64_t bh = tc_desc(tBh + st * kTcTileB), bl = tc_desc(tBl + st * kTcTileB);
+          const uint32_t d = tmem + 16 * st;
+          tc_mma(d, al, bh, 0);
+          tc_mma(d, ah, bl, 1);
+          tc_mma(d, ah, bh, 1);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(mmab))
+                     : "memory");
+        if (u + kTcStages < u_end) issue(u + kTcStages);
+      }
+      tc_wait(mmab, mma_parity, err);
+      mma_parity ^= 1u;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int st = 0; st < nsteps; ++st) {
+        float f[16];
+        tc_ld16(tlane + 16 * st, f);
+#pragma unroll
+        for (int n = 0; n < 16; ++n) acc[n] = __fadd_rn(acc[n], f[n]);
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    }
+    if (tid < O) {
+      float* out = xz + (size_t)(task.out_row + tid) * RS;
+      if constexpr (RS % 4 == 0) {
+#pragma unroll
+        for (int n = 0; n < RS; n += 4)
+          *reinterpret_cast<float4*>(out + n) = make_float4(acc[n], acc[n + 1], acc[n + 2], acc[n + 3]);
+      } else {
+#pragma unroll
+        for (int n = 0; n < RS; ++n) out[n] = acc[n];
+      }
+    }
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
+}
+
+template <int RS>
+void launch_umma_t(const GemvLaunch& L, const GemvUnit* units, const float* arena, float* xz, int* err,
+                   cudaStream_t s) {
+  auto kern = umma_stream_kernel<RS>;
+  const size_t smem = (size_t)kTcStages * kTcStage + 2 * kTcSteps * (kTcTileA + kTcTileB) + (kTcStages + 1) * 8 +
+                      16 + kTcStages * sizeof(GemvUnit);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  kern<<<L.ncta, kTcThreads, smem, s>>>(L.tasks, L.cta_begin, units, arena, xz, err);
+}
+
 // y in client order from the partial rows of the 'N' y tasks:
 // y[i, q0 + q] = alpha * sum_p xz[pos + p * O, q] + beta * y[i, q0 + q].  A CTA takes 32
 // client rows: the partial rows are read along q (contiguous), transposed through shared
@@ -780,6 +1007,12 @@ template <typename T, int R, int RS, bool TRANSP>
 void launch_stream(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, int conj, const int* perm_out,
                    T* y, int ldy, int q0, int r, T alpha, T beta, int* err, cudaStream_t s) {
   if (L.ntasks <= 0) return;
+  if constexpr (std::is_same<T, float>::value && !TRANSP) {
+    if (L.map == 4) {
+      launch_umma_t<RS>(L, units, arena, xz, err, s);
+      return;
+    }
+  }
   if (L.warp_level) {
     if constexpr (std::is_same<T, float>::value) {
       if (L.map == 3) {
@@ -831,7 +1064,7 @@ void run_tile(const GemvPlan& p, int nrhs, int q0, T alpha, T beta, const T* x, 
   if (tm) cudaEventRecord(tm->ev[2], s);
   launch_stream<T, R, RS, TRANSP>(side.y, side.units, arena, xz, conj, perm_out, y, ld_out, q0, nrhs, alpha, beta,
                                   err, s);
-  if (side.y.warp_level) {
+  if (side.y.warp_level || side.y.map == 4) {
     const unsigned nb = (unsigned)((side.nyrows + kFinalRows - 1) / kFinalRows);
     yfinal_kernel<T, R, RS><<<nb, 256, 0, s>>>(side.yrows, side.nyrows, xz, y, ld_out, q0, nrhs, alpha, beta);
   }
@@ -955,13 +1188,18 @@ size_t warp_stream_smem_bytes(int elem_bytes) {
 }
 int warp_stream_warps_per_cta() { return kWarpCTA; }
 
+size_t umma_smem_bytes() {
+  return (size_t)kTcStages * kTcStage + 2 * kTcSteps * (kTcTileA + kTcTileB) + (kTcStages + 1) * 8 + 16 +
+         kTcStages * sizeof(GemvUnit);
+}
+
 int gemv_launch_count(const GemvPlan& p, char trans, int nrhs, int elem_bytes) {
   const GemvSide& side = p.side[(trans == 'N' || trans == 'n') ? 0 : 1];
   int per_tile = 1;  // gather
   for (int c = 0; c < side.nz; ++c) per_tile += side.z[c].ntasks > 0;
   per_tile += side.nzred > 0;
   per_tile += side.y.ntasks > 0;
-  per_tile += side.y.warp_level;  // final pass
+  per_tile += side.y.warp_level || side.y.map == 4;  // final pass
   const int maxR = elem_bytes >= 16 ? 4 : 16;
   return per_tile * ((nrhs + maxR - 1) / maxR);
 }

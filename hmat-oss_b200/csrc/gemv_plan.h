@@ -50,8 +50,17 @@ struct GemvLaunch {
   // window over tasks of at most 32 rows (rpt rows per lane); map 1: half-warp row groups
   // (at most 64 rows); map 0: lanes over rows (at most 128).
   bool warp_level = false;
+  // map 4 (FP32 'N' y launches, not warp-level): the tensor-memory kernel, one task at a time
+  // per CTA, units of at most kTcCols columns and kTcPieceBytes bytes; it writes partial rows
+  // like the warp-level launches.
   int map = 0;
 };
+
+// Unit capacities of the tensor-memory kernel: columns, piece bytes (128 rows x kTcCols),
+// X rows bytes (kTcCols rows of 16 floats).
+constexpr int kTcCols = 32;
+constexpr int kTcPieceBytes = 128 * kTcCols * 4;
+constexpr int kTcXBytes = kTcCols * 16 * 4;
 
 // Per-stage capacities of the warp-level pipeline (bytes): one P piece and its X rows.
 constexpr int kWarpPieceBytes = 4096;

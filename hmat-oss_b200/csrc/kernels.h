@@ -145,6 +145,7 @@ int gemv_launch_count(const GemvPlan& p, char trans, int nrhs, int elem_bytes);
 // Dynamic shared memory of one streamed-task CTA, and of one warp-level CTA (and its warps).
 size_t stream_smem_bytes(int elem_bytes, int R, int RS, int omax, bool transposed);
 size_t warp_stream_smem_bytes(int elem_bytes);
+size_t umma_smem_bytes();
 int warp_stream_warps_per_cta();
 
 // Leaf-factor gradients of y = H x for the output gradient r (real types; x, r device,

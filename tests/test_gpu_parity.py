@@ -185,3 +185,41 @@ def test_single_rhs_transposed_products(hb, oracle, name):
         assert rel(got, 2.0 * o.gemv(x1, "T") - y0) < tol
     finally:
         h.close()
+
+
+@pytest.mark.parametrize("nrhs", [16, 5])
+def test_tensor_memory_y_phase_matches_warp_level(hb, nrhs, monkeypatch):
+    """The opt-in tensor-memory y-phase (tcgen05.mma with tensor-memory accumulators,
+    HMAT_B200_TC_Y=1) computes the FP32 'N' product to the accuracy of the default
+    warp-level tensor-core kernel: both within 2e-6 of the FP64 product, and within 1e-6
+    of each other."""
+    import importlib.util
+    import os
+    from conftest import ROOT
+    spec = importlib.util.spec_from_file_location("wl_tc", os.path.join(ROOT, "hmat-oss_b200", "workloads.py"))
+    wl = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(wl)
+    pts = wl.cylinder(60, 120)
+    hb.set_parameters(compressionMinLeafSize=0)
+    k = hb.kernel(hb.LAPLACE_REG, delta=0.01)
+    h64 = hb.HMatrix(pts, k, value_type=hb.HMAT_DOUBLE_PRECISION, leaf_size=64, eta=2.0, epsilon=1e-6)
+    h32 = hb.HMatrix(pts, k, value_type=hb.HMAT_SIMPLE_PRECISION, leaf_size=64, eta=2.0, epsilon=1e-6)
+    monkeypatch.setenv("HMAT_B200_TC_Y", "1")
+    htc = hb.HMatrix(pts, k, value_type=hb.HMAT_SIMPLE_PRECISION, leaf_size=64, eta=2.0, epsilon=1e-6)
+    try:
+        x = wl.rhs(len(pts), nrhs, 13)
+        y64 = h64.gemv(x)
+        y32 = h32.gemv(x.astype(np.float32)).astype(np.float64)
+        ytc = htc.gemv(x.astype(np.float32)).astype(np.float64)
+        assert np.isfinite(ytc).all()
+        assert rel(y32, y64) < 2e-6
+        assert rel(ytc, y64) < 2e-6
+        assert rel(ytc, y32) < 1e-6
+        # alpha / beta through the final pass
+        y0 = np.ones_like(x, dtype=np.float32)
+        got = htc.gemv(x.astype(np.float32), alpha=0.5, beta=2.0, y=y0).astype(np.float64)
+        assert rel(got, 0.5 * y64 + 2.0) < 2e-6
+    finally:
+        h64.close()
+        h32.close()
+        htc.close()
