@@ -60,7 +60,6 @@ size_t workspace_budget() {
   if (mb < 64) mb = 64;
   return (size_t)mb << 20;
 }
-// Initial ACA rank capacity per leaf; leaves that reach it are rerun with twice as much.
 // The tensor-memory y-phase kernel (map 4) is opt-in: HMAT_B200_TC_Y=1.  With 16
 // right-hand sides each M=128, N=16, K=8 tf32 MMA costs about 90 cycles (measured), so the
 // three-term split caps it below the warp-level tensor-core kernel's rate.
@@ -69,6 +68,7 @@ bool tc_y_enabled() {
   return s && s[0] == '1';
 }
 
+// Initial ACA rank capacity per leaf; leaves that reach it are rerun with twice as much.
 int initial_kcap() {
   const char* s = getenv("HMAT_B200_ACA_KCAP");
   int k = s ? atoi(s) : 48;
@@ -839,7 +839,11 @@ class Engine : public EngineBase {
       }
       if (!large.empty() || !svd_good.empty()) {
         slab = truncate_slab_elems<T>(big_m, big_n, big_k);
-        const size_t budget = workspace_budget();
+        // the slabs are sized for the largest leaf: let them use a third of the free memory
+        // when that is more than the ACA budget, so long high-rank leaves still fill the grid
+        size_t budget = workspace_budget();
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget = std::max(budget, free_b / 3);
         grid = std::min<long long>((long long)std::max(large.size(), svd_good.size()), persistent_grid(2));
         grid = std::max(1LL, std::min<long long>(grid, (long long)(budget / (slab * sizeof(W)))));
         d_scratch.alloc((size_t)(grid * slab));
