@@ -766,21 +766,83 @@ class Engine : public EngineBase {
     std::vector<TsItem> ts_seg[3], ts_stack[3];
     std::vector<TsCore> ts_core[3];
     bool any_ts = false;
+    // high-rank leaves: the same phases with a CTA per item
+    std::vector<TsItem> tb_seg, tb_stack;
+    std::vector<TsCore> tb_core;
+    DevArray<TsItem> d_tb_seg, d_tb_stack;
+    DevArray<TsCore> d_tb_core;
+    DevArray<W> d_tb_tri, d_tb_maps, d_tb_scratch;
+    long long tb_slab = 0;
+    int tb_grid = 0;
     if (!good.empty()) {
       // Leaves up to rank ts_kmax go to the tall-skinny phases (row segments of A and B
-      // reduced to triangles, stacks of triangles reduced again, core, apply); the others,
-      // and the dense-SVD jobs whose rank is only known on the device, to the CTA-per-leaf
-      // kernel.
+      // reduced to triangles, stacks of triangles reduced again, core, apply), higher ranks
+      // to the same phases with a CTA per item; the dense-SVD jobs, whose rank is only known
+      // on the device, to the CTA-per-leaf kernel.
       int big_m = 1, big_n = 1, big_k = 1;
-      long long tri_n = 0, map_n = 0;
+      long long tri_n = 0, map_n = 0, tb_tri = 0, tb_map = 0;
+      int tb_rows = 1, tb_k = 1;
       const int kmax = ts_kmax<T>();
       for (int b : good) {
-        const int K = jobs[b].svd ? 0 : ts_bucket(h_ranks[b], kmax);
-        if (!K) {
+        if (jobs[b].svd) {
           large.push_back(b);
           big_m = std::max(big_m, desc[b].m);
           big_n = std::max(big_n, desc[b].n);
           big_k = std::max(big_k, h_ranks[b]);
+          continue;
+        }
+        const int K = ts_bucket(h_ranks[b], kmax);
+        if (!K) {
+          // segments of at least k rows (the last one takes the remainder)
+          const RkLeafDesc& d = desc[b];
+          const int k = h_ranks[b];
+          TsCore c{};
+          c.leaf = b;
+          c.k = k;
+          for (int side = 0; side < 2; ++side) {
+            const int len = side ? d.n : d.m;
+            const long long base = d.ws_off + (side ? (long long)d.m * d.kcap : 0);
+            const int S = std::max(kTsSegRows, k);
+            const int p = std::max(1, len / S);
+            const long long fin = tb_tri, mo = tb_map;
+            tb_tri += (long long)k * k;
+            tb_map += (long long)k * k;
+            (side ? c.rb : c.ra) = fin;
+            (side ? c.mb : c.ma) = mo;
+            long long stk = 0;
+            if (p > 1) {
+              stk = tb_tri;
+              tb_tri += (long long)p * k * k;
+            }
+            for (int sg = 0; sg < p; ++sg) {
+              TsItem it{};
+              it.src = base + (long long)sg * S;
+              it.rows = sg == p - 1 ? len - sg * S : S;
+              it.ld = len;
+              it.r_out = p == 1 ? fin : stk + (long long)sg * k;
+              it.ld_r = p == 1 ? k : p * k;
+              it.map = mo;
+              it.leaf = b;
+              it.k = k;
+              tb_rows = std::max(tb_rows, it.rows);
+              tb_seg.push_back(it);
+            }
+            if (p > 1) {
+              TsItem it{};
+              it.src = stk;
+              it.rows = p * k;
+              it.ld = p * k;
+              it.r_out = fin;
+              it.ld_r = k;
+              it.map = mo;
+              it.leaf = b;
+              it.k = k;
+              tb_rows = std::max(tb_rows, it.rows);
+              tb_stack.push_back(it);
+            }
+          }
+          tb_k = std::max(tb_k, k);
+          tb_core.push_back(c);
           continue;
         }
         const int q = K == 8 ? 0 : (K == 16 ? 1 : 2);
@@ -862,6 +924,25 @@ class Engine : public EngineBase {
           d_ts_core[q].upload(ts_core[q], stream_);
         }
       }
+      if (!tb_core.empty()) {
+        // slab a CTA: a segment (rows x k) with tau and R, or the core's two k x k blocks
+        tb_slab = (long long)tb_rows * tb_k + tb_k + 3LL * tb_k * tb_k + 2LL * tb_k + 64;
+        size_t budget = workspace_budget();
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget = std::max(budget, free_b / 3);
+        long long g = std::min<long long>((long long)tb_seg.size(), persistent_grid(2));
+        g = std::max(1LL, std::min<long long>(g, (long long)(budget / (tb_slab * sizeof(W)))));
+        tb_grid = (int)g;
+        d_tb_scratch.alloc((size_t)(g * tb_slab));
+        d_tb_tri.alloc((size_t)tb_tri);
+        d_tb_maps.alloc((size_t)tb_map);
+        std::stable_sort(tb_seg.begin(), tb_seg.end(), [](const TsItem& x, const TsItem& y) { return x.rows > y.rows; });
+        std::stable_sort(tb_stack.begin(), tb_stack.end(),
+                         [](const TsItem& x, const TsItem& y) { return x.rows > y.rows; });
+        d_tb_seg.upload(tb_seg, stream_);
+        d_tb_stack.upload(tb_stack, stream_);
+        d_tb_core.upload(tb_core, stream_);
+      }
       d_svd_good.upload(svd_good, stream_);
       d_good.upload(large, stream_);
       HB_CUDA(cudaStreamSynchronize(stream_));
@@ -895,6 +976,17 @@ class Engine : public EngineBase {
         HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
         launch_truncate<T>(d_desc.p, d_good.p, (int)large.size(), eps_trunc, d_ws.p, d_ranks.p, d_status.p,
                            d_counter.p, d_scratch.p, slab, (int)grid, stream_);
+        HB_CUDA(cudaGetLastError());
+      }
+      if (!tb_core.empty()) {
+        launch_tsqr_cta<T>(d_tb_seg.p, (int)tb_seg.size(), d_ws.p, d_tb_tri.p, false, d_tb_scratch.p, tb_slab,
+                           tb_grid, d_counter.p, stream_);
+        launch_tsqr_cta<T>(d_tb_stack.p, (int)tb_stack.size(), d_ws.p, d_tb_tri.p, true, d_tb_scratch.p, tb_slab,
+                           tb_grid, d_counter.p, stream_);
+        launch_tscore_cta<T>(d_tb_core.p, (int)tb_core.size(), d_tb_tri.p, d_tb_maps.p, d_ranks.p, d_status.p,
+                             eps_trunc, d_tb_scratch.p, tb_slab, tb_grid, d_counter.p, stream_);
+        launch_tsapply_cta<T>(d_tb_seg.p, (int)tb_seg.size(), d_ws.p, d_tb_maps.p, d_ranks.p, d_tb_scratch.p, tb_slab,
+                              tb_grid, d_counter.p, stream_);
         HB_CUDA(cudaGetLastError());
       }
       if (any_ts) HB_CUDA(cudaStreamWaitEvent(stream_, fork_[1], 0));

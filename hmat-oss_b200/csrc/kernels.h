@@ -127,6 +127,20 @@ void launch_tscore(int K, const TsCore* items, int nitems, const typename Traits
 template <typename T>
 void launch_tsapply(int K, const TsItem* items, int nitems, T* ws, const typename Traits<T>::wide* maps,
                     const int* ranks, cudaStream_t s);
+// The same phases for ranks above the register buckets: a CTA per item with an FP64 slab of
+// `slab` wide elements per CTA (tsqr: rows x k + k + k^2; core: 2 k^2 + 2 k; apply: rows x k'
+// scalars), `grid` CTAs, one work counter.
+template <typename T>
+void launch_tsqr_cta(const TsItem* items, int nitems, const T* ws, typename Traits<T>::wide* tri, bool from_tri,
+                     typename Traits<T>::wide* scratch, long long slab, int grid, int* counter, cudaStream_t s);
+template <typename T>
+void launch_tscore_cta(const TsCore* items, int nitems, const typename Traits<T>::wide* tri,
+                       typename Traits<T>::wide* maps, int* ranks, int* status, double eps,
+                       typename Traits<T>::wide* scratch, long long slab, int grid, int* counter, cudaStream_t s);
+template <typename T>
+void launch_tsapply_cta(const TsItem* items, int nitems, T* ws, const typename Traits<T>::wide* maps,
+                        const int* ranks, typename Traits<T>::wide* scratch, long long slab, int grid, int* counter,
+                        cudaStream_t s);
 
 // ---- gemv ----
 }  // namespace hmatb200

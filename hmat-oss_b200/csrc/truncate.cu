@@ -9,6 +9,8 @@
 // small core is one-sided Jacobi with a round-robin pair schedule; both run in FP64 (or
 // complex FP64) whatever the storage type, and the new factors are narrowed back into the
 // leaf's workspace slot.
+#include <cstdlib>
+
 #include "block_reduce.cuh"
 #include "kernels.h"
 
@@ -713,6 +715,165 @@ __global__ void __launch_bounds__(kTsWarps * 32) tsapply_kernel(const TsItem* __
   }
 }
 
+// ---------------------------------------------------------------------------------
+// Tall-skinny truncation of the leaves above the register buckets (rank > 32 real / 16
+// complex, not dense-SVD jobs): the same algorithm as tsqr / tscore / tsapply (triangles of
+// row segments, stacks of triangles, core, factors times maps), each item taken by a CTA of
+// kTruncThreads threads with the CTA-level Householder QR and one-sided Jacobi of
+// truncate_kernel on an FP64 slab of its own.  Segments hold at least k rows.
+
+// Triangle of one item: rows x k (ld d.ld) widened into the slab, Householder QR, R written
+// with leading dimension d.ld_r.
+template <typename W, typename S>
+__global__ void __launch_bounds__(kTruncThreads) tsqr_cta_kernel(const TsItem* __restrict__ items, int nitems,
+                                                                  const S* src, W* tri, W* scratch,
+                                                                  long long slab_elems, int* counter) {
+  __shared__ RedScratch rs;
+  __shared__ int s_item;
+  W* slab = scratch + (size_t)blockIdx.x * slab_elems;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= nitems) break;
+    const TsItem d = items[item];
+    const int k = d.k, rows = d.rows;
+    W* X = slab;
+    W* tau = X + (size_t)rows * k;
+    W* R = tau + k;
+    for (size_t e = threadIdx.x; e < (size_t)rows * k; e += blockDim.x) {
+      const int c = (int)(e / rows), i = (int)(e % rows);
+      X[e] = widen(src[d.src + (size_t)c * d.ld + i]);
+    }
+    __syncthreads();
+    householder_qr(X, rows, k, tau, R, rs);
+    __syncthreads();
+    for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+      const int i = e % k, c = e / k;
+      tri[d.r_out + (size_t)c * d.ld_r + i] = R[e];
+    }
+  }
+}
+
+// Core of one leaf: Ra Rb^T, Jacobi, sigma order, k', and the maps (k x k, ld k, columns at
+// or past k' zero), as tscore_kernel.
+template <typename W>
+__global__ void __launch_bounds__(kTruncThreads) tscore_cta_kernel(const TsCore* __restrict__ items, int nitems,
+                                                                    const W* __restrict__ tri, W* maps, int* ranks,
+                                                                    int* status, double eps, W* scratch,
+                                                                    long long slab_elems, int* counter) {
+  __shared__ RedScratch rs;
+  __shared__ int s_item, s_newk;
+  W* slab = scratch + (size_t)blockIdx.x * slab_elems;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= nitems) break;
+    const TsCore d = items[item];
+    const int k = d.k;
+    const W* Ra = tri + d.ra;
+    const W* Rb = tri + d.rb;
+    W* Rm = slab;
+    W* Vm = Rm + (size_t)k * k;
+    double* sig = reinterpret_cast<double*>(Vm + (size_t)k * k);
+    int* ord = reinterpret_cast<int*>(sig + k);
+    for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+      const int i = e % k, j = e / k;
+      W s = zero<W>();
+      for (int l = max(i, j); l < k; ++l) s = s + Ra[i + (size_t)l * k] * Rb[j + (size_t)l * k];
+      Rm[e] = s;
+    }
+    __syncthreads();
+    const bool conv = jacobi_svd(Rm, Vm, k, rs);
+    for (int j = threadIdx.x; j < k; j += blockDim.x) {
+      double s2 = 0.0;
+      for (int i = 0; i < k; ++i) s2 += abs2(Rm[i + (size_t)j * k]);
+      sig[j] = sqrt(s2);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < k; j += blockDim.x) {
+      int r = 0;
+      for (int i = 0; i < k; ++i) r += (sig[i] > sig[j]) || (sig[i] == sig[j] && i < j);
+      ord[r] = j;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const double thr = sig[ord[0]] * eps;
+      int nk = 0;
+      while (nk < k && !(sig[ord[nk]] <= thr)) nk++;
+      s_newk = nk;
+    }
+    __syncthreads();
+    const int nk = s_newk;
+    // Ma[i, c] = (Rb^T V[:, o])_i / sqrt(s_o), Mb[i, c] = (Ra^T conj(W[:, o]))_i / s_o^3/2
+    for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+      const int i = e % k, c = e / k;
+      W ma = zero<W>(), mb = zero<W>();
+      if (c < nk) {
+        const int o = ord[c];
+        const double so = sig[o];
+        for (int l = 0; l <= i; ++l) {
+          ma = ma + Rb[l + (size_t)i * k] * Vm[l + (size_t)o * k];
+          mb = mb + Ra[l + (size_t)i * k] * conjg(Rm[l + (size_t)o * k]);
+        }
+        const double rsq = 1.0 / sqrt(so);
+        ma = scal(rsq, ma);
+        mb = scal(rsq / so, mb);
+      }
+      maps[d.ma + e] = ma;
+      maps[d.mb + e] = mb;
+    }
+    if (threadIdx.x == 0) {
+      ranks[d.leaf] = nk;
+      if (!conv && status[d.leaf] == kLeafOk) status[d.leaf] = kLeafSvdNoConverge;
+    }
+  }
+}
+
+// New factor columns of one segment: each thread takes rows, forms the k' outputs of a row
+// (eight at a time, sums in increasing l) into the slab, then writes them over the row.
+template <typename T, typename W>
+__global__ void __launch_bounds__(kTruncThreads) tsapply_cta_kernel(const TsItem* __restrict__ items, int nitems,
+                                                                     T* ws, const W* __restrict__ maps,
+                                                                     const int* __restrict__ ranks, W* scratch,
+                                                                     long long slab_elems, int* counter) {
+  __shared__ int s_item;
+  T* out = reinterpret_cast<T*>(scratch + (size_t)blockIdx.x * slab_elems);
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= nitems) break;
+    const TsItem d = items[item];
+    const int k = d.k, nk = ranks[d.leaf], rows = d.rows;
+    if (nk <= 0) continue;
+    T* base = ws + d.src;
+    const W* M = maps + d.map;
+    for (int row = threadIdx.x; row < rows; row += blockDim.x) {
+      for (int c0 = 0; c0 < nk; c0 += 8) {
+        W acc[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q] = zero<W>();
+        for (int l = 0; l < k; ++l) {
+          const W a = widen(base[(size_t)l * d.ld + row]);
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (c0 + q < nk) acc[q] = acc[q] + a * M[l + (size_t)(c0 + q) * k];
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (c0 + q < nk) out[(size_t)(c0 + q) * rows + row] = narrow<T>(acc[q]);
+      }
+      // every input of this row is read: the outputs replace its first k' columns
+      for (int c = 0; c < nk; ++c) base[(size_t)c * d.ld + row] = out[(size_t)c * rows + row];
+    }
+  }
+}
+
 }  // namespace
 
 template <typename T>
@@ -746,9 +907,17 @@ void launch_compact(const RkLeafDesc* d_leaves, int nleaves, const T* ws, const 
   compact_kernel<T><<<nleaves, 256, 0, s>>>(d_leaves, nleaves, ws, ranks, store, panels, arena);
 }
 
+// HMAT_B200_TS_KMAX lowers the largest register-bucket rank (8, 16; tests use it to send
+// leaves through the CTA-per-item phases).
 template <typename T>
 int ts_kmax() {
-  return Traits<T>::is_complex ? 16 : 32;
+  int k = Traits<T>::is_complex ? 16 : 32;
+  const char* s = getenv("HMAT_B200_TS_KMAX");
+  if (s) {
+    const int c = atoi(s);
+    if (c >= 0 && c < k) k = c < 8 ? 0 : (c < 16 ? 8 : 16);
+  }
+  return k;
 }
 int ts_bucket(int k, int kmax) {
   if (k <= 0 || k > kmax) return 0;
@@ -868,6 +1037,55 @@ void launch_tsapply(int K, const TsItem* items, int nitems, T* ws, const typenam
   }
 }
 
+// High-rank tall-skinny phases (tsqr_cta / tscore_cta / tsapply_cta), one launch each on a
+// persistent grid of `grid` CTAs with a work counter (zeroed here, on the stream).
+template <typename T>
+void launch_tsqr_cta(const TsItem* items, int nitems, const T* ws, typename Traits<T>::wide* tri, bool from_tri,
+                     typename Traits<T>::wide* scratch, long long slab, int grid, int* counter, cudaStream_t s) {
+  typedef typename Traits<T>::wide W;
+  if (nitems <= 0) {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, tsqr_cta_kernel<W, T>);
+    cudaFuncGetAttributes(&a, tsqr_cta_kernel<W, W>);
+    return;
+  }
+  cudaMemsetAsync(counter, 0, sizeof(int), s);
+  const int g = grid < nitems ? grid : nitems;
+  if (from_tri)
+    tsqr_cta_kernel<W, W><<<g, kTruncThreads, 0, s>>>(items, nitems, tri, tri, scratch, slab, counter);
+  else
+    tsqr_cta_kernel<W, T><<<g, kTruncThreads, 0, s>>>(items, nitems, ws, tri, scratch, slab, counter);
+}
+template <typename T>
+void launch_tscore_cta(const TsCore* items, int nitems, const typename Traits<T>::wide* tri,
+                       typename Traits<T>::wide* maps, int* ranks, int* status, double eps,
+                       typename Traits<T>::wide* scratch, long long slab, int grid, int* counter, cudaStream_t s) {
+  typedef typename Traits<T>::wide W;
+  if (nitems <= 0) {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, tscore_cta_kernel<W>);
+    return;
+  }
+  cudaMemsetAsync(counter, 0, sizeof(int), s);
+  const int g = grid < nitems ? grid : nitems;
+  tscore_cta_kernel<W><<<g, kTruncThreads, 0, s>>>(items, nitems, tri, maps, ranks, status, eps, scratch, slab,
+                                                   counter);
+}
+template <typename T>
+void launch_tsapply_cta(const TsItem* items, int nitems, T* ws, const typename Traits<T>::wide* maps,
+                        const int* ranks, typename Traits<T>::wide* scratch, long long slab, int grid, int* counter,
+                        cudaStream_t s) {
+  typedef typename Traits<T>::wide W;
+  if (nitems <= 0) {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, tsapply_cta_kernel<T, W>);
+    return;
+  }
+  cudaMemsetAsync(counter, 0, sizeof(int), s);
+  const int g = grid < nitems ? grid : nitems;
+  tsapply_cta_kernel<T, W><<<g, kTruncThreads, 0, s>>>(items, nitems, ws, maps, ranks, scratch, slab, counter);
+}
+
 // Loads every truncation kernel of the storage type T (the CUDA runtime otherwise loads a
 // kernel at its first launch, inside the first assembly).
 template <typename T>
@@ -884,6 +1102,9 @@ void preload_truncate_kernels() {
     launch_tscore<T>(K, nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0.0, 0);
     launch_tsapply<T>(K, nullptr, 0, nullptr, nullptr, nullptr, 0);
   }
+  launch_tsqr_cta<T>(nullptr, 0, nullptr, nullptr, false, nullptr, 0, 0, nullptr, 0);
+  launch_tscore_cta<T>(nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0.0, nullptr, 0, 0, nullptr, 0);
+  launch_tsapply_cta<T>(nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, 0);
 }
 
 #define HB_INST(T)                                                                                         \
@@ -895,6 +1116,13 @@ void preload_truncate_kernels() {
   template void launch_unpack<T>(const RkLeafDesc*, int, const int*, const RkStoreDesc*, const PanelDesc*,  \
                                  const T*, T*, cudaStream_t);                                             \
   template void preload_truncate_kernels<T>();                                                            \
+  template void launch_tsqr_cta<T>(const TsItem*, int, const T*, typename Traits<T>::wide*, bool,            \
+                                   typename Traits<T>::wide*, long long, int, int*, cudaStream_t);         \
+  template void launch_tscore_cta<T>(const TsCore*, int, const typename Traits<T>::wide*,                    \
+                                     typename Traits<T>::wide*, int*, int*, double, typename Traits<T>::wide*, \
+                                     long long, int, int*, cudaStream_t);                                  \
+  template void launch_tsapply_cta<T>(const TsItem*, int, T*, const typename Traits<T>::wide*, const int*,   \
+                                      typename Traits<T>::wide*, long long, int, int*, cudaStream_t);      \
   template int ts_kmax<T>();                                                                               \
   template void launch_tsqr<T>(int, const TsItem*, int, const T*, typename Traits<T>::wide*, bool,         \
                                cudaStream_t);                                                              \

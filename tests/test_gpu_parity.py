@@ -223,3 +223,24 @@ def test_tensor_memory_y_phase_matches_warp_level(hb, nrhs, monkeypatch):
         h64.close()
         h32.close()
         htc.close()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_high_rank_truncation_path_matches_reference(hb, name, monkeypatch):
+    """The truncation phases for ranks above the register buckets (a CTA per row segment, per
+    stack of triangles and per core) give the reference's ranks and products: with
+    HMAT_B200_TS_KMAX=0 every leaf that is not a dense-SVD job takes them."""
+    monkeypatch.setenv("HMAT_B200_TS_KMAX", "0")
+    g = golden(name)
+    h, pts, x, kern, tree = build_engine(hb, name)
+    try:
+        T = h.leaf_table()
+        assert np.array_equal(T[:, :5], g["leaves"][:, :5])
+        rk = g["leaves"][:, 4] == 1
+        mism = int((T[rk, 5] != g["leaves"][rk, 5]).sum())
+        assert mism <= max(1, rk.sum() // 100), f"{mism} rank mismatches"
+        tol = GEMV_TOL.get(name, 1e-12)
+        assert rel(h.gemv(x, "N"), g["y"]) < tol
+        assert rel(h.gemv(x, "T"), g["y_T"]) < tol
+    finally:
+        h.close()
