@@ -19,6 +19,7 @@ namespace hmatb200 {
 namespace {
 
 constexpr int kAcaThreads = 128;
+constexpr int kAcaBigThreads = 512;  // leaves with m + n >= kAcaBigRows
 
 template <typename T>
 struct Aca {
@@ -317,8 +318,8 @@ struct Aca {
   }
 };
 
-template <typename T>
-__global__ void __launch_bounds__(kAcaThreads) aca_kernel(const RkLeafDesc* __restrict__ leaves,
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) aca_kernel(const RkLeafDesc* __restrict__ leaves,
                                                           const int* __restrict__ order, int nleaves,
                                                           KernelParams kp, Points pts, double eps, T* ws,
                                                           unsigned char* flags, int* ranks, int* status,
@@ -716,18 +717,29 @@ int persistent_grid(int blocks_per_sm) {
   return sms * blocks_per_sm;
 }
 
+template <typename T, int NT>
+static void aca_run(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, const KernelParams& kp, Points pts,
+                    double epsilon, T* ws, unsigned char* flags, int* ranks, int* status, int* counter, int kcap_max,
+                    int grid, cudaStream_t s) {
+  typedef typename Traits<T>::wide W;
+  size_t smem = (size_t)kcap_max * (2 * sizeof(W) + sizeof(T));
+  if (smem > 48 * 1024) cudaFuncSetAttribute(aca_kernel<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int g = grid < nleaves ? grid : nleaves;
+  aca_kernel<T, NT><<<g, NT, smem, s>>>(d_leaves, d_order, nleaves, kp, pts, epsilon, ws, flags, ranks, status,
+                                        counter, kcap_max);
+}
+
 template <typename T>
 void launch_aca(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, const KernelParams& kp, Points pts,
                 double epsilon, T* ws, unsigned char* flags, int* ranks, int* status, int* counter, int kcap_max,
-                int grid, cudaStream_t s) {
+                int grid, cudaStream_t s, int threads) {
   if (nleaves <= 0) return;
-  typedef typename Traits<T>::wide W;
-  size_t smem = (size_t)kcap_max * (2 * sizeof(W) + sizeof(T));
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(aca_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int g = grid < nleaves ? grid : nleaves;
-  aca_kernel<T><<<g, kAcaThreads, smem, s>>>(d_leaves, d_order, nleaves, kp, pts, epsilon, ws, flags, ranks,
-                                             status, counter, kcap_max);
+  if (threads >= kAcaBigThreads)
+    aca_run<T, kAcaBigThreads>(d_leaves, d_order, nleaves, kp, pts, epsilon, ws, flags, ranks, status, counter,
+                               kcap_max, grid, s);
+  else
+    aca_run<T, kAcaThreads>(d_leaves, d_order, nleaves, kp, pts, epsilon, ws, flags, ranks, status, counter,
+                            kcap_max, grid, s);
 }
 
 // Rank capacity of the warp-per-leaf kernel's shared factors (its slots are 2 x 64 x kc
@@ -766,7 +778,8 @@ void launch_aca_warp(const RkLeafDesc* d_leaves, const int* d_order, int nleaves
 template <typename T>
 void preload_aca_kernels() {
   cudaFuncAttributes a;
-  cudaFuncGetAttributes(&a, aca_kernel<T>);
+  cudaFuncGetAttributes(&a, aca_kernel<T, kAcaThreads>);
+  cudaFuncGetAttributes(&a, aca_kernel<T, kAcaBigThreads>);
   cudaFuncGetAttributes(&a, dense_to_rk_kernel<T>);
   launch_aca_warp<T>(nullptr, nullptr, 0, KernelParams{}, Points{}, 0.0, nullptr, nullptr, nullptr, nullptr, 1, 0);
 }
@@ -776,7 +789,7 @@ void preload_aca_kernels() {
   template void launch_aca_warp<T>(const RkLeafDesc*, const int*, int, const KernelParams&, Points, double, T*, \
                                    int*, int*, int*, int, cudaStream_t);                                    \
   template void launch_aca<T>(const RkLeafDesc*, const int*, int, const KernelParams&, Points, double, T*, \
-                              unsigned char*, int*, int*, int*, int, int, cudaStream_t);                    \
+                              unsigned char*, int*, int*, int*, int, int, cudaStream_t, int);               \
   template void launch_dense_to_rk<T>(const RkLeafDesc*, const int*, int, const KernelParams&, Points, T*, \
                                       int*, int*, cudaStream_t);
 HB_INST(float)

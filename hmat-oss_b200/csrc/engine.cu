@@ -114,6 +114,7 @@ class Engine : public EngineBase {
   Engine(const ClusterTree* rows, const ClusterTree* cols, const BlockTree* bt) : R_(rows), C_(cols), bt_(bt) {
     HB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     HB_CUDA(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking));
+    HB_CUDA(cudaStreamCreateWithFlags(&stream3_, cudaStreamNonBlocking));
     for (auto& e : ev_) HB_CUDA(cudaEventCreate(&e));
     for (auto& e : fork_) HB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     ranks.assign(bt_->leaves.size(), -1);
@@ -135,6 +136,7 @@ class Engine : public EngineBase {
     for (auto& e : ev_) cudaEventDestroy(e);
     for (auto& e : fork_) cudaEventDestroy(e);
     cudaStreamDestroy(stream2_);
+    cudaStreamDestroy(stream3_);
     cudaStreamDestroy(stream_);
   }
 
@@ -655,6 +657,19 @@ class Engine : public EngineBase {
     }
     auto cost = [&](int b) { return (double)(desc[b].m + desc[b].n) * std::min(desc[b].m, desc[b].n); };
     std::stable_sort(aca_order.begin(), aca_order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+    // long leaves to 512-thread CTAs on a third stream: capacity retries (rank above the
+    // initial capacity) from m + n >= kAcaBigRows, any leaf from four times that.  Their fills
+    // and Gram terms are long chains a thread at 128 threads; shorter leaves of rank ~16
+    // measured faster on the 128-thread kernel.
+    std::vector<int> big_order;
+    {
+      std::vector<int> rest;
+      for (int b : aca_order) {
+        const int len = desc[b].m + desc[b].n;
+        (len >= 4 * kAcaBigRows || (jobs[b].cta && len >= kAcaBigRows) ? big_order : rest).push_back(b);
+      }
+      aca_order.swap(rest);
+    }
     std::stable_sort(aw_order.begin(), aw_order.end(), [&](int x, int y) { return cost(x) > cost(y); });
     DevArray<RkLeafDesc> d_desc;
     d_desc.upload(desc, stream_);
@@ -662,14 +677,15 @@ class Engine : public EngineBase {
     d_ws.alloc((size_t)ws);
     DevArray<unsigned char> d_flags;
     d_flags.alloc((size_t)std::max(fl, 1LL));
-    DevArray<int> d_ranks, d_status, d_counter, d_aca_order, d_aw_order, d_svd_order;
+    DevArray<int> d_ranks, d_status, d_counter, d_aca_order, d_aw_order, d_big_order, d_svd_order;
     d_ranks.alloc(nb);
     d_status.alloc(nb);
-    d_counter.alloc(2);
+    d_counter.alloc(3);
     HB_CUDA(cudaMemsetAsync(d_ranks.p, 0, nb * sizeof(int), stream_));
     HB_CUDA(cudaMemsetAsync(d_status.p, 0, nb * sizeof(int), stream_));
     d_aca_order.upload(aca_order, stream_);
     d_aw_order.upload(aw_order, stream_);
+    d_big_order.upload(big_order, stream_);
     d_svd_order.upload(svd_order, stream_);
     HB_CUDA(cudaStreamSynchronize(stream_));
 
@@ -694,6 +710,7 @@ class Engine : public EngineBase {
       }
       aca_order.clear();
       aw_order.clear();
+      big_order.clear();
       svd_order.clear();
       d_ranks.upload(k0, stream_);
       DevArray<RkStoreDesc> d_ostore;
@@ -715,6 +732,15 @@ class Engine : public EngineBase {
       HB_CUDA(cudaGetLastError());
       HB_CUDA(cudaEventRecord(fork_[1], stream2_));
     }
+    if (!big_order.empty()) {
+      HB_CUDA(cudaEventRecord(fork_[2], stream_));
+      HB_CUDA(cudaStreamWaitEvent(stream3_, fork_[2], 0));
+      HB_CUDA(cudaMemsetAsync(d_counter.p + 2, 0, sizeof(int), stream3_));
+      launch_aca<T>(d_desc.p, d_big_order.p, (int)big_order.size(), kp_, pts_, eps_aca, d_ws.p, d_flags.p, d_ranks.p,
+                    d_status.p, d_counter.p + 2, max_cap, persistent_grid(2), stream3_, 512);
+      HB_CUDA(cudaGetLastError());
+      HB_CUDA(cudaEventRecord(fork_[3], stream3_));
+    }
     if (!aca_order.empty()) {
       HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
       launch_aca<T>(d_desc.p, d_aca_order.p, (int)aca_order.size(), kp_, pts_, eps_aca, d_ws.p, d_flags.p,
@@ -727,6 +753,7 @@ class Engine : public EngineBase {
       HB_CUDA(cudaGetLastError());
     }
     if (!aw_order.empty()) HB_CUDA(cudaStreamWaitEvent(stream_, fork_[1], 0));
+    if (!big_order.empty()) HB_CUDA(cudaStreamWaitEvent(stream_, fork_[3], 0));
     HB_CUDA(cudaEventRecord(ev_[3], stream_));
     std::vector<int> h_status(nb), h_ranks(nb);
     HB_CUDA(cudaMemcpyAsync(h_status.data(), d_status.p, nb * sizeof(int), cudaMemcpyDeviceToHost, stream_));
@@ -1462,8 +1489,9 @@ class Engine : public EngineBase {
   std::vector<int> rstarts_, cstarts_;
   cudaStream_t stream_ = nullptr;
   cudaStream_t stream2_ = nullptr;  // runs the tall-skinny truncation beside the CTA kernel
+  cudaStream_t stream3_ = nullptr;  // runs the long leaves' ACA beside the other ACA kernels
   cudaEvent_t ev_[8];
-  cudaEvent_t fork_[2];
+  cudaEvent_t fork_[4];
   KernelParams kp_{};
   Points pts_{};
   DevArray<double> d_pts_;

@@ -50,11 +50,15 @@ void launch_full_from_canonical(const FullLeafDesc* d_leaves, const long long* g
                                 const PanelDesc* panels, const T* src, T* arena, cudaStream_t s);
 
 // ACA+ (compression.cpp:553-724), delegating to partial ACA when n * 100 < m.  Leaves are
-// taken in `order` from a device work counter that must be zero at launch.
+// taken in `order` from a device work counter that must be zero at launch.  `threads` is the
+// CTA size: 128, or 512 for long leaves (m + n >= 4 kAcaBigRows, or capacity retries from
+// kAcaBigRows), whose residual fills and Gram terms then have a quarter of the entries a
+// thread.
+constexpr int kAcaBigRows = 2048;
 template <typename T>
 void launch_aca(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, const KernelParams& kp, Points pts,
                 double epsilon, T* ws, unsigned char* flags, int* ranks, int* status, int* counter, int kcap_max,
-                int grid, cudaStream_t s);
+                int grid, cudaStream_t s, int threads = 128);
 
 // Warp-per-leaf ACA+ of the small leaves (m, n <= 64, not the partial-ACA delegate): same
 // pivots and factors as launch_aca, the factors growing in shared memory.  Its rank
