@@ -1278,7 +1278,7 @@ class Engine : public EngineBase {
     const std::vector<Block>& oblocks = trans ? cblocks_ : rblocks_;
     const std::vector<int>& ostarts = trans ? cstarts_ : rstarts_;
     std::vector<GemvUnit> units;
-    const int kMaxUnits = 64;  // a longer z task is cut into chunks summed afterwards
+    const int kMaxUnits = 16;  // a longer z task is cut into chunks summed afterwards (spreads long leaves over warps)
     // FP32 'N' y-phase on the tensor-memory kernel when HMAT_B200_TC_Y=1
     const bool tc_y = !trans && std::is_same<T, float>::value && tc_y_enabled();
 
