@@ -1343,11 +1343,12 @@ class Engine : public EngineBase {
     for (size_t t = 0; t < rk_leaf.size(); ++t) rk_index[rk_leaf[t]] = (int)t;
     std::vector<GemvTask> yt;
     int maxlen = 1;
-    // 'N': each output block is cut into chunks of at most kYChunkUnits units whose partial
-    // rows go to xz; a final pass sums them into y (client order)
+    // each output block is cut into chunks of at most kYChunkUnits units whose partial rows go
+    // to xz; a final pass sums them into y (client order).  The chunks spread the blocks with
+    // many leaves over the grid.
     const int kYChunkUnits = 16;
-    std::vector<int2> yrows;
-    if (!trans) yrows.assign(R_->n, int2{0, 0});
+    const ClusterTree* otree = trans ? C_ : R_;
+    std::vector<int2> yrows(otree->n, int2{0, 0});
     for (size_t b = 0; b < oblocks.size(); ++b) {
       const Block& ob = oblocks[b];
       const int first = (int)units.size();
@@ -1377,10 +1378,6 @@ class Engine : public EngineBase {
       }
       maxlen = std::max(maxlen, ob.len);
       const int nu = (int)units.size() - first;
-      if (trans) {
-        yt.push_back(GemvTask{ob.len, first, nu, ob.off});
-        continue;
-      }
       const int nparts = (nu + kYChunkUnits - 1) / kYChunkUnits;
       const int part_row = (int)next_row;
       next_row += (long long)nparts * ob.len;
@@ -1388,7 +1385,7 @@ class Engine : public EngineBase {
         const int u0 = pidx * kYChunkUnits, u1 = std::min(nu, u0 + kYChunkUnits);
         yt.push_back(GemvTask{ob.len, first + u0, u1 - u0, part_row + pidx * ob.len});
       }
-      for (int l = 0; l < ob.len; ++l) yrows[R_->perm[ob.off + l]] = int2{part_row + l, (nparts << 8) | ob.len};
+      for (int l = 0; l < ob.len; ++l) yrows[otree->perm[ob.off + l]] = int2{part_row + l, (nparts << 8) | ob.len};
     }
     // launches
     side.nz = 0;
@@ -1409,7 +1406,7 @@ class Engine : public EngineBase {
       side.y.map = 4;
     else if (!trans)
       warp_shape(side.y, maxlen);
-    finish_launch(side.y, sb, GemvSide::kMaxLaunch, yt, units, 32, rpt, trans, true);
+    finish_launch(side.y, sb, GemvSide::kMaxLaunch, yt, units, 32, rpt, trans, false);
     sb.units.upload(units, stream_);
     side.units = sb.units.p;
     sb.zred.upload(zred, stream_);

@@ -1064,7 +1064,7 @@ void run_tile(const GemvPlan& p, int nrhs, int q0, T alpha, T beta, const T* x, 
   if (tm) cudaEventRecord(tm->ev[2], s);
   launch_stream<T, R, RS, TRANSP>(side.y, side.units, arena, xz, conj, perm_out, y, ld_out, q0, nrhs, alpha, beta,
                                   err, s);
-  if (side.y.warp_level || side.y.map == 4) {
+  if (side.nyrows > 0) {
     const unsigned nb = (unsigned)((side.nyrows + kFinalRows - 1) / kFinalRows);
     yfinal_kernel<T, R, RS><<<nb, 256, 0, s>>>(side.yrows, side.nyrows, xz, y, ld_out, q0, nrhs, alpha, beta);
   }
@@ -1199,7 +1199,7 @@ int gemv_launch_count(const GemvPlan& p, char trans, int nrhs, int elem_bytes) {
   for (int c = 0; c < side.nz; ++c) per_tile += side.z[c].ntasks > 0;
   per_tile += side.nzred > 0;
   per_tile += side.y.ntasks > 0;
-  per_tile += side.y.warp_level || side.y.map == 4;  // final pass
+  per_tile += side.nyrows > 0;  // final pass
   const int maxR = elem_bytes >= 16 ? 4 : 16;
   return per_tile * ((nrhs + maxR - 1) / maxR);
 }

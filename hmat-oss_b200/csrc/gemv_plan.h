@@ -80,8 +80,8 @@ struct GemvSide {
   const GemvZred* zred = nullptr;
   GemvLaunch y;
   const GemvUnit* units = nullptr;
-  // Warp-level y launches write partial rows (chunks of the output blocks) into xz; the
-  // final pass reads, per client row i, yrows[i] = {xz row of part 0, nparts << 8 | O}.
+  // The y launches write partial rows (chunks of the output blocks) into xz; the final pass
+  // reads, per client row i, yrows[i] = {xz row of part 0, nparts << 8 | O}.
   int nyrows = 0;
   const int2* yrows = nullptr;
 };
