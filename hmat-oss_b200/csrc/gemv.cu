@@ -1088,9 +1088,11 @@ void run_all(const GemvPlan& p, int nrhs, T alpha, T beta, const T* x, T* y, T* 
 // ---------------------------------------------------------------------------------
 // Leaf-factor gradients (adjoint of y = H x with respect to the stored leaves), written in
 // the canonical layout (full: m x n, Rk: A m x k then B n x k, column-major).
-template <typename T, int RS>
+// R is the right-hand-side tile (compile time): columns past the caller's count hold exact
+// zeros in xs and rs (the gather pads them), so they add nothing.
+template <typename T, int RS, int R>
 __global__ void grad_full_kernel(const GemvFullLeaf* __restrict__ full, int nfull, const T* __restrict__ xs,
-                                 const T* __restrict__ rs, int R, T* __restrict__ g, bool accumulate) {
+                                 const T* __restrict__ rs, T* __restrict__ g, bool accumulate) {
   // warp per column j of a leaf, lanes over its rows: coalesced column writes, no division
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int f = blockIdx.x; f < nfull; f += gridDim.x) {
@@ -1101,6 +1103,7 @@ __global__ void grad_full_kernel(const GemvFullLeaf* __restrict__ full, int nful
       for (int i = lane; i < F.m; i += 32) {
         const T* rv = rs + (size_t)(F.row_off + i) * RS;
         T acc = accumulate ? dF[i] : zero<T>();
+#pragma unroll
         for (int q = 0; q < R; ++q) acc = fmadd(rv[q], xv[q], acc);
         dF[i] = acc;
       }
@@ -1108,9 +1111,9 @@ __global__ void grad_full_kernel(const GemvFullLeaf* __restrict__ full, int nful
   }
 }
 
-template <typename T, int RS>
+template <typename T, int RS, int R>
 __global__ void grad_rk_kernel(const GemvRkLeaf* __restrict__ rk, int nrk, const T* __restrict__ xs,
-                               const T* __restrict__ rs, int R, T* __restrict__ g, bool accumulate) {
+                               const T* __restrict__ rs, T* __restrict__ g, bool accumulate) {
   // warp per factor column l, lanes over rows: coalesced column writes, no division
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int t = blockIdx.x; t < nrk; t += gridDim.x) {
@@ -1124,6 +1127,7 @@ __global__ void grad_rk_kernel(const GemvRkLeaf* __restrict__ rk, int nrk, const
       for (int i = lane; i < L.m; i += 32) {
         const T* rv = rs + (size_t)(L.row_off + i) * RS;
         T acc = accumulate ? col[i] : zero<T>();
+#pragma unroll
         for (int q = 0; q < R; ++q) acc = fmadd(rv[q], zv[q], acc);
         col[i] = acc;
       }
@@ -1135,6 +1139,7 @@ __global__ void grad_rk_kernel(const GemvRkLeaf* __restrict__ rk, int nrk, const
       for (int j = lane; j < L.n; j += 32) {
         const T* xv = xs + (size_t)(L.col_off + j) * RS;
         T acc = accumulate ? col[j] : zero<T>();
+#pragma unroll
         for (int q = 0; q < R; ++q) acc = fmadd(xv[q], wv[q], acc);
         col[j] = acc;
       }
@@ -1167,8 +1172,8 @@ void grads_tile(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* r
   if (st.nzred > 0) zred_kernel<T, RS><<<st.nzred, 128, 0, s>>>(st.zred, rz);
   const int grid = persistent_grid(4);
   if (p.nfull > 0 && gfull)
-    grad_full_kernel<T, RS><<<grid, 256, 0, s>>>(p.full, p.nfull, xz, rz, nrhs, gfull, accumulate);
-  if (p.nrk > 0 && grk) grad_rk_kernel<T, RS><<<grid, 256, 0, s>>>(p.rk, p.nrk, xz, rz, nrhs, grk, accumulate);
+    grad_full_kernel<T, RS, R><<<grid, 256, 0, s>>>(p.full, p.nfull, xz, rz, gfull, accumulate);
+  if (p.nrk > 0 && grk) grad_rk_kernel<T, RS, R><<<grid, 256, 0, s>>>(p.rk, p.nrk, xz, rz, grk, accumulate);
 }
 
 }  // namespace
