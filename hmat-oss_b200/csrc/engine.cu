@@ -786,12 +786,12 @@ class Engine : public EngineBase {
     typedef typename Traits<T>::wide W;
     DevArray<W> d_scratch, d_tri, d_maps;
     DevArray<int> d_good, d_svd_good;
-    DevArray<TsItem> d_ts_seg[3], d_ts_stack[3];
-    DevArray<TsCore> d_ts_core[3];
+    DevArray<TsItem> d_ts_seg[4], d_ts_stack[4];
+    DevArray<TsCore> d_ts_core[4];
     long long slab = 0, grid = 0;
     std::vector<int> svd_good, large;
-    std::vector<TsItem> ts_seg[3], ts_stack[3];
-    std::vector<TsCore> ts_core[3];
+    std::vector<TsItem> ts_seg[4], ts_stack[4];
+    std::vector<TsCore> ts_core[4];
     bool any_ts = false;
     // high-rank leaves: the same phases with a CTA per item
     std::vector<TsItem> tb_seg, tb_stack;
@@ -872,7 +872,7 @@ class Engine : public EngineBase {
           tb_core.push_back(c);
           continue;
         }
-        const int q = K == 8 ? 0 : (K == 16 ? 1 : 2);
+        const int q = K == 8 ? 0 : (K == 16 ? 1 : (K == 24 ? 2 : 3));
         const RkLeafDesc& d = desc[b];
         TsCore c{};
         c.leaf = b;
@@ -940,7 +940,7 @@ class Engine : public EngineBase {
       if (any_ts) {
         d_tri.alloc((size_t)tri_n);
         d_maps.alloc((size_t)map_n);
-        for (int q = 0; q < 3; ++q) {
+        for (int q = 0; q < 4; ++q) {
           // longest segments first: the warps take items in order
           std::stable_sort(ts_seg[q].begin(), ts_seg[q].end(),
                            [](const TsItem& x, const TsItem& y) { return x.rows > y.rows; });
@@ -988,8 +988,8 @@ class Engine : public EngineBase {
       if (any_ts) {
         HB_CUDA(cudaEventRecord(fork_[0], stream_));
         HB_CUDA(cudaStreamWaitEvent(stream2_, fork_[0], 0));
-        for (int q = 0; q < 3; ++q) {
-          const int K = 8 << q;
+        for (int q = 0; q < 4; ++q) {
+          const int K = 8 * (q + 1);
           launch_tsqr<T>(K, d_ts_seg[q].p, (int)ts_seg[q].size(), d_ws.p, d_tri.p, false, stream2_);
           launch_tsqr<T>(K, d_ts_stack[q].p, (int)ts_stack[q].size(), d_ws.p, d_tri.p, true, stream2_);
           launch_tscore<T>(K, d_ts_core[q].p, (int)ts_core[q].size(), d_tri.p, d_maps.p, d_ranks.p, d_status.p,

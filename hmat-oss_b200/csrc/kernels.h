@@ -117,7 +117,7 @@ struct TsCore {
   int leaf, k;
 };
 // Largest rank the tall-skinny path takes (32 real, 16 complex), and the rank bucket
-// (8, 16 or 32) of rank k (0 when above the largest).
+// (8, 16, 24 or 32) of rank k (0 when above the largest).
 template <typename T>
 int ts_kmax();
 int ts_bucket(int k, int kmax);

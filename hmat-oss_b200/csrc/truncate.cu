@@ -502,19 +502,20 @@ __global__ void __launch_bounds__(NW * 32) tscore_kernel(const TsCore* __restric
                                                           const W* __restrict__ tri, W* __restrict__ maps,
                                                           int* ranks, int* status, double eps) {
   constexpr int G = 32 / K;  // leaves per warp
+  constexpr int SW = (K & (K - 1)) == 0 ? K : 32;  // shuffle width (a power of two; one leaf a warp otherwise)
   __shared__ W s_ra[NW][G][K * K];
   __shared__ W s_rb[NW][G][K * K];
   __shared__ signed char s_partner[NW][K][32];
   __shared__ int s_ord[NW][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int grp = lane / K, j = lane % K;  // leaf slot in the warp, column in the leaf
-  W* Ra = s_ra[warp][grp];
-  W* Rb = s_rb[warp][grp];
+  W* Ra = s_ra[warp][grp < G ? grp : 0];
+  W* Rb = s_rb[warp][grp < G ? grp : 0];
   int* ord = s_ord[warp] + grp * K;
   const int nwarps = gridDim.x * NW;
   for (int base = (blockIdx.x * NW + warp) * G; base < nitems; base += nwarps * G) {
     const int it = base + grp;
-    const bool live = it < nitems;
+    const bool live = grp < G && it < nitems;
     TsCore d{};
     if (live) d = items[it];
     const int k = live ? d.k : 0;
@@ -560,7 +561,7 @@ __global__ void __launch_bounds__(NW * 32) tscore_kernel(const TsCore* __restric
         const int src = partner < 0 ? j : partner;
         W pw[K];
 #pragma unroll
-        for (int i = 0; i < K; ++i) pw[i] = wt_shfl_w(w[i], src, K);
+        for (int i = 0; i < K; ++i) pw[i] = wt_shfl_w(w[i], src, SW);
         const bool pair = partner >= 0 && j < k && partner < k;
         const bool is_p = j < partner;
         // both lanes of a pair sum the same squares in the same order; <p, q> is formed on
@@ -573,7 +574,7 @@ __global__ void __launch_bounds__(NW * 32) tscore_kernel(const TsCore* __restric
           n_oth += abs2(pw[i]);
           g_own = g_own + conjg(w[i]) * pw[i];
         }
-        const W g_p = wt_shfl_w(g_own, src, K);
+        const W g_p = wt_shfl_w(g_own, src, SW);
         const double al = is_p ? n_own : n_oth, be = is_p ? n_oth : n_own;
         const W g = is_p ? g_own : g_p;
         const double ag = sqrt(abs2(g));
@@ -596,7 +597,7 @@ __global__ void __launch_bounds__(NW * 32) tscore_kernel(const TsCore* __restric
           }
         }
 #pragma unroll
-        for (int i = 0; i < K; ++i) pw[i] = wt_shfl_w(v[i], src, K);
+        for (int i = 0; i < K; ++i) pw[i] = wt_shfl_w(v[i], src, SW);
         if (do_rot) {
 #pragma unroll
           for (int i = 0; i < K; ++i) {
@@ -620,18 +621,18 @@ __global__ void __launch_bounds__(NW * 32) tscore_kernel(const TsCore* __restric
     int rnk = 0;
 #pragma unroll
     for (int i = 0; i < K; ++i) {
-      const double si = __shfl_sync(0xffffffffu, sg, i, K);
+      const double si = __shfl_sync(0xffffffffu, sg, i, SW);
       if (i < k) rnk += (si > sg) || (si == sg && i < j);
     }
     if (j < k) ord[rnk] = j;
     __syncwarp();
     int nk = 0;
     {
-      const double thr = __shfl_sync(0xffffffffu, sg, k > 0 ? ord[0] : j, K) * eps;
+      const double thr = __shfl_sync(0xffffffffu, sg, k > 0 ? ord[0] : j, SW) * eps;
       bool run = true;
 #pragma unroll
       for (int i = 0; i < K; ++i) {
-        const double si = __shfl_sync(0xffffffffu, sg, i < k ? ord[i] : j, K);
+        const double si = __shfl_sync(0xffffffffu, sg, i < k ? ord[i] : j, SW);
         run = run && i < k && !(si <= thr);
         nk += run ? 1 : 0;
       }
@@ -639,11 +640,11 @@ __global__ void __launch_bounds__(NW * 32) tscore_kernel(const TsCore* __restric
     // Ma[:, c] = Rb^T V[:, o] / sqrt(s_o), Mb[:, c] = Ra^T conj(W[:, o]) / s_o^3/2 (lane = row)
     for (int c = 0; c < K; ++c) {
       const int o = c < nk ? ord[c] : j;
-      const double so = __shfl_sync(0xffffffffu, sg, o, K);
+      const double so = __shfl_sync(0xffffffffu, sg, o, SW);
       W ma = zero<W>(), mb = zero<W>();
 #pragma unroll
       for (int l = 0; l < K; ++l) {
-        const W vl = wt_shfl_w(v[l], o, K), wl = wt_shfl_w(w[l], o, K);
+        const W vl = wt_shfl_w(v[l], o, SW), wl = wt_shfl_w(w[l], o, SW);
         if (c < nk && j < k && l <= j) {
           ma = ma + Rb[l + j * K] * vl;
           mb = mb + Ra[l + j * K] * conjg(wl);
@@ -921,7 +922,7 @@ int ts_kmax() {
 }
 int ts_bucket(int k, int kmax) {
   if (k <= 0 || k > kmax) return 0;
-  return k <= 8 ? 8 : (k <= 16 ? 16 : 32);
+  return k <= 8 ? 8 : (k <= 16 ? 16 : (k <= 24 ? 24 : 32));
 }
 
 // Grid of a warp-per-item launch: the resident CTAs of `kernel`, at most one warp per item.
@@ -977,12 +978,15 @@ static void tsqr_k(const TsItem* items, int n, const T* ws, typename Traits<T>::
 template <typename T>
 void launch_tsqr(int K, const TsItem* items, int nitems, const T* ws, typename Traits<T>::wide* tri,
                  bool from_tri, cudaStream_t s) {
-    if (K == 8)
+  if (K == 8)
     tsqr_k<T, 8>(items, nitems, ws, tri, from_tri, s);
   else if (K == 16)
     tsqr_k<T, 16>(items, nitems, ws, tri, from_tri, s);
   else if constexpr (!Traits<T>::is_complex) {
-    if (K == 32) tsqr_k<T, 32>(items, nitems, ws, tri, from_tri, s);
+    if (K == 24)
+      tsqr_k<T, 24>(items, nitems, ws, tri, from_tri, s);
+    else if (K == 32)
+      tsqr_k<T, 32>(items, nitems, ws, tri, from_tri, s);
   }
 }
 
@@ -1003,12 +1007,15 @@ static void tscore_k(const TsCore* items, int n, const typename Traits<T>::wide*
 template <typename T>
 void launch_tscore(int K, const TsCore* items, int nitems, const typename Traits<T>::wide* tri,
                    typename Traits<T>::wide* maps, int* ranks, int* status, double eps, cudaStream_t s) {
-    if (K == 8)
+  if (K == 8)
     tscore_k<T, 8>(items, nitems, tri, maps, ranks, status, eps, s);
   else if (K == 16)
     tscore_k<T, 16>(items, nitems, tri, maps, ranks, status, eps, s);
   else if constexpr (!Traits<T>::is_complex) {
-    if (K == 32) tscore_k<T, 32>(items, nitems, tri, maps, ranks, status, eps, s);
+    if (K == 24)
+      tscore_k<T, 24>(items, nitems, tri, maps, ranks, status, eps, s);
+    else if (K == 32)
+      tscore_k<T, 32>(items, nitems, tri, maps, ranks, status, eps, s);
   }
 }
 
@@ -1028,12 +1035,15 @@ static void tsapply_k(const TsItem* items, int n, T* ws, const typename Traits<T
 template <typename T>
 void launch_tsapply(int K, const TsItem* items, int nitems, T* ws, const typename Traits<T>::wide* maps,
                     const int* ranks, cudaStream_t s) {
-    if (K == 8)
+  if (K == 8)
     tsapply_k<T, 8>(items, nitems, ws, maps, ranks, s);
   else if (K == 16)
     tsapply_k<T, 16>(items, nitems, ws, maps, ranks, s);
   else if constexpr (!Traits<T>::is_complex) {
-    if (K == 32) tsapply_k<T, 32>(items, nitems, ws, maps, ranks, s);
+    if (K == 24)
+      tsapply_k<T, 24>(items, nitems, ws, maps, ranks, s);
+    else if (K == 32)
+      tsapply_k<T, 32>(items, nitems, ws, maps, ranks, s);
   }
 }
 
@@ -1096,7 +1106,8 @@ void preload_truncate_kernels() {
   cudaFuncGetAttributes(&a, compact_kernel<T>);
   cudaFuncGetAttributes(&a, unpack_kernel<T>);
   const int kmax = ts_kmax<T>();
-  for (int K = 8; K <= kmax; K *= 2) {
+  for (int K : {8, 16, 24, 32}) {
+    if (K > kmax) break;
     launch_tsqr<T>(K, nullptr, 0, nullptr, nullptr, false, 0);
     launch_tsqr<T>(K, nullptr, 0, nullptr, nullptr, true, 0);
     launch_tscore<T>(K, nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0.0, 0);
