@@ -957,7 +957,7 @@ class Engine : public EngineBase {
         size_t budget = workspace_budget();
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget = std::max(budget, free_b / 3);
-        long long g = std::min<long long>((long long)tb_seg.size(), persistent_grid(2));
+        long long g = std::min<long long>((long long)tb_seg.size(), persistent_grid(4));
         g = std::max(1LL, std::min<long long>(g, (long long)(budget / (tb_slab * sizeof(W)))));
         tb_grid = (int)g;
         d_tb_scratch.alloc((size_t)(g * tb_slab));
