@@ -379,6 +379,7 @@ def main():
     # ---- mixed precision engine (headline) ----
     h32, wall32 = build(hb.HMAT_SIMPLE_PRECISION)
     pt32 = h32.phase_times()
+    aca32 = {k: v["threads"] for k, v in h32.aca_tuning().items()}
     T32 = h32.leaf_table()
     n_rk = int((T32[:, 4] == 1).sum())
     bytes32 = h32.gemv_bytes(nrhs)
@@ -451,7 +452,7 @@ def main():
                        f"{bytes32 / 1e9:.3f} GB)", "leaves": int(len(T32)), "rk_leaves": n_rk,
                        "bytes_per_step": bytes32, "assembly_device_ms": asm32, "assembly_wall_s": wall32,
                        "aca_leaves_per_s": n_rk / ((pt32["aca_ms"] + pt32["truncate_ms"]) * 1e-3),
-                       "phase_ms": pt32},
+                       "phase_ms": pt32, "aca_shapes": aca32},
             "roofline": {"bound": "hbm", "kernel": f"gemv {dom}", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": measured_traffic(dom),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture "

@@ -142,7 +142,8 @@ EXPORTED = [
     "hmat_b200_create_assembly", "hmat_b200_delete_assembly", "hmat_b200_gemv_device", "hmat_b200_gemv_device_noalloc",
     "hmat_b200_leaf_count",
     "hmat_b200_leaf_table", "hmat_b200_leaf_payload", "hmat_b200_payload_layout", "hmat_b200_leaf_gradients",
-    "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_gemv_launches", "hmat_b200_last_error",
+    "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_gemv_launches", "hmat_b200_aca_shapes",
+    "hmat_b200_last_error",
     "hmat_b200_clear_last_error",
 ]
 
@@ -186,6 +187,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "hmat_b200_phase_times": (C.c_int, [_P, _P]),
         "hmat_b200_gemv_profile": (C.c_int, [_P, C.c_char, _P, _P, C.c_int, _P, _P]),
         "hmat_b200_gemv_launches": (C.c_int, [_P, C.c_char, C.c_int]),
+        "hmat_b200_aca_shapes": (C.c_int, [_P, _P, _P, _P]),
         "hmat_b200_last_error": (C.c_char_p, []),
         "hmat_b200_clear_last_error": (None, []),
     }
@@ -519,6 +521,25 @@ class HMatrix:
         out = np.zeros(4, dtype=np.float64)
         _check(self.lib.hmat_b200_phase_times(self.m, out.ctypes.data), "hmat_b200_phase_times")
         return {"full_ms": out[0], "aca_ms": out[1], "truncate_ms": out[2], "gemv_ms": out[3]}
+
+    def aca_tuning(self) -> dict:
+        """ACA kernel shape per leaf-size bucket of the last assembly: bucket name ->
+        {"threads": 0 (warp per leaf) / 64 / 128 / 512, "how": "default" / "measured" /
+        "cached", "rates": leaf cost per ms of each sampled shape}; empty buckets omitted."""
+        shape = np.zeros(4, dtype=np.int32)
+        tuned = np.zeros(4, dtype=np.int32)
+        rate = np.zeros(16, dtype=np.float64)
+        _check(self.lib.hmat_b200_aca_shapes(self.m, shape.ctypes.data, tuned.ctypes.data, rate.ctypes.data),
+               "hmat_b200_aca_shapes")
+        names = ("m,n<=64", "m+n<2048", "m+n<8192", "m+n>=8192")
+        shapes = ("warp", "64", "128", "512")
+        out = {}
+        for b in range(4):
+            if shape[b] < 0:
+                continue
+            out[names[b]] = {"threads": int(shape[b]), "how": ("default", "measured", "cached")[int(tuned[b])],
+                             "rates": {shapes[s]: float(rate[4 * b + s]) for s in range(4) if rate[4 * b + s] > 0}}
+        return out
 
     def gemv_bytes(self, nrhs: int) -> int:
         """Algorithmic bytes of one product: every stored leaf scalar read once, x read and

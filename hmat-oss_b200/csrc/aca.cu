@@ -18,8 +18,9 @@
 namespace hmatb200 {
 namespace {
 
+constexpr int kAcaSmallThreads = 64;
 constexpr int kAcaThreads = 128;
-constexpr int kAcaBigThreads = 512;  // leaves with m + n >= kAcaBigRows
+constexpr int kAcaBigThreads = 512;
 
 template <typename T>
 struct Aca {
@@ -737,9 +738,24 @@ void launch_aca(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, con
   if (threads >= kAcaBigThreads)
     aca_run<T, kAcaBigThreads>(d_leaves, d_order, nleaves, kp, pts, epsilon, ws, flags, ranks, status, counter,
                                kcap_max, grid, s);
+  else if (threads <= kAcaSmallThreads)
+    aca_run<T, kAcaSmallThreads>(d_leaves, d_order, nleaves, kp, pts, epsilon, ws, flags, ranks, status, counter,
+                                 kcap_max, grid, s);
   else
     aca_run<T, kAcaThreads>(d_leaves, d_order, nleaves, kp, pts, epsilon, ws, flags, ranks, status, counter,
                             kcap_max, grid, s);
+}
+
+template <typename T, int NT>
+static int aca_resident_per_sm(int kcap_max) {
+  typedef typename Traits<T>::wide W;
+  const size_t smem = (size_t)kcap_max * (2 * sizeof(W) + sizeof(T));
+  if (smem > 48 * 1024) cudaFuncSetAttribute(aca_kernel<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, aca_kernel<T, NT>, NT, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  return per_sm;
 }
 
 // Rank capacity of the warp-per-leaf kernel's shared factors (its slots are 2 x 64 x kc
@@ -776,8 +792,26 @@ void launch_aca_warp(const RkLeafDesc* d_leaves, const int* d_order, int nleaves
 }
 
 template <typename T>
+int aca_concurrency(int threads, int kcap_max) {
+  if (threads == 0) {
+    const int kc = kcap_max < aca_warp_cap<T>() ? kcap_max : aca_warp_cap<T>();
+    const size_t smem = (size_t)kAwWarps * 2 * kc * kAwLen * sizeof(T);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, aca_warp_kernel<T>, kAwWarps * 32, smem) !=
+            cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    return persistent_grid(per_sm) * kAwWarps;
+  }
+  if (threads >= kAcaBigThreads) return persistent_grid(aca_resident_per_sm<T, kAcaBigThreads>(kcap_max));
+  if (threads <= kAcaSmallThreads) return persistent_grid(aca_resident_per_sm<T, kAcaSmallThreads>(kcap_max));
+  return persistent_grid(aca_resident_per_sm<T, kAcaThreads>(kcap_max));
+}
+
+template <typename T>
 void preload_aca_kernels() {
   cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, aca_kernel<T, kAcaSmallThreads>);
   cudaFuncGetAttributes(&a, aca_kernel<T, kAcaThreads>);
   cudaFuncGetAttributes(&a, aca_kernel<T, kAcaBigThreads>);
   cudaFuncGetAttributes(&a, dense_to_rk_kernel<T>);
@@ -786,6 +820,7 @@ void preload_aca_kernels() {
 
 #define HB_INST(T)                                                                                           \
   template void preload_aca_kernels<T>();                                                                  \
+  template int aca_concurrency<T>(int, int);                                                               \
   template void launch_aca_warp<T>(const RkLeafDesc*, const int*, int, const KernelParams&, Points, double, T*, \
                                    int*, int*, int*, int, cudaStream_t);                                    \
   template void launch_aca<T>(const RkLeafDesc*, const int*, int, const KernelParams&, Points, double, T*, \

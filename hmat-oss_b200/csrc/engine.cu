@@ -1,10 +1,14 @@
 // B200 engine: device residency and phase orchestration (see engine.h).
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <numeric>
 #include <string>
+#include <tuple>
 #include <type_traits>
 
 #include "engine.h"
@@ -68,6 +72,45 @@ bool tc_y_enabled() {
   return s && s[0] == '1';
 }
 
+// ACA autotuner.  Leaf-size buckets: leaves the warp-per-leaf kernel takes (m, n <= 64), then
+// m + n below kAcaBigRows, below 4 kAcaBigRows, and above.  Shapes: warp per leaf, CTAs of 64,
+// 128 and 512 threads; each bucket has two candidates and a default (the measured best on the
+// cylinder benchmark).  Every shape builds the same factors, so the choice only moves time.
+enum AcaShape { kShapeWarp = 0, kShape64 = 1, kShape128 = 2, kShape512 = 3 };
+constexpr int kAcaBuckets = 4;
+constexpr int kAcaShapes = 4;
+constexpr int kShapeThreads[kAcaShapes] = {0, 64, 128, 512};
+constexpr int kAcaCand[kAcaBuckets][2] = {
+    {kShapeWarp, kShape64}, {kShape64, kShape128}, {kShape128, kShape512}, {kShape128, kShape512}};
+constexpr int kAcaDefault[kAcaBuckets] = {kShapeWarp, kShape128, kShape128, kShape512};
+constexpr size_t kTuneRuns = 2 * kAcaBuckets;
+
+int aca_bucket(int m, int n) {
+  if (aca_warp_eligible(m, n)) return 0;
+  const int len = m + n;
+  return len < kAcaBigRows ? 1 : (len < 4 * kAcaBigRows ? 2 : 3);
+}
+// HMAT_B200_ACA_SHAPE=warp|64|128|512 forces one shape wherever it applies (the warp kernel
+// only takes bucket 0); -1 when unset.
+int forced_aca_shape() {
+  const char* s = getenv("HMAT_B200_ACA_SHAPE");
+  if (!s || !*s) return -1;
+  if (!strcmp(s, "warp")) return kShapeWarp;
+  const int t = atoi(s);
+  return t == 64 ? kShape64 : t == 128 ? kShape128 : t == 512 ? kShape512 : -1;
+}
+// HMAT_B200_ACA_TUNE=0 keeps the defaults; =2 samples every bucket of two leaves or more,
+// however small, and neither reads nor writes the process's choices (a test mode).
+int aca_tuning_mode() {
+  const char* s = getenv("HMAT_B200_ACA_TUNE");
+  if (!s || !*s) return 1;
+  return s[0] == '0' ? 0 : (s[0] == '2' ? 2 : 1);
+}
+// Choices measured so far in this process, by (scalar type, kernel kind, epsilon decade,
+// bucket).
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
+
 // Initial ACA rank capacity per leaf; leaves that reach it are rerun with twice as much.
 int initial_kcap() {
   const char* s = getenv("HMAT_B200_ACA_KCAP");
@@ -115,7 +158,9 @@ class Engine : public EngineBase {
     HB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     HB_CUDA(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking));
     HB_CUDA(cudaStreamCreateWithFlags(&stream3_, cudaStreamNonBlocking));
+    HB_CUDA(cudaStreamCreateWithFlags(&stream4_, cudaStreamNonBlocking));
     for (auto& e : ev_) HB_CUDA(cudaEventCreate(&e));
+    for (auto& e : tune_ev_) HB_CUDA(cudaEventCreate(&e));
     for (auto& e : fork_) HB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     ranks.assign(bt_->leaves.size(), -1);
     for (size_t i = 0; i < bt_->leaves.size(); ++i)
@@ -135,8 +180,10 @@ class Engine : public EngineBase {
     if (gexec_) cudaGraphExecDestroy(gexec_);
     for (auto& e : ev_) cudaEventDestroy(e);
     for (auto& e : fork_) cudaEventDestroy(e);
+    for (auto& e : tune_ev_) cudaEventDestroy(e);
     cudaStreamDestroy(stream2_);
     cudaStreamDestroy(stream3_);
+    cudaStreamDestroy(stream4_);
     cudaStreamDestroy(stream_);
   }
 
@@ -645,48 +692,130 @@ class Engine : public EngineBase {
       max_n = std::max(max_n, l.n);
       max_cap = std::max(max_cap, d.kcap);
     }
-    // small leaves to the warp-per-leaf ACA kernel, the others to the CTA-per-leaf one
-    std::vector<int> aca_order, aw_order, svd_order;
-    for (int b = 0; b < nb; ++b) {
-      if (jobs[b].svd)
-        svd_order.push_back(b);
-      else if (!jobs[b].cta && aca_warp_eligible(desc[b].m, desc[b].n))
-        aw_order.push_back(b);
-      else
-        aca_order.push_back(b);
-    }
+    // ACA shape of each leaf: the autotuner's choice for its size bucket; capacity retries run
+    // on CTAs (512 threads from m + n >= kAcaBigRows, where the retried ranks are high).
+    std::vector<int> svd_order, bucket_list[kAcaBuckets], shape_order[kAcaShapes];
     auto cost = [&](int b) { return (double)(desc[b].m + desc[b].n) * std::min(desc[b].m, desc[b].n); };
-    std::stable_sort(aca_order.begin(), aca_order.end(), [&](int x, int y) { return cost(x) > cost(y); });
-    // long leaves to 512-thread CTAs on a third stream: capacity retries (rank above the
-    // initial capacity) from m + n >= kAcaBigRows, any leaf from four times that.  Their fills
-    // and Gram terms are long chains a thread at 128 threads; shorter leaves of rank ~16
-    // measured faster on the 128-thread kernel.
-    std::vector<int> big_order;
-    {
-      std::vector<int> rest;
-      for (int b : aca_order) {
-        const int len = desc[b].m + desc[b].n;
-        (len >= 4 * kAcaBigRows || (jobs[b].cta && len >= kAcaBigRows) ? big_order : rest).push_back(b);
+    auto by_cost = [&](std::vector<int>& v) {
+      std::stable_sort(v.begin(), v.end(), [&](int x, int y) { return cost(x) > cost(y); });
+    };
+    const int forced = forced_aca_shape();
+    if (!src) {
+      for (int b = 0; b < nb; ++b) {
+        if (jobs[b].svd)
+          svd_order.push_back(b);
+        else if (jobs[b].cta)
+          shape_order[forced > kShapeWarp ? forced
+                                          : (desc[b].m + desc[b].n >= kAcaBigRows ? kShape512 : kShape128)]
+              .push_back(b);
+        else
+          bucket_list[aca_bucket(desc[b].m, desc[b].n)].push_back(b);
       }
-      aca_order.swap(rest);
     }
-    std::stable_sort(aw_order.begin(), aw_order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+    for (auto& v : bucket_list) by_cost(v);
+
+    // Autotuner: a bucket without a choice yet (for this scalar type, kernel kind and epsilon
+    // decade) runs one or two waves of each candidate shape on interleaved samples of its
+    // cost-sorted leaves, so that both samples are alike, timed alone on stream_; the shape
+    // with the most leaf cost per millisecond takes the rest of the bucket and is kept for
+    // the process.  The sampled leaves are compressed for good.
+    struct TuneRun {
+      int bucket, shape;
+      size_t begin, count;
+      double cost;
+    };
+    std::vector<TuneRun> runs;
+    std::vector<int> tune_order;
+    int choice[kAcaBuckets];
+    size_t sampled[kAcaBuckets] = {0, 0, 0, 0};
+    const int eps_dec = (int)std::floor(std::log10(std::max(eps_aca, 1e-300)) + 1e-9);
+    auto tune_key = [&](int bk) {
+      return std::make_tuple((int)sizeof(T) * 2 + (Traits<T>::is_complex ? 1 : 0), (int)kp_.kind, eps_dec, bk);
+    };
+    for (int bk = 0; bk < kAcaBuckets; ++bk) {
+      choice[bk] = kAcaDefault[bk];
+      const auto& lst = bucket_list[bk];
+      if (lst.empty()) continue;
+      aca_shape[bk] = kShapeThreads[choice[bk]];
+      if (forced >= 0) {
+        if (forced != kShapeWarp || bk == 0) choice[bk] = forced;
+        continue;
+      }
+      const int mode = aca_tuning_mode();
+      if (mode == 0) continue;
+      if (mode == 1) {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        auto it = g_tune_cache.find(tune_key(bk));
+        if (it != g_tune_cache.end()) {
+          choice[bk] = it->second;
+          if (aca_tuned[bk] != 1) aca_tuned[bk] = 2;  // an earlier batch of this assembly may have measured it
+          continue;
+        }
+      }
+      long long conc[2], wave = 0;
+      for (int v = 0; v < 2; ++v) {
+        conc[v] = aca_concurrency<T>(kShapeThreads[kAcaCand[bk][v]], max_cap);
+        wave += conc[v];
+      }
+      const long long n = (long long)lst.size();
+      // only where the samples are at most an eighth of the bucket: their serial runs and
+      // tails then cost about 1 % of the bucket's time
+      const int waves = n >= 16 * wave ? 2 : (n >= 8 * wave ? 1 : 0);
+      if (waves)
+        sampled[bk] = (size_t)(waves * wave);
+      else if (mode == 2 && n >= 2)
+        sampled[bk] = (size_t)(n / 2);
+      else
+        continue;
+      // position i goes to the shape furthest below its share (shares in proportion to the
+      // leaves each shape has in flight)
+      std::vector<int> samp[2];
+      for (size_t i = 0; i < sampled[bk]; ++i) {
+        const int v = (double)samp[0].size() * conc[1] <= (double)samp[1].size() * conc[0] ? 0 : 1;
+        samp[v].push_back(lst[i]);
+      }
+      for (int v = 0; v < 2; ++v) {
+        double c = 0;
+        for (int b : samp[v]) c += cost(b);
+        runs.push_back(TuneRun{bk, kAcaCand[bk][v], tune_order.size(), samp[v].size(), c});
+        tune_order.insert(tune_order.end(), samp[v].begin(), samp[v].end());
+      }
+    }
+    if (runs.size() > kTuneRuns) throw Error("ACA autotuner: too many sample runs");
+
     DevArray<RkLeafDesc> d_desc;
     d_desc.upload(desc, stream_);
     DevArray<T> d_ws;
     d_ws.alloc((size_t)ws);
     DevArray<unsigned char> d_flags;
     d_flags.alloc((size_t)std::max(fl, 1LL));
-    DevArray<int> d_ranks, d_status, d_counter, d_aca_order, d_aw_order, d_big_order, d_svd_order;
+    DevArray<int> d_ranks, d_status, d_counter, d_tune_order, d_svd_order, d_shape_order[kAcaShapes];
     d_ranks.alloc(nb);
     d_status.alloc(nb);
-    d_counter.alloc(3);
+    d_counter.alloc(kAcaShapes + kTuneRuns);
     HB_CUDA(cudaMemsetAsync(d_ranks.p, 0, nb * sizeof(int), stream_));
     HB_CUDA(cudaMemsetAsync(d_status.p, 0, nb * sizeof(int), stream_));
-    d_aca_order.upload(aca_order, stream_);
-    d_aw_order.upload(aw_order, stream_);
-    d_big_order.upload(big_order, stream_);
+    HB_CUDA(cudaMemsetAsync(d_counter.p, 0, (kAcaShapes + kTuneRuns) * sizeof(int), stream_));
+    d_tune_order.upload(tune_order, stream_);
     d_svd_order.upload(svd_order, stream_);
+    for (auto& d : d_shape_order) d.alloc((size_t)nb);
+    // the rest of each bucket goes to its chosen shape; without sample runs the lists are
+    // complete (and on the device) before the timed region
+    auto finish_shapes = [&]() {
+      for (int bk = 0; bk < kAcaBuckets; ++bk) {
+        if (bucket_list[bk].empty()) continue;
+        aca_shape[bk] = kShapeThreads[choice[bk]];
+        shape_order[choice[bk]].insert(shape_order[choice[bk]].end(), bucket_list[bk].begin() + sampled[bk],
+                                       bucket_list[bk].end());
+      }
+      for (int sh = 0; sh < kAcaShapes; ++sh) {
+        by_cost(shape_order[sh]);
+        if (!shape_order[sh].empty())
+          HB_CUDA(cudaMemcpyAsync(d_shape_order[sh].p, shape_order[sh].data(), shape_order[sh].size() * sizeof(int),
+                                  cudaMemcpyHostToDevice, stream_));
+      }
+    };
+    if (runs.empty()) finish_shapes();
     HB_CUDA(cudaStreamSynchronize(stream_));
 
     if (src) {
@@ -708,10 +837,6 @@ class Engine : public EngineBase {
         }
         ostore[b].bt_off = p;
       }
-      aca_order.clear();
-      aw_order.clear();
-      big_order.clear();
-      svd_order.clear();
       d_ranks.upload(k0, stream_);
       DevArray<RkStoreDesc> d_ostore;
       DevArray<PanelDesc> d_opanels;
@@ -721,39 +846,64 @@ class Engine : public EngineBase {
       HB_CUDA(cudaGetLastError());
       HB_CUDA(cudaStreamSynchronize(stream_));
     }
+    auto launch_shape = [&](int shape, const int* order, int count, int* counter, cudaStream_t s) {
+      if (count <= 0) return;
+      if (shape == kShapeWarp)
+        launch_aca_warp<T>(d_desc.p, order, count, kp_, pts_, eps_aca, d_ws.p, d_ranks.p, d_status.p, counter,
+                           max_cap, s);
+      else
+        launch_aca<T>(d_desc.p, order, count, kp_, pts_, eps_aca, d_ws.p, d_flags.p, d_ranks.p, d_status.p,
+                      counter, max_cap, aca_concurrency<T>(kShapeThreads[shape], max_cap), s, kShapeThreads[shape]);
+      HB_CUDA(cudaGetLastError());
+    };
     HB_CUDA(cudaEventRecord(ev_[2], stream_));
-    if (!aw_order.empty()) {
-      // beside the CTA kernel, on the second stream with its own work counter
-      HB_CUDA(cudaEventRecord(fork_[0], stream_));
-      HB_CUDA(cudaStreamWaitEvent(stream2_, fork_[0], 0));
-      HB_CUDA(cudaMemsetAsync(d_counter.p + 1, 0, sizeof(int), stream2_));
-      launch_aca_warp<T>(d_desc.p, d_aw_order.p, (int)aw_order.size(), kp_, pts_, eps_aca, d_ws.p, d_ranks.p,
-                         d_status.p, d_counter.p + 1, max_cap, stream2_);
-      HB_CUDA(cudaGetLastError());
-      HB_CUDA(cudaEventRecord(fork_[1], stream2_));
+    if (!runs.empty()) {
+      for (size_t r = 0; r < runs.size(); ++r) {
+        HB_CUDA(cudaEventRecord(tune_ev_[2 * r], stream_));
+        launch_shape(runs[r].shape, d_tune_order.p + runs[r].begin, (int)runs[r].count,
+                     d_counter.p + kAcaShapes + r, stream_);
+        HB_CUDA(cudaEventRecord(tune_ev_[2 * r + 1], stream_));
+      }
+      HB_CUDA(cudaStreamSynchronize(stream_));
+      double best[kAcaBuckets] = {0, 0, 0, 0};
+      for (size_t r = 0; r < runs.size(); ++r) {
+        float ms = 0;
+        HB_CUDA(cudaEventElapsedTime(&ms, tune_ev_[2 * r], tune_ev_[2 * r + 1]));
+        const int bk = runs[r].bucket;
+        const double rate = runs[r].cost / std::max((double)ms, 1e-6);
+        aca_rate[bk][runs[r].shape] = rate;
+        if (rate > best[bk]) {
+          best[bk] = rate;
+          choice[bk] = runs[r].shape;
+        }
+      }
+      const bool keep = aca_tuning_mode() == 1;
+      std::lock_guard<std::mutex> g(g_tune_mu);
+      for (const auto& r : runs) {
+        if (keep) g_tune_cache[tune_key(r.bucket)] = choice[r.bucket];
+        aca_tuned[r.bucket] = 1;
+      }
     }
-    if (!big_order.empty()) {
-      HB_CUDA(cudaEventRecord(fork_[2], stream_));
-      HB_CUDA(cudaStreamWaitEvent(stream3_, fork_[2], 0));
-      HB_CUDA(cudaMemsetAsync(d_counter.p + 2, 0, sizeof(int), stream3_));
-      launch_aca<T>(d_desc.p, d_big_order.p, (int)big_order.size(), kp_, pts_, eps_aca, d_ws.p, d_flags.p, d_ranks.p,
-                    d_status.p, d_counter.p + 2, max_cap, persistent_grid(2), stream3_, 512);
-      HB_CUDA(cudaGetLastError());
-      HB_CUDA(cudaEventRecord(fork_[3], stream3_));
+    if (!runs.empty()) finish_shapes();
+    // each shape on its own stream, beside the others: warp per leaf, 512, 64 on the side
+    // streams, 128 and the dense-SVD fills on stream_
+    const cudaStream_t side[kAcaShapes] = {stream2_, stream4_, stream_, stream3_};
+    for (int sh = 0; sh < kAcaShapes; ++sh) {
+      if (shape_order[sh].empty() || side[sh] == stream_) continue;
+      HB_CUDA(cudaEventRecord(fork_[2 * sh], stream_));
+      HB_CUDA(cudaStreamWaitEvent(side[sh], fork_[2 * sh], 0));
+      launch_shape(sh, d_shape_order[sh].p, (int)shape_order[sh].size(), d_counter.p + sh, side[sh]);
+      HB_CUDA(cudaEventRecord(fork_[2 * sh + 1], side[sh]));
     }
-    if (!aca_order.empty()) {
-      HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
-      launch_aca<T>(d_desc.p, d_aca_order.p, (int)aca_order.size(), kp_, pts_, eps_aca, d_ws.p, d_flags.p,
-                    d_ranks.p, d_status.p, d_counter.p, max_cap, persistent_grid(8), stream_);
-      HB_CUDA(cudaGetLastError());
-    }
+    launch_shape(kShape128, d_shape_order[kShape128].p, (int)shape_order[kShape128].size(), d_counter.p + kShape128,
+                 stream_);
     if (!svd_order.empty()) {
       launch_dense_to_rk<T>(d_desc.p, d_svd_order.p, (int)svd_order.size(), kp_, pts_, d_ws.p, d_ranks.p,
                             d_status.p, stream_);
       HB_CUDA(cudaGetLastError());
     }
-    if (!aw_order.empty()) HB_CUDA(cudaStreamWaitEvent(stream_, fork_[1], 0));
-    if (!big_order.empty()) HB_CUDA(cudaStreamWaitEvent(stream_, fork_[3], 0));
+    for (int sh = 0; sh < kAcaShapes; ++sh)
+      if (!shape_order[sh].empty() && side[sh] != stream_) HB_CUDA(cudaStreamWaitEvent(stream_, fork_[2 * sh + 1], 0));
     HB_CUDA(cudaEventRecord(ev_[3], stream_));
     std::vector<int> h_status(nb), h_ranks(nb);
     HB_CUDA(cudaMemcpyAsync(h_status.data(), d_status.p, nb * sizeof(int), cudaMemcpyDeviceToHost, stream_));
@@ -1078,6 +1228,11 @@ class Engine : public EngineBase {
     const int nleaves = (int)L.size();
     piece_of_.assign(nleaves, -1);
     pieces_.clear();
+    for (int bk = 0; bk < kAcaBuckets; ++bk) {
+      aca_shape[bk] = -1;
+      aca_tuned[bk] = 0;
+      for (double& r : aca_rate[bk]) r = 0.0;
+    }
     std::vector<RkJob> queue;
     const int k0 = initial_kcap();
     for (int i = 0; i < nleaves; ++i) {
@@ -1486,9 +1641,11 @@ class Engine : public EngineBase {
   std::vector<int> rstarts_, cstarts_;
   cudaStream_t stream_ = nullptr;
   cudaStream_t stream2_ = nullptr;  // runs the tall-skinny truncation beside the CTA kernel
-  cudaStream_t stream3_ = nullptr;  // runs the long leaves' ACA beside the other ACA kernels
+  cudaStream_t stream3_ = nullptr;  // runs the 512-thread ACA beside the other ACA kernels
+  cudaStream_t stream4_ = nullptr;  // runs the 64-thread ACA beside the other ACA kernels
   cudaEvent_t ev_[8];
-  cudaEvent_t fork_[4];
+  cudaEvent_t fork_[2 * kAcaShapes];
+  cudaEvent_t tune_ev_[2 * kTuneRuns];  // brackets of the autotuner's sample runs
   KernelParams kp_{};
   Points pts_{};
   DevArray<double> d_pts_;

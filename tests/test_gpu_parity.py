@@ -167,6 +167,59 @@ def test_mixed_gemv_accuracy_wide_leaves(hb, nrhs):
         h32.close()
 
 
+@pytest.mark.parametrize("nrhs", [1, 5, 16])
+def test_fp32_product_error_on_stored_leaves(hb, nrhs):
+    """The FP32 products' own rounding, apart from assembly and compression: the mixed
+    engine's 'N' and 'T' products against the product of its stored FP32 leaves summed in
+    FP64.  The tensor-core split (its dropped lo x lo term and the TF32 rounding of the lo
+    parts cost up to 2^-21 a product) with round-to-nearest partial sums stays below 1e-6
+    relative, within four times a float32 BLAS evaluation of the same leaves (numpy, leaf by
+    leaf)."""
+    import importlib.util
+    import os
+    from conftest import ROOT
+    spec = importlib.util.spec_from_file_location("wl_rnd", os.path.join(ROOT, "hmat-oss_b200", "workloads.py"))
+    wl = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(wl)
+    pts = wl.cylinder(60, 120)
+    hb.set_parameters(compressionMinLeafSize=0)
+    h = hb.HMatrix(pts, hb.kernel(hb.LAPLACE_REG, delta=0.01), value_type=hb.HMAT_SIMPLE_PRECISION,
+                   leaf_size=64, eta=2.0, epsilon=1e-6)
+    try:
+        n = len(pts)
+        x = wl.rhs(n, nrhs, 17).astype(np.float32)
+        x64 = x.astype(np.float64)
+        pr, pc = h.perm(), h.perm(cols=True)
+        ex = {"N": np.zeros((n, nrhs)), "T": np.zeros((n, nrhs))}
+        f32 = {"N": np.zeros((n, nrhs), np.float32), "T": np.zeros((n, nrhs), np.float32)}
+        for i, (r0, m, c0, nn, t, k) in enumerate(h.leaf_table()):
+            rows, cols = pr[r0:r0 + m], pc[c0:c0 + nn]
+            p = h.leaf_payload(i)
+            if t == 0:
+                F = p.reshape(nn, m).T
+                ex["N"][rows] += F.astype(np.float64) @ x64[cols]
+                ex["T"][cols] += F.T.astype(np.float64) @ x64[rows]
+                f32["N"][rows] += F @ x[cols]
+                f32["T"][cols] += F.T @ x[rows]
+            elif k > 0:
+                A = p[:k * m].reshape(k, m).T
+                B = p[k * m:].reshape(k, nn).T
+                A64, B64 = A.astype(np.float64), B.astype(np.float64)
+                ex["N"][rows] += A64 @ (B64.T @ x64[cols])
+                ex["T"][cols] += B64 @ (A64.T @ x64[rows])
+                f32["N"][rows] += A @ (B.T @ x[cols])
+                f32["T"][cols] += B @ (A.T @ x[rows])
+        for trans in ("N", "T"):
+            got = h.gemv(x, trans).astype(np.float64)
+            e_dev = rel(got, ex[trans])
+            e_np = rel(f32[trans].astype(np.float64), ex[trans])
+            print(f"nrhs {nrhs} {trans}: device {e_dev:.3e}, float32 BLAS {e_np:.3e}")
+            assert e_dev < 1e-6
+            assert e_dev < 4 * e_np + 1e-8
+    finally:
+        h.close()
+
+
 @pytest.mark.parametrize("name", ["cfg0_laplace", "cube_expcov", "helmholtz_small", "tall_partial"])
 def test_single_rhs_transposed_products(hb, oracle, name):
     """Transposed products ('T', and 'C' for complex values) with one right-hand side agree
