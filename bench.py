@@ -176,6 +176,17 @@ def reference_arm(args, rank, world):
     return 0
 
 
+def max_over_ranks(value, dist, device="cuda"):
+    """The largest per-rank value (a step time): every rank times its own replica alone, so
+    the job's step time is the slowest rank's.  All ranks must call it, in the same order."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _time_device(fn, steps, warmup, stream):
     """Mean device ms of fn(stream) over `steps` calls after `warmup`, CUDA events on `stream`."""
     import torch
@@ -369,11 +380,7 @@ def main():
             h.gemv_device(xd.data_ptr(), yd.data_ptr(), nrhs, stream=sp)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / args.steps
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist)
         return ms, yd.T.cpu().numpy().astype(np.float64)
 
     # ---- mixed precision engine (headline) ----
@@ -405,11 +412,14 @@ def main():
     for _ in range(args.warmup):
         h32.hi.gemv(b"N", a.ctypes.data, h32.m, x_pin.data_ptr(), b.ctypes.data, y_pin.data_ptr(), nrhs)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         rc = h32.hi.gemv(b"N", a.ctypes.data, h32.m, x_pin.data_ptr(), b.ctypes.data, y_pin.data_ptr(), nrhs)
         assert rc == 0
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    # each call is synchronous (the result is in host memory when it returns)
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, dist)
 
     # ---- FP64 engine on the same inputs ----
     fp64 = None
@@ -434,7 +444,7 @@ def main():
         h64.close()
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cpu = cpu_baseline_reference(pts, x_host, cfg, steps=1, warmup=0)
         except Exception as e:  # reported, not fatal
@@ -460,8 +470,8 @@ def main():
                          "phase_ms": ph_ms, "phase_bytes": ph_bytes,
                          "whole_gemv_frac": bytes32 / (ms32 * 1e-3) / 1e9 / peak},
             "mixed_vs_fp64": fp64,
-            "e2e": {"value": bytes32 / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": e2e_ms,
-                    "h2d_bytes_per_step": n * nrhs * 4, "d2h_bytes_per_step": n * nrhs * 4,
+            "e2e": {"value": world * bytes32 / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": world * n * nrhs * 4, "d2h_bytes_per_step": world * n * nrhs * 4,
                     "path": "hmat_interface_t.gemv (C ABI), pinned host x/y"},
             "cpu_baseline": None if cpu is None or "error" in cpu else {
                 "value": cpu["gbs"], "unit": "GB/s", "cores": 1, "kind": "reference",
