@@ -1288,7 +1288,7 @@ class Engine : public EngineBase {
     const int xrow_bytes = gemv_rhs_stride((int)sizeof(T), Rmax) * (int)sizeof(T);
     // pieces start 16-byte aligned when cols * O * sizeof(T) is a multiple of 16
     const int g = sizeof(T) >= 16 ? 1 : 16 / (int)sizeof(T);
-    int cols = std::min(kWarpXBytes / xrow_bytes, kWarpPieceBytes / (O * (int)sizeof(T)));
+    int cols = std::min(kWarpXBytes / xrow_bytes, warp_piece_bytes((int)sizeof(T)) / (O * (int)sizeof(T)));
     cols -= cols % g;
     if (cols < g) throw Error("gemv plan: output too tall for a warp-level unit");
     return cols;
@@ -1335,7 +1335,9 @@ class Engine : public EngineBase {
     const size_t smem = map == 4      ? umma_smem_bytes()
                         : warp_level ? warp_stream_smem_bytes((int)sizeof(T))
                                      : stream_smem_bytes((int)sizeof(T), Rmax, RS16, omax, transposed);
-    int per_sm = (int)std::min<size_t>(8, (226 * 1024) / (smem + 1024));
+    // warp-level kernels: 228 KB of shared memory an SM, 1 KB reserved a CTA (their launch
+    // bounds guarantee the registers for that many CTAs)
+    int per_sm = (int)std::min<size_t>(8, ((warp_level ? 228 : 226) * 1024) / (smem + 1024));
     per_sm = std::max(per_sm, 1);
     const int wpc = warp_level ? warp_stream_warps_per_cta() : 1;
     const int nt = (int)tasks.size();
@@ -1406,7 +1408,7 @@ class Engine : public EngineBase {
       for (auto& t : tasks)
         for (int u = t.first_unit; u < t.first_unit + t.nunits; ++u) {
           const GemvUnit& g = units[u];
-          if ((long long)g.pel * sizeof(T) > kWarpPieceBytes || g.shift != 0 || g.c * xrow_bytes > kWarpXBytes)
+          if ((long long)g.pel * sizeof(T) > warp_piece_bytes((int)sizeof(T)) || g.shift != 0 || g.c * xrow_bytes > kWarpXBytes)
             throw Error("gemv plan: unit above the warp-level stage capacity");
         }
     }

@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(kThreads) stream_kernel(const GemvTask* __rest
 // instruction).  Summation orders are fixed, so repeated products are bitwise identical.
 constexpr int kWarpCTA = 4;
 constexpr int kWarpStages = 2;
-constexpr int kWarpStageBytes = kWarpPieceBytes + kWarpXBytes;
+__host__ __device__ constexpr int warp_stage_bytes(int elem_bytes) { return warp_piece_bytes(elem_bytes) + kWarpXBytes; }
 
 // R accumulators of one output row, and one X row as the FMAs consume it.
 template <typename T, int R, bool PAIR = std::is_same<T, float>::value && (R % 2 == 0)>
@@ -362,11 +362,11 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
   constexpr int OL = MODE == 0 ? 32 : 16;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  unsigned char* wbase = smem_raw + (size_t)warp * kWarpStages * kWarpStageBytes;
+  unsigned char* wbase = smem_raw + (size_t)warp * kWarpStages * warp_stage_bytes((int)sizeof(T));
   GemvUnit* uslot =
-      reinterpret_cast<GemvUnit*>(smem_raw + (size_t)kWarpCTA * kWarpStages * kWarpStageBytes) + warp * kWarpStages;
+      reinterpret_cast<GemvUnit*>(smem_raw + (size_t)kWarpCTA * kWarpStages * warp_stage_bytes((int)sizeof(T))) + warp * kWarpStages;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWarpCTA * kWarpStages *
-                                                               (kWarpStageBytes + sizeof(GemvUnit))) +
+                                                               (warp_stage_bytes((int)sizeof(T)) + sizeof(GemvUnit))) +
                    warp * kWarpStages;
   const int gw = blockIdx.x * kWarpCTA + warp;
   const int t0 = warp_begin[gw], t1 = warp_begin[gw + 1];
@@ -387,10 +387,10 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
     uslot[s] = U;
     const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(T));
     const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(T);
-    unsigned char* st = wbase + (size_t)s * kWarpStageBytes;
+    unsigned char* st = wbase + (size_t)s * warp_stage_bytes((int)sizeof(T));
     mbar_expect_tx(&bars[s], pbytes + xbytes);
     bulk_g2s(st, arena + U.poff, pbytes, &bars[s]);
-    bulk_g2s(st + kWarpPieceBytes, xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
+    bulk_g2s(st + warp_piece_bytes((int)sizeof(T)), xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
   };
   auto issue_next = [&](int v) {  // nxt holds units[v]
     issue(v, nxt);
@@ -445,8 +445,8 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
         }
       }
       const int c = uslot[s].c;
-      const T* P = reinterpret_cast<const T*>(wbase + (size_t)s * kWarpStageBytes);
-      const T* X = reinterpret_cast<const T*>(wbase + (size_t)s * kWarpStageBytes + kWarpPieceBytes);
+      const T* P = reinterpret_cast<const T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)));
+      const T* X = reinterpret_cast<const T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)) + warp_piece_bytes((int)sizeof(T)));
       // Rows of a lane past O read the next column (or, in the last column, the first
       // elements of the X rows of the same stage); they are never written.
       if constexpr (MODE == 2) {
@@ -464,11 +464,11 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
     if constexpr (MODE == 2) {
       // slices summed in slice order through the stage just consumed, QC right-hand sides
       // per round: lane's partial of (its row a, q) at sc[(lane * A2 + a) * QC + q - q0]
-      constexpr int QC0 = kWarpPieceBytes / (32 * A2 * (int)sizeof(T));
+      constexpr int QC0 = warp_piece_bytes((int)sizeof(T)) / (32 * A2 * (int)sizeof(T));
       constexpr int QC1 = QC0 >= 16 ? 16 : (QC0 >= 8 ? 8 : (QC0 >= 4 ? 4 : (QC0 >= 2 ? 2 : 1)));  // power of two
       constexpr int QC = QC1 < R ? QC1 : R;
       static_assert(QC >= 1 && (R % QC) == 0, "reduction chunk");
-      T* sc = reinterpret_cast<T*>(wbase + (size_t)s * kWarpStageBytes);
+      T* sc = reinterpret_cast<T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)));
       if (task.nunits > 0) {
 #pragma unroll
         for (int qc0 = 0; qc0 < R; qc0 += QC) {
@@ -590,18 +590,18 @@ __device__ __forceinline__ void mma_kstep(const float* P, const float* X, int k0
 }
 
 template <int R, int RS, int MT>
-__global__ void __launch_bounds__(kWarpCTA * 32, 4)
+__global__ void __launch_bounds__(kWarpCTA * 32, 5)
     mma_stream_kernel(const GemvTask* __restrict__ tasks, const int* __restrict__ warp_begin,
                       const GemvUnit* __restrict__ units, const float* __restrict__ arena, float* xz, int* err) {
   constexpr int NT = (R + 7) / 8;  // 8-column tiles of the right-hand sides
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, tg = lane & 3;
-  unsigned char* wbase = smem_raw + (size_t)warp * kWarpStages * kWarpStageBytes;
+  unsigned char* wbase = smem_raw + (size_t)warp * kWarpStages * warp_stage_bytes(4);
   GemvUnit* uslot =
-      reinterpret_cast<GemvUnit*>(smem_raw + (size_t)kWarpCTA * kWarpStages * kWarpStageBytes) + warp * kWarpStages;
+      reinterpret_cast<GemvUnit*>(smem_raw + (size_t)kWarpCTA * kWarpStages * warp_stage_bytes(4)) + warp * kWarpStages;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWarpCTA * kWarpStages *
-                                                               (kWarpStageBytes + sizeof(GemvUnit))) +
+                                                               (warp_stage_bytes(4) + sizeof(GemvUnit))) +
                    warp * kWarpStages;
   const int gw = blockIdx.x * kWarpCTA + warp;
   const int t0 = warp_begin[gw], t1 = warp_begin[gw + 1];
@@ -620,10 +620,10 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 4)
     uslot[s] = U;
     const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(float));
     const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(float);
-    unsigned char* st = wbase + (size_t)s * kWarpStageBytes;
+    unsigned char* st = wbase + (size_t)s * warp_stage_bytes(4);
     mbar_expect_tx(&bars[s], pbytes + xbytes);
     bulk_g2s(st, arena + U.poff, pbytes, &bars[s]);
-    bulk_g2s(st + kWarpPieceBytes, xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
+    bulk_g2s(st + warp_piece_bytes(4), xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
   };
   auto issue_next = [&](int v) {
     issue(v, nxt);
@@ -661,8 +661,8 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 4)
         }
       }
       const int c = uslot[s].c;
-      const float* P = reinterpret_cast<const float*>(wbase + (size_t)s * kWarpStageBytes);
-      const float* X = reinterpret_cast<const float*>(wbase + (size_t)s * kWarpStageBytes + kWarpPieceBytes);
+      const float* P = reinterpret_cast<const float*>(wbase + (size_t)s * warp_stage_bytes(4));
+      const float* X = reinterpret_cast<const float*>(wbase + (size_t)s * warp_stage_bytes(4) + warp_piece_bytes(4));
       int k0 = 0;
       // two steps per iteration: their MMA chains are independent and overlap
 #pragma unroll 2
@@ -1188,8 +1188,7 @@ size_t stream_smem_bytes(int elem_bytes, int R, int RS, int omax, bool transpose
 int gemv_rhs_stride(int elem_bytes, int R) { return R * elem_bytes >= 16 ? R : 16 / elem_bytes; }
 
 size_t warp_stream_smem_bytes(int elem_bytes) {
-  (void)elem_bytes;
-  return (size_t)kWarpCTA * kWarpStages * (kWarpStageBytes + sizeof(GemvUnit) + sizeof(uint64_t));
+  return (size_t)kWarpCTA * kWarpStages * (warp_stage_bytes(elem_bytes) + sizeof(GemvUnit) + sizeof(uint64_t));
 }
 int warp_stream_warps_per_cta() { return kWarpCTA; }
 
