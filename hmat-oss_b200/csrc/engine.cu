@@ -171,6 +171,8 @@ class Engine : public EngineBase {
     for (auto& b : cblocks_) cstarts_.push_back(b.off);
     err_.alloc(1);
     HB_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
+    HB_CUDA(cudaMallocHost(&h_err_, sizeof(int)));
+    *h_err_ = 0;
     preload_full_kernels<T>();
     preload_aca_kernels<T>();
     preload_truncate_kernels<T>();
@@ -181,6 +183,7 @@ class Engine : public EngineBase {
     for (auto& e : ev_) cudaEventDestroy(e);
     for (auto& e : fork_) cudaEventDestroy(e);
     for (auto& e : tune_ev_) cudaEventDestroy(e);
+    if (h_err_) cudaFreeHost(h_err_);
     cudaStreamDestroy(stream2_);
     cudaStreamDestroy(stream3_);
     cudaStreamDestroy(stream4_);
@@ -307,9 +310,14 @@ class Engine : public EngineBase {
       HB_CUDA(cudaMemcpyAsync(stage_y_.p, y, n_out * nrhs * sizeof(T), cudaMemcpyHostToDevice, stream_));
     gemv_device(trans, alpha, stage_x_.p, beta, stage_y_.p, nrhs, stream_);
     HB_CUDA(cudaMemcpyAsync(y, stage_y_.p, n_out * nrhs * sizeof(T), cudaMemcpyDeviceToHost, stream_));
+    // the pipeline-wait flag comes back with y (one synchronisation per call)
+    HB_CUDA(cudaMemcpyAsync(h_err_, err_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
     HB_CUDA(cudaStreamSynchronize(stream_));
     HB_CUDA(cudaGetLastError());
-    check_err_flag();
+    if (*h_err_) {
+      HB_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
+      throw Error("gemv: a shared-memory pipeline wait gave up (copy did not complete)");
+    }
     float ms = 0;
     if (cudaEventElapsedTime(&ms, ev_[6], ev_[7]) == cudaSuccess) times_ms[3] = ms;
   }
@@ -1293,16 +1301,32 @@ class Engine : public EngineBase {
     if (cols < g) throw Error("gemv plan: output too tall for a warp-level unit");
     return cols;
   }
+  // Columns and X offset of the FP32 units of a short piece (O rows): the stage split the
+  // other way (kWarpXBytesWide of X rows) when that gives wider units, as for B^T blocks of
+  // ranks below 16 (40 columns at rank 12 instead of 32).  Other types keep the fixed split.
+  static int warp_unit_cols_wide(int O, int* xoff) {
+    const int cols = warp_unit_cols(O);
+    *xoff = warp_piece_bytes((int)sizeof(T));
+    if (!std::is_same<T, float>::value) return cols;
+    const int stage = warp_piece_bytes(4) + kWarpXBytes;
+    const int xrow_bytes = gemv_rhs_stride(4, 16) * 4;
+    int wide = std::min(kWarpXBytesWide / xrow_bytes, (stage - kWarpXBytesWide) / (O * 4));
+    wide -= wide % 4;
+    if (wide <= cols) return cols;
+    *xoff = stage - kWarpXBytesWide;
+    return wide;
+  }
 
   // Units of out(O rows) += P X for a column-major O x C block at `poff`, X rows from `xrow`,
   // `cols` columns per unit.
-  void px_units(std::vector<GemvUnit>& u, long long poff, int O, int C, int xrow, int cols = 32) {
+  void px_units(std::vector<GemvUnit>& u, long long poff, int O, int C, int xrow, int cols = 32,
+                int xoff = warp_piece_bytes((int)sizeof(T))) {
     for (int j0 = 0; j0 < C; j0 += cols) {
       GemvUnit g;
       g.poff = poff + (long long)j0 * O;
       g.xrow = xrow + j0;
       g.c = std::min(cols, C - j0);
-      g.o0 = 0;
+      g.o0 = xoff;  // X rows' offset in a warp-level stage
       g.ow = O;
       g.pel = O * g.c;
       g.shift = (int)(g.poff % kPad);
@@ -1408,7 +1432,11 @@ class Engine : public EngineBase {
       for (auto& t : tasks)
         for (int u = t.first_unit; u < t.first_unit + t.nunits; ++u) {
           const GemvUnit& g = units[u];
-          if ((long long)g.pel * sizeof(T) > warp_piece_bytes((int)sizeof(T)) || g.shift != 0 || g.c * xrow_bytes > kWarpXBytes)
+          // FP32 tensor-core units carry their stage split; the other kernels use the fixed one
+          const long long stage = warp_piece_bytes((int)sizeof(T)) + kWarpXBytes;
+          const long long xoff = L.map == 3 ? g.o0 : warp_piece_bytes((int)sizeof(T));
+          if (xoff % 16 != 0 || xoff <= 0 || xoff > stage || (long long)g.pel * sizeof(T) > xoff || g.shift != 0 ||
+              (L.map != 3 && g.o0 != xoff) || g.c * xrow_bytes > stage - xoff)
             throw Error("gemv plan: unit above the warp-level stage capacity");
         }
     }
@@ -1451,7 +1479,9 @@ class Engine : public EngineBase {
       lu.clear();
       if (!trans) {
         // z = B^T x_J: B^T is k x n column-major after the A panels
-        px_units(lu, bt_offset(leaf), k.k, k.n, k.col_off, warp_unit_cols(k.k));
+        int xoff = 0;
+        const int zc = warp_unit_cols_wide(k.k, &xoff);
+        px_units(lu, bt_offset(leaf), k.k, k.n, k.col_off, zc, xoff);
       } else {
         // z' = A^T x_I: each A panel (len x k) is a transposed piece
         auto br = block_range(rblocks_, rstarts_, k.row_off, k.m);
@@ -1664,6 +1694,7 @@ class Engine : public EngineBase {
   GemvPlan plan_;
   DevArray<T> xz_, rz_, stage_x_, stage_y_;
   DevArray<int> err_;
+  int* h_err_ = nullptr;  // pinned copy of err_ for the host-buffer product
   cudaGraphExec_t gexec_ = nullptr;
   GraphKey gkey_;
 };

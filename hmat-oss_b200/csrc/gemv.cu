@@ -623,7 +623,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 5)
     unsigned char* st = wbase + (size_t)s * warp_stage_bytes(4);
     mbar_expect_tx(&bars[s], pbytes + xbytes);
     bulk_g2s(st, arena + U.poff, pbytes, &bars[s]);
-    bulk_g2s(st + warp_piece_bytes(4), xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
+    bulk_g2s(st + U.o0, xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
   };
   auto issue_next = [&](int v) {
     issue(v, nxt);
@@ -662,7 +662,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 5)
       }
       const int c = uslot[s].c;
       const float* P = reinterpret_cast<const float*>(wbase + (size_t)s * warp_stage_bytes(4));
-      const float* X = reinterpret_cast<const float*>(wbase + (size_t)s * warp_stage_bytes(4) + warp_piece_bytes(4));
+      const float* X = reinterpret_cast<const float*>(wbase + (size_t)s * warp_stage_bytes(4) + uslot[s].o0);
       int k0 = 0;
       // two steps per iteration: their MMA chains are independent and overlap
 #pragma unroll 2

@@ -22,7 +22,9 @@ struct GemvUnit {
   long long poff;  // element offset of the piece P in the arena (16-byte aligned)
   int xrow;        // first row of the X piece in the xz buffer
   int c;           // inner extent (rows of X)
-  int o0, ow;      // transposed units: output rows [o0, o0 + ow) this piece covers
+  int o0, ow;      // transposed units: output rows [o0, o0 + ow) this piece covers;
+                   // other units: o0 = byte offset of the X rows in a warp-level pipeline
+                   // stage (the piece's capacity; the FP32 tensor-core kernel reads it per unit)
   int pel;         // elements of the piece P (O x c, or c x ow when transposed)
   int shift;       // elements between the 16-byte aligned copy start and the piece
 };
@@ -68,6 +70,9 @@ constexpr int kTcXBytes = kTcCols * 16 * 4;
 // measured 8 % faster than 4 KB pieces, the kernel being issue-bound.
 __host__ __device__ constexpr int warp_piece_bytes(int elem_bytes) { return elem_bytes == 4 ? 3584 : 4096; }
 constexpr int kWarpXBytes = 2048;
+// FP32 units of short pieces (the z-phase's k x c blocks of B^T) may split the same stage the
+// other way, kWarpXBytesWide bytes of X rows after a piece of the rest.
+constexpr int kWarpXBytesWide = 3584;
 
 // A long leaf whose z is computed in several chunks: the chunks' partial slots
 // (nparts consecutive slots of k rows from part_row) are summed into final_row.
