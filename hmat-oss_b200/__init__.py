@@ -528,17 +528,17 @@ class HMatrix:
         "cached", "rates": leaf cost per ms of each sampled shape}; empty buckets omitted."""
         shape = np.zeros(4, dtype=np.int32)
         tuned = np.zeros(4, dtype=np.int32)
-        rate = np.zeros(16, dtype=np.float64)
+        rate = np.zeros(20, dtype=np.float64)
         _check(self.lib.hmat_b200_aca_shapes(self.m, shape.ctypes.data, tuned.ctypes.data, rate.ctypes.data),
                "hmat_b200_aca_shapes")
         names = ("m,n<=64", "m+n<2048", "m+n<8192", "m+n>=8192")
-        shapes = ("warp", "64", "128", "512")
+        shapes = ("warp", "64", "128", "256", "512")
         out = {}
         for b in range(4):
             if shape[b] < 0:
                 continue
             out[names[b]] = {"threads": int(shape[b]), "how": ("default", "measured", "cached")[int(tuned[b])],
-                             "rates": {shapes[s]: float(rate[4 * b + s]) for s in range(4) if rate[4 * b + s] > 0}}
+                             "rates": {shapes[s]: float(rate[5 * b + s]) for s in range(5) if rate[5 * b + s] > 0}}
         return out
 
     def gemv_bytes(self, nrhs: int) -> int:

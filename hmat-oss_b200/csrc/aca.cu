@@ -20,6 +20,7 @@ namespace {
 
 constexpr int kAcaSmallThreads = 64;
 constexpr int kAcaThreads = 128;
+constexpr int kAcaMidThreads = 256;
 constexpr int kAcaBigThreads = 512;
 
 template <typename T>
@@ -738,6 +739,9 @@ void launch_aca(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, con
   if (threads >= kAcaBigThreads)
     aca_run<T, kAcaBigThreads>(d_leaves, d_order, nleaves, kp, pts, epsilon, ws, flags, ranks, status, counter,
                                kcap_max, grid, s);
+  else if (threads >= kAcaMidThreads)
+    aca_run<T, kAcaMidThreads>(d_leaves, d_order, nleaves, kp, pts, epsilon, ws, flags, ranks, status, counter,
+                               kcap_max, grid, s);
   else if (threads <= kAcaSmallThreads)
     aca_run<T, kAcaSmallThreads>(d_leaves, d_order, nleaves, kp, pts, epsilon, ws, flags, ranks, status, counter,
                                  kcap_max, grid, s);
@@ -804,6 +808,7 @@ int aca_concurrency(int threads, int kcap_max) {
     return persistent_grid(per_sm) * kAwWarps;
   }
   if (threads >= kAcaBigThreads) return persistent_grid(aca_resident_per_sm<T, kAcaBigThreads>(kcap_max));
+  if (threads >= kAcaMidThreads) return persistent_grid(aca_resident_per_sm<T, kAcaMidThreads>(kcap_max));
   if (threads <= kAcaSmallThreads) return persistent_grid(aca_resident_per_sm<T, kAcaSmallThreads>(kcap_max));
   return persistent_grid(aca_resident_per_sm<T, kAcaThreads>(kcap_max));
 }
@@ -813,6 +818,7 @@ void preload_aca_kernels() {
   cudaFuncAttributes a;
   cudaFuncGetAttributes(&a, aca_kernel<T, kAcaSmallThreads>);
   cudaFuncGetAttributes(&a, aca_kernel<T, kAcaThreads>);
+  cudaFuncGetAttributes(&a, aca_kernel<T, kAcaMidThreads>);
   cudaFuncGetAttributes(&a, aca_kernel<T, kAcaBigThreads>);
   cudaFuncGetAttributes(&a, dense_to_rk_kernel<T>);
   launch_aca_warp<T>(nullptr, nullptr, 0, KernelParams{}, Points{}, 0.0, nullptr, nullptr, nullptr, nullptr, 1, 0);

@@ -1109,12 +1109,12 @@ int hmat_b200_phase_times(hmat_matrix_t* m, double* out4) {
   return 0;
 }
 
-int hmat_b200_aca_shapes(hmat_matrix_t* m, int* shape4, int* tuned4, double* rate16) {
-  if (!m || !shape4 || !tuned4 || !rate16) return fail("hmat_b200_aca_shapes", "null argument");
+int hmat_b200_aca_shapes(hmat_matrix_t* m, int* shape4, int* tuned4, double* rate20) {
+  if (!m || !shape4 || !tuned4 || !rate20) return fail("hmat_b200_aca_shapes", "null argument");
   for (int b = 0; b < 4; ++b) {
     shape4[b] = m->engine ? m->engine->aca_shape[b] : -1;
     tuned4[b] = m->engine ? m->engine->aca_tuned[b] : 0;
-    for (int s = 0; s < 4; ++s) rate16[4 * b + s] = m->engine ? m->engine->aca_rate[b][s] : 0.0;
+    for (int s = 0; s < 5; ++s) rate20[5 * b + s] = m->engine ? m->engine->aca_rate[b][s] : 0.0;
   }
   return 0;
 }

@@ -74,15 +74,15 @@ bool tc_y_enabled() {
 
 // ACA autotuner.  Leaf-size buckets: leaves the warp-per-leaf kernel takes (m, n <= 64), then
 // m + n below kAcaBigRows, below 4 kAcaBigRows, and above.  Shapes: warp per leaf, CTAs of 64,
-// 128 and 512 threads; each bucket has two candidates and a default (the measured best on the
-// cylinder benchmark).  Every shape builds the same factors, so the choice only moves time.
-enum AcaShape { kShapeWarp = 0, kShape64 = 1, kShape128 = 2, kShape512 = 3 };
+// 128, 256 and 512 threads; each bucket has two candidates and a default (the measured best on
+// the cylinder benchmark).  Every shape builds the same factors, so the choice only moves time.
+enum AcaShape { kShapeWarp = 0, kShape64 = 1, kShape128 = 2, kShape256 = 3, kShape512 = 4 };
 constexpr int kAcaBuckets = 4;
-constexpr int kAcaShapes = 4;
-constexpr int kShapeThreads[kAcaShapes] = {0, 64, 128, 512};
+constexpr int kAcaShapes = 5;
+constexpr int kShapeThreads[kAcaShapes] = {0, 64, 128, 256, 512};
 constexpr int kAcaCand[kAcaBuckets][2] = {
-    {kShapeWarp, kShape64}, {kShape64, kShape128}, {kShape128, kShape512}, {kShape128, kShape512}};
-constexpr int kAcaDefault[kAcaBuckets] = {kShapeWarp, kShape128, kShape128, kShape512};
+    {kShapeWarp, kShape64}, {kShape128, kShape256}, {kShape128, kShape256}, {kShape256, kShape512}};
+constexpr int kAcaDefault[kAcaBuckets] = {kShapeWarp, kShape128, kShape256, kShape256};
 constexpr size_t kTuneRuns = 2 * kAcaBuckets;
 
 int aca_bucket(int m, int n) {
@@ -90,14 +90,14 @@ int aca_bucket(int m, int n) {
   const int len = m + n;
   return len < kAcaBigRows ? 1 : (len < 4 * kAcaBigRows ? 2 : 3);
 }
-// HMAT_B200_ACA_SHAPE=warp|64|128|512 forces one shape wherever it applies (the warp kernel
+// HMAT_B200_ACA_SHAPE=warp|64|128|256|512 forces one shape wherever it applies (the warp kernel
 // only takes bucket 0); -1 when unset.
 int forced_aca_shape() {
   const char* s = getenv("HMAT_B200_ACA_SHAPE");
   if (!s || !*s) return -1;
   if (!strcmp(s, "warp")) return kShapeWarp;
   const int t = atoi(s);
-  return t == 64 ? kShape64 : t == 128 ? kShape128 : t == 512 ? kShape512 : -1;
+  return t == 64 ? kShape64 : t == 128 ? kShape128 : t == 256 ? kShape256 : t == 512 ? kShape512 : -1;
 }
 // HMAT_B200_ACA_TUNE=0 keeps the defaults; =2 samples every bucket of two leaves or more,
 // however small, and neither reads nor writes the process's choices (a test mode).
@@ -159,6 +159,7 @@ class Engine : public EngineBase {
     HB_CUDA(cudaStreamCreateWithFlags(&stream2_, cudaStreamNonBlocking));
     HB_CUDA(cudaStreamCreateWithFlags(&stream3_, cudaStreamNonBlocking));
     HB_CUDA(cudaStreamCreateWithFlags(&stream4_, cudaStreamNonBlocking));
+    HB_CUDA(cudaStreamCreateWithFlags(&stream5_, cudaStreamNonBlocking));
     for (auto& e : ev_) HB_CUDA(cudaEventCreate(&e));
     for (auto& e : tune_ev_) HB_CUDA(cudaEventCreate(&e));
     for (auto& e : fork_) HB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -187,6 +188,7 @@ class Engine : public EngineBase {
     cudaStreamDestroy(stream2_);
     cudaStreamDestroy(stream3_);
     cudaStreamDestroy(stream4_);
+    cudaStreamDestroy(stream5_);
     cudaStreamDestroy(stream_);
   }
 
@@ -723,10 +725,10 @@ class Engine : public EngineBase {
     for (auto& v : bucket_list) by_cost(v);
 
     // Autotuner: a bucket without a choice yet (for this scalar type, kernel kind and epsilon
-    // decade) runs one or two waves of each candidate shape on interleaved samples of its
-    // cost-sorted leaves, so that both samples are alike, timed alone on stream_; the shape
-    // with the most leaf cost per millisecond takes the rest of the bucket and is kept for
-    // the process.  The sampled leaves are compressed for good.
+    // decade) runs one or two waves of each candidate shape on samples spread evenly over its
+    // cost-sorted leaves and dealt alternately, so that both samples are alike, timed alone on
+    // stream_; the shape with the most leaf cost per millisecond takes the rest of the bucket
+    // and is kept for the process.  The sampled leaves are compressed for good.
     struct TuneRun {
       int bucket, shape;
       size_t begin, count;
@@ -735,7 +737,6 @@ class Engine : public EngineBase {
     std::vector<TuneRun> runs;
     std::vector<int> tune_order;
     int choice[kAcaBuckets];
-    size_t sampled[kAcaBuckets] = {0, 0, 0, 0};
     const int eps_dec = (int)std::floor(std::log10(std::max(eps_aca, 1e-300)) + 1e-9);
     auto tune_key = [&](int bk) {
       return std::make_tuple((int)sizeof(T) * 2 + (Traits<T>::is_complex ? 1 : 0), (int)kp_.kind, eps_dec, bk);
@@ -769,19 +770,28 @@ class Engine : public EngineBase {
       // only where the samples are at most an eighth of the bucket: their serial runs and
       // tails then cost about 1 % of the bucket's time
       const int waves = n >= 16 * wave ? 2 : (n >= 8 * wave ? 1 : 0);
+      size_t ns = 0;
       if (waves)
-        sampled[bk] = (size_t)(waves * wave);
+        ns = (size_t)(waves * wave);
       else if (mode == 2 && n >= 2)
-        sampled[bk] = (size_t)(n / 2);
+        ns = (size_t)(n / 2);
       else
         continue;
-      // position i goes to the shape furthest below its share (shares in proportion to the
-      // leaves each shape has in flight)
-      std::vector<int> samp[2];
-      for (size_t i = 0; i < sampled[bk]; ++i) {
+      // the samples are spread evenly over the cost-sorted bucket (the largest leaves alone
+      // misjudge a bucket of mostly small ones); sample leaf i goes to the shape furthest below
+      // its share (shares in proportion to the leaves each shape has in flight)
+      std::vector<int> samp[2], rest_bk;
+      std::vector<char> taken(lst.size(), 0);
+      for (size_t i = 0; i < ns; ++i) taken[(size_t)((double)i * lst.size() / ns)] = 1;
+      for (size_t i = 0; i < lst.size(); ++i) {
+        if (!taken[i]) {
+          rest_bk.push_back(lst[i]);
+          continue;
+        }
         const int v = (double)samp[0].size() * conc[1] <= (double)samp[1].size() * conc[0] ? 0 : 1;
         samp[v].push_back(lst[i]);
       }
+      bucket_list[bk].swap(rest_bk);  // the rest, still in cost order
       for (int v = 0; v < 2; ++v) {
         double c = 0;
         for (int b : samp[v]) c += cost(b);
@@ -813,7 +823,7 @@ class Engine : public EngineBase {
       for (int bk = 0; bk < kAcaBuckets; ++bk) {
         if (bucket_list[bk].empty()) continue;
         aca_shape[bk] = kShapeThreads[choice[bk]];
-        shape_order[choice[bk]].insert(shape_order[choice[bk]].end(), bucket_list[bk].begin() + sampled[bk],
+        shape_order[choice[bk]].insert(shape_order[choice[bk]].end(), bucket_list[bk].begin(),
                                        bucket_list[bk].end());
       }
       for (int sh = 0; sh < kAcaShapes; ++sh) {
@@ -893,9 +903,9 @@ class Engine : public EngineBase {
       }
     }
     if (!runs.empty()) finish_shapes();
-    // each shape on its own stream, beside the others: warp per leaf, 512, 64 on the side
-    // streams, 128 and the dense-SVD fills on stream_
-    const cudaStream_t side[kAcaShapes] = {stream2_, stream4_, stream_, stream3_};
+    // each shape on its own stream, beside the others: warp per leaf, 64, 256 and 512 on the
+    // side streams, 128 and the dense-SVD fills on stream_
+    const cudaStream_t side[kAcaShapes] = {stream2_, stream4_, stream_, stream5_, stream3_};
     for (int sh = 0; sh < kAcaShapes; ++sh) {
       if (shape_order[sh].empty() || side[sh] == stream_) continue;
       HB_CUDA(cudaEventRecord(fork_[2 * sh], stream_));
@@ -1675,6 +1685,7 @@ class Engine : public EngineBase {
   cudaStream_t stream2_ = nullptr;  // runs the tall-skinny truncation beside the CTA kernel
   cudaStream_t stream3_ = nullptr;  // runs the 512-thread ACA beside the other ACA kernels
   cudaStream_t stream4_ = nullptr;  // runs the 64-thread ACA beside the other ACA kernels
+  cudaStream_t stream5_ = nullptr;  // runs the 256-thread ACA beside the other ACA kernels
   cudaEvent_t ev_[8];
   cudaEvent_t fork_[2 * kAcaShapes];
   cudaEvent_t tune_ev_[2 * kTuneRuns];  // brackets of the autotuner's sample runs

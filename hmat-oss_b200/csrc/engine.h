@@ -57,12 +57,13 @@ class EngineBase {
   std::vector<int> ranks;  // per leaf, -1 for full leaves
   double times_ms[4] = {0, 0, 0, 0};
   // ACA autotuner report of the last assembly, per leaf-size bucket (m, n <= 64; m + n below
-  // 2,048; below 8,192; above): the CTA size used (0 = warp per leaf, 64, 128, 512; -1 = no
-  // leaves), how it was chosen (0 default or forced, 1 measured now, 2 cached from an earlier
-  // assembly of the process) and the measured leaf cost per ms of each shape (0 = not run).
+  // 2,048; below 8,192; above): the CTA size used (0 = warp per leaf, 64, 128, 256, 512; -1 =
+  // no leaves), how it was chosen (0 default or forced, 1 measured now, 2 cached from an
+  // earlier assembly of the process) and the measured leaf cost per ms of each shape (0 = not
+  // run).
   int aca_shape[4] = {-1, -1, -1, -1};
   int aca_tuned[4] = {0, 0, 0, 0};
-  double aca_rate[4][4] = {};
+  double aca_rate[4][5] = {};
 };
 
 std::unique_ptr<EngineBase> make_engine(int value_type, const ClusterTree* rows, const ClusterTree* cols,

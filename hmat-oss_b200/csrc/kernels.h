@@ -51,7 +51,7 @@ void launch_full_from_canonical(const FullLeafDesc* d_leaves, const long long* g
 
 // ACA+ (compression.cpp:553-724), delegating to partial ACA when n * 100 < m.  Leaves are
 // taken in `order` from a device work counter that must be zero at launch.  `threads` is the
-// CTA size: 64, 128 or 512.  Every size builds the same factors (the Gram terms are summed a
+// CTA size: 64, 128, 256 or 512.  Every size builds the same factors (the Gram terms are summed a
 // warp per term, pivot searches break ties by first index), so the size is a pure speed
 // choice, made per leaf-size bucket by the engine's autotuner.
 constexpr int kAcaBigRows = 2048;
@@ -59,7 +59,7 @@ template <typename T>
 void launch_aca(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, const KernelParams& kp, Points pts,
                 double epsilon, T* ws, unsigned char* flags, int* ranks, int* status, int* counter, int kcap_max,
                 int grid, cudaStream_t s, int threads = 128);
-// Leaves in flight at once on the whole GPU: resident CTAs of `threads` (64, 128, 512), or
+// Leaves in flight at once on the whole GPU: resident CTAs of `threads` (64 ... 512), or
 // resident warps of the warp-per-leaf kernel for threads == 0, at rank capacity kcap_max.
 template <typename T>
 int aca_concurrency(int threads, int kcap_max);

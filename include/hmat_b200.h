@@ -437,11 +437,12 @@ int hmat_b200_phase_times(hmat_matrix_t* hmatrix, double* out4);
 
 /* ACA autotuner report of the last assembly, per leaf-size bucket b (0: m, n <= 64; 1: m + n
  * below 2,048; 2: below 8,192; 3: above): shape4[b] = CTA size of the ACA kernel that ran the
- * bucket (0 = a warp per leaf, 64, 128 or 512; -1 = no leaf), tuned4[b] = 0 (default shape or
- * HMAT_B200_ACA_SHAPE), 1 (measured during that assembly), 2 (measured by an earlier assembly
- * of the process), rate16[4 b + s] = leaf cost ((m + n) min(m, n)) per ms that shape s (warp,
- * 64, 128, 512) reached on its sample, 0 when not run.  No counterpart in the reference. */
-int hmat_b200_aca_shapes(hmat_matrix_t* hmatrix, int* shape4, int* tuned4, double* rate16);
+ * bucket (0 = a warp per leaf, 64, 128, 256 or 512; -1 = no leaf), tuned4[b] = 0 (default
+ * shape or HMAT_B200_ACA_SHAPE), 1 (measured during that assembly), 2 (measured by an earlier
+ * assembly of the process), rate20[5 b + s] = leaf cost ((m + n) min(m, n)) per ms that shape
+ * s (warp, 64, 128, 256, 512) reached on its sample, 0 when not run.  No counterpart in the
+ * reference. */
+int hmat_b200_aca_shapes(hmat_matrix_t* hmatrix, int* shape4, int* tuned4, double* rate20);
 
 /* Last error message of the calling thread ("" if none). */
 const char* hmat_b200_last_error(void);

@@ -1,7 +1,8 @@
-"""ACA autotuner: the warp-per-leaf kernel and the CTA kernels of 64, 128 and 512 threads
-build the same factors (Gram terms summed a warp per term, pivot ties broken by first index),
-so the shape the autotuner picks per leaf-size bucket only moves time.  Each shape forced on
-every leaf it can take, and the autotuner's own sample runs, must give bit-identical leaves."""
+"""ACA autotuner: the warp-per-leaf kernel and the CTA kernels of 64, 128, 256 and 512
+threads build the same factors (Gram terms summed a warp per term, pivot ties broken by first
+index), so the shape the autotuner picks per leaf-size bucket only moves time.  Each shape
+forced on every leaf it can take, and the autotuner's own sample runs, must give bit-identical
+leaves."""
 import importlib.util
 import os
 
@@ -11,8 +12,8 @@ from conftest import ROOT
 
 pytestmark = pytest.mark.gpu
 
-ENVS = [{"HMAT_B200_ACA_SHAPE": "64"}, {"HMAT_B200_ACA_SHAPE": "128"}, {"HMAT_B200_ACA_SHAPE": "512"},
-        {"HMAT_B200_ACA_SHAPE": "warp"}, {"HMAT_B200_ACA_TUNE": "2"}]
+ENVS = [{"HMAT_B200_ACA_SHAPE": "64"}, {"HMAT_B200_ACA_SHAPE": "128"}, {"HMAT_B200_ACA_SHAPE": "256"},
+        {"HMAT_B200_ACA_SHAPE": "512"}, {"HMAT_B200_ACA_SHAPE": "warp"}, {"HMAT_B200_ACA_TUNE": "2"}]
 
 
 def _workloads():
