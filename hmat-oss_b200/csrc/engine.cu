@@ -767,9 +767,10 @@ class Engine : public EngineBase {
         wave += conc[v];
       }
       const long long n = (long long)lst.size();
-      // only where the samples are at most an eighth of the bucket: their serial runs and
-      // tails then cost about 1 % of the bucket's time
-      const int waves = n >= 16 * wave ? 2 : (n >= 8 * wave ? 1 : 0);
+      // only where the samples are at most a thirty-second of the bucket: each serial run
+      // lasts as long as its slowest leaf, about 0.5 ms for a bucket's largest leaves, which
+      // only a bucket of many waves amortises
+      const int waves = n >= 64 * wave ? 2 : (n >= 32 * wave ? 1 : 0);
       size_t ns = 0;
       if (waves)
         ns = (size_t)(waves * wave);
