@@ -327,13 +327,45 @@ static double complex complex_eval(const oracle_hmat* h, const oracle_kernel* k,
   return CMPLX(cos(kr) * s, sin(kr) * s);
 }
 
+/* Stratum `stratum` of a multi-strata kernel, or the sum of its strata in order for -1
+ * (the callback convention of hmat.h:552-583). */
+static double real_eval_s(const oracle_hmat* h, const oracle_kernel* k, int row, int col, int stratum) {
+  if (k->nstrata < 1) return real_eval(h, k, row, col);
+  double r = point_dist(h->pts + 3 * (size_t)row, h->pts + 3 * (size_t)col);
+  double sum = 0.0;
+  for (int q = 0; q < k->nstrata; ++q) {
+    if (stratum >= 0 && q != stratum) continue;
+    double w = k->sweight[q], a = k->sparam[q];
+    double v = k->kind == 0 ? w * (1.0 / (kFourPi * (r + a))) : w * exp(-r / a);
+    if (stratum >= 0) return v;
+    sum = sum + v;
+  }
+  return sum;
+}
+
+static double complex complex_eval_s(const oracle_hmat* h, const oracle_kernel* k, int row, int col, int stratum) {
+  if (k->nstrata < 1) return complex_eval(h, k, row, col);
+  double r = point_dist(h->pts + 3 * (size_t)row, h->pts + 3 * (size_t)col);
+  double sc = 1.0 / (kFourPi * (r + k->delta));
+  double re = 0.0, im = 0.0;
+  for (int q = 0; q < k->nstrata; ++q) {
+    if (stratum >= 0 && q != stratum) continue;
+    double w = k->sweight[q], kr = k->sparam[q] * r;
+    double vr = w * (cos(kr) * sc), vi = w * (sin(kr) * sc);
+    if (stratum >= 0) return CMPLX(vr, vi);
+    re = re + vr;
+    im = im + vi;
+  }
+  return CMPLX(re, im);
+}
+
 void oracle_kernel_eval(const oracle_hmat* h, const oracle_kernel* k, int row, int col, double* out) {
   if (k->kind == 2) {
-    double complex v = complex_eval(h, k, row, col);
+    double complex v = complex_eval_s(h, k, row, col, -1);
     out[0] = creal(v);
     out[1] = cimag(v);
   } else {
-    out[0] = real_eval(h, k, row, col);
+    out[0] = real_eval_s(h, k, row, col, -1);
   }
 }
 
@@ -350,7 +382,7 @@ static double complex complex_recip(double complex z) {
 #define REALP(x) (x)
 #define IAMAX_KEY(x) fabs(x)
 #define RECIP(x) (1.0 / (x))
-#define SC_EVAL(h, k, r, c) real_eval(h, k, r, c)
+#define SC_EVAL(h, k, r, c, s) real_eval_s(h, k, r, c, s)
 #include "oracle_leaf.inc"
 #undef SC
 #undef FN
@@ -369,7 +401,7 @@ static double complex complex_recip(double complex z) {
 #define REALP(x) creal(x)
 #define IAMAX_KEY(x) (fabs(creal(x)) + fabs(cimag(x)))
 #define RECIP(x) complex_recip(x)
-#define SC_EVAL(h, k, r, c) complex_eval(h, k, r, c)
+#define SC_EVAL(h, k, r, c, s) complex_eval_s(h, k, r, c, s)
 #include "oracle_leaf.inc"
 #undef SC
 #undef FN

@@ -30,6 +30,13 @@ typedef struct oracle_hmat oracle_hmat;
 typedef struct {
   int kind;
   double delta, ell, nugget, wavenumber;
+  /* Strata kernels (nstrata >= 1, at most 8; 0 for the plain kernel; assembly through
+   * advanced_compute, hmat.h:552-583): stratum s is sweight[s] times the kernel with its
+   * parameter (ell, delta or wavenumber) replaced by sparam[s], the nugget left out; full
+   * leaves and dense-SVD compressions take the sum of the strata in order, and with two
+   * strata or more ACA+ leaves are compressed stratum by stratum (compression.cpp:745-773). */
+  int nstrata;
+  double sparam[8], sweight[8];
 } oracle_kernel;
 
 /* Builds the cluster tree on n points (point-major xyz) with leaves of at most

@@ -22,7 +22,22 @@ REF_DRIVER = os.path.join(HERE, "_ref", "ref_driver")
 
 class Kernel(C.Structure):
     _fields_ = [("kind", C.c_int), ("delta", C.c_double), ("ell", C.c_double), ("nugget", C.c_double),
-                ("wavenumber", C.c_double)]
+                ("wavenumber", C.c_double), ("nstrata", C.c_int), ("sparam", C.c_double * 8),
+                ("sweight", C.c_double * 8)]
+
+
+def make_kernel(kind, delta=0.01, ell=0.3, nugget=0.0, wavenumber=0.0, strata_param=None, strata_weight=None):
+    """Kernel descriptor; strata_param / strata_weight give a multi-strata kernel (stratum s =
+    w_s times the kernel with parameter a_s: ell, delta or wavenumber)."""
+    k = Kernel(kind, delta, ell, nugget, wavenumber)
+    if strata_param is not None:
+        if len(strata_param) != len(strata_weight) or not 1 <= len(strata_param) <= 8:
+            raise ValueError("strata_param and strata_weight: same length, 1 to 8 strata")
+        k.nstrata = len(strata_param)
+        for s, (a, w) in enumerate(zip(strata_param, strata_weight)):
+            k.sparam[s] = a
+            k.sweight[s] = w
+    return k
 
 
 _lib = None
@@ -90,8 +105,9 @@ class OracleHMatrix:
                 "largest_rk_mem_cols", "largest_rk_mem_rank"]
         return dict(zip(keys, [int(v) for v in out]))
 
-    def assemble(self, kind, eps, delta=0.01, ell=0.3, nugget=0.0, wavenumber=0.0, min_leaf=0):
-        self.kernel = Kernel(kind, delta, ell, nugget, wavenumber)
+    def assemble(self, kind, eps, delta=0.01, ell=0.3, nugget=0.0, wavenumber=0.0, min_leaf=0, strata_param=None,
+                 strata_weight=None):
+        self.kernel = make_kernel(kind, delta, ell, nugget, wavenumber, strata_param, strata_weight)
         self.is_complex = kind == 2
         rc = lib().oracle_assemble2(self.h, C.byref(self.kernel), eps, int(self.is_complex), min_leaf)
         assert rc == 0
@@ -170,8 +186,10 @@ def have_reference():
 
 def run_reference(points, kind, eps, leaf=64, eta=2.0, delta=0.01, ell=0.3, nugget=0.0, wavenumber=0.0, x=None,
                   nrhs=1, trans="N", scalar="D", dump_factors=False, gemv_reps=1, min_leaf=0, leaf_cols=0,
-                  gemv_warmup=0, retrunc=0.0):
-    """Runs the reference library (oracle/_ref/ref_driver) and returns its outputs."""
+                  gemv_warmup=0, retrunc=0.0, strata_param=None, strata_weight=None):
+    """Runs the reference library (oracle/_ref/ref_driver) and returns its outputs.  With
+    strata_param / strata_weight, the matrix is assembled through advanced_compute with one
+    stratum per entry (w_s times the kernel with parameter a_s: ell, delta or wavenumber)."""
     if not have_reference():
         raise FileNotFoundError(REF_DRIVER)
     kname = {0: "laplace", 1: "expcov", 2: "helmholtz"}[kind]
@@ -184,6 +202,9 @@ def run_reference(points, kind, eps, leaf=64, eta=2.0, delta=0.01, ell=0.3, nugg
                  f"gemv_reps={gemv_reps}", f"gemv_warmup={gemv_warmup}", f"min_leaf={min_leaf}",
                  f"leaf_cols={leaf_cols}", f"retrunc={retrunc!r}",
                  f"out={os.path.join(d, 'out')}"]
+        if strata_param is not None:
+            lines.append("strata_param=" + ",".join(repr(float(a)) for a in strata_param))
+            lines.append("strata_weight=" + ",".join(repr(float(w)) for w in strata_weight))
         dt = {"D": np.float64, "S": np.float32, "Z": np.complex128, "C": np.complex64}[scalar]
         if x is not None:
             xp = os.path.join(d, "x.bin")

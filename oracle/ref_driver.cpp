@@ -6,7 +6,8 @@
 //   hmat_create_admissibility_standard                                (c_default_interface.cpp:215)
 //   hmat_create_compression_aca_plus                                  (compression.hpp:137)
 //   hi.create_empty_hmatrix_admissibility / set_low_rank_epsilon /
-//   assemble_generic (simple_compute callback) / gemv / get_info      (c_wrapping.hpp:41-96,233-252)
+//   assemble_generic (simple_compute callback, or advanced_compute +
+//   prepare for multi-strata kernels) / gemv / get_info               (c_wrapping.hpp:41-96,233-252)
 // and dumps what the parity tests compare: the cluster permutation, the leaf list,
 // the leaf payloads (optional), the gemv result and wall-clock timings.
 //
@@ -126,6 +127,89 @@ void complex_kernel(void* vctx, int row, int col, void* result) {
   out[1] = std::sin(kr) * s;
 }
 
+// Multi-strata kernel through advanced_compute (hmat.h:552-583): stratum s is w_s times the
+// base kernel with its own parameter (exp_cov: ell_s; laplace: delta_s; helmholtz:
+// wavenumber_s); stratum -1 sums the strata in order, as the full blocks and dense-SVD
+// compressions ask for (assembly.cpp:168-180, compression.cpp:745-773).
+struct StrataCtx {
+  KernelCtx base;
+  std::vector<double> param, weight;
+};
+
+std::complex<double> strata_value(const StrataCtx* s, int row, int col, int stratum) {
+  const KernelCtx* c = &s->base;
+  const double r = dist(c->pts + 3 * (size_t)row, c->pts + 3 * (size_t)col);
+  std::complex<double> sum(0.0, 0.0);
+  const int S = (int)s->param.size();
+  for (int q = 0; q < S; ++q) {
+    if (stratum >= 0 && q != stratum) continue;
+    const double w = s->weight[q], a = s->param[q];
+    std::complex<double> v;
+    if (c->kind == 0) {
+      v = std::complex<double>(w * (1.0 / (kFourPi * (r + a))), 0.0);
+    } else if (c->kind == 1) {
+      v = std::complex<double>(w * std::exp(-r / a), 0.0);
+    } else {
+      const double sc = 1.0 / (kFourPi * (r + c->delta));
+      const double kr = a * r;
+      v = std::complex<double>(w * (std::cos(kr) * sc), w * (std::sin(kr) * sc));
+    }
+    sum = stratum >= 0 ? v : std::complex<double>(sum.real() + v.real(), sum.imag() + v.imag());
+  }
+  return sum;
+}
+
+struct StrataBlock {
+  const StrataCtx* s;
+  std::vector<int> rows, cols;  // client indices of the block's rows and columns
+  bool complex_;
+};
+
+void strata_release(void* p) { delete (StrataBlock*)p; }
+
+bool g_strata_complex = false;
+
+void strata_prepare(int row_start, int row_count, int col_start, int col_count, int* row_hmat2client, int*,
+                    int* col_hmat2client, int*, void* context, hmat_block_info_t* info) {
+  StrataBlock* b = new StrataBlock;
+  b->s = (const StrataCtx*)context;
+  b->rows.assign(row_hmat2client + row_start, row_hmat2client + row_start + row_count);
+  b->cols.assign(col_hmat2client + col_start, col_hmat2client + col_start + col_count);
+  b->complex_ = g_strata_complex;
+  info->user_data = b;
+  info->release_user_data = strata_release;
+  info->number_of_strata = (int)b->s->param.size();
+}
+
+void strata_compute(struct hmat_block_compute_context_t* c) {
+  const StrataBlock* b = (const StrataBlock*)c->user_data;
+  double* out = (double*)c->block;
+  for (int j = 0; j < c->col_count; ++j)
+    for (int i = 0; i < c->row_count; ++i) {
+      const std::complex<double> v =
+          strata_value(b->s, b->rows[c->row_start + i], b->cols[c->col_start + j], c->stratum);
+      const size_t e = i + (size_t)j * c->row_count;
+      if (b->complex_) {
+        out[2 * e] = v.real();
+        out[2 * e + 1] = v.imag();
+      } else {
+        out[e] = v.real();
+      }
+    }
+}
+
+std::vector<double> parse_list(const std::string& s) {
+  std::vector<double> v;
+  size_t p = 0;
+  while (p < s.size()) {
+    size_t q = s.find(',', p);
+    if (q == std::string::npos) q = s.size();
+    if (q > p) v.push_back(atof(s.substr(p, q - p).c_str()));
+    p = q + 1;
+  }
+  return v;
+}
+
 double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -217,6 +301,22 @@ int run(const Params& p, hmat_value_t vt) {
   ctx.compression = hmat_create_compression_aca_plus(eps);
   ctx.user_context = &kctx;
   ctx.simple_compute = (vt == HMAT_DOUBLE_COMPLEX || vt == HMAT_SIMPLE_COMPLEX) ? complex_kernel : real_kernel;
+  // optional multi-strata assembly: strata_param=a0,a1,... strata_weight=w0,w1,...
+  StrataCtx sctx;
+  sctx.base = kctx;
+  sctx.param = parse_list(p.get("strata_param"));
+  sctx.weight = parse_list(p.get("strata_weight"));
+  if (!sctx.param.empty()) {
+    if (sctx.weight.size() != sctx.param.size()) {
+      fprintf(stderr, "strata_param and strata_weight differ in length\n");
+      return 2;
+    }
+    g_strata_complex = vt == HMAT_DOUBLE_COMPLEX || vt == HMAT_SIMPLE_COMPLEX;
+    ctx.simple_compute = nullptr;
+    ctx.advanced_compute = strata_compute;
+    ctx.prepare = strata_prepare;
+    ctx.user_context = &sctx;
+  }
   ctx.lower_symmetric = 0;
   ctx.factorization = hmat_factorization_none;
   t0 = now_s();

@@ -32,10 +32,25 @@ CASES = {
 }
 
 
+# Multi-strata kernels assembled through advanced_compute (one stratum a material: w_s times the
+# kernel with parameter a_s).  Kept apart from CASES: the device engine does not assemble them;
+# they pin the oracle's restatement of compress() over strata (compression.cpp:745-773) and of
+# formattedAddParts (rk_matrix.cpp:846-1009).
+STRATA_CASES = {
+    "strata_expcov": (lambda: wl.cube(800, 41),
+                      dict(kind=1, strata_param=[0.1, 0.3, 1.0], strata_weight=[1.0, 0.5, 0.25]),
+                      dict(leaf=32, eta=2.0, eps=1e-6), 2, 42, "D", True),
+    "strata_laplace_signed": (lambda: wl.cylinder(20, 30),
+                              dict(kind=0, strata_param=[0.01, 0.2], strata_weight=[1.0, -0.5]),
+                              dict(leaf=16, eta=2.0, eps=1e-10), 1, 44, "D", False),
+    "strata_helmholtz": (lambda: wl.cylinder(15, 20),
+                         dict(kind=2, delta=0.01, strata_param=[5.0, 12.0], strata_weight=[1.0, 0.5]),
+                         dict(leaf=16, eta=3.0, eps=1e-6), 1, 45, "Z", False),
+}
 
 
 def inputs(name):
-    build, kern, tree, nrhs, seed, scalar, dump = CASES[name]
+    build, kern, tree, nrhs, seed, scalar, dump = CASES[name] if name in CASES else STRATA_CASES[name]
     pts = build()
     x = wl.rhs(len(pts), nrhs, seed, complex_=scalar in ("Z", "C"))
     return pts, x

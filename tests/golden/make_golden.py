@@ -5,7 +5,8 @@ oracle/_ref/ (libhmat_ref.so + ref_driver, a driver over the reference's public 
 This script runs that driver on small seeded inputs and stores what the parity tests
 compare against: cluster permutations, leaf lists (offsets, sizes, type, rank), gemv
 results for 'N' and 'T', hmat_info_t fields and, for the smallest cases, the leaf
-payloads.  Inputs are regenerated from their seeds by the tests, so only outputs are
+payloads.  The multi-strata cases assemble through advanced_compute with one stratum a
+material.  Inputs are regenerated from their seeds by the tests, so only outputs are
 stored.
 
 Usage (where the reference tree and oracle/_ref exist):  python tests/golden/make_golden.py
@@ -22,11 +23,11 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, HERE)
 import oracle as O  # noqa: E402
 
-from cases import CASES, inputs  # noqa: E402
+from cases import CASES, STRATA_CASES, inputs  # noqa: E402
 
 
 def make(name):
-    _, kern, tree, nrhs, _, scalar, dump = CASES[name]
+    _, kern, tree, nrhs, _, scalar, dump = CASES[name] if name in CASES else STRATA_CASES[name]
     pts, x = inputs(name)
     out = {}
     rn = O.run_reference(pts, x=x, nrhs=nrhs, trans="N", scalar=scalar, dump_factors=dump, **kern, **tree)
@@ -58,5 +59,5 @@ def make(name):
 
 
 if __name__ == "__main__":
-    for n in (sys.argv[1:] or CASES):
+    for n in (sys.argv[1:] or list(CASES) + list(STRATA_CASES)):
         make(n)

@@ -2,7 +2,7 @@
 library's own outputs, stored as golden fixtures by tests/golden/make_golden.py."""
 import numpy as np
 import pytest
-from cases import CASES, inputs
+from cases import CASES, STRATA_CASES, inputs
 from conftest import golden, rel
 
 # gemv tolerance against the reference.  Real cases reproduce the reference's pivots and
@@ -86,3 +86,48 @@ def test_oracle_rk_factors_match_reference(oracle, name):
         assert rel(Mr, ex) < tol and rel(Mo, ex) < tol
     assert off == len(pay)
     assert flips <= max(1, nrk // 100)
+
+
+@pytest.mark.parametrize("name", sorted(STRATA_CASES))
+def test_oracle_multi_strata_assembly_matches_reference(oracle, name):
+    """compress() over strata (compression.cpp:745-773) and formattedAddParts
+    (rk_matrix.cpp:846-1009), restated: the reference assembled these matrices through
+    advanced_compute with one stratum a material; the oracle must give the same partition
+    and ranks, the same products to 1e-12 and, where stored, the same Rk blocks.  The cases
+    take both branches of formattedAddParts (concatenation, and the full-block sum compressed
+    by SVD once the summed rank reaches min(m, n)), real and complex, one with a negative
+    stratum weight."""
+    g = golden(name)
+    _, kern, tree, nrhs, seed, scalar, dump = STRATA_CASES[name]
+    pts, x = inputs(name)
+    o = oracle.OracleHMatrix(pts, leaf=tree["leaf"], eta=tree["eta"])
+    o.assemble(eps=tree["eps"], **kern)
+    L = o.leaves()
+    assert np.array_equal(o.perm(), g["perm"])
+    assert np.array_equal(L, g["leaves"]), "partition or ranks differ from the reference"
+    assert rel(o.gemv(x, "N"), g["y"]) < 1e-12
+    assert rel(o.gemv(x, "T"), g["y_T"]) < 1e-12
+    if "y_C" in g:
+        assert rel(o.gemv(x, "C"), g["y_C"]) < 1e-12
+    if dump:
+        pay, off = g["rk_payload"], 0
+        for i, (r0, m, c0, n, t, k) in enumerate(g["leaves"]):
+            if t != 1 or k <= 0:
+                continue
+            A = pay[off:off + k * m].reshape(k, m).T
+            B = pay[off + k * m:off + k * (m + n)].reshape(k, n).T
+            off += k * (m + n)
+            assert rel(o.block(i, L), A @ B.T) < 1e-11, i
+        assert off == len(pay)
+
+
+def test_oracle_single_stratum_equals_plain_kernel(oracle):
+    """One stratum of weight 1 is the plain kernel: the same leaves as the simple
+    interaction callback's assembly."""
+    pts, x = inputs("cube_expcov")
+    a = oracle.OracleHMatrix(pts, leaf=32, eta=2.0)
+    a.assemble(kind=1, eps=1e-6, ell=0.3)
+    b = oracle.OracleHMatrix(pts, leaf=32, eta=2.0)
+    b.assemble(kind=1, eps=1e-6, strata_param=[0.3], strata_weight=[1.0])
+    assert np.array_equal(a.leaves(), b.leaves())
+    assert rel(a.gemv(x), b.gemv(x)) == 0.0
