@@ -109,3 +109,17 @@ def test_vector_reorder_restore_roundtrip(hb):
         assert np.array_equal(w, v)
     finally:
         h.close()
+
+
+def test_aca_report_before_assembly(hb):
+    """The ACA autotuner report of a matrix that was never assembled: no bucket ran."""
+    pts = np.random.default_rng(3).random((300, 3))
+    h = hb.HMatrix(pts, hb.kernel(hb.LAPLACE_REG), assemble=False, leaf_size=16)
+    try:
+        assert h.aca_tuning() == {}
+        lib = hb.load_library()
+        assert lib.hmat_b200_aca_shapes(None, None, None, None) != 0
+        assert b"null argument" in lib.hmat_b200_last_error()
+        lib.hmat_b200_clear_last_error()
+    finally:
+        h.close()
