@@ -139,7 +139,7 @@ EXPORTED = [
     "hmat_create_compression_rrqr", "hmat_delete_compression", "hmat_default_progress",
     "hmat_assemble_context_init", "hmat_factorization_context_init", "hmat_solve_context_init",
     "hmat_init_default_interface", "hmat_get_parameters", "hmat_set_parameters", "hmat_get_version",
-    "hmat_b200_create_assembly", "hmat_b200_delete_assembly", "hmat_b200_gemv_device", "hmat_b200_gemv_device_noalloc",
+    "hmat_b200_create_assembly", "hmat_b200_delete_assembly", "hmat_b200_gemv_device", "hmat_b200_gemv_device_noalloc", "hmat_b200_gemv_status",
     "hmat_b200_leaf_count",
     "hmat_b200_leaf_table", "hmat_b200_leaf_payload", "hmat_b200_payload_layout", "hmat_b200_leaf_gradients",
     "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_gemv_launches", "hmat_b200_aca_shapes",
@@ -179,6 +179,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "hmat_b200_delete_assembly": (None, [_P]),
         "hmat_b200_gemv_device": (C.c_int, [_P, C.c_char, _P, _P, _P, _P, C.c_int, _P]),
         "hmat_b200_gemv_device_noalloc": (C.c_int, [_P, C.c_char, _P, _P, _P, _P, C.c_int, _P]),
+        "hmat_b200_gemv_status": (C.c_int, [_P, _P, C.POINTER(C.c_int)]),
         "hmat_b200_leaf_count": (C.c_int, [_P]),
         "hmat_b200_leaf_table": (C.c_int, [_P, _P]),
         "hmat_b200_leaf_payload": (C.c_longlong, [_P, C.c_int, _P]),
@@ -335,6 +336,13 @@ class HMatrix:
         b = np.array([beta], dtype=self.dtype)
         return self.lib.hmat_b200_gemv_device_noalloc(self.m, trans.encode(), a.ctypes.data, C.c_void_p(x_ptr),
                                                       b.ctypes.data, C.c_void_p(y_ptr), nrhs, C.c_void_p(stream))
+
+    def gemv_status(self, stream=0) -> bool:
+        """True if a device product of this matrix stopped since the last query because a
+        kernel's wait for a bulk copy gave up (hmat_b200_gemv_status; clears the flag)."""
+        failed = C.c_int(0)
+        _check(self.lib.hmat_b200_gemv_status(self.m, C.c_void_p(stream), C.byref(failed)), "hmat_b200_gemv_status")
+        return bool(failed.value)
 
     def info(self) -> dict:
         return self.hi.get_info(self.m).as_dict()

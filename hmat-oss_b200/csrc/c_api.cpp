@@ -1040,6 +1040,15 @@ int hmat_b200_gemv_device(hmat_matrix_t* m, char trans, const void* alpha, const
   return 0;
 }
 
+int hmat_b200_gemv_status(hmat_matrix_t* m, void* stream, int* failed) {
+  HB_TRY("hmat_b200_gemv_status", {
+    if (!m || !failed) throw Error("null argument");
+    if (!m->engine || !m->engine->assembled) throw Error("matrix is not assembled");
+    *failed = m->engine->gemv_status((cudaStream_t)stream);
+  });
+  return 0;
+}
+
 int hmat_b200_leaf_count(hmat_matrix_t* m) { return m ? (int)m->bt.leaves.size() : -1; }
 
 int hmat_b200_leaf_table(hmat_matrix_t* m, int* out) {

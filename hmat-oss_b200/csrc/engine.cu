@@ -111,6 +111,24 @@ int aca_tuning_mode() {
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
 
+// Bound of each gemv kernel's wait for a bulk copy (polls of the stage barrier).
+// HMAT_B200_GEMV_WAIT_LIMIT changes it for the matrices created while it is set; a negative
+// value makes every wait give up at once (a test hook: the kernels flag the product, let
+// their copies land and stop, so that the status path is checked without a fault).
+long long gemv_wait_limit() {
+  const char* s = getenv("HMAT_B200_GEMV_WAIT_LIMIT");
+  const long long v = (s && *s) ? atoll(s) : kGemvWaitLimit;
+  return v < 0 ? -1 : (v < 1 ? 1 : v);
+}
+
+// Cap on the Jacobi sweeps of the truncation's core SVDs.  HMAT_B200_JACOBI_SWEEPS lowers it
+// (a test hook: with one sweep most cores do not converge and the assembly reports it).
+int jacobi_sweeps() {
+  const char* s = getenv("HMAT_B200_JACOBI_SWEEPS");
+  const int v = (s && *s) ? atoi(s) : kJacobiDefaultSweeps;
+  return v < 1 ? 1 : v;
+}
+
 // Initial ACA rank capacity per leaf; leaves that reach it are rerun with twice as much.
 int initial_kcap() {
   const char* s = getenv("HMAT_B200_ACA_KCAP");
@@ -170,10 +188,13 @@ class Engine : public EngineBase {
     cblocks_ = output_blocks(*C_);
     for (auto& b : rblocks_) rstarts_.push_back(b.off);
     for (auto& b : cblocks_) cstarts_.push_back(b.off);
+    HB_CUDA(cudaGetDevice(&device));
     err_.alloc(1);
-    HB_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
-    HB_CUDA(cudaMallocHost(&h_err_, sizeof(int)));
-    *h_err_ = 0;
+    HB_CUDA(cudaMallocHost(&h_err_, sizeof(GemvStatus)));
+    h_err_->failed = 0;
+    h_err_->pad = 0;
+    h_err_->wait_limit = gemv_wait_limit();
+    HB_CUDA(cudaMemcpy(err_.p, h_err_, sizeof(GemvStatus), cudaMemcpyHostToDevice));
     preload_full_kernels<T>();
     preload_aca_kernels<T>();
     preload_truncate_kernels<T>();
@@ -312,13 +333,13 @@ class Engine : public EngineBase {
       HB_CUDA(cudaMemcpyAsync(stage_y_.p, y, n_out * nrhs * sizeof(T), cudaMemcpyHostToDevice, stream_));
     gemv_device(trans, alpha, stage_x_.p, beta, stage_y_.p, nrhs, stream_);
     HB_CUDA(cudaMemcpyAsync(y, stage_y_.p, n_out * nrhs * sizeof(T), cudaMemcpyDeviceToHost, stream_));
-    // the pipeline-wait flag comes back with y (one synchronisation per call)
-    HB_CUDA(cudaMemcpyAsync(h_err_, err_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    // the status flag comes back with y (one synchronisation per call)
+    HB_CUDA(cudaMemcpyAsync(&h_err_->failed, &err_.p->failed, sizeof(int), cudaMemcpyDeviceToHost, stream_));
     HB_CUDA(cudaStreamSynchronize(stream_));
     HB_CUDA(cudaGetLastError());
-    if (*h_err_) {
-      HB_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
-      throw Error("gemv: a shared-memory pipeline wait gave up (copy did not complete)");
+    if (h_err_->failed) {
+      clear_status(stream_);
+      throw Error(kWaitGaveUp);
     }
     float ms = 0;
     if (cudaEventElapsedTime(&ms, ev_[6], ev_[7]) == cudaSuccess) times_ms[3] = ms;
@@ -370,6 +391,7 @@ class Engine : public EngineBase {
     if (!assembled) throw Error("matrix is not assembled");
     if (Traits<T>::is_complex) throw Error("leaf gradients are implemented for real value types");
     if (nrhs < 1 || nrhs > 16) throw Error("leaf gradients take 1 to 16 right-hand sides");
+    check_device();
     xz_.ensure(xz_elems());
     rz_.ensure(xz_elems());
     cudaStream_t s = user_stream ? user_stream : stream_;
@@ -484,6 +506,8 @@ class Engine : public EngineBase {
   // assembly's truncation kernels, then the arena and the gemv schedule rebuilt.
   void retruncate(double eps) override {
     if (!assembled) throw Error("matrix not assembled");
+    check_device();
+    HB_CUDA(set_jacobi_max_sweeps(jacobi_sweeps()));
     const auto& L = bt_->leaves;
     const int nleaves = (int)L.size();
     double saved[4];
@@ -586,7 +610,7 @@ class Engine : public EngineBase {
     bytes3[2] = (full + (trans == 'N' ? fa : fb)) * s + n_out * nrhs * s;
   }
 
-  size_t gemv_scratch_bytes() const override { return 256 + xz_elems() * sizeof(T); }
+  size_t gemv_scratch_bytes() const override { return xz_elems() * sizeof(T); }
   int gemv_launches(char trans, int nrhs) const override {
     if (!assembled) throw Error("matrix not assembled");
     return gemv_launch_count(plan_, trans, nrhs, (int)sizeof(T));
@@ -597,12 +621,21 @@ class Engine : public EngineBase {
     check_gemv_args(trans, nrhs);
     if (nrhs == 0) return;
     if (gemv_scratch_bytes() > scratch_bytes) throw Error("scratch buffer too small for this matrix");
-    int* err = (int*)scratch;
-    T* xz = (T*)((char*)scratch + 256);
     cudaStream_t s = stream ? stream : stream_;
-    HB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-    launch_gemv<T>(plan_, trans, nrhs, *(const T*)alpha, *(const T*)beta, (const T*)x, (T*)y, xz, err, s);
+    // the status flag is the matrix's own (allocated with the engine), read by gemv_status
+    launch_gemv<T>(plan_, trans, nrhs, *(const T*)alpha, *(const T*)beta, (const T*)x, (T*)y, (T*)scratch, err_.p,
+                   s);
     HB_CUDA(cudaGetLastError());
+  }
+
+  int gemv_status(cudaStream_t user_stream) override {
+    check_device();
+    cudaStream_t s = user_stream ? user_stream : stream_;
+    HB_CUDA(cudaMemcpyAsync(&h_err_->failed, &err_.p->failed, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    const int failed = h_err_->failed;
+    if (failed) clear_status(s);
+    return failed;
   }
 
  private:
@@ -626,18 +659,39 @@ class Engine : public EngineBase {
     return (size_t)std::max(plan_.xz_rows, 1LL) * gemv_rhs_stride((int)sizeof(T), 16);
   }
 
+  static constexpr const char* kWaitGaveUp =
+      "gemv: a kernel's wait for a bulk copy gave up, in this product or an earlier device product of this matrix "
+      "(its result is not valid)";
+
+  // The engine's streams, arena and status block live on the device that was current when
+  // the matrix was created; products must be issued with that device current.
+  void check_device() const {
+    int d = -1;
+    HB_CUDA(cudaGetDevice(&d));
+    if (d != device)
+      throw Error("the current CUDA device (" + std::to_string(d) + ") is not the matrix's device (" +
+                  std::to_string(device) + ")");
+  }
+
+  void clear_status(cudaStream_t s) {
+    h_err_->failed = 0;
+    HB_CUDA(cudaMemsetAsync(&err_.p->failed, 0, sizeof(int), s));
+    HB_CUDA(cudaStreamSynchronize(s));
+  }
+
   void check_gemv_args(char trans, int nrhs) {
     if (!assembled) throw Error("matrix is not assembled");
+    check_device();
     if (trans != 'N' && trans != 'T' && trans != 'C') throw Error("gemv: trans must be 'N', 'T' or 'C'");
     if (nrhs < 0) throw Error("gemv: negative number of right-hand sides");
   }
 
   void check_err_flag() {
     int e = 0;
-    HB_CUDA(cudaMemcpy(&e, err_.p, sizeof(int), cudaMemcpyDeviceToHost));
+    HB_CUDA(cudaMemcpy(&e, &err_.p->failed, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
-      HB_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
-      throw Error("gemv: a shared-memory pipeline wait gave up (copy did not complete)");
+      clear_status(stream_);
+      throw Error(kWaitGaveUp);
     }
   }
 
@@ -1193,8 +1247,15 @@ class Engine : public EngineBase {
     HB_CUDA(cudaStreamSynchronize(stream_));
     HB_CUDA(cudaEventElapsedTime(&ms, ev_[4], ev_[5]));
     times_ms[2] += ms;
-    for (int b = 0; b < nb; ++b)
+    for (int b = 0; b < nb; ++b) {
       if (h_status[b] == kLeafAcaCapacity) h_ranks[b] = 0;
+      else if (h_status[b] != kLeafOk)
+        throw Error("truncation failed on leaf " + std::to_string(jobs[b].leaf) +
+                    (h_status[b] == kLeafSvdNoConverge
+                         ? ": the Jacobi SVD of its core did not converge within " + std::to_string(jacobi_sweeps()) +
+                               " sweeps"
+                         : " (status " + std::to_string(h_status[b]) + ")"));
+    }
     // storage of each leaf in the new piece: A row panels, then B^T
     std::vector<RkStoreDesc> store(nb);
     std::vector<PanelDesc> panels;
@@ -1242,6 +1303,7 @@ class Engine : public EngineBase {
   }
 
   void assemble_rk(int method, double eps_aca, double eps_trunc, int svd_below) {
+    HB_CUDA(set_jacobi_max_sweeps(jacobi_sweeps()));
     (void)method;
     const auto& L = bt_->leaves;
     const int nleaves = (int)L.size();
@@ -1705,8 +1767,8 @@ class Engine : public EngineBase {
   SideBuf side_buf_[2];
   GemvPlan plan_;
   DevArray<T> xz_, rz_, stage_x_, stage_y_;
-  DevArray<int> err_;
-  int* h_err_ = nullptr;  // pinned copy of err_ for the host-buffer product
+  DevArray<GemvStatus> err_;       // status block of this matrix's products (flag, wait bound)
+  GemvStatus* h_err_ = nullptr;    // pinned host copy
   cudaGraphExec_t gexec_ = nullptr;
   GraphKey gkey_;
 };

@@ -52,8 +52,13 @@ class EngineBase {
   virtual int gemv_launches(char trans, int nrhs) const = 0;
   virtual void gemv_device_with_scratch(char trans, const void* alpha, const void* x, const void* beta, void* y,
                                         int nrhs, cudaStream_t stream, void* scratch, size_t scratch_bytes) = 0;
+  // 1 if a product of this matrix on the device entry points stopped because a kernel's wait
+  // for a bulk copy gave up since the last query (the flag is then cleared), else 0.
+  // Synchronises `stream` (NULL: the matrix's own stream).
+  virtual int gemv_status(cudaStream_t stream) = 0;
 
   bool assembled = false;
+  int device = 0;  // the CUDA device the matrix lives on (current when it was created)
   std::vector<int> ranks;  // per leaf, -1 for full leaves
   double times_ms[4] = {0, 0, 0, 0};
   // ACA autotuner report of the last assembly, per leaf-size bucket (m, n <= 64; m + n below

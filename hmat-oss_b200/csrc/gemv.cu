@@ -31,7 +31,6 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kPieceCols = 32;         // inner extent of a non-transposed unit
 constexpr int kPieceElems = 128 * 32;  // P capacity of a stage (elements)
 constexpr int kMaxInner = 128;         // inner extent of a transposed unit
-constexpr long long kWaitLimit = 1LL << 26;
 
 // ---------------------------------------------------------------------------------
 // TMA bulk copy + mbarrier helpers
@@ -59,6 +58,26 @@ __device__ inline bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "r"(smem_u32(bar)), "r"(parity)
       : "memory");
   return ok != 0;
+}
+
+// Bounded wait for a barrier phase: false once `limit` polls went by without it completing.
+// A negative limit gives up at once (a test mode of the status path: the caller still drains
+// its copies with a positive limit before it stops).
+__device__ inline bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long limit) {
+  if (limit < 0) return false;
+  long long spins = 0;
+  while (!mbar_try_wait(bar, parity))
+    if (++spins > limit) return false;
+  return true;
+}
+
+// A warp whose wait gave up: sets the status flag, then waits (bounded) for the copies of
+// the units it has issued and not consumed (u .. last_issued, one stage each) to land, so
+// that no bulk copy is still writing its shared memory when it exits.
+__device__ inline void warp_give_up(GemvStatus* st, uint64_t* bars, int nstages, int u_begin, int u, int last_issued) {
+  atomicExch(&st->failed, 1);
+  for (int v = u; v <= last_issued; ++v)
+    mbar_wait_bounded(&bars[(v - u_begin) % nstages], (uint32_t)(((v - u_begin) / nstages) & 1), kGemvDrainLimit);
 }
 
 __device__ inline uint32_t round16(uint64_t b) { return (uint32_t)((b + 15) & ~15ull); }
@@ -121,7 +140,7 @@ __global__ void __launch_bounds__(kThreads) stream_kernel(const GemvTask* __rest
                                                           const T* __restrict__ arena, T* xz, int conj,
                                                           int out_is_y, const int* __restrict__ perm_out,
                                                           T* __restrict__ y, int ldy, int q0, int r, T alpha,
-                                                          T beta, int* err) {
+                                                          T beta, GemvStatus* err) {
   constexpr int LS = 32 / OL;
   constexpr int OMAX = OL * RPT;
   constexpr int XCAP = (TRANSP ? kMaxInner : kPieceCols) * RS;
@@ -136,6 +155,7 @@ __global__ void __launch_bounds__(kThreads) stream_kernel(const GemvTask* __rest
   if (t0 >= t1) return;
   const int u_begin = tasks[t0].first_unit;
   const int u_end = tasks[t1 - 1].first_unit + tasks[t1 - 1].nunits;
+  const long long wlim = err->wait_limit;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ol = lane % OL, ls = lane / OL;
@@ -171,13 +191,7 @@ __global__ void __launch_bounds__(kThreads) stream_kernel(const GemvTask* __rest
     for (int k = 0; k < task.nunits; ++k, ++u) {
       const int s = (u - u_begin) % NSTAGE;
       const uint32_t parity = (uint32_t)(((u - u_begin) / NSTAGE) & 1);
-      long long spins = 0;
-      while (!mbar_try_wait(&bars[s], parity)) {
-        if (++spins > kWaitLimit) {
-          if (tid == 0) atomicExch(err, 1);
-          return;  // a copy that never lands: stop this CTA, the host sees the error flag
-        }
-      }
+      const bool ok = mbar_wait_bounded(&bars[s], parity, wlim);
       const GemvUnit U = units[u];
       const T* P = Ps + (size_t)s * PCAP + U.shift;
       const T* X = Xs + (size_t)s * XCAP;
@@ -215,7 +229,17 @@ __global__ void __launch_bounds__(kThreads) stream_kernel(const GemvTask* __rest
           }
         }
       }
-      __syncthreads();  // stage s is free again
+      // stage s is free again; a copy that did not land in time stops the whole CTA, after
+      // the copies it has in flight (units u .. u + NSTAGE - 1) have landed
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicExch(&err->failed, 1);
+          for (int v = u; v < u_end && v < u + NSTAGE; ++v)
+            mbar_wait_bounded(&bars[(v - u_begin) % NSTAGE], (uint32_t)(((v - u_begin) / NSTAGE) & 1),
+                              kGemvDrainLimit);
+        }
+        return;
+      }
       if (tid == 0 && u + NSTAGE < u_end) issue(u + NSTAGE);
     }
 
@@ -357,7 +381,7 @@ constexpr int warp_min_blocks() {
 template <typename T, int R, int RS, int MODE, int A2>
 __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
     warp_stream_kernel(const GemvTask* __restrict__ tasks, const int* __restrict__ warp_begin,
-                       const GemvUnit* __restrict__ units, const T* __restrict__ arena, T* xz, int* err) {
+                       const GemvUnit* __restrict__ units, const T* __restrict__ arena, T* xz, GemvStatus* err) {
   using Ops = RowOps<T, R>;
   constexpr int OL = MODE == 0 ? 32 : 16;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -373,6 +397,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
   if (t0 >= t1) return;
   const int u_begin = tasks[t0].first_unit;
   const int u_end = tasks[t1 - 1].first_unit + tasks[t1 - 1].nunits;
+  const long long wlim = err->wait_limit;
 
   if (lane == 0) {
     for (int s = 0; s < kWarpStages; ++s) mbar_init(&bars[s], 1);
@@ -382,8 +407,10 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
   // lane 0: descriptor into the stage, then the unit's two bulk copies.  The descriptor of
   // the next unit to issue is loaded one issue ahead, off the critical path.
   GemvUnit nxt;
+  int last_issued = u_begin - 1;  // lane 0: the last unit whose copies were issued
   auto issue = [&](int u, const GemvUnit& U) {
     const int s = (u - u_begin) % kWarpStages;
+    last_issued = u;
     uslot[s] = U;
     const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(T));
     const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(T);
@@ -437,12 +464,10 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
     for (int kk = 0; kk < task.nunits; ++kk, ++u) {
       s = (u - u_begin) % kWarpStages;
       const uint32_t parity = (uint32_t)(((u - u_begin) / kWarpStages) & 1);
-      long long spins = 0;
-      while (!mbar_try_wait(&bars[s], parity)) {
-        if (++spins > kWaitLimit) {
-          if (lane == 0) atomicExch(err, 1);
-          return;
-        }
+      if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bars[s], parity, wlim))) {
+        // a copy did not land in time: flag it, let the copies in flight land, stop the warp
+        if (lane == 0) warp_give_up(err, bars, kWarpStages, u_begin, u, last_issued);
+        return;
       }
       const int c = uslot[s].c;
       const T* P = reinterpret_cast<const T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)));
@@ -592,7 +617,7 @@ __device__ __forceinline__ void mma_kstep(const float* P, const float* X, int k0
 template <int R, int RS, int MT>
 __global__ void __launch_bounds__(kWarpCTA * 32, 5)
     mma_stream_kernel(const GemvTask* __restrict__ tasks, const int* __restrict__ warp_begin,
-                      const GemvUnit* __restrict__ units, const float* __restrict__ arena, float* xz, int* err) {
+                      const GemvUnit* __restrict__ units, const float* __restrict__ arena, float* xz, GemvStatus* err) {
   constexpr int NT = (R + 7) / 8;  // 8-column tiles of the right-hand sides
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -608,6 +633,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 5)
   if (t0 >= t1) return;
   const int u_begin = tasks[t0].first_unit;
   const int u_end = tasks[t1 - 1].first_unit + tasks[t1 - 1].nunits;
+  const long long wlim = err->wait_limit;
 
   if (lane == 0) {
     for (int s = 0; s < kWarpStages; ++s) mbar_init(&bars[s], 1);
@@ -615,8 +641,10 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 5)
   }
   __syncwarp();
   GemvUnit nxt;
+  int last_issued = u_begin - 1;  // lane 0: the last unit whose copies were issued
   auto issue = [&](int u, const GemvUnit& U) {
     const int s = (u - u_begin) % kWarpStages;
+    last_issued = u;
     uslot[s] = U;
     const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(float));
     const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(float);
@@ -653,12 +681,9 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 5)
     for (int kk = 0; kk < task.nunits; ++kk, ++u) {
       const int s = (u - u_begin) % kWarpStages;
       const uint32_t parity = (uint32_t)(((u - u_begin) / kWarpStages) & 1);
-      long long spins = 0;
-      while (!mbar_try_wait(&bars[s], parity)) {
-        if (++spins > kWaitLimit) {
-          if (lane == 0) atomicExch(err, 1);
-          return;
-        }
+      if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bars[s], parity, wlim))) {
+        if (lane == 0) warp_give_up(err, bars, kWarpStages, u_begin, u, last_issued);
+        return;
       }
       const int c = uslot[s].c;
       const float* P = reinterpret_cast<const float*>(wbase + (size_t)s * warp_stage_bytes(4));
@@ -755,21 +780,11 @@ __device__ __forceinline__ float4 tc_hi(float4 v, float4& lo) {
   lo = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
   return h;
 }
-__device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity, int* err) {
-  long long spins = 0;
-  while (!mbar_try_wait(bar, parity)) {
-    if (++spins > kWaitLimit) {
-      atomicExch(err, 1);
-      return false;
-    }
-  }
-  return true;
-}
 
 template <int RS>
 __global__ void __launch_bounds__(kTcThreads, 1)
     umma_stream_kernel(const GemvTask* __restrict__ tasks, const int* __restrict__ cta_begin,
-                       const GemvUnit* __restrict__ units, const float* __restrict__ arena, float* xz, int* err) {
+                       const GemvUnit* __restrict__ units, const float* __restrict__ arena, float* xz, GemvStatus* err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* ring = smem_raw;
   unsigned char* tAh = ring + kTcStages * kTcStage;
@@ -785,6 +800,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (t0 >= t1) return;
   const int u_begin = tasks[t0].first_unit;
   const int u_end = tasks[t1 - 1].first_unit + tasks[t1 - 1].nunits;
+  const long long wlim = err->wait_limit;
   if (tid == 0) {
     for (int s = 0; s < kTcStages; ++s) mbar_init(&full[s], 1);
     mbar_init(mmab, 1);
@@ -801,9 +817,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const uint32_t tmem = *tslot;
   const uint32_t tlane = tmem + ((uint32_t)(warp * 32) << 16);
 
+  int last_issued = u_begin - 1;  // thread 0: the last unit whose copies were issued
   auto issue = [&](int v) {
     const GemvUnit U = units[v];
     const int s = (v - u_begin) % kTcStages;
+    last_issued = v;
     uslot[s] = U;
     const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(float));
     const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(float);
@@ -817,7 +835,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
   uint32_t mma_parity = 0;
   int u = u_begin;
-  for (int t = t0; t < t1; ++t) {
+  // a wait that gives up stops the CTA (CTA-uniform): `pending` is the first unit whose
+  // copies are not consumed, `mma_pending` whether a commit is not waited for
+  bool failed = false, mma_pending = false;
+  int pending = u_begin;
+  for (int t = t0; t < t1 && !failed; ++t) {
     const GemvTask task = tasks[t];
     const int O = task.O;
     float acc[16];
@@ -825,7 +847,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     for (int n = 0; n < 16; ++n) acc[n] = 0.f;
     for (int kk = 0; kk < task.nunits; ++kk, ++u) {
       const int s = (u - u_begin) % kTcStages;
-      tc_wait(&full[s], (uint32_t)(((u - u_begin) / kTcStages) & 1), err);
+      if (__syncthreads_or(!mbar_wait_bounded(&full[s], (uint32_t)(((u - u_begin) / kTcStages) & 1), wlim))) {
+        failed = true;
+        pending = u;
+        break;
+      }
       const int c = uslot[s].c;
       const float* P = reinterpret_cast<const float*>(ring + (size_t)s * kTcStage);
       const float* X = reinterpret_cast<const float*>(ring + (size_t)s * kTcStage + kTcPieceBytes);
@@ -876,7 +902,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                      : "memory");
         if (u + kTcStages < u_end) issue(u + kTcStages);
       }
-      tc_wait(mmab, mma_parity, err);
+      if (__syncthreads_or(!mbar_wait_bounded(mmab, mma_parity, wlim))) {
+        failed = mma_pending = true;
+        pending = u + 1;
+        break;
+      }
       mma_parity ^= 1u;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       for (int st = 0; st < nsteps; ++st) {
@@ -887,6 +917,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     }
+    if (failed) break;
     if (tid < O) {
       float* out = xz + (size_t)(task.out_row + tid) * RS;
       if constexpr (RS % 4 == 0) {
@@ -899,6 +930,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
     }
   }
+  if (failed && tid == 0) {
+    // flag the product, then let the MMAs and copies in flight finish before the tensor
+    // memory is freed and the CTA exits
+    atomicExch(&err->failed, 1);
+    if (mma_pending) mbar_wait_bounded(mmab, mma_parity, kGemvDrainLimit);
+    for (int v = pending; v <= last_issued; ++v)
+      mbar_wait_bounded(&full[(v - u_begin) % kTcStages], (uint32_t)(((v - u_begin) / kTcStages) & 1),
+                        kGemvDrainLimit);
+  }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (warp == 0)
@@ -906,7 +946,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 }
 
 template <int RS>
-void launch_umma_t(const GemvLaunch& L, const GemvUnit* units, const float* arena, float* xz, int* err,
+void launch_umma_t(const GemvLaunch& L, const GemvUnit* units, const float* arena, float* xz, GemvStatus* err,
                    cudaStream_t s) {
   auto kern = umma_stream_kernel<RS>;
   const size_t smem = (size_t)kTcStages * kTcStage + 2 * kTcSteps * (kTcTileA + kTcTileB) + (kTcStages + 1) * 8 +
@@ -965,7 +1005,7 @@ __global__ void zred_kernel(const GemvZred* __restrict__ zr, T* xz) {
 // ---------------------------------------------------------------------------------
 template <typename T, int R, int RS, int OL, int RPT, bool TRANSP>
 void launch_stream_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, int conj,
-                     const int* perm_out, T* y, int ldy, int q0, int r, T alpha, T beta, int* err, cudaStream_t s) {
+                     const int* perm_out, T* y, int ldy, int q0, int r, T alpha, T beta, GemvStatus* err, cudaStream_t s) {
   constexpr int NSTAGE = nstage_of<T>();
   auto kern = stream_kernel<T, R, RS, OL, RPT, TRANSP, NSTAGE>;
   const size_t smem = stream_smem_bytes(sizeof(T), R, RS, OL * RPT, TRANSP);
@@ -979,7 +1019,7 @@ void launch_stream_t(const GemvLaunch& L, const GemvUnit* units, const T* arena,
 }
 
 template <typename T, int R, int RS, int MODE, int A2>
-void launch_warp_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, int* err, cudaStream_t s) {
+void launch_warp_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, GemvStatus* err, cudaStream_t s) {
   auto kern = warp_stream_kernel<T, R, RS, MODE, A2>;
   const size_t smem = warp_stream_smem_bytes((int)sizeof(T));
   static bool attr = false;
@@ -991,7 +1031,7 @@ void launch_warp_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T
 }
 
 template <int R, int RS, int MT>
-void launch_mma_t(const GemvLaunch& L, const GemvUnit* units, const float* arena, float* xz, int* err,
+void launch_mma_t(const GemvLaunch& L, const GemvUnit* units, const float* arena, float* xz, GemvStatus* err,
                   cudaStream_t s) {
   auto kern = mma_stream_kernel<R, RS, MT>;
   const size_t smem = warp_stream_smem_bytes((int)sizeof(float));
@@ -1005,7 +1045,7 @@ void launch_mma_t(const GemvLaunch& L, const GemvUnit* units, const float* arena
 
 template <typename T, int R, int RS, bool TRANSP>
 void launch_stream(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, int conj, const int* perm_out,
-                   T* y, int ldy, int q0, int r, T alpha, T beta, int* err, cudaStream_t s) {
+                   T* y, int ldy, int q0, int r, T alpha, T beta, GemvStatus* err, cudaStream_t s) {
   if (L.ntasks <= 0) return;
   if constexpr (std::is_same<T, float>::value && !TRANSP) {
     if (L.map == 4) {
@@ -1044,7 +1084,7 @@ void launch_stream(const GemvLaunch& L, const GemvUnit* units, const T* arena, T
 }
 
 template <typename T, int R, bool TRANSP>
-void run_tile(const GemvPlan& p, int nrhs, int q0, T alpha, T beta, const T* x, T* y, T* xz, int conj, int* err,
+void run_tile(const GemvPlan& p, int nrhs, int q0, T alpha, T beta, const T* x, T* y, T* xz, int conj, GemvStatus* err,
               cudaStream_t s, const GemvTiming* tm) {
   constexpr int RS = rs_of<T>(R);
   const GemvSide& side = p.side[TRANSP ? 1 : 0];
@@ -1072,7 +1112,7 @@ void run_tile(const GemvPlan& p, int nrhs, int q0, T alpha, T beta, const T* x, 
 }
 
 template <typename T, bool TRANSP>
-void run_all(const GemvPlan& p, int nrhs, T alpha, T beta, const T* x, T* y, T* xz, int conj, int* err,
+void run_all(const GemvPlan& p, int nrhs, T alpha, T beta, const T* x, T* y, T* xz, int conj, GemvStatus* err,
              cudaStream_t s, const GemvTiming* tm) {
   // complex double keeps tiles of at most 4 right-hand sides (shared-memory budget)
   constexpr int maxR = sizeof(T) >= 16 ? 4 : 16;
@@ -1149,7 +1189,7 @@ __global__ void grad_rk_kernel(const GemvRkLeaf* __restrict__ rk, int nrk, const
 
 template <typename T, int R>
 void grads_tile(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* rz, T* gfull, T* grk, bool accumulate,
-                int* err, cudaStream_t s) {
+                GemvStatus* err, cudaStream_t s) {
   constexpr int RS = rs_of<T>(R);
   const T* arena = (const T*)p.arena;
   // x in cluster order (columns) and z = B^T x
@@ -1210,7 +1250,7 @@ int gemv_launch_count(const GemvPlan& p, char trans, int nrhs, int elem_bytes) {
 
 template <typename T>
 void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* rz, T* gfull, T* grk,
-                           bool accumulate, int* err, cudaStream_t s) {
+                           bool accumulate, GemvStatus* err, cudaStream_t s) {
   constexpr bool big = sizeof(T) < 16;
   if (big && nrhs > 8) grads_tile<T, big ? 16 : 4>(p, nrhs, x, r, xz, rz, gfull, grk, accumulate, err, s);
   else if (big && nrhs > 4) grads_tile<T, big ? 8 : 4>(p, nrhs, x, r, xz, rz, gfull, grk, accumulate, err, s);
@@ -1220,7 +1260,7 @@ void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, 
 
 template <typename T>
 void launch_gemv(const GemvPlan& p, char trans, int nrhs, T alpha, T beta, const T* x_client, T* y_client, T* xz,
-                 int* err, cudaStream_t s, const GemvTiming* tm) {
+                 GemvStatus* err, cudaStream_t s, const GemvTiming* tm) {
   if (trans == 'N') run_all<T, false>(p, nrhs, alpha, beta, x_client, y_client, xz, 0, err, s, tm);
   else
     run_all<T, true>(p, nrhs, alpha, beta, x_client, y_client, xz, (trans == 'C' && Traits<T>::is_complex) ? 1 : 0,
@@ -1228,9 +1268,9 @@ void launch_gemv(const GemvPlan& p, char trans, int nrhs, T alpha, T beta, const
 }
 
 #define HB_INST(T)                                                                                            \
-  template void launch_gemv<T>(const GemvPlan&, char, int, T, T, const T*, T*, T*, int*, cudaStream_t,         \
+  template void launch_gemv<T>(const GemvPlan&, char, int, T, T, const T*, T*, T*, GemvStatus*, cudaStream_t,         \
                                const GemvTiming*);                                                             \
-  template void launch_leaf_gradients<T>(const GemvPlan&, int, const T*, const T*, T*, T*, T*, T*, bool, int*, \
+  template void launch_leaf_gradients<T>(const GemvPlan&, int, const T*, const T*, T*, T*, T*, T*, bool, GemvStatus*, \
                                          cudaStream_t);
 HB_INST(float)
 HB_INST(double)

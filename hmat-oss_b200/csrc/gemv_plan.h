@@ -104,6 +104,18 @@ struct GemvRkLeaf {
   int zrow_n, zrow_t;  // xz rows of z = B^T x ('N') and z' = A^T x ('T' / 'C')
 };
 
+// Status block of the products of one matrix, in device memory.  A kernel whose bounded
+// wait for a bulk copy gives up sets `failed` (after waiting, again bounded, for the copies
+// it has in flight) and stops; the host reads and clears it.  `wait_limit` bounds each wait
+// (polls of a stage barrier); the drain after a give-up uses kGemvDrainLimit.
+struct GemvStatus {
+  int failed;
+  int pad;
+  long long wait_limit;
+};
+constexpr long long kGemvWaitLimit = 1LL << 26;
+constexpr long long kGemvDrainLimit = 1LL << 26;
+
 struct GemvTiming {
   cudaEvent_t ev[4];
 };

@@ -159,7 +159,7 @@ namespace hmatb200 {
 // a pipeline wait gives up.
 template <typename T>
 void launch_gemv(const GemvPlan& p, char trans, int nrhs, T alpha, T beta, const T* x_client, T* y_client, T* xz,
-                 int* err, cudaStream_t s, const GemvTiming* timing = nullptr);
+                 GemvStatus* err, cudaStream_t s, const GemvTiming* timing = nullptr);
 // Row stride (scalars) of the xz buffer for R right-hand sides.
 int gemv_rhs_stride(int elem_bytes, int R);
 // Kernel launches of one product with nrhs right-hand sides.
@@ -175,7 +175,7 @@ int warp_stream_warps_per_cta();
 // written (or added) into gradient arenas laid out like the leaf arenas.
 template <typename T>
 void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* rz, T* gfull, T* grk,
-                           bool accumulate, int* err, cudaStream_t s);
+                           bool accumulate, GemvStatus* err, cudaStream_t s);
 
 // Load the assembly kernels of the storage type T ahead of the first assembly.
 template <typename T>
@@ -184,6 +184,10 @@ template <typename T>
 void preload_full_kernels();
 template <typename T>
 void preload_truncate_kernels();
+// Cap on the one-sided Jacobi sweeps of the truncation's core SVDs, for the device that is
+// current (default kJacobiDefaultSweeps).
+constexpr int kJacobiDefaultSweeps = 60;
+cudaError_t set_jacobi_max_sweeps(int sweeps);
 
 // Grid size of a persistent launch: a multiple of the SM count.
 int persistent_grid(int blocks_per_sm);

@@ -27,6 +27,8 @@ using namespace hmatb200;
 namespace {
 
 // 16 MiB: the cluster-ordered x (N x 16 scalars) plus the z buffer of the matrix must fit.
+// The address looked up for a device stays valid for the life of the process's context on
+// that device; a cudaDeviceReset (which destroys that context) is not supported.
 constexpr size_t kNoAllocScratchBytes = 16u << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -60,9 +62,13 @@ extern "C" int hmat_b200_gemv_device_noalloc(hmat_matrix_t* m, char trans, const
     if (need > kNoAllocScratchBytes)
       throw Error("matrix needs " + std::to_string(need) + " bytes of gemv scratch, more than the " +
                   std::to_string(kNoAllocScratchBytes) + " bytes this entry point holds; use hmat_b200_gemv_device");
+    // the scratch address is looked up on the matrix's own device, which must be current
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess) throw Error(std::string("cudaGetDevice failed: ") + cudaGetErrorString(ce));
+    if (dev != e->device)
+      throw Error("the current CUDA device (" + std::to_string(dev) + ") is not the matrix's device (" +
+                  std::to_string(e->device) + ")");
     if (dev < 0 || dev >= kMaxDevices) throw Error("device index out of range");
     void* scratch = scratch_address(dev);
     e->gemv_device_with_scratch(trans, alpha, x_dev, beta, y_dev, nrhs, (cudaStream_t)stream, scratch,

@@ -18,7 +18,9 @@ namespace hmatb200 {
 namespace {
 
 constexpr int kTruncThreads = 256;
-constexpr int kJacobiMaxSweeps = 60;
+// Cap on the one-sided Jacobi sweeps of a core SVD (a leaf that reaches it is flagged
+// kLeafSvdNoConverge and its assembly fails).  Set by the host before each assembly.
+__device__ int g_jacobi_max_sweeps = kJacobiDefaultSweeps;
 
 __device__ inline double sqrt_abs2(double a) { return fabs(a); }
 __device__ inline double sqrt_abs2(cdouble a) { return sqrt(a.x * a.x + a.y * a.y); }
@@ -106,8 +108,9 @@ __device__ bool jacobi_svd(W* Wm, W* V, int k, RedScratch& rs) {
   for (int i = threadIdx.x; i < k * k; i += blockDim.x) V[i] = (i % (k + 1) == 0) ? one<W>() : zero<W>();
   __syncthreads();
   const int kk = (k + 1) & ~1;  // even number of players (the extra one sits out)
+  const int max_sweeps = g_jacobi_max_sweeps;
   __shared__ int s_rot;
-  for (int sweep = 0; sweep < kJacobiMaxSweeps; ++sweep) {
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
     if (threadIdx.x == 0) s_rot = 0;
     __syncthreads();
     for (int round = 0; round < kk - 1; ++round) {
@@ -554,7 +557,8 @@ __global__ void __launch_bounds__(NW * 32) tscore_kernel(const TsCore* __restric
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) rounds = max(rounds, __shfl_xor_sync(0xffffffffu, rounds, off));
     bool conv = false;
-    for (int sweep = 0; sweep < kJacobiMaxSweeps; ++sweep) {
+    const int max_sweeps = g_jacobi_max_sweeps;
+    for (int sweep = 0; sweep < max_sweeps; ++sweep) {
       bool rot = false;
       for (int round = 0; round < rounds; ++round) {
         const int partner = (j < kk && round < kk - 1) ? (int)s_partner[warp][round][lane] : -1;
@@ -1098,6 +1102,11 @@ void launch_tsapply_cta(const TsItem* items, int nitems, T* ws, const typename T
 
 // Loads every truncation kernel of the storage type T (the CUDA runtime otherwise loads a
 // kernel at its first launch, inside the first assembly).
+cudaError_t set_jacobi_max_sweeps(int sweeps) {
+  const int v = sweeps < 1 ? 1 : sweeps;
+  return cudaMemcpyToSymbol(g_jacobi_max_sweeps, &v, sizeof(int));
+}
+
 template <typename T>
 void preload_truncate_kernels() {
   typedef typename Traits<T>::wide W;

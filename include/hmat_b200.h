@@ -372,16 +372,29 @@ void hmat_b200_delete_assembly(void* assembly);
 
 /* gemv on device buffers (x, y column-major, client numbering, leading dimension = the
  * vector length), enqueued on `stream` (a cudaStream_t, NULL for the engine's own) and
- * not synchronised.  Same maths and return convention as hmat_interface_t.gemv. */
+ * not synchronised.  Same maths and return convention as hmat_interface_t.gemv (reference:
+ * c_wrapping.hpp:233-252, with the buffers on the device).  The device that was current when
+ * the matrix was assembled must be current (otherwise the call fails).  The return code
+ * covers the arguments and the launches only: a kernel whose bounded wait for a bulk copy
+ * gives up marks the matrix's status flag and leaves y invalid; read it with
+ * hmat_b200_gemv_status once the product is complete. */
 int hmat_b200_gemv_device(hmat_matrix_t* hmatrix, char trans, const void* alpha, const void* x_dev,
                           const void* beta, void* y_dev, int nrhs, void* stream);
+
+/* Status of the device products of `hmatrix` (hmat_b200_gemv_device, _noalloc, and the
+ * leaf gradients): synchronises `stream` (NULL: the matrix's own stream), then sets *failed
+ * to 1 if one of them stopped since the last query because a kernel's wait for a bulk copy
+ * gave up (their results are not valid), else 0, and clears the flag.  Allocates nothing.
+ * The C table's gemv checks the same flag itself and returns 1.  Returns 0, or non-zero
+ * on a bad argument.  No counterpart in the reference (its products run on the host). */
+int hmat_b200_gemv_status(hmat_matrix_t* hmatrix, void* stream, int* failed);
 
 /* hmat_b200_gemv_device for callers that cannot allocate device memory when they
  * multiply (no counterpart in the reference's C API).  Callers inside a caching
  * allocator or memory pool they do not control, inside callbacks where cudaMalloc /
  * cudaFree would synchronise or deadlock, or in loops that forbid allocation after
- * start-up can use it: it calls no cudaMalloc, cudaFree or other allocating routine and
- * builds no CUDA graph.  Its scratch (x in cluster order and the per-leaf B^T x values) is
+ * start-up can use it: it calls no cudaMalloc, cudaFree or other allocating routine.
+ * Its scratch (x in cluster order and the per-leaf B^T x values) is
  * one fixed 16 MiB device array compiled into the library: every GPU on which the
  * library's device code is loaded holds it until the process exits.  Matrices whose
  * product needs more scratch than that are rejected with a non-zero return and an
@@ -391,8 +404,11 @@ int hmat_b200_gemv_device(hmat_matrix_t* hmatrix, char trans, const void* alpha,
  * on the GPU (different streams, or different host threads, without ordering between
  * them) race: order them on one stream.  The array keeps the previous call's contents;
  * nothing in it needs to start at zero, since each product overwrites what it reads.
- * Same arguments, maths and return convention as hmat_b200_gemv_device; `stream` NULL
- * means the matrix's own stream. */
+ * The address is looked up once per process and device; a cudaDeviceReset is not supported.
+ * Same arguments, maths and return convention as hmat_b200_gemv_device (the matrix's device
+ * current; a bulk-copy wait that gives up is reported by hmat_b200_gemv_status, through a
+ * flag allocated with the matrix, not in the shared array); `stream` NULL means the
+ * matrix's own stream. */
 int hmat_b200_gemv_device_noalloc(hmat_matrix_t* hmatrix, char trans, const void* alpha, const void* x_dev,
                                   const void* beta, void* y_dev, int nrhs, void* stream);
 

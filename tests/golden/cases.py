@@ -26,6 +26,12 @@ CASES = {
                      dict(leaf=2048, leaf_cols=16, eta=2.0, eps=1e-5), 1, 3, "D", False),
     "svd_small": (lambda: wl.cylinder(40, 50), dict(kind=0, delta=0.01), dict(leaf=32, eta=2.0, eps=1e-4, min_leaf=100),
                   2, 14, "D", False),
+    # the headline workload: 100,000-point cylinder (250 x 400 grid), eps 1e-6, 2 of its 16 RHS
+    "cfg1_cylinder": (lambda: wl.cylinder(250, 400), dict(kind=0, delta=0.01), dict(leaf=64, eta=2.0, eps=1e-6), 2, 1,
+                      "D", False),
+    # the adjoint workload's shape at 20,000 points: uniform cube, exponential covariance l=0.3
+    "cfg4_cube": (lambda: wl.cube(20000, 2), dict(kind=1, ell=0.3, nugget=1e-6), dict(leaf=64, eta=2.0, eps=1e-6), 2,
+                  2, "D", False),
     # assembled at 1e-6, then set_low_rank_epsilon(1e-3) + truncate
     "retrunc_expcov": (lambda: wl.cube(800, 31), dict(kind=1, ell=0.3, nugget=1e-6),
                        dict(leaf=32, eta=2.0, eps=1e-6, retrunc=1e-3), 2, 32, "D", True),

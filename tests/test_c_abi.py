@@ -123,3 +123,21 @@ def test_aca_report_before_assembly(hb):
         lib.hmat_b200_clear_last_error()
     finally:
         h.close()
+
+
+def test_gemv_status_rejects_bad_arguments(hb):
+    """hmat_b200_gemv_status before any product: null arguments and an unassembled matrix are
+    refused with a non-zero return (no device call)."""
+    lib = hb.load_library()
+    failed = C.c_int(7)
+    assert lib.hmat_b200_gemv_status(None, None, C.byref(failed)) != 0
+    pts = np.random.default_rng(4).random((300, 3))
+    h = hb.HMatrix(pts, hb.kernel(hb.LAPLACE_REG), assemble=False, leaf_size=16)
+    try:
+        assert lib.hmat_b200_gemv_status(h.m, None, None) != 0
+        assert lib.hmat_b200_gemv_status(h.m, None, C.byref(failed)) != 0
+        assert b"not assembled" in lib.hmat_b200_last_error()
+        assert failed.value == 7
+        lib.hmat_b200_clear_last_error()
+    finally:
+        h.close()

@@ -16,7 +16,16 @@ pytestmark = pytest.mark.gpu
 
 VT = {"D": 1, "Z": 3}
 # Complex cases on the symmetric cylinder meet exact pivot ties (see test_oracle_golden).
-GEMV_TOL = {"helmholtz_small": 2e-6, "helmholtz_payload": 2e-6}
+# On the 100,000-point cylinder 43 of the 35,084 Rk leaves meet such ties against the
+# reference (the oracle shows the same 43): same ranks, a different approximation of the
+# block within epsilon of it, 1.5e-8 on the product.
+GEMV_TOL = {"helmholtz_small": 2e-6, "helmholtz_payload": 2e-6, "cfg1_cylinder": 5e-8}
+# Rank mismatches allowed against the reference: none, except in the complex tie cases.
+TIE_CASES = ("helmholtz_small", "helmholtz_payload")
+
+
+def rank_mismatches_allowed(name, n_rk):
+    return max(1, n_rk // 100) if name in TIE_CASES else 0
 
 
 def build_engine(hb, name, value_type=None, **over):
@@ -44,7 +53,7 @@ def test_fp64_engine_matches_reference(hb, name):
         assert np.array_equal(T[:, :5], g["leaves"][:, :5])
         rk = g["leaves"][:, 4] == 1
         mism = int((T[rk, 5] != g["leaves"][rk, 5]).sum())
-        assert mism <= max(1, rk.sum() // 100), f"{mism} rank mismatches"
+        assert mism <= rank_mismatches_allowed(name, int(rk.sum())), f"{mism} rank mismatches"
         tol = GEMV_TOL.get(name, 1e-12)
         assert rel(h.gemv(x, "N"), g["y"]) < tol
         assert rel(h.gemv(x, "T"), g["y_T"]) < tol
@@ -291,7 +300,74 @@ def test_high_rank_truncation_path_matches_reference(hb, name, monkeypatch):
         assert np.array_equal(T[:, :5], g["leaves"][:, :5])
         rk = g["leaves"][:, 4] == 1
         mism = int((T[rk, 5] != g["leaves"][rk, 5]).sum())
-        assert mism <= max(1, rk.sum() // 100), f"{mism} rank mismatches"
+        assert mism <= rank_mismatches_allowed(name, int(rk.sum())), f"{mism} rank mismatches"
+        tol = GEMV_TOL.get(name, 1e-12)
+        assert rel(h.gemv(x, "N"), g["y"]) < tol
+        assert rel(h.gemv(x, "T"), g["y_T"]) < tol
+    finally:
+        h.close()
+
+
+def test_headline_cylinder_100k(hb, oracle):
+    """The benchmark's workload (100,000-point cylinder, leaf 64, eta 2, epsilon 1e-6) pinned to
+    the reference: the FP64 engine gives the reference's partition and every rank, its 'N' and
+    'T' products within the tie-flip tolerance, and the oracle's product (same pivot rules)
+    within 1e-12.  The mixed engine (FP32 bulk, FP64 truncation) keeps the partition and stays
+    within 1e-6 of the FP64 H-matrix product on the benchmark's 16 right-hand sides."""
+    import importlib.util
+    import os
+    from conftest import ROOT
+    spec = importlib.util.spec_from_file_location("wl_cfg1", os.path.join(ROOT, "hmat-oss_b200", "workloads.py"))
+    wl = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(wl)
+    name = "cfg1_cylinder"
+    g = golden(name)
+    h64, pts, x, kern, tree = build_engine(hb, name)
+    h32 = None
+    try:
+        T = h64.leaf_table()
+        assert np.array_equal(h64.perm(), g["perm"])
+        assert np.array_equal(T[:, :5], g["leaves"][:, :5])
+        assert np.array_equal(T[:, 5], g["leaves"][:, 5]), "ranks differ from the reference"
+        y = h64.gemv(x, "N")
+        assert rel(y, g["y"]) < GEMV_TOL[name]
+        assert rel(h64.gemv(x, "T"), g["y_T"]) < GEMV_TOL[name]
+        o = oracle.OracleHMatrix(pts, leaf=tree["leaf"], eta=tree["eta"])
+        o.assemble(eps=tree["eps"], **kern)
+        assert np.array_equal(o.leaves(), T)
+        assert rel(y, o.gemv(x, "N")) < 1e-12
+        o.close()
+        h32, _, _, _, _ = build_engine(hb, name, value_type=hb.HMAT_SIMPLE_PRECISION)
+        assert np.array_equal(h32.leaf_table()[:, :5], T[:, :5])
+        x16 = wl.rhs(len(pts), 16, 1)
+        y64 = h64.gemv(x16)
+        y32 = h32.gemv(x16.astype(np.float32)).astype(np.float64)
+        err = rel(y32, y64)
+        print(f"mixed vs FP64 H-matrix, 16 RHS: {err:.3e}")
+        assert err <= 1e-6
+    finally:
+        h64.close()
+        if h32 is not None:
+            h32.close()
+
+
+@pytest.mark.parametrize("name", ["cfg4_cube", "cfg0_laplace", "helmholtz_small"])
+def test_aca_capacity_retries_and_workspace_batches_match_reference(hb, name, monkeypatch):
+    """The ACA rank-capacity retry (leaves that fill their factor slots are rerun with twice
+    the capacity) and the batching of the ACA workspace give the reference's ranks and
+    products: an initial capacity of 4 makes most leaves retry, some several times, and a
+    64 MiB workspace budget cuts the 20,000-point cube's leaves into many batches."""
+    monkeypatch.setenv("HMAT_B200_ACA_KCAP", "4")
+    monkeypatch.setenv("HMAT_B200_WORKSPACE_MB", "64")
+    g = golden(name)
+    h, pts, x, kern, tree = build_engine(hb, name)
+    try:
+        T = h.leaf_table()
+        assert np.array_equal(T[:, :5], g["leaves"][:, :5])
+        rk = g["leaves"][:, 4] == 1
+        assert int((T[rk, 5] > 4).sum()) > 0  # leaves above the initial capacity exist
+        mism = int((T[rk, 5] != g["leaves"][rk, 5]).sum())
+        assert mism <= rank_mismatches_allowed(name, int(rk.sum())), f"{mism} rank mismatches"
         tol = GEMV_TOL.get(name, 1e-12)
         assert rel(h.gemv(x, "N"), g["y"]) < tol
         assert rel(h.gemv(x, "T"), g["y_T"]) < tol

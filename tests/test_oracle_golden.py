@@ -11,7 +11,9 @@ from conftest import golden, rel
 # bit; the reference's OpenBLAS summation order and the restatement's break those ties
 # differently, giving a different but equally accurate rank-k approximation of those
 # leaves (both within the compression epsilon of the exact block, checked below).
-GEMV_TOL = {"helmholtz_small": 2e-6}
+# On the 100,000-point cylinder, 43 of the 35,084 Rk leaves meet such ties (same ranks, both
+# approximations within epsilon of the exact block): 1.5e-8 on the product.
+GEMV_TOL = {"helmholtz_small": 2e-6, "cfg1_cylinder": 5e-8}
 
 INFO_KEYS = ["full_count", "rk_count", "full_size", "rk_size", "compressed_size", "uncompressed_size",
              "nr_block_clusters", "largest_rk_dim_rows", "largest_rk_dim_cols", "largest_rk_mem_rows",

@@ -56,6 +56,17 @@ def test_noalloc_gemv_matches_device_gemv_twice(hb, vt, tol):
             a = y_ref.cpu().numpy()
             b = y_na.cpu().numpy()
             assert np.linalg.norm(a - b) / np.linalg.norm(a) <= tol
+        # alpha and beta on the output, against the regular device gemv with the same y
+        x = torch.from_numpy(np.ascontiguousarray(wl.rhs(n, 2, 44).T)).to("cuda", dt)
+        y0 = torch.from_numpy(np.ascontiguousarray(wl.rhs(n, 2, 45).T)).to("cuda", dt)
+        y_ref, y_na = y0.clone(), y0.clone()
+        h.gemv_device(x.data_ptr(), y_ref.data_ptr(), 2, alpha=2.0, beta=0.5, stream=stream.cuda_stream)
+        assert h.gemv_device_noalloc(x.data_ptr(), y_na.data_ptr(), 2, alpha=2.0, beta=0.5,
+                                     stream=stream.cuda_stream) == 0
+        assert h.gemv_status(stream.cuda_stream) is False
+        a = y_ref.cpu().numpy()
+        b = y_na.cpu().numpy()
+        assert np.linalg.norm(a - b) / np.linalg.norm(a) <= tol
     finally:
         h.close()
 
