@@ -153,6 +153,43 @@ def cpu_baseline_reference(pts, x, wl_cfg, steps=1, warmup=0, scalar="S"):
             "rk_count": r["json"]["rk_count"], "wall_s": wall, "scalar": scalar}
 
 
+def batch_cpu_baseline(batch):
+    """The reference's CPU build on every matrix of the batch, one process per matrix (the
+    library has global state), as many at once as the host has cores: wall time of the whole
+    batch, matrices/s and ACA+ leaves/s over it, FP32 storage as the mixed engine."""
+    import concurrent.futures as cf
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.have_reference():
+        return None
+    cores = os.cpu_count() or 1
+
+    def one(c):
+        r = O.run_reference(c["points"], 1, c["eps"], leaf=c["leaf"], eta=c["eta"], ell=c["ell"], nugget=c["nugget"],
+                            scalar="S")
+        return r["json"]["rk_count"], r["json"]["t_assemble"]
+
+    t0 = time.time()
+    with cf.ThreadPoolExecutor(max_workers=cores) as ex:  # each call runs the reference in its own process
+        out = list(ex.map(one, batch))
+    wall = time.time() - t0
+    rk = sum(o[0] for o in out)
+    return {"matrices_per_s": len(batch) / wall, "aca_leaves_per_s": rk / wall, "wall_s": wall,
+            "assembly_s_sum": sum(o[1] for o in out), "cores": cores, "kind": "reference",
+            "cpu": cpu_model(),
+            "sample": f"all {len(batch)} matrices, one reference process each, {cores} at a time (assembly)"}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -259,26 +296,40 @@ def supplementary(args):
                     "results": res, "mixed_rel_err_vs_fp64_hmatrix": err,
                     "gemv_speedup_mixed_vs_fp64": res[hi]["gemv_ms"] / res[lo]["gemv_ms"]})
     elif name == "cfg2":
+        # the 64 matrices as one batch (hmat_b200_batch_*): one assembly and one product for all
+        # of them, one launch per phase
         batch = wl.batch_config(64, seed=0)
-        res = {}
-        for label, vt in (("S", 0), ("D", 1)):
-            dev_ms = wall = 0.0
-            leaves = rk = dof = 0
-            for c in batch:
-                h, w = make(c, vt)
-                a_ms, _ = asm_ms(h)
-                T = h.leaf_table()
-                dev_ms += a_ms
-                wall += w
-                leaves += len(T)
-                rk += int((T[:, 4] == 1).sum())
-                dof += len(c["points"])
-                h.close()
-            res[label] = {"matrices": len(batch), "dof": dof, "leaves": leaves, "rk_leaves": rk,
-                          "assembly_device_ms_total": dev_ms, "assembly_wall_s_total": wall,
-                          "aca_leaves_per_s_device": rk / (dev_ms * 1e-3),
-                          "matrices_per_s_device": len(batch) / (dev_ms * 1e-3)}
-        out.update({"metric": "ACA+ leaves/s over the batch (device assembly time)", "results": res})
+        pts = [c["points"] for c in batch]
+        kers = [hb.kernel(hb.EXP_COV, ell=c["ell"], nugget=c["nugget"]) for c in batch]
+        hb.set_parameters(compressionMinLeafSize=0)
+        nrhs = 1
+        X = np.concatenate([wl.rhs(len(c["points"]), nrhs, c["seed"]) for c in batch], axis=0)
+        res, ys = {}, {}
+        for label, vt, dt in (("S", 0, torch.float32), ("D", 1, torch.float64)):
+            t0 = time.time()
+            b = hb.HMatrixBatch(pts, kers, value_type=vt, leaf_size=64, eta=2.0, epsilon=1e-5)
+            torch.cuda.synchronize()
+            wall = time.time() - t0
+            a_ms, parts = asm_ms(b)
+            T = b.leaf_table()
+            rk = int((T[:, 4] == 1).sum())
+            ms, ys[label] = gemv_ms(b, np.asfortranarray(X), dt)
+            res[label] = {"matrices": len(batch), "dof": int(X.shape[0]), "leaves": int(len(T)), "rk_leaves": rk,
+                          "assembly_device_ms": a_ms, "phase_ms": parts, "assembly_wall_s": wall,
+                          "aca_leaves_per_s": rk / ((parts["aca_ms"] + parts["truncate_ms"]) * 1e-3),
+                          "matrices_per_s": len(batch) / (a_ms * 1e-3), "gemv_ms": ms,
+                          "gemv_gbs": b.gemv_bytes(nrhs) / (ms * 1e-3) / 1e9,
+                          "gemv_launches": b.gemv_launches(nrhs)}
+            b.close()
+        err = float(np.linalg.norm(ys["S"] - ys["D"]) / np.linalg.norm(ys["D"]))
+        cpu = None
+        if not args.no_cpu_baseline:
+            cpu = batch_cpu_baseline(batch)
+        out.update({"metric": "ACA+ leaves/s and matrices/s over the batch (device assembly time); batched H-gemv GB/s",
+                    "nrhs": nrhs, "results": res, "mixed_rel_err_vs_fp64_hmatrix": err,
+                    "assembly_speedup_mixed_vs_fp64": res["D"]["assembly_device_ms"] / res["S"]["assembly_device_ms"],
+                    "gemv_speedup_mixed_vs_fp64": res["D"]["gemv_ms"] / res["S"]["gemv_ms"],
+                    "cpu_baseline": cpu})
     elif name == "cfg4":
         c = wl.config(name)
         n = len(c["points"])

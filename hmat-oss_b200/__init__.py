@@ -140,6 +140,7 @@ EXPORTED = [
     "hmat_assemble_context_init", "hmat_factorization_context_init", "hmat_solve_context_init",
     "hmat_init_default_interface", "hmat_get_parameters", "hmat_set_parameters", "hmat_get_version",
     "hmat_b200_create_assembly", "hmat_b200_delete_assembly", "hmat_b200_gemv_device", "hmat_b200_gemv_device_noalloc", "hmat_b200_gemv_status",
+    "hmat_b200_batch_create", "hmat_b200_batch_offsets", "hmat_b200_batch_assemble",
     "hmat_b200_leaf_count",
     "hmat_b200_leaf_table", "hmat_b200_leaf_payload", "hmat_b200_payload_layout", "hmat_b200_leaf_gradients",
     "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_gemv_launches", "hmat_b200_aca_shapes",
@@ -180,6 +181,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "hmat_b200_gemv_device": (C.c_int, [_P, C.c_char, _P, _P, _P, _P, C.c_int, _P]),
         "hmat_b200_gemv_device_noalloc": (C.c_int, [_P, C.c_char, _P, _P, _P, _P, C.c_int, _P]),
         "hmat_b200_gemv_status": (C.c_int, [_P, _P, C.POINTER(C.c_int)]),
+        "hmat_b200_batch_create": (_P, [_P, C.c_int]),
+        "hmat_b200_batch_offsets": (C.c_int, [_P, _P, _P]),
+        "hmat_b200_batch_assemble": (C.c_int, [_P, _P, _P]),
         "hmat_b200_leaf_count": (C.c_int, [_P]),
         "hmat_b200_leaf_table": (C.c_int, [_P, _P]),
         "hmat_b200_leaf_payload": (C.c_longlong, [_P, C.c_int, _P]),
@@ -579,6 +583,62 @@ class HMatrix:
             self.close()
         except Exception:
             pass
+
+
+class HMatrixBatch(HMatrix):
+    """Independent H-matrices assembled and multiplied together (hmat_b200_batch_*): member i
+    is built on points[i] with kernels[i] (one kernel kind and nugget; each its own correlation
+    length, regularisation or wavenumber), all with the same value type, leaf size, eta and
+    epsilon.  The object is the block-diagonal matrix of the members: gemv takes the members'
+    vectors stacked (offsets()[0] gives each member's first row), leaf_table() lists the
+    members' leaves in order (offsets()[1])."""
+
+    def __init__(self, points: list, kernels: list, *, value_type: int = HMAT_DOUBLE_PRECISION, leaf_size: int = 64,
+                 eta: float = 2.0, epsilon: float = 1e-4, compression: str = "aca_plus", assemble: bool = True):
+        if len(points) != len(kernels) or not points:
+            raise ValueError("one kernel per member matrix")
+        lib = load_library()
+        self.lib = lib
+        self.value_type = value_type
+        self.dtype = DTYPES[value_type]
+        self.hi = HMatInterface(value_type)
+        self.members = [HMatrix(p, k, value_type=value_type, leaf_size=leaf_size, eta=eta, epsilon=epsilon,
+                                compression=compression, assemble=False) for p, k in zip(points, kernels)]
+        arr = (C.c_void_p * len(self.members))(*[mm.m for mm in self.members])
+        self.m = lib.hmat_b200_batch_create(arr, len(self.members))
+        if not self.m:
+            raise HMatError("hmat_b200_batch_create failed: " + lib.hmat_b200_last_error().decode())
+        self.n = int(sum(len(p) for p in points))
+        self.tree = self.tree_cols = None
+        self._borrowed_trees = None
+        self._comp = self.members[0]._comp
+        if assemble:
+            self.assemble()
+
+    def assemble(self):
+        arr = (C.c_void_p * len(self.members))(*[mm._assembly for mm in self.members])
+        _check(self.lib.hmat_b200_batch_assemble(self.m, arr, self._comp), "hmat_b200_batch_assemble")
+
+    def offsets(self):
+        """(first row of each member, first leaf of each member), count + 1 entries each."""
+        rb = np.zeros(len(self.members) + 1, np.int32)
+        lb = np.zeros(len(self.members) + 1, np.int32)
+        _check(self.lib.hmat_b200_batch_offsets(self.m, rb.ctypes.data, lb.ctypes.data), "hmat_b200_batch_offsets")
+        return rb, lb
+
+    def perm(self, cols: bool = False) -> np.ndarray:
+        rt, ct = C.c_void_p(), C.c_void_p()
+        self.hi.fn("get_cluster_trees")(self.m, C.byref(rt), C.byref(ct))
+        p = self.lib.hmat_cluster_get_indices(ct if cols else rt)
+        return np.ctypeslib.as_array(p, shape=(self.n,)).copy()
+
+    def close(self):
+        if getattr(self, "m", None):
+            self.hi.destroy(self.m)
+            self.m = None
+        for mm in getattr(self, "members", []):
+            mm.close()
+        self.members = []
 
 
 def kernel(kind: int, delta: float = 0.01, ell: float = 0.3, nugget: float = 0.0, wavenumber: float = 0.0):

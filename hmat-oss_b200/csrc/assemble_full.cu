@@ -67,11 +67,31 @@ void launch_full_from_canonical(const FullLeafDesc* d_leaves, const long long* g
   full_from_canonical_kernel<T><<<grid, 256, 0, s>>>(d_leaves, goff, nleaves, panels, src, arena);
 }
 
+// Segmented copy between two device buffers (relayout of stored leaves): segment g copies
+// count elements from src + src_off to dst + dst_off.  A CTA per segment, threads over elements.
+template <typename T>
+__global__ void __launch_bounds__(256) copy_segments_kernel(const CopySeg* __restrict__ segs, int nseg,
+                                                            const T* __restrict__ src, T* __restrict__ dst) {
+  for (int g = blockIdx.x; g < nseg; g += gridDim.x) {
+    const CopySeg c = segs[g];
+    for (long long e = threadIdx.x; e < c.count; e += blockDim.x) dst[c.dst + e] = src[c.src + e];
+  }
+}
+
+template <typename T>
+void launch_copy_segments(const CopySeg* segs, int nseg, const T* src, T* dst, cudaStream_t s) {
+  if (nseg <= 0) return;
+  int grid = persistent_grid(8);
+  if (grid > nseg) grid = nseg;
+  copy_segments_kernel<T><<<grid, 256, 0, s>>>(segs, nseg, src, dst);
+}
+
 template <typename T>
 void preload_full_kernels() {
   cudaFuncAttributes a;
   cudaFuncGetAttributes(&a, assemble_full_kernel<T>);
   cudaFuncGetAttributes(&a, full_from_canonical_kernel<T>);
+  cudaFuncGetAttributes(&a, copy_segments_kernel<T>);
 }
 
 #define HB_INST(T)                                                                                      \
@@ -79,7 +99,8 @@ void preload_full_kernels() {
   template void launch_assemble_full<T>(const FullLeafDesc*, int, const PanelDesc*, const KernelParams&, \
                                         Points, T*, cudaStream_t);                                       \
   template void launch_full_from_canonical<T>(const FullLeafDesc*, const long long*, int, const PanelDesc*, \
-                                              const T*, T*, cudaStream_t);
+                                              const T*, T*, cudaStream_t);                                 \
+  template void launch_copy_segments<T>(const CopySeg*, int, const T*, T*, cudaStream_t);
 HB_INST(float)
 HB_INST(double)
 HB_INST(cfloat)

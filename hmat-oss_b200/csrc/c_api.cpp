@@ -36,6 +36,9 @@ struct hmat_matrix_struct {
   BlockTree bt;
   double low_rank_eps = 1e-4;  // LocalSettings default (h_matrix.cpp:151)
   std::unique_ptr<EngineBase> engine;
+  // A batch (hmat_b200_batch_create): the first row and the first leaf of each member matrix
+  // in the block-diagonal combination (count + 1 entries each); empty for a plain matrix.
+  std::vector<int> batch_rows, batch_leaves;
 };
 
 namespace {
@@ -1045,6 +1048,108 @@ int hmat_b200_gemv_status(hmat_matrix_t* m, void* stream, int* failed) {
     if (!m || !failed) throw Error("null argument");
     if (!m->engine || !m->engine->assembled) throw Error("matrix is not assembled");
     *failed = m->engine->gemv_status((cudaStream_t)stream);
+  });
+  return 0;
+}
+
+// ---- batches of independent matrices ----
+// The batch is the block-diagonal matrix of its members: their cluster trees side by side (row
+// and column numbering offset by the rows before each member), their leaves in member order.
+// It is an ordinary hmat_matrix_t for every other entry point (one assembly and one product
+// for all members, one launch per phase), and owns its combined tree.
+hmat_matrix_t* hmat_b200_batch_create(hmat_matrix_t* const* matrices, int count) {
+  try {
+    if (!matrices || count <= 0) throw Error("bad argument");
+    std::unique_ptr<hmat_cluster_tree_t> tree(new hmat_cluster_tree_t());
+    tree->t.reset(new ClusterTree());
+    ClusterTree& t = *tree->t;
+    std::unique_ptr<hmat_matrix_t> b(new hmat_matrix_t());
+    b->vt = matrices[0] ? matrices[0]->vt : 1;
+    b->low_rank_eps = matrices[0] ? matrices[0]->low_rank_eps : 1e-4;
+    b->batch_rows.push_back(0);
+    b->batch_leaves.push_back(0);
+    for (int i = 0; i < count; ++i) {
+      const hmat_matrix_t* m = matrices[i];
+      if (!m) throw Error("null member matrix");
+      if (!m->batch_rows.empty()) throw Error("a batch cannot be a member of a batch");
+      if (m->vt != b->vt) throw Error("the members of a batch must have one value type");
+      if (m->rows_h != m->cols_h) throw Error("batch members must be built on one cluster tree (rows = columns)");
+      if (m->low_rank_eps != b->low_rank_eps) throw Error("the members of a batch must have one low-rank epsilon");
+      const ClusterTree& s = *m->rows_h->t;
+      const int base = t.n, nbase = (int)t.nodes.size();
+      t.pts.insert(t.pts.end(), s.pts.begin(), s.pts.end());
+      for (int v : s.perm) t.perm.push_back(v + base);
+      for (int v : s.rev) t.rev.push_back(v + base);
+      for (ClusterNode c : s.nodes) {
+        c.offset += base;
+        for (int& ch : c.child)
+          if (ch >= 0) ch += nbase;
+        t.nodes.push_back(c);
+      }
+      for (int l : s.leaf_nodes) t.leaf_nodes.push_back(l + nbase);
+      t.n += s.n;
+      for (LeafInfo l : m->bt.leaves) {
+        l.row_node += nbase;
+        l.col_node += nbase;
+        l.row_off += base;
+        l.col_off += base;
+        b->bt.leaves.push_back(l);
+      }
+      b->bt.nr_block_clusters += m->bt.nr_block_clusters;
+      b->batch_rows.push_back(t.n);
+      b->batch_leaves.push_back((int)b->bt.leaves.size());
+    }
+    b->rows_h = b->cols_h = tree.release();
+    b->own_rows = true;
+    return b.release();
+  } catch (const std::exception& e) {
+    fail("hmat_b200_batch_create", e.what());
+    return nullptr;
+  }
+}
+
+int hmat_b200_batch_offsets(hmat_matrix_t* b, int* row_base, int* leaf_base) {
+  if (!b || b->batch_rows.empty()) return fail("hmat_b200_batch_offsets", "not a batch");
+  for (size_t i = 0; i < b->batch_rows.size(); ++i) {
+    if (row_base) row_base[i] = b->batch_rows[i];
+    if (leaf_base) leaf_base[i] = b->batch_leaves[i];
+  }
+  return 0;
+}
+
+int hmat_b200_batch_assemble(hmat_matrix_t* b, void* const* assemblies, const hmat_compression_algorithm_t* comp) {
+  HB_TRY("hmat_b200_batch_assemble", {
+    if (!b || !assemblies || !comp) throw Error("null argument");
+    const int count = (int)b->batch_rows.size() - 1;
+    if (count <= 0) throw Error("not a batch");
+    int method;
+    switch (comp->method) {
+      case hmat_compress_aca_plus: method = 0; break;
+      case hmat_compress_aca_partial: method = 1; break;
+      default: throw Error("only ACA+ and partial-ACA compression are implemented by the B200 engine");
+    }
+    AssemblyDesc d;
+    bool uniform = true;
+    std::vector<double> param;
+    for (int i = 0; i < count; ++i) {
+      const AssemblyObj* a = (const AssemblyObj*)assemblies[i];
+      if (!a || a->magic != kAssemblyMagic) throw Error("member assembly is not a descriptor from hmat_b200_create_assembly");
+      const int n = b->batch_rows[i + 1] - b->batch_rows[i];
+      if ((long long)a->d.pts.size() != 3LL * n) throw Error("member assembly has another point count than its matrix");
+      const KernelParams& k = a->d.kp;
+      if (i == 0) d.kp = k;
+      if (k.kind != d.kp.kind) throw Error("the members of a batch must share the kernel kind");
+      if (k.nugget != d.kp.nugget) throw Error("the members of a batch must share the covariance nugget");
+      if (k.kind == kHelmholtzReg && k.delta != d.kp.delta)
+        throw Error("the members of a Helmholtz batch must share the regularisation");
+      const double own = k.kind == kExpCov ? k.ell : (k.kind == kLaplaceReg ? k.delta : k.wavenumber);
+      const double first = d.kp.kind == kExpCov ? d.kp.ell : (d.kp.kind == kLaplaceReg ? d.kp.delta : d.kp.wavenumber);
+      if (own != first) uniform = false;
+      d.pts.insert(d.pts.end(), a->d.pts.begin(), a->d.pts.end());
+      param.insert(param.end(), (size_t)n, own);
+    }
+    if (!uniform) d.param.swap(param);  // each member's own parameter, point by point
+    engine_of(b).assemble(d, method, comp->eps, b->low_rank_eps, g_settings.compressionMinLeafSize);
   });
   return 0;
 }

@@ -223,6 +223,10 @@ struct Points {
   const double *cx, *cy, *cz;
   const int* rid;
   const int* cid;
+  // Optional per-row-point kernel parameter (cluster order), replacing the kernel's own ell
+  // (exponential covariance), delta (regularised Laplace and Helmholtz amplitude) or
+  // wavenumber (Helmholtz phase) -- see param_of.
+  const double* rprm = nullptr;
 };
 
 #define HB_FOUR_PI 12.566370614359172  // 4 * M_PI in double
@@ -251,12 +255,15 @@ __device__ inline float dist_fp32(const Points& p, int i, int j) {
 template <typename T>
 struct KernelEval;
 
+// The kernel's parameter for row point i: its own (per-point array) or the kernel's.
+__device__ inline double param_of(const Points& p, int i, double own) { return p.rprm ? p.rprm[i] : own; }
+
 template <>
 struct KernelEval<double> {
   __device__ static inline double eval(const KernelParams& k, const Points& p, int i, int j) {
     double r = dist_fp64(p, i, j);
-    if (k.kind == kLaplaceReg) return __ddiv_rn(1.0, __dmul_rn(HB_FOUR_PI, __dadd_rn(r, k.delta)));
-    double v = exp(__ddiv_rn(-r, k.ell));
+    if (k.kind == kLaplaceReg) return __ddiv_rn(1.0, __dmul_rn(HB_FOUR_PI, __dadd_rn(r, param_of(p, i, k.delta))));
+    double v = exp(__ddiv_rn(-r, param_of(p, i, k.ell)));
     if (p.rid[i] == p.cid[j]) v = __dadd_rn(v, k.nugget);
     return v;
   }
@@ -266,8 +273,8 @@ template <>
 struct KernelEval<float> {
   __device__ static inline float eval(const KernelParams& k, const Points& p, int i, int j) {
     float r = dist_fp32(p, i, j);
-    if (k.kind == kLaplaceReg) return 1.0f / ((float)HB_FOUR_PI * (r + (float)k.delta));
-    float v = expf(-r / (float)k.ell);
+    if (k.kind == kLaplaceReg) return 1.0f / ((float)HB_FOUR_PI * (r + (float)param_of(p, i, k.delta)));
+    float v = expf(-r / (float)param_of(p, i, k.ell));
     if (p.rid[i] == p.cid[j]) v += (float)k.nugget;
     return v;
   }
@@ -279,7 +286,7 @@ struct KernelEval<cdouble> {
     double r = dist_fp64(p, i, j);
     double s = __ddiv_rn(1.0, __dmul_rn(HB_FOUR_PI, __dadd_rn(r, k.delta)));
     double sn, cs;
-    sincos(__dmul_rn(k.wavenumber, r), &sn, &cs);
+    sincos(__dmul_rn(param_of(p, i, k.wavenumber), r), &sn, &cs);
     return cdouble{cs * s, sn * s};
   }
 };
@@ -291,7 +298,7 @@ struct KernelEval<cfloat> {
     // hundreds of radians, where an FP32 argument would lose most of its digits.
     double r = dist_fp64(p, i, j);
     float s = 1.0f / ((float)HB_FOUR_PI * ((float)r + (float)k.delta));
-    double kr = k.wavenumber * r;
+    double kr = param_of(p, i, k.wavenumber) * r;
     float ph = (float)(kr - 6.283185307179586 * rint(kr * 0.15915494309189535));
     float sn, cs;
     sincosf(ph, &sn, &cs);

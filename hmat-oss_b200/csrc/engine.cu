@@ -230,36 +230,20 @@ class Engine : public EngineBase {
     upload_points(a);
     const auto& L = bt_->leaves;
     const int nleaves = (int)L.size();
-    leaf_off_.assign(nleaves, -1);
+    piece_loff_.assign(nleaves, -1);
     times_ms[0] = times_ms[1] = times_ms[2] = 0;
-
-    // ---- layout of the full leaves (row panels) ----
-    std::vector<FullLeafDesc> fd;
-    std::vector<PanelDesc> fpanels;
-    long long pos = 0;
-    for (int i = 0; i < nleaves; ++i) {
-      if (L[i].type != 0 || L[i].m == 0 || L[i].n == 0) continue;
-      FullLeafDesc d{L[i].row_off, L[i].m, L[i].col_off, L[i].n, (int)fpanels.size(), 0};
-      leaf_off_[i] = pos;
-      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
-      for (int b = br.first; b < br.second; ++b) {
-        fpanels.push_back(PanelDesc{rblocks_[b].off - L[i].row_off, rblocks_[b].len, pos});
-        pos += padded((long long)rblocks_[b].len * L[i].n);
-        d.npanel++;
-      }
-      fd.push_back(d);
-    }
-    const long long full_total = pad32(pos);
-    full_total_ = full_total;
 
     // ---- admissible leaves: ACA / SVD, truncation, compaction into pieces ----
     assemble_rk(method, eps_aca, eps_trunc, svd_below);
-    long long rk_total = 0;
-    for (auto& pc : pieces_) rk_total += pad32(pc.elems);
 
-    // ---- final arena: full leaves, then the Rk pieces ----
-    arena_.alloc((size_t)(full_total + rk_total + 256));
-    arena_elems_ = full_total + rk_total;
+    // ---- final arena (the ranks fix the layout): full leaves evaluated in place, the Rk
+    // factors moved from their pieces ----
+    compute_layout();
+    std::vector<FullLeafDesc> fd;
+    std::vector<PanelDesc> fpanels;
+    full_descs(fd, fpanels, nullptr);
+    arena_.alloc((size_t)(layout_.total + 256));
+    HB_CUDA(cudaMemsetAsync(arena_.p, 0, (size_t)layout_.total * sizeof(T), stream_));  // padding columns
     DevArray<FullLeafDesc> d_fd;
     DevArray<PanelDesc> d_fp;
     d_fd.upload(fd, stream_);
@@ -268,17 +252,7 @@ class Engine : public EngineBase {
     launch_assemble_full<T>(d_fd.p, (int)fd.size(), d_fp.p, kp_, pts_, arena_.p, stream_);
     HB_CUDA(cudaGetLastError());
     HB_CUDA(cudaEventRecord(ev_[1], stream_));
-    long long base = full_total;
-    std::vector<long long> piece_base(pieces_.size());
-    for (size_t p = 0; p < pieces_.size(); ++p) {
-      piece_base[p] = base;
-      if (pieces_[p].elems)
-        HB_CUDA(cudaMemcpyAsync(arena_.p + base, pieces_[p].arena.p, pieces_[p].elems * sizeof(T),
-                                cudaMemcpyDeviceToDevice, stream_));
-      base += pad32(pieces_[p].elems);
-    }
-    for (int i = 0; i < nleaves; ++i)
-      if (L[i].type == 1 && piece_of_[i] >= 0) leaf_off_[i] += piece_base[piece_of_[i]];
+    scatter_pieces(arena_.p);
     HB_CUDA(cudaStreamSynchronize(stream_));
     float ms = 0;
     HB_CUDA(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
@@ -349,29 +323,26 @@ class Engine : public EngineBase {
   long long leaf_payload(int leaf, void* out) override {
     if (!assembled || leaf < 0 || leaf >= (int)bt_->leaves.size()) return -1;
     const LeafInfo& L = bt_->leaves[leaf];
-    if (leaf_off_[leaf] < 0) return 0;
+    if (layout_.first[leaf] < 0) return 0;
     const int k = ranks[leaf];
-    if (L.type == 1 && k <= 0) return 0;
-    auto br = block_range(rblocks_, rstarts_, L.row_off, L.m);
     const int w = L.type == 0 ? L.n : k;  // columns of a row panel
-    long long span = 0;
-    for (int b = br.first; b < br.second; ++b) span += padded((long long)rblocks_[b].len * w);
-    const long long bt_off = span;
-    if (L.type == 1) span += (long long)k * L.n;
-    std::vector<T> h((size_t)span);
-    HB_CUDA(cudaMemcpy(h.data(), arena_.p + leaf_off_[leaf], span * sizeof(T), cudaMemcpyDeviceToHost));
+    auto br = block_range(rblocks_, rstarts_, L.row_off, L.m);
     T* o = (T*)out;
-    long long p = 0;
+    std::vector<T> h;
     for (int b = br.first; b < br.second; ++b) {  // row panels -> column-major m x w
       const int rs = rblocks_[b].off - L.row_off, len = rblocks_[b].len;
+      h.resize((size_t)len * w);
+      HB_CUDA(cudaMemcpy(h.data(), arena_.p + layout_.panel[layout_.first[leaf] + (b - br.first)],
+                         h.size() * sizeof(T), cudaMemcpyDeviceToHost));
       for (int j = 0; j < w; ++j)
-        for (int i = 0; i < len; ++i) o[(size_t)rs + i + (size_t)j * L.m] = h[p + i + (size_t)j * len];
-      p += padded((long long)len * w);
+        for (int i = 0; i < len; ++i) o[(size_t)rs + i + (size_t)j * L.m] = h[i + (size_t)j * len];
     }
     if (L.type == 0) return (long long)L.m * L.n;
+    h.resize((size_t)k * L.n);
+    HB_CUDA(cudaMemcpy(h.data(), arena_.p + layout_.bt[leaf], h.size() * sizeof(T), cudaMemcpyDeviceToHost));
     T* Bo = o + (size_t)L.m * k;  // B^T (k x n) -> B (n x k)
     for (int j = 0; j < L.n; ++j)
-      for (int l = 0; l < k; ++l) Bo[j + (size_t)l * L.n] = h[bt_off + l + (size_t)j * k];
+      for (int l = 0; l < k; ++l) Bo[j + (size_t)l * L.n] = h[l + (size_t)j * k];
     return (long long)k * (L.m + L.n);
   }
 
@@ -421,32 +392,17 @@ class Engine : public EngineBase {
     std::vector<long long> goff(nleaves);
     long long total = 0;
     payload_layout(goff.data(), &total);
-    leaf_off_.assign(nleaves, -1);
-    // full leaves: row panels, as assemble lays them out
+    compute_layout();
+    // full leaves: canonical m x n into their row panels
     std::vector<FullLeafDesc> fd;
     std::vector<long long> fgoff;
     std::vector<PanelDesc> fpanels;
-    long long pos = 0;
-    for (int i = 0; i < nleaves; ++i) {
-      if (L[i].type != 0 || L[i].m == 0 || L[i].n == 0) continue;
-      FullLeafDesc d{L[i].row_off, L[i].m, L[i].col_off, L[i].n, (int)fpanels.size(), 0};
-      leaf_off_[i] = pos;
-      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
-      for (int b = br.first; b < br.second; ++b) {
-        fpanels.push_back(PanelDesc{rblocks_[b].off - L[i].row_off, rblocks_[b].len, pos});
-        pos += padded((long long)rblocks_[b].len * L[i].n);
-        d.npanel++;
-      }
-      fd.push_back(d);
-      fgoff.push_back(goff[i]);
-    }
-    full_total_ = pad32(pos);
-    // Rk leaves: A row panels then B^T, from the canonical A (m x k) and B (n x k)
+    full_descs(fd, fpanels, &fgoff, &goff);
+    // Rk leaves: canonical A (m x k) and B (n x k) into the A panels and B^T
     std::vector<RkLeafDesc> rd;
     std::vector<int> rk;
     std::vector<RkStoreDesc> store;
     std::vector<PanelDesc> panels;
-    long long pe = 0;
     for (int i = 0; i < nleaves; ++i) {
       const int k = ranks[i];
       if (L[i].type != 1 || k <= 0) continue;
@@ -461,20 +417,10 @@ class Engine : public EngineBase {
       d.pad = 0;
       rd.push_back(d);
       rk.push_back(k);
-      RkStoreDesc st{(int)panels.size(), 0, 0};
-      leaf_off_[i] = full_total_ + pe;
-      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
-      for (int q = br.first; q < br.second; ++q) {
-        panels.push_back(PanelDesc{rblocks_[q].off - L[i].row_off, rblocks_[q].len, pe});
-        pe += padded((long long)rblocks_[q].len * k);
-        st.npanel++;
-      }
-      st.bt_off = pe;
-      pe += padded((long long)k * L[i].n);
-      store.push_back(st);
+      store.push_back(rk_store(i, panels));
     }
-    arena_.alloc((size_t)(full_total_ + pad32(pe) + 256));
-    arena_elems_ = full_total_ + pad32(pe);
+    arena_.alloc((size_t)(layout_.total + 256));
+    HB_CUDA(cudaMemsetAsync(arena_.p, 0, (size_t)layout_.total * sizeof(T), stream_));
     DevArray<T> src;
     src.alloc((size_t)std::max(total, 1LL));
     if (total) HB_CUDA(cudaMemcpyAsync(src.p, canonical, total * sizeof(T), cudaMemcpyHostToDevice, stream_));
@@ -493,7 +439,7 @@ class Engine : public EngineBase {
     d_panels.upload(panels, stream_);
     launch_full_from_canonical<T>(d_fd.p, d_fgoff.p, (int)fd.size(), d_fp.p, src.p, arena_.p, stream_);
     HB_CUDA(cudaGetLastError());
-    launch_compact<T>(d_rd.p, (int)rd.size(), src.p, d_rk.p, d_store.p, d_panels.p, arena_.p + full_total_, stream_);
+    launch_compact<T>(d_rd.p, (int)rd.size(), src.p, d_rk.p, d_store.p, d_panels.p, arena_.p, stream_);
     HB_CUDA(cudaGetLastError());
     HB_CUDA(cudaStreamSynchronize(stream_));
     build_plan();
@@ -522,6 +468,7 @@ class Engine : public EngineBase {
         queue.push_back(j);
       }
     piece_of_.assign(nleaves, -1);
+    piece_loff_.assign(nleaves, -1);
     pieces_.clear();
     const size_t budget = workspace_budget();
     size_t pos = 0;
@@ -535,33 +482,35 @@ class Engine : public EngineBase {
         bytes += b;
         batch.push_back(queue[pos++]);
       }
-      run_batch(batch, eps, eps, retry, arena_.p);
+      run_batch(batch, eps, eps, retry, arena_.p);  // unpacks with the current layout
       if (!retry.empty()) throw Error("re-truncation: unexpected capacity retry");
     }
-    // new arena: the full leaves unchanged, then the re-truncated pieces
-    long long rk_total = 0;
-    for (auto& pc : pieces_) rk_total += pad32(pc.elems);
+    // new arena for the new ranks: the full leaves' panels moved, the re-truncated factors
+    // from their pieces
+    const Layout old = layout_;
+    compute_layout();
     DevArray<T> na;
-    na.alloc((size_t)(full_total_ + rk_total + 256));
-    if (full_total_) HB_CUDA(cudaMemcpyAsync(na.p, arena_.p, full_total_ * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
-    long long base = full_total_;
-    std::vector<long long> piece_base(pieces_.size());
-    for (size_t p = 0; p < pieces_.size(); ++p) {
-      piece_base[p] = base;
-      if (pieces_[p].elems)
-        HB_CUDA(cudaMemcpyAsync(na.p + base, pieces_[p].arena.p, pieces_[p].elems * sizeof(T),
-                                cudaMemcpyDeviceToDevice, stream_));
-      base += pad32(pieces_[p].elems);
+    na.alloc((size_t)(layout_.total + 256));
+    HB_CUDA(cudaMemsetAsync(na.p, 0, (size_t)layout_.total * sizeof(T), stream_));
+    std::vector<CopySeg> segs;
+    for (int i = 0; i < nleaves; ++i) {
+      if (L[i].type != 0 || layout_.first[i] < 0) continue;
+      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
+      for (int b = br.first; b < br.second; ++b)
+        segs.push_back(CopySeg{old.panel[old.first[i] + (b - br.first)], layout_.panel[layout_.first[i] + (b - br.first)],
+                               (long long)rblocks_[b].len * L[i].n});
     }
-    for (int i = 0; i < nleaves; ++i)
-      if (L[i].type == 1) leaf_off_[i] = piece_of_[i] >= 0 ? leaf_off_[i] + piece_base[piece_of_[i]] : -1;
+    DevArray<CopySeg> d_segs;
+    d_segs.upload(segs, stream_);
+    launch_copy_segments<T>(d_segs.p, (int)segs.size(), arena_.p, na.p, stream_);
+    HB_CUDA(cudaGetLastError());
+    scatter_pieces(na.p);
     HB_CUDA(cudaStreamSynchronize(stream_));
     arena_.release();
     arena_.p = na.p;
     arena_.n = na.n;
     na.p = nullptr;
     na.n = 0;
-    arena_elems_ = full_total_ + rk_total;
     pieces_.clear();
     if (gexec_) {
       cudaGraphExecDestroy(gexec_);
@@ -598,7 +547,7 @@ class Engine : public EngineBase {
     const auto& L = bt_->leaves;
     double full = 0, fa = 0, fb = 0;
     for (size_t i = 0; i < L.size(); ++i) {
-      if (L[i].type == 0 && leaf_off_[i] >= 0) full += (double)L[i].m * L[i].n;
+      if (L[i].type == 0 && layout_.first[i] >= 0) full += (double)L[i].m * L[i].n;
       if (L[i].type == 1 && ranks[i] > 0) {
         fa += (double)L[i].m * ranks[i];
         fb += (double)L[i].n * ranks[i];
@@ -714,6 +663,15 @@ class Engine : public EngineBase {
     pts_.cz = pts_.cx + 2 * (size_t)nc;
     pts_.rid = d_perm_rows_.p;
     pts_.cid = d_perm_cols_.p;
+    pts_.rprm = nullptr;
+    if (!a.param.empty()) {
+      // per-point kernel parameter, taken from the row point (cluster order)
+      if ((long long)a.param.size() != nr) throw Error("one kernel parameter per point is needed");
+      std::vector<double> hp(nr);
+      for (int i = 0; i < nr; ++i) hp[i] = a.param[R_->perm[i]];
+      d_prm_.upload(hp, stream_);
+      pts_.rprm = d_prm_.p;
+    }
   }
 
   struct RkJob {
@@ -897,18 +855,8 @@ class Engine : public EngineBase {
       std::vector<RkStoreDesc> ostore(nb);
       std::vector<PanelDesc> opanels;
       for (int b = 0; b < nb; ++b) {
-        const int leaf = jobs[b].leaf;
-        const LeafInfo& l = L[leaf];
         k0[b] = jobs[b].kcap;
-        ostore[b] = RkStoreDesc{(int)opanels.size(), 0, 0};
-        long long p = leaf_off_[leaf];
-        auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
-        for (int q = br.first; q < br.second; ++q) {
-          opanels.push_back(PanelDesc{rblocks_[q].off - l.row_off, rblocks_[q].len, p});
-          p += padded((long long)rblocks_[q].len * k0[b]);
-          ostore[b].npanel++;
-        }
-        ostore[b].bt_off = p;
+        ostore[b] = rk_store(jobs[b].leaf, opanels);  // the stored leaf in the current layout
       }
       d_ranks.upload(k0, stream_);
       DevArray<RkStoreDesc> d_ostore;
@@ -1297,7 +1245,7 @@ class Engine : public EngineBase {
       const int leaf = jobs[b].leaf;
       ranks[leaf] = h_ranks[b];
       piece_of_[leaf] = h_ranks[b] > 0 ? pid : -1;
-      leaf_off_[leaf] = loff[b];
+      piece_loff_[leaf] = loff[b];
     }
     pieces_.push_back(std::move(piece));
   }
@@ -1347,6 +1295,133 @@ class Engine : public EngineBase {
   }
 
   // ------------------------------------------------------------------------------
+  // Arena layout.  Region Y: per output block b (rblocks_, O_b rows), the row panels of every
+  // leaf whose rows cover b, side by side in leaf order as one column-major O_b x W_b matrix
+  // (a full leaf's panel has n columns, an Rk leaf's A panel k columns), W_b rounded up to a
+  // multiple of kYColAlign with zero columns; so a leaf's panel for b is still one contiguous
+  // O_b x w chunk.  Region BT: per Rk leaf of rank k > 0, B^T (k x n, column-major), 16-byte
+  // aligned.  The 'N' product streams each block's matrix in one pass; every piece of it and
+  // every B^T starts on a 16-byte boundary (the TMA rule).
+  struct Layout {
+    std::vector<int> first;         // per leaf: its first entry in `panel`, -1 without storage
+    std::vector<long long> panel;   // per (leaf, block of its rows): offset of the leaf's panel
+    std::vector<int> pcol;          // its first column in the block's matrix
+    std::vector<long long> bt;      // per leaf: offset of B^T, -1 unless Rk with rank > 0
+    std::vector<long long> yblock;  // per output block: offset of its matrix
+    std::vector<int> ywidth;        // per output block: columns (a multiple of kYColAlign)
+    long long total = 0;
+  };
+
+  bool has_storage(int i) const {
+    const LeafInfo& l = bt_->leaves[i];
+    if (l.m == 0 || l.n == 0) return false;
+    return l.type == 0 || ranks[i] > 0;
+  }
+
+  void compute_layout() {
+    const auto& L = bt_->leaves;
+    const int nleaves = (int)L.size();
+    Layout y;
+    y.first.assign(nleaves, -1);
+    y.bt.assign(nleaves, -1);
+    std::vector<int> width(rblocks_.size(), 0);
+    for (int i = 0; i < nleaves; ++i) {
+      if (!has_storage(i)) continue;
+      const int w = L[i].type == 0 ? L[i].n : ranks[i];
+      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
+      y.first[i] = (int)y.pcol.size();
+      for (int b = br.first; b < br.second; ++b) {
+        y.pcol.push_back(width[b]);
+        width[b] += w;
+      }
+    }
+    long long pos = 0;
+    y.yblock.resize(rblocks_.size());
+    y.ywidth.resize(rblocks_.size());
+    for (size_t b = 0; b < rblocks_.size(); ++b) {
+      y.yblock[b] = pos;
+      y.ywidth[b] = (width[b] + kYColAlign - 1) / kYColAlign * kYColAlign;
+      pos += (long long)rblocks_[b].len * y.ywidth[b];
+    }
+    y.panel.resize(y.pcol.size());
+    for (int i = 0; i < nleaves; ++i) {
+      if (y.first[i] < 0) continue;
+      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
+      for (int b = br.first; b < br.second; ++b) {
+        const int e = y.first[i] + (b - br.first);
+        y.panel[e] = y.yblock[b] + (long long)y.pcol[e] * rblocks_[b].len;
+      }
+    }
+    pos = pad32(pos);
+    for (int i = 0; i < nleaves; ++i) {
+      if (L[i].type != 1 || y.first[i] < 0) continue;
+      y.bt[i] = pos;
+      pos += padded((long long)ranks[i] * L[i].n);
+    }
+    y.total = pad32(pos);
+    layout_ = std::move(y);
+  }
+
+  // Descriptors of the full leaves' row panels in the current layout (and, with `goff`, their
+  // canonical offsets).
+  void full_descs(std::vector<FullLeafDesc>& fd, std::vector<PanelDesc>& fp, std::vector<long long>* fgoff,
+                  const std::vector<long long>* goff = nullptr) const {
+    const auto& L = bt_->leaves;
+    for (int i = 0; i < (int)L.size(); ++i) {
+      if (L[i].type != 0 || layout_.first[i] < 0) continue;
+      FullLeafDesc d{L[i].row_off, L[i].m, L[i].col_off, L[i].n, (int)fp.size(), 0};
+      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
+      for (int b = br.first; b < br.second; ++b) {
+        fp.push_back(PanelDesc{rblocks_[b].off - L[i].row_off, rblocks_[b].len,
+                               layout_.panel[layout_.first[i] + (b - br.first)]});
+        d.npanel++;
+      }
+      fd.push_back(d);
+      if (fgoff) fgoff->push_back((*goff)[i]);
+    }
+  }
+
+  // Where Rk leaf i's factors live in the current layout: its A panels appended to `panels`.
+  RkStoreDesc rk_store(int i, std::vector<PanelDesc>& panels) const {
+    const LeafInfo& l = bt_->leaves[i];
+    RkStoreDesc st{(int)panels.size(), 0, layout_.bt[i]};
+    if (layout_.first[i] < 0) return st;
+    auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
+    for (int b = br.first; b < br.second; ++b) {
+      panels.push_back(PanelDesc{rblocks_[b].off - l.row_off, rblocks_[b].len,
+                                 layout_.panel[layout_.first[i] + (b - br.first)]});
+      st.npanel++;
+    }
+    return st;
+  }
+
+  // The compacted factors of every piece (A row panels, then B^T, per leaf at piece_loff_)
+  // into their places in `dst` (laid out by layout_).
+  void scatter_pieces(T* dst) {
+    const auto& L = bt_->leaves;
+    std::vector<std::vector<CopySeg>> segs(pieces_.size());
+    for (int i = 0; i < (int)L.size(); ++i) {
+      if (L[i].type != 1 || piece_of_[i] < 0 || layout_.first[i] < 0) continue;
+      const int k = ranks[i];
+      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
+      long long p = piece_loff_[i];
+      for (int b = br.first; b < br.second; ++b) {
+        const long long len = (long long)rblocks_[b].len * k;
+        segs[piece_of_[i]].push_back(CopySeg{p, layout_.panel[layout_.first[i] + (b - br.first)], len});
+        p += padded(len);
+      }
+      segs[piece_of_[i]].push_back(CopySeg{p, layout_.bt[i], (long long)k * L[i].n});
+    }
+    std::vector<DevArray<CopySeg>> d_segs(pieces_.size());
+    for (size_t q = 0; q < pieces_.size(); ++q) {
+      d_segs[q].upload(segs[q], stream_);
+      launch_copy_segments<T>(d_segs[q].p, (int)segs[q].size(), pieces_[q].arena.p, dst, stream_);
+      HB_CUDA(cudaGetLastError());
+    }
+    HB_CUDA(cudaStreamSynchronize(stream_));
+  }
+
+  // ------------------------------------------------------------------------------
   // gemv schedule
   struct SideBuf {
     DevArray<GemvUnit> units;
@@ -1390,12 +1465,25 @@ class Engine : public EngineBase {
     return wide;
   }
 
+  // FP32 tensor-core units: the widest multiple of 8 columns whose piece (O x c) and X rows
+  // (c rows of 16 floats) fit one pipeline stage, the X rows right after the piece (16-byte
+  // aligned); *xoff is their offset in the stage.
+  static int mma_unit_cols(int O, int* xoff) {
+    const int stage = warp_piece_bytes(4) + kWarpXBytes;
+    auto need = [&](int c) { return (((long long)O * c * 4 + 15) / 16) * 16 + (long long)c * 64; };
+    int c = 8;
+    while (need(c + 8) <= stage) c += 8;
+    if (need(c) > stage) throw Error("gemv plan: output too tall for a tensor-core unit");
+    *xoff = (int)(((long long)O * c * 4 + 15) / 16 * 16);
+    return c;
+  }
+
   // Units of out(O rows) += P X for a column-major O x C block at `poff`, X rows from `xrow`,
   // `cols` columns per unit.
   void px_units(std::vector<GemvUnit>& u, long long poff, int O, int C, int xrow, int cols = 32,
                 int xoff = warp_piece_bytes((int)sizeof(T))) {
     for (int j0 = 0; j0 < C; j0 += cols) {
-      GemvUnit g;
+      GemvUnit g{};  // nruns = 0: contiguous X rows
       g.poff = poff + (long long)j0 * O;
       g.xrow = xrow + j0;
       g.c = std::min(cols, C - j0);
@@ -1411,7 +1499,7 @@ class Engine : public EngineBase {
   void ptx_units(std::vector<GemvUnit>& u, long long poff, int C, int W, int o_base, int xrow) {
     if (C > 128) throw Error("gemv plan: transposed inner extent above 128 (rank or block too large)");
     for (int w0 = 0; w0 < W; w0 += 32) {
-      GemvUnit g;
+      GemvUnit g{};  // nruns = 0: contiguous X rows
       g.poff = poff + (long long)w0 * C;
       g.xrow = xrow;
       g.c = C;
@@ -1425,8 +1513,8 @@ class Engine : public EngineBase {
 
   // Contiguous ranges of tasks of about equal bytes for a persistent grid: one range per
   // CTA, or per warp for warp-level launches.  Returns the range starts; *ncta is the grid.
-  std::vector<int> partition(const std::vector<GemvTask>& tasks, const std::vector<GemvUnit>& units, int omax,
-                             bool transposed, bool warp_level, int map, int* ncta) {
+  // CTAs of the persistent grid of a launch: as many as fit the SMs at once.
+  static int launch_ctas(int omax, bool transposed, bool warp_level, int map) {
     const int Rmax = sizeof(T) >= 16 ? 4 : 16;
     const int RS16 = gemv_rhs_stride((int)sizeof(T), Rmax);
     const size_t smem = map == 4      ? umma_smem_bytes()
@@ -1436,9 +1524,16 @@ class Engine : public EngineBase {
     // bounds guarantee the registers for that many CTAs)
     int per_sm = (int)std::min<size_t>(8, ((warp_level ? 228 : 226) * 1024) / (smem + 1024));
     per_sm = std::max(per_sm, 1);
+    return persistent_grid(per_sm);
+  }
+
+  std::vector<int> partition(const std::vector<GemvTask>& tasks, const std::vector<GemvUnit>& units, int omax,
+                             bool transposed, bool warp_level, int map, int* ncta) {
+    const int Rmax = sizeof(T) >= 16 ? 4 : 16;
+    const int RS16 = gemv_rhs_stride((int)sizeof(T), Rmax);
     const int wpc = warp_level ? warp_stream_warps_per_cta() : 1;
     const int nt = (int)tasks.size();
-    const int cta = std::max(1, std::min((nt + wpc - 1) / wpc, persistent_grid(per_sm)));
+    const int cta = std::max(1, std::min((nt + wpc - 1) / wpc, launch_ctas(omax, transposed, warp_level, map)));
     *ncta = cta;
     const int G = cta * wpc;
     std::vector<double> cost(tasks.size());
@@ -1470,17 +1565,20 @@ class Engine : public EngineBase {
     L.warp_level = true;
     L.ol = 32;
     if (std::is_same<T, float>::value) {
-      // FP32: tensor-core tiles of 16 rows (map 3, rpt = row tiles held per warp)
+      // FP32: tensor-core tiles of 8 output rows (map 3, rpt = row tiles held per warp)
       L.map = 3;
-      L.rpt = omax <= 32 ? 2 : (omax <= 64 ? 4 : 8);
+      L.rpt = omax <= 16 ? 2 : (omax <= 32 ? 4 : (omax <= 64 ? 8 : 16));
       return;
     }
     L.map = omax <= 32 ? 2 : (omax <= 64 ? 1 : 0);
     L.rpt = omax <= 32 ? 2 : 4;
   }
 
+  // With `begin` given (one range of tasks per warp, or per CTA, of the full persistent grid),
+  // the ranges are taken as they are instead of being cut by cost here.
   void finish_launch(GemvLaunch& L, SideBuf& sb, int slot, std::vector<GemvTask>& tasks,
-                     const std::vector<GemvUnit>& units, int ol, int rpt, bool transposed, bool out_is_y) {
+                     const std::vector<GemvUnit>& units, int ol, int rpt, bool transposed, bool out_is_y,
+                     const std::vector<int>* begin_given = nullptr) {
     L.ntasks = (int)tasks.size();
     if (!L.warp_level) {
       L.ol = ol;
@@ -1489,12 +1587,24 @@ class Engine : public EngineBase {
     L.transposed = transposed;
     L.out_is_y = out_is_y;
     if (tasks.empty()) return;
+    // X rows of every unit: contiguous, or at most kUnitRuns runs covering exactly c rows
+    for (auto& t : tasks)
+      for (int u = t.first_unit; u < t.first_unit + t.nunits; ++u) {
+        const GemvUnit& g = units[u];
+        if (g.nruns < 0 || g.nruns > kUnitRuns) throw Error("gemv plan: unit with a bad run count");
+        if (g.nruns > 0) {
+          long long rows = 0;
+          for (int r = 0; r < g.nruns; ++r) rows += g.run_len[r];
+          if (rows != g.c) throw Error("gemv plan: unit runs do not cover its columns");
+          if (transposed) throw Error("gemv plan: runs of X rows in a transposed unit");  // read as one block
+        }
+      }
     // the kernel walks units sequentially across the tasks of a CTA
     for (size_t t = 1; t < tasks.size(); ++t)
       if (tasks[t].first_unit != tasks[t - 1].first_unit + tasks[t - 1].nunits)
         throw Error("gemv plan: units of a launch are not contiguous");
     const int omax = L.map == 4       ? 128
-                     : L.warp_level ? (L.map == 3 ? 16 * L.rpt : (L.map == 2 ? 32 : (L.map == 1 ? 64 : 128)))
+                     : L.warp_level ? (L.map == 3 ? 8 * L.rpt : (L.map == 2 ? 32 : (L.map == 1 ? 64 : 128)))
                                     : ol * rpt;
     for (auto& t : tasks)
       if (t.O > omax) throw Error("gemv plan: task taller than its launch shape");
@@ -1522,7 +1632,16 @@ class Engine : public EngineBase {
             throw Error("gemv plan: unit above the tensor-memory stage capacity");
         }
     }
-    std::vector<int> begin = partition(tasks, units, omax, transposed, L.warp_level, L.map, &L.ncta);
+    std::vector<int> begin;
+    if (begin_given) {
+      const int wpc = L.warp_level ? warp_stream_warps_per_cta() : 1;
+      L.ncta = launch_ctas(omax, transposed, L.warp_level, L.map);
+      begin = *begin_given;
+      if ((int)begin.size() != L.ncta * wpc + 1 || begin.front() != 0 || begin.back() != (int)tasks.size())
+        throw Error("gemv plan: task ranges do not match the launch grid");
+    } else {
+      begin = partition(tasks, units, omax, transposed, L.warp_level, L.map, &L.ncta);
+    }
     sb.tasks[slot].upload(tasks, stream_);
     sb.begin[slot].upload(begin, stream_);
     L.tasks = sb.tasks[slot].p;
@@ -1548,21 +1667,18 @@ class Engine : public EngineBase {
     for (size_t t = 0; t < K.size(); ++t) {
       const GemvRkLeaf& k = K[t];
       const int leaf = rk_leaf[t];
-      const long long base = leaf_off_[leaf];
       lu.clear();
       if (!trans) {
-        // z = B^T x_J: B^T is k x n column-major after the A panels
+        // z = B^T x_J: B^T is k x n column-major
         int xoff = 0;
-        const int zc = warp_unit_cols_wide(k.k, &xoff);
-        px_units(lu, bt_offset(leaf), k.k, k.n, k.col_off, zc, xoff);
+        const int zc = std::is_same<T, float>::value ? mma_unit_cols(k.k, &xoff) : warp_unit_cols_wide(k.k, &xoff);
+        px_units(lu, layout_.bt[leaf], k.k, k.n, k.col_off, zc, xoff);
       } else {
         // z' = A^T x_I: each A panel (len x k) is a transposed piece
         auto br = block_range(rblocks_, rstarts_, k.row_off, k.m);
-        long long p = base;
-        for (int b = br.first; b < br.second; ++b) {
-          ptx_units(lu, p, rblocks_[b].len, k.k, 0, rblocks_[b].off);
-          p += padded((long long)rblocks_[b].len * k.k);
-        }
+        for (int b = br.first; b < br.second; ++b)
+          ptx_units(lu, layout_.panel[layout_.first[leaf] + (b - br.first)], rblocks_[b].len, k.k, 0,
+                    rblocks_[b].off);
       }
       if (k.k > 128) throw Error("gemv plan: ranks above 128 are not supported by the streamed kernels");
       // 'N' launches take every rank up to 32 in one column-slice window launch
@@ -1590,62 +1706,168 @@ class Engine : public EngineBase {
       for (auto& t : zt[c]) t.first_unit += shift;
       units.insert(units.end(), zunits[c].begin(), zunits[c].end());
     }
-    // ---- y-phase: one task per output block ----
-    std::vector<std::vector<std::pair<int, int>>> per_block(oblocks.size());  // (leaf, 0 full / 1 rk index)
+    // ---- y-phase ----
+    std::vector<std::vector<int>> per_block(oblocks.size());  // leaves with storage covering each block
     for (int i = 0; i < (int)L.size(); ++i) {
-      if (leaf_off_[i] < 0) continue;
-      if (L[i].type == 1 && ranks[i] <= 0) continue;
+      if (layout_.first[i] < 0) continue;
       auto br = trans ? block_range(oblocks, ostarts, L[i].col_off, L[i].n)
                       : block_range(oblocks, ostarts, L[i].row_off, L[i].m);
-      for (int b = br.first; b < br.second; ++b) per_block[b].push_back({i, 0});
+      for (int b = br.first; b < br.second; ++b) per_block[b].push_back(i);
     }
     std::vector<int> rk_index(L.size(), -1);
     for (size_t t = 0; t < rk_leaf.size(); ++t) rk_index[rk_leaf[t]] = (int)t;
     std::vector<GemvTask> yt;
+    std::vector<int> ybegin;  // 'N': the warps' task ranges, cut here by cost
     int maxlen = 1;
-    // each output block is cut into chunks of at most kYChunkUnits units whose partial rows go
-    // to xz; a final pass sums them into y (client order).  The chunks spread the blocks with
-    // many leaves over the grid.
-    const int kYChunkUnits = 16;
+    for (const Block& ob : oblocks) maxlen = std::max(maxlen, ob.len);
     const ClusterTree* otree = trans ? C_ : R_;
     std::vector<int2> yrows(otree->n, int2{0, 0});
-    for (size_t b = 0; b < oblocks.size(); ++b) {
-      const Block& ob = oblocks[b];
-      const int first = (int)units.size();
-      for (auto& pr : per_block[b]) {
-        const int i = pr.first;
-        const LeafInfo& l = L[i];
-        if (!trans) {
-          // row panel of leaf i for block b
-          const int w = l.type == 0 ? l.n : ranks[i];
-          const long long poff = row_panel_offset(i, ob.off, w);
-          const int xrow = l.type == 0 ? l.col_off : K[rk_index[i]].zrow_n;
-          px_units(units, poff, ob.len, w, xrow, tc_y ? kTcCols : warp_unit_cols(ob.len));
-        } else if (l.type == 0) {
-          // columns of block b in every row panel of full leaf i
-          auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
-          long long p = leaf_off_[i];
-          for (int q = br.first; q < br.second; ++q) {
-            const int len = rblocks_[q].len;
-            ptx_units(units, p + (long long)(ob.off - l.col_off) * len, len, ob.len, 0, rblocks_[q].off);
-            p += padded((long long)len * l.n);
+    if (!trans) {
+      // Each output block's matrix (the y region of the arena) in units of whole columns; the X
+      // rows of its columns are the leaves' x rows (full) and z rows (Rk), merged into runs where
+      // adjacent, and the zero rows for the padding columns.
+      const int RS16 = gemv_rhs_stride((int)sizeof(T), sizeof(T) >= 16 ? 4 : 16);
+      const int galign = sizeof(T) >= 16 ? 1 : 16 / (int)sizeof(T);  // columns keeping a piece aligned
+      std::vector<int> ublock;  // output block of each y unit
+      std::vector<int> colrow;
+      const int first_y = (int)units.size();
+      for (size_t b = 0; b < oblocks.size(); ++b) {
+        const int O = oblocks[b].len, W = layout_.ywidth[b];
+        if (W == 0) continue;
+        colrow.clear();
+        for (int i : per_block[b]) {
+          const bool full = L[i].type == 0;
+          const int w = full ? L[i].n : ranks[i], row = full ? L[i].col_off : K[rk_index[i]].zrow_n;
+          if ((int)colrow.size() != layout_.pcol[layout_.first[i] + (int)b - block_range(rblocks_, rstarts_,
+                                                                                          L[i].row_off, L[i].m).first])
+            throw Error("gemv plan: block matrix columns out of order");
+          for (int j = 0; j < w; ++j) colrow.push_back(row + j);
+        }
+        const int used = (int)colrow.size();  // at most kYColAlign - 1 = kZeroRows - 1 padding columns
+        for (int j = used; j < W; ++j) colrow.push_back(plan_.n_in_max + (j - used));
+        int xoff = warp_piece_bytes((int)sizeof(T)), cols;
+        if (tc_y)
+          cols = kTcCols;
+        else if (std::is_same<T, float>::value)
+          cols = mma_unit_cols(O, &xoff);
+        else
+          cols = warp_unit_cols(O);
+        for (int j0 = 0; j0 < W;) {
+          const int want = std::min(cols, W - j0);
+          // the columns the unit can take with at most kUnitRuns runs of X rows
+          int c = 0, nr = 0;
+          while (c < want) {
+            if (c == 0 || colrow[j0 + c] != colrow[j0 + c - 1] + 1) {
+              if (nr == kUnitRuns) break;
+              ++nr;
+            }
+            ++c;
           }
-        } else {
-          const int k = ranks[i];
-          ptx_units(units, bt_offset(i) + (long long)(ob.off - l.col_off) * k, k, ob.len, 0,
-                    K[rk_index[i]].zrow_t);
+          if (c < want) c -= c % galign;  // cut short: the next piece must start 16-byte aligned
+          if (c <= 0) throw Error("gemv plan: unit without columns");
+          GemvUnit u{};
+          u.poff = layout_.yblock[b] + (long long)j0 * O;
+          u.xrow = colrow[j0];
+          u.c = c;
+          u.o0 = xoff;
+          u.ow = O;
+          u.pel = O * c;
+          u.shift = (int)(u.poff % kPad);
+          if (u.shift) throw Error("gemv plan: misaligned block piece");
+          u.nruns = 0;
+          for (int j = 0; j < c; ++j) {
+            if (j == 0 || colrow[j0 + j] != colrow[j0 + j - 1] + 1) {
+              u.run_row[u.nruns] = colrow[j0 + j];
+              u.run_len[u.nruns] = 0;
+              ++u.nruns;
+            }
+            ++u.run_len[u.nruns - 1];
+          }
+          units.push_back(u);
+          ublock.push_back((int)b);
+          j0 += c;
         }
       }
-      maxlen = std::max(maxlen, ob.len);
-      const int nu = (int)units.size() - first;
-      const int nparts = (nu + kYChunkUnits - 1) / kYChunkUnits;
-      const int part_row = (int)next_row;
-      next_row += (long long)nparts * ob.len;
-      for (int pidx = 0; pidx < nparts; ++pidx) {
-        const int u0 = pidx * kYChunkUnits, u1 = std::min(nu, u0 + kYChunkUnits);
-        yt.push_back(GemvTask{ob.len, first + u0, u1 - u0, part_row + pidx * ob.len});
+      // Tasks: the y units cut into one range of about equal cost per warp of the launch, and
+      // at block boundaries; a task writes its block's partial rows, summed by the final pass.
+      GemvLaunch probe;
+      if (tc_y) probe.map = 4;
+      else warp_shape(probe, maxlen);
+      const int wpc = probe.map == 4 ? 1 : warp_stream_warps_per_cta();
+      const int G = launch_ctas(maxlen, false, probe.map != 4, probe.map) * wpc;
+      const int nyu = (int)units.size() - first_y;
+      std::vector<double> cum(nyu + 1, 0.0);
+      for (int v = 0; v < nyu; ++v) {
+        const GemvUnit& u = units[first_y + v];
+        cum[v + 1] = cum[v] + (double)u.pel + (double)u.c * RS16 + 64;
       }
-      for (int l = 0; l < ob.len; ++l) yrows[otree->perm[ob.off + l]] = int2{part_row + l, (nparts << 8) | ob.len};
+      const double tot = std::max(cum[nyu], 1.0);
+      ybegin.assign(G + 1, 0);
+      int w = 0;
+      std::vector<int> task_block;
+      for (int v = 0; v < nyu;) {
+        // the warp of unit v: the last w with cum[v] >= tot * w / G
+        while (w + 1 < G && cum[v] >= tot * (w + 1) / G) {
+          ++w;
+          ybegin[w] = (int)yt.size();
+        }
+        const double wend = w + 1 < G ? tot * (w + 1) / G : 1e300;
+        int v1 = v + 1;
+        while (v1 < nyu && ublock[v1] == ublock[v] && cum[v1] < wend) ++v1;
+        yt.push_back(GemvTask{oblocks[ublock[v]].len, first_y + v, v1 - v, 0});
+        task_block.push_back(ublock[v]);
+        v = v1;
+      }
+      for (++w; w <= G; ++w) ybegin[w] = (int)yt.size();
+      // partial-row slots: the tasks of a block (consecutive) take consecutive slots
+      std::vector<int> nparts(oblocks.size(), 0), part_row(oblocks.size(), 0);
+      for (size_t t = 0; t < yt.size(); ++t) {
+        const int b = task_block[t];
+        if (nparts[b] == 0) {
+          part_row[b] = (int)next_row;
+        }
+        yt[t].out_row = part_row[b] + nparts[b] * oblocks[b].len;
+        nparts[b]++;
+        next_row += oblocks[b].len;
+      }
+      for (size_t b = 0; b < oblocks.size(); ++b) {
+        const Block& ob = oblocks[b];
+        for (int l = 0; l < ob.len; ++l)
+          yrows[otree->perm[ob.off + l]] = int2{part_row[b] + l, (nparts[b] << 8) | ob.len};
+      }
+    } else {
+      // each output block is cut into chunks of at most kYChunkUnits units whose partial rows go
+      // to xz; a final pass sums them into y (client order).  The chunks spread the blocks with
+      // many leaves over the grid.
+      const int kYChunkUnits = 16;
+      for (size_t b = 0; b < oblocks.size(); ++b) {
+        const Block& ob = oblocks[b];
+        const int first = (int)units.size();
+        for (int i : per_block[b]) {
+          const LeafInfo& l = L[i];
+          if (l.type == 0) {
+            // columns of block b in every row panel of full leaf i
+            auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
+            for (int q = br.first; q < br.second; ++q) {
+              const int len = rblocks_[q].len;
+              ptx_units(units, layout_.panel[layout_.first[i] + (q - br.first)] + (long long)(ob.off - l.col_off) * len,
+                        len, ob.len, 0, rblocks_[q].off);
+            }
+          } else {
+            const int k = ranks[i];
+            ptx_units(units, layout_.bt[i] + (long long)(ob.off - l.col_off) * k, k, ob.len, 0, K[rk_index[i]].zrow_t);
+          }
+        }
+        const int nu = (int)units.size() - first;
+        const int nparts = (nu + kYChunkUnits - 1) / kYChunkUnits;
+        const int part_row = (int)next_row;
+        next_row += (long long)nparts * ob.len;
+        for (int pidx = 0; pidx < nparts; ++pidx) {
+          const int u0 = pidx * kYChunkUnits, u1 = std::min(nu, u0 + kYChunkUnits);
+          yt.push_back(GemvTask{ob.len, first + u0, u1 - u0, part_row + pidx * ob.len});
+        }
+        for (int l = 0; l < ob.len; ++l) yrows[otree->perm[ob.off + l]] = int2{part_row + l, (nparts << 8) | ob.len};
+      }
     }
     // launches
     side.nz = 0;
@@ -1666,7 +1888,7 @@ class Engine : public EngineBase {
       side.y.map = 4;
     else if (!trans)
       warp_shape(side.y, maxlen);
-    finish_launch(side.y, sb, GemvSide::kMaxLaunch, yt, units, 32, rpt, trans, false);
+    finish_launch(side.y, sb, GemvSide::kMaxLaunch, yt, units, 32, rpt, trans, false, trans ? nullptr : &ybegin);
     sb.units.upload(units, stream_);
     side.units = sb.units.p;
     sb.zred.upload(zred, stream_);
@@ -1675,24 +1897,6 @@ class Engine : public EngineBase {
     sb.yrows.upload(yrows, stream_);
     side.nyrows = (int)yrows.size();
     side.yrows = sb.yrows.p;
-  }
-
-  long long bt_offset(int leaf) const {
-    const LeafInfo& l = bt_->leaves[leaf];
-    auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
-    long long p = leaf_off_[leaf];
-    for (int b = br.first; b < br.second; ++b) p += padded((long long)rblocks_[b].len * ranks[leaf]);
-    return p;
-  }
-  long long row_panel_offset(int leaf, int block_off, int w) const {
-    const LeafInfo& l = bt_->leaves[leaf];
-    auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
-    long long p = leaf_off_[leaf];
-    for (int b = br.first; b < br.second; ++b) {
-      if (rblocks_[b].off == block_off) return p;
-      p += padded((long long)rblocks_[b].len * w);
-    }
-    throw Error("gemv plan: block outside the leaf");
   }
 
   void build_plan() {
@@ -1705,9 +1909,9 @@ class Engine : public EngineBase {
     plan_.n_rows = R_->n;
     plan_.n_cols = C_->n;
     plan_.n_in_max = std::max(R_->n, C_->n);
-    long long next_row = plan_.n_in_max;
+    long long next_row = plan_.n_in_max + kZeroRows;
     for (size_t i = 0; i < L.size(); ++i) {
-      if (L[i].type == 0 && leaf_off_[i] >= 0) {
+      if (L[i].type == 0 && layout_.first[i] >= 0) {
         F.push_back(GemvFullLeaf{L[i].row_off, L[i].m, L[i].col_off, L[i].n, goff});
         goff += (long long)L[i].m * L[i].n;
       } else if (L[i].type == 1 && ranks[i] > 0) {
@@ -1726,6 +1930,15 @@ class Engine : public EngineBase {
     if (!d_perm_rows_.p || !d_perm_cols_.p) throw Error("gemv plan: cluster permutations are not on the device");
     plan_.perm_rows = d_perm_rows_.p;
     plan_.perm_cols = d_perm_cols_.p;
+    std::vector<int> inv(R_->n);
+    for (int i = 0; i < R_->n; ++i) inv[R_->perm[i]] = i;
+    d_iperm_rows_.upload(inv, stream_);
+    inv.assign(C_->n, 0);
+    for (int i = 0; i < C_->n; ++i) inv[C_->perm[i]] = i;
+    d_iperm_cols_.upload(inv, stream_);
+    HB_CUDA(cudaStreamSynchronize(stream_));
+    plan_.iperm_rows = d_iperm_rows_.p;
+    plan_.iperm_cols = d_iperm_cols_.p;
     plan_.arena = arena_.p;
     g_full_.upload(F, stream_);
     g_rk_.upload(K, stream_);
@@ -1755,13 +1968,14 @@ class Engine : public EngineBase {
   KernelParams kp_{};
   Points pts_{};
   DevArray<double> d_pts_;
+  DevArray<double> d_prm_;  // per-point kernel parameter (cluster order), when the points carry one
   DevArray<int> d_perm_rows_, d_perm_cols_;
-  std::vector<long long> leaf_off_;
+  DevArray<int> d_iperm_rows_, d_iperm_cols_;  // client -> cluster order (the gemv's gather)
+  std::vector<long long> piece_loff_;  // per Rk leaf: offset of its factors in its piece (assembly)
   std::vector<int> piece_of_;
   std::vector<Piece> pieces_;
   DevArray<T> arena_;
-  long long arena_elems_ = 0;
-  long long full_total_ = 0;  // elements of the full-leaf region at the start of the arena
+  Layout layout_;
   DevArray<GemvFullLeaf> g_full_;
   DevArray<GemvRkLeaf> g_rk_;
   SideBuf side_buf_[2];

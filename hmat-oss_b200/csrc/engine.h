@@ -18,7 +18,12 @@ namespace hmatb200 {
 
 struct AssemblyDesc {
   KernelParams kp;
-  std::vector<double> pts;  // client numbering, point-major
+  std::vector<double> pts;    // client numbering, point-major
+  // Optional, one per point (client numbering): the kernel's parameter for the blocks of that
+  // point's rows, in place of kp's (the correlation length of the exponential covariance, the
+  // regularisation of the Laplace kernels, the Helmholtz wavenumber).  Batches of independent
+  // matrices with their own kernels use it: a block's rows and columns belong to one matrix.
+  std::vector<double> param;
 };
 
 struct LeafGrad;

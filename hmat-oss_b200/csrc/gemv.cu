@@ -121,13 +121,50 @@ constexpr int nstage_of() {
 }
 
 // ---------------------------------------------------------------------------------
+// x (client order, column-major with leading dimension ldx; right-hand sides q0 .. q0 + R - 1
+// of r) into xz in cluster order (row-major, RS columns, zeros past R).  A CTA takes
+// kGatherRows client rows: it reads each column of x along the rows (coalesced), transposes
+// through shared memory, and writes each client row's RS values as one contiguous xz row at
+// its cluster position iperm[j].  One more CTA clears the kZeroRows zero rows from row `zrow0`
+// (the X rows of the y matrices' padding columns).
+constexpr int kGatherRows = 64;
 template <typename T, int R, int RS>
-__global__ void gather_kernel(const T* __restrict__ x, int N, int ldx, int q0, int r, const int* __restrict__ perm,
-                              T* __restrict__ xz) {
-  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (long long)N * RS) return;
-  const int i = (int)(e / RS), q = (int)(e % RS);
-  xz[e] = (q < R && q0 + q < r) ? x[(size_t)perm[i] + (size_t)(q0 + q) * ldx] : zero<T>();
+__global__ void __launch_bounds__(256) gather_kernel(const T* __restrict__ x, int N, int ldx, int q0, int r,
+                                                     const int* __restrict__ iperm, T* __restrict__ xz, int zrow0) {
+  __shared__ T tile[RS][kGatherRows + 1];
+  const int nblk = (N + kGatherRows - 1) / kGatherRows;
+  if ((int)blockIdx.x >= nblk) {
+    for (int e = threadIdx.x; e < kZeroRows * RS; e += blockDim.x) xz[(size_t)zrow0 * RS + e] = zero<T>();
+    return;
+  }
+  const int j0 = blockIdx.x * kGatherRows;
+  for (int e = threadIdx.x; e < RS * kGatherRows; e += blockDim.x) {
+    const int q = e / kGatherRows, jl = e % kGatherRows, j = j0 + jl;
+    T v = zero<T>();
+    if (j < N && q < R && q0 + q < r) v = x[(size_t)j + (size_t)(q0 + q) * ldx];
+    tile[q][jl] = v;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < RS * kGatherRows; e += blockDim.x) {
+    const int jl = e / RS, q = e % RS, j = j0 + jl;
+    if (j < N) xz[(size_t)iperm[j] * RS + q] = tile[q][jl];
+  }
+}
+inline unsigned gather_grid(int N) { return (unsigned)((N + kGatherRows - 1) / kGatherRows + 1); }
+
+// The X rows of a unit into a pipeline stage: one bulk copy, or one per run.
+template <typename T, int RS>
+__device__ inline void issue_x(unsigned char* dst, const T* xz, const GemvUnit& U, uint64_t* bar) {
+  if (U.nruns == 0) {
+    bulk_g2s(dst, xz + (size_t)U.xrow * RS, (uint32_t)U.c * RS * (uint32_t)sizeof(T), bar);
+    return;
+  }
+  uint32_t off = 0;
+  for (int r = 0; r < U.nruns; ++r) {
+    const uint32_t b = (uint32_t)U.run_len[r] * RS * (uint32_t)sizeof(T);
+    bulk_g2s(dst + off, xz + (size_t)U.run_row[r] * RS, b, bar);
+    off += b;
+  }
 }
 
 // ---------------------------------------------------------------------------------
@@ -417,7 +454,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
     unsigned char* st = wbase + (size_t)s * warp_stage_bytes((int)sizeof(T));
     mbar_expect_tx(&bars[s], pbytes + xbytes);
     bulk_g2s(st, arena + U.poff, pbytes, &bars[s]);
-    bulk_g2s(st + warp_piece_bytes((int)sizeof(T)), xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
+    issue_x<T, RS>(st + warp_piece_bytes((int)sizeof(T)), xz, U, &bars[s]);
   };
   auto issue_next = [&](int v) {  // nxt holds units[v]
     issue(v, nxt);
@@ -548,12 +585,17 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
 
 // Warp-level streamed tasks on the tensor cores (FP32 'N' products).  Same per-warp TMA
 // pipeline as warp_stream_kernel; the product of a unit is a sequence of warp MMAs
-// (mma.sync m16n8k8, TF32 operands, FP32 accumulators) over 16-row tiles of the piece P and
-// 8-column tiles of the right-hand sides.  FP32 accuracy is kept with the three-term split
-// a = a_hi + a_lo (a_hi = a truncated to TF32): P X ~ P_lo X_hi + P_hi X_lo + P_hi X_hi, the
-// P_lo X_lo term (2^-20 relative at most) dropped.  Operands are read from the stage in fragment
-// order (rows g, g + 8 and columns t, t + 4 of each tile, g = lane / 4, t = lane % 4);
-// rows at or past O are computed and never written, columns past the piece are zeros.
+// (mma.sync m16n8k8, TF32 operands, FP32 accumulators) computing out^T = X^T P^T: the
+// right-hand sides are the 16 rows of the MMA (A = X^T, one fragment per 8-column step for
+// the whole task), the output rows its 8 columns (B = P^T, one fragment per 8-row tile), so an
+// output of O rows takes ceil(O / 8) tiles.  FP32 accuracy is kept with the three-term split
+// a = a_hi + a_lo (a_hi = a truncated to TF32): X P ~ X_lo P_hi + X_hi P_lo + X_hi P_hi, the
+// lo x lo term (2^-20 relative at most) dropped, and every 8-column step goes to fresh
+// fragments that are added to the running FP32 sums with round-to-nearest adds (the tensor
+// core's own sums are not rounded to nearest).  Operands are read from the stage in fragment
+// order (g = lane / 4, t = lane % 4): A holds X[k0 + t (+4)][g (+8)], B holds
+// P[k0 + t (+4)][row 8 tile + g]; rows at or past O are computed and never written.  Only the
+// last step of a unit whose width is not a multiple of 8 masks its columns (TAIL).
 // a_hi = a with its low 13 mantissa bits cleared (a TF32 value), a_lo = a - a_hi (exact in
 // FP32; the MMA reads its leading 11 bits).
 __device__ __forceinline__ void tf32_split(float v, uint32_t& hi, uint32_t& lo) {
@@ -568,57 +610,74 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// One 8-column step k0 of a unit: B fragments from the X rows, then every row tile.  TAIL
-// masks the columns at or past c.
-template <int R, int RS, int MT, int NT, bool TAIL>
+// One 8-column step k0 of a unit: the A fragment (X^T) once, then the NT 8-row tiles of the
+// output (NT a compile-time count, so that the tiles' MMA chains are independent straight-line
+// code the scheduler interleaves).  TAIL masks the columns at or past c (both operands: the
+// stage past a short piece holds stale data).
+template <int RS, int NT, int NTILE, bool TAIL>
 __device__ __forceinline__ void mma_kstep(const float* P, const float* X, int k0, int c, int O, int g, int tg,
-                                          int mtn, float (&acc)[MT][NT][4]) {
+                                          float (&acc)[NTILE][4]) {
   const int ka = k0 + tg, kb = k0 + tg + 4;
   const bool va = !TAIL || ka < c, vb = !TAIL || kb < c;
-  uint32_t bh[NT][2], bl[NT][2];
-#pragma unroll
-  for (int nt = 0; nt < NT; ++nt) {
-    const int n = nt * 8 + g;
-    const bool vn = (R % 8 == 0) || n < R;
-    tf32_split((va && vn) ? X[ka * RS + n] : 0.f, bh[nt][0], bl[nt][0]);
-    tf32_split((vb && vn) ? X[kb * RS + n] : 0.f, bh[nt][1], bl[nt][1]);
-  }
+  // right-hand sides g and g + 8 of the xz rows (RS columns; the rest are zeros)
+  const bool q0 = g < RS, q1 = g + 8 < RS;
+  uint32_t ah[4], al[4];
+  tf32_split((va && q0) ? X[ka * RS + g] : 0.f, ah[0], al[0]);
+  tf32_split((va && q1) ? X[ka * RS + g + 8] : 0.f, ah[1], al[1]);
+  tf32_split((vb && q0) ? X[kb * RS + g] : 0.f, ah[2], al[2]);
+  tf32_split((vb && q1) ? X[kb * RS + g + 8] : 0.f, ah[3], al[3]);
   const float* pa = P + ka * O + g;
   const float* pb = P + kb * O + g;
 #pragma unroll
-  for (int mt = 0; mt < MT; ++mt) {
-    if (mt < mtn) {
-      uint32_t ah[4], al[4];
-      tf32_split(va ? pa[mt * 16] : 0.f, ah[0], al[0]);
-      tf32_split(va ? pa[mt * 16 + 8] : 0.f, ah[1], al[1]);
-      tf32_split(vb ? pb[mt * 16] : 0.f, ah[2], al[2]);
-      tf32_split(vb ? pb[mt * 16 + 8] : 0.f, ah[3], al[3]);
-      // the tensor core's FP32 sums are not rounded to nearest: each 8-column step goes to
-      // fresh fragments, added to the running sums with FP32 adds
-      float d[NT][4];
+  for (int t = 0; t < NT; ++t) {
+    uint32_t bh0, bl0, bh1, bl1;
+    tf32_split(va ? pa[t * 8] : 0.f, bh0, bl0);
+    tf32_split(vb ? pb[t * 8] : 0.f, bh1, bl1);
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    mma_tf32(d, al, bh0, bh1);
+    mma_tf32(d, ah, bl0, bl1);
+    mma_tf32(d, ah, bh0, bh1);
 #pragma unroll
-      for (int nt = 0; nt < NT; ++nt) {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) d[nt][e] = 0.f;
-        mma_tf32(d[nt], al, bh[nt][0], bh[nt][1]);
-      }
-#pragma unroll
-      for (int nt = 0; nt < NT; ++nt) mma_tf32(d[nt], ah, bl[nt][0], bl[nt][1]);
-#pragma unroll
-      for (int nt = 0; nt < NT; ++nt) mma_tf32(d[nt], ah, bh[nt][0], bh[nt][1]);
-#pragma unroll
-      for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) acc[mt][nt][e] += d[nt][e];
-    }
+    for (int e = 0; e < 4; ++e) acc[t][e] += d[e];
   }
 }
 
-template <int R, int RS, int MT>
+// All steps of one unit with NT output tiles.
+template <int RS, int NT, int NTILE>
+__device__ __forceinline__ void mma_unit(const float* P, const float* X, int c, int O, int g, int tg,
+                                         float (&acc)[NTILE][4]) {
+  int k0 = 0;
+  if constexpr (NT <= 3) {
+    // two steps per iteration: their MMA chains are independent and overlap (wider tasks
+    // have enough independent tiles in one step, and the registers go to their sums)
+#pragma unroll 2
+    for (; k0 + 8 <= c; k0 += 8) mma_kstep<RS, NT, NTILE, false>(P, X, k0, c, O, g, tg, acc);
+  } else {
+#pragma unroll 1
+    for (; k0 + 8 <= c; k0 += 8) mma_kstep<RS, NT, NTILE, false>(P, X, k0, c, O, g, tg, acc);
+  }
+  if (k0 < c) mma_kstep<RS, NT, NTILE, true>(P, X, k0, c, O, g, tg, acc);
+}
+
+// The unit with the task's tile count (1 .. NTILE) as a compile-time constant.
+template <int RS, int NTILE, int NT = 1>
+__device__ __forceinline__ void mma_unit_dispatch(int ntn, const float* P, const float* X, int c, int O, int g,
+                                                  int tg, float (&acc)[NTILE][4]) {
+  if constexpr (NT < NTILE) {
+    if (ntn == NT) {
+      mma_unit<RS, NT, NTILE>(P, X, c, O, g, tg, acc);
+      return;
+    }
+    mma_unit_dispatch<RS, NTILE, NT + 1>(ntn, P, X, c, O, g, tg, acc);
+  } else {
+    mma_unit<RS, NTILE, NTILE>(P, X, c, O, g, tg, acc);
+  }
+}
+
+template <int R, int RS, int NTILE>
 __global__ void __launch_bounds__(kWarpCTA * 32, 5)
     mma_stream_kernel(const GemvTask* __restrict__ tasks, const int* __restrict__ warp_begin,
                       const GemvUnit* __restrict__ units, const float* __restrict__ arena, float* xz, GemvStatus* err) {
-  constexpr int NT = (R + 7) / 8;  // 8-column tiles of the right-hand sides
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, tg = lane & 3;
@@ -651,7 +710,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 5)
     unsigned char* st = wbase + (size_t)s * warp_stage_bytes(4);
     mbar_expect_tx(&bars[s], pbytes + xbytes);
     bulk_g2s(st, arena + U.poff, pbytes, &bars[s]);
-    bulk_g2s(st + U.o0, xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
+    issue_x<float, RS>(st + U.o0, xz, U, &bars[s]);
   };
   auto issue_next = [&](int v) {
     issue(v, nxt);
@@ -669,14 +728,12 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 5)
     const GemvTask task = task_next;
     if (t + 1 < t1) task_next = tasks[t + 1];
     const int O = task.O;
-    const int mtn = (O + 15) >> 4;  // row tiles holding rows of this task (warp-uniform)
-    float acc[MT][NT][4];
+    const int ntn = (O + 7) >> 3;  // 8-row tiles holding rows of this task (warp-uniform)
+    float acc[NTILE][4];
 #pragma unroll
-    for (int mt = 0; mt < MT; ++mt)
+    for (int i = 0; i < NTILE; ++i)
 #pragma unroll
-      for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) acc[mt][nt][e] = 0.f;
+      for (int e = 0; e < 4; ++e) acc[i][e] = 0.f;
 
     for (int kk = 0; kk < task.nunits; ++kk, ++u) {
       const int s = (u - u_begin) % kWarpStages;
@@ -688,29 +745,25 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 5)
       const int c = uslot[s].c;
       const float* P = reinterpret_cast<const float*>(wbase + (size_t)s * warp_stage_bytes(4));
       const float* X = reinterpret_cast<const float*>(wbase + (size_t)s * warp_stage_bytes(4) + uslot[s].o0);
-      int k0 = 0;
-      // two steps per iteration: their MMA chains are independent and overlap
-#pragma unroll 2
-      for (; k0 + 8 <= c; k0 += 8) mma_kstep<R, RS, MT, NT, false>(P, X, k0, c, O, g, tg, mtn, acc);
-      if (k0 < c) mma_kstep<R, RS, MT, NT, true>(P, X, k0, c, O, g, tg, mtn, acc);
+      mma_unit_dispatch<RS, NTILE>(ntn, P, X, c, O, g, tg, acc);
       __syncwarp();  // every lane is done with stage s
       if (lane == 0 && u + kWarpStages < u_end) issue_next(u + kWarpStages);
     }
 
-    // ---- epilogue: rows mt * 16 + g (+ 8), columns nt * 8 + 2 t (+ 1); columns past R
+    // ---- epilogue: accumulator (rhs g (+8), rows 8 i + 2 t (+1)); right-hand sides past R
     // hold exact zeros (their X columns were zeros), which pads the row to RS ----
     float* out = xz + (size_t)task.out_row * RS;
 #pragma unroll
-    for (int mt = 0; mt < MT; ++mt) {
-      if (mt < mtn) {
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt) {
-          const int n = nt * 8 + 2 * tg;
-          const int m0 = mt * 16 + g, m1 = m0 + 8;
-          if (n < RS) {
-            if (m0 < O) *reinterpret_cast<float2*>(out + (size_t)m0 * RS + n) = make_float2(acc[mt][nt][0], acc[mt][nt][1]);
-            if (m1 < O) *reinterpret_cast<float2*>(out + (size_t)m1 * RS + n) = make_float2(acc[mt][nt][2], acc[mt][nt][3]);
-          }
+    for (int i = 0; i < NTILE; ++i) {
+      if (i < ntn) {
+        const int r0 = i * 8 + 2 * tg, r1 = r0 + 1;
+        if (g < RS) {
+          if (r0 < O) out[(size_t)r0 * RS + g] = acc[i][0];
+          if (r1 < O) out[(size_t)r1 * RS + g] = acc[i][1];
+        }
+        if (g + 8 < RS) {
+          if (r0 < O) out[(size_t)r0 * RS + g + 8] = acc[i][2];
+          if (r1 < O) out[(size_t)r1 * RS + g + 8] = acc[i][3];
         }
       }
     }
@@ -828,7 +881,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     unsigned char* st = ring + (size_t)s * kTcStage;
     mbar_expect_tx(&full[s], pbytes + xbytes);
     bulk_g2s(st, arena + U.poff, pbytes, &full[s]);
-    bulk_g2s(st + kTcPieceBytes, xz + (size_t)U.xrow * RS, xbytes, &full[s]);
+    issue_x<float, RS>(st + kTcPieceBytes, xz, U, &full[s]);
   };
   if (tid == 0)
     for (int v = u_begin; v < u_end && v < u_begin + kTcStages; ++v) issue(v);
@@ -1030,10 +1083,10 @@ void launch_warp_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T
   kern<<<L.ncta, kWarpCTA * 32, smem, s>>>(L.tasks, L.cta_begin, units, arena, xz, err);
 }
 
-template <int R, int RS, int MT>
+template <int R, int RS, int NTILE>
 void launch_mma_t(const GemvLaunch& L, const GemvUnit* units, const float* arena, float* xz, GemvStatus* err,
                   cudaStream_t s) {
-  auto kern = mma_stream_kernel<R, RS, MT>;
+  auto kern = mma_stream_kernel<R, RS, NTILE>;
   const size_t smem = warp_stream_smem_bytes((int)sizeof(float));
   static bool attr = false;
   if (!attr) {
@@ -1055,13 +1108,15 @@ void launch_stream(const GemvLaunch& L, const GemvUnit* units, const T* arena, T
   }
   if (L.warp_level) {
     if constexpr (std::is_same<T, float>::value) {
-      if (L.map == 3) {
+      if (L.map == 3) {  // rpt = 8-row tiles per task
         if (L.rpt <= 2)
           launch_mma_t<R, RS, 2>(L, units, arena, xz, err, s);
         else if (L.rpt <= 4)
           launch_mma_t<R, RS, 4>(L, units, arena, xz, err, s);
-        else
+        else if (L.rpt <= 8)
           launch_mma_t<R, RS, 8>(L, units, arena, xz, err, s);
+        else
+          launch_mma_t<R, RS, 16>(L, units, arena, xz, err, s);
         return;
       }
     }
@@ -1089,13 +1144,12 @@ void run_tile(const GemvPlan& p, int nrhs, int q0, T alpha, T beta, const T* x, 
   constexpr int RS = rs_of<T>(R);
   const GemvSide& side = p.side[TRANSP ? 1 : 0];
   const int n_in = TRANSP ? p.n_rows : p.n_cols;
-  const int* perm_in = TRANSP ? p.perm_rows : p.perm_cols;
+  const int* iperm_in = TRANSP ? p.iperm_rows : p.iperm_cols;
   const int* perm_out = TRANSP ? p.perm_cols : p.perm_rows;
   const int ld_in = n_in, ld_out = TRANSP ? p.n_cols : p.n_rows;
   const T* arena = (const T*)p.arena;
   if (tm) cudaEventRecord(tm->ev[0], s);
-  const long long tot = (long long)n_in * RS;
-  gather_kernel<T, R, RS><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(x, n_in, ld_in, q0, nrhs, perm_in, xz);
+  gather_kernel<T, R, RS><<<gather_grid(n_in), 256, 0, s>>>(x, n_in, ld_in, q0, nrhs, iperm_in, xz, p.n_in_max);
   if (tm) cudaEventRecord(tm->ev[1], s);
   for (int c = 0; c < side.nz; ++c)
     launch_stream<T, R, RS, TRANSP>(side.z[c], side.units, arena, xz, conj, nullptr, nullptr, 0, 0, 0, alpha, beta,
@@ -1193,18 +1247,16 @@ void grads_tile(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* r
   constexpr int RS = rs_of<T>(R);
   const T* arena = (const T*)p.arena;
   // x in cluster order (columns) and z = B^T x
-  long long tot = (long long)p.n_cols * RS;
-  gather_kernel<T, R, RS><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(x, p.n_cols, p.n_cols, 0, nrhs, p.perm_cols,
-                                                                         xz);
+  gather_kernel<T, R, RS><<<gather_grid(p.n_cols), 256, 0, s>>>(x, p.n_cols, p.n_cols, 0, nrhs, p.iperm_cols, xz,
+                                                                   p.n_in_max);
   const GemvSide& sn = p.side[0];
   for (int c = 0; c < sn.nz; ++c)
     launch_stream<T, R, RS, false>(sn.z[c], sn.units, arena, xz, 0, nullptr, nullptr, 0, 0, 0, one<T>(), zero<T>(),
                                    err, s);
   if (sn.nzred > 0) zred_kernel<T, RS><<<sn.nzred, 128, 0, s>>>(sn.zred, xz);
   // r in cluster order (rows) and w = A^T r
-  tot = (long long)p.n_rows * RS;
-  gather_kernel<T, R, RS><<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(r, p.n_rows, p.n_rows, 0, nrhs, p.perm_rows,
-                                                                         rz);
+  gather_kernel<T, R, RS><<<gather_grid(p.n_rows), 256, 0, s>>>(r, p.n_rows, p.n_rows, 0, nrhs, p.iperm_rows, rz,
+                                                                   p.n_in_max);
   const GemvSide& st = p.side[1];
   for (int c = 0; c < st.nz; ++c)
     launch_stream<T, R, RS, true>(st.z[c], st.units, arena, rz, 0, nullptr, nullptr, 0, 0, 0, one<T>(), zero<T>(),

@@ -18,15 +18,22 @@
 
 namespace hmatb200 {
 
+// X rows of a unit come from at most kUnitRuns runs of consecutive xz rows (the columns of a
+// block's matrix belong to several leaves, whose x or z rows are not adjacent).
+constexpr int kUnitRuns = 4;
+
 struct GemvUnit {
   long long poff;  // element offset of the piece P in the arena (16-byte aligned)
-  int xrow;        // first row of the X piece in the xz buffer
+  int xrow;        // first row of the X piece in the xz buffer (nruns == 0)
   int c;           // inner extent (rows of X)
   int o0, ow;      // transposed units: output rows [o0, o0 + ow) this piece covers;
                    // other units: o0 = byte offset of the X rows in a warp-level pipeline
                    // stage (the piece's capacity; the FP32 tensor-core kernel reads it per unit)
   int pel;         // elements of the piece P (O x c, or c x ow when transposed)
   int shift;       // elements between the 16-byte aligned copy start and the piece
+  int nruns;       // 0: X rows xrow .. xrow + c - 1; else X rows from the runs below, in order
+  int run_row[kUnitRuns];
+  unsigned short run_len[kUnitRuns];
 };
 
 struct GemvTask {
@@ -57,6 +64,13 @@ struct GemvLaunch {
   // like the warp-level launches.
   int map = 0;
 };
+
+// The arena's y region: per output block, the row panels of every leaf covering it side by side
+// (full leaves n columns, Rk leaves their A panel of k columns) as one column-major matrix
+// whose width is a multiple of kYColAlign (zero columns at the end, their X rows the zero rows
+// of the xz buffer, kZeroRows of them after the x part).
+constexpr int kYColAlign = 8;
+constexpr int kZeroRows = 8;
 
 // Unit capacities of the tensor-memory kernel: columns, piece bytes (128 rows x kTcCols),
 // X rows bytes (kTcCols rows of 16 floats).
@@ -122,10 +136,12 @@ struct GemvTiming {
 
 struct GemvPlan {
   int n_rows = 0, n_cols = 0;
-  int n_in_max = 0;      // rows of the x part of the xz buffer
-  long long xz_rows = 0; // total rows of the xz buffer (x part + z slots + partial slots)
+  int n_in_max = 0;      // rows of the x part of the xz buffer (kZeroRows zero rows follow it)
+  long long xz_rows = 0; // total rows of the xz buffer (x part, zero rows, z slots, partial slots)
   const int* perm_rows = nullptr;  // internal -> client
   const int* perm_cols = nullptr;
+  const int* iperm_rows = nullptr;  // client -> internal
+  const int* iperm_cols = nullptr;
   const void* arena = nullptr;
   int nfull = 0, nrk = 0;
   const GemvFullLeaf* full = nullptr;

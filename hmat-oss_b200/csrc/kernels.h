@@ -34,6 +34,13 @@ struct FullLeafDesc {
   int panel_first, npanel;
 };
 
+// One contiguous copy of a segmented relayout (elements).
+struct CopySeg {
+  long long src, dst, count;
+};
+template <typename T>
+void launch_copy_segments(const CopySeg* segs, int nseg, const T* src, T* dst, cudaStream_t s);
+
 // Where the truncated factors of an Rk leaf go: A as row panels, B transposed (k x n).
 struct RkStoreDesc {
   int panel_first, npanel;

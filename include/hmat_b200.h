@@ -412,6 +412,27 @@ int hmat_b200_gemv_status(hmat_matrix_t* hmatrix, void* stream, int* failed);
 int hmat_b200_gemv_device_noalloc(hmat_matrix_t* hmatrix, char trans, const void* alpha, const void* x_dev,
                                   const void* beta, void* y_dev, int nrhs, void* stream);
 
+/* Batches of independent H-matrices (no counterpart in the reference, whose
+ * assemble_generic and gemv take one matrix, c_wrapping.hpp:57-96 and 233-252).
+ * hmat_b200_batch_create combines `count` matrices made by create_empty_hmatrix_admissibility
+ * (each on one cluster tree for rows and columns, one value type and one low-rank epsilon; they
+ * are not assembled and stay owned by the caller) into one block-diagonal matrix: their
+ * cluster trees side by side, member i's rows and columns numbered from row_base[i], its leaves
+ * from leaf_base[i] (hmat_b200_batch_offsets, count + 1 entries each).  The batch is an
+ * ordinary matrix for every other entry point (gemv, hmat_b200_gemv_device, the leaf table and
+ * payloads, get_info, destroy through the table), so all members are assembled and multiplied
+ * by one launch per phase; vectors are the members' vectors stacked (column-major, N_total x
+ * nrhs).  Each member's leaves and ranks are those of its own assembly.  It owns the combined
+ * cluster tree; NULL on error.
+ * hmat_b200_batch_assemble assembles every member with its own descriptor from
+ * hmat_b200_create_assembly (assemblies[i] on member i's points; one kernel kind and nugget,
+ * each member its own correlation length, regularisation or wavenumber) and one compression
+ * algorithm (ACA+ or partial ACA). */
+hmat_matrix_t* hmat_b200_batch_create(hmat_matrix_t* const* matrices, int count);
+int hmat_b200_batch_offsets(hmat_matrix_t* batch, int* row_base, int* leaf_base);
+int hmat_b200_batch_assemble(hmat_matrix_t* batch, void* const* assemblies,
+                             const hmat_compression_algorithm_t* compression);
+
 /* Leaf table: `n` leaves in the reference's depth-first order, 6 ints each: row offset,
  * rows, col offset, cols (cluster numbering), type (0 full, 1 rk), rank (-1 for full). */
 int hmat_b200_leaf_count(hmat_matrix_t* hmatrix);

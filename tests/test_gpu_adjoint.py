@@ -42,6 +42,7 @@ class HGemv:
                 nrhs = x.shape[0]
                 y = torch.empty_like(x)
                 stream = torch.cuda.current_stream().cuda_stream
+                assert stream != 0, "run under a torch stream of its own (handle 0 is the matrix's own stream)"
                 h.gemv_device(x.data_ptr(), y.data_ptr(), nrhs, trans="N", stream=stream)
                 ctx.h = h
                 ctx.save_for_backward(x)
@@ -79,14 +80,19 @@ def _theta(h):
 
 
 def _loss_and_grads(torch, h, x, b):
+    # A stream of its own: torch's default stream has the handle 0, which the engine's device
+    # entry points read as "the matrix's own stream" (unordered with torch's work).
     F = HGemv.make(torch)
-    theta = torch.from_numpy(_theta(h)).to("cuda").requires_grad_(True)
-    xt = torch.from_numpy(np.ascontiguousarray(x.T)).to("cuda", theta.dtype).requires_grad_(True)
-    bt = torch.from_numpy(np.ascontiguousarray(b.T)).to("cuda", torch.float64)
-    y = F.apply(xt, theta, h)
-    L = 0.5 * ((y.double() - bt) ** 2).sum()  # the residual in FP64, handed back in the engine's type
-    L.backward()
-    return float(L), xt.grad.T.cpu().numpy().astype(np.float64), theta.grad.cpu().numpy().astype(np.float64)
+    with torch.cuda.stream(torch.cuda.Stream()):
+        theta = torch.from_numpy(_theta(h)).to("cuda").requires_grad_(True)
+        xt = torch.from_numpy(np.ascontiguousarray(x.T)).to("cuda", theta.dtype).requires_grad_(True)
+        bt = torch.from_numpy(np.ascontiguousarray(b.T)).to("cuda", torch.float64)
+        y = F.apply(xt, theta, h)
+        L = 0.5 * ((y.double() - bt) ** 2).sum()  # the residual in FP64, handed back in the engine's type
+        L.backward()
+        torch.cuda.current_stream().synchronize()
+        return (float(L.detach()), xt.grad.T.cpu().numpy().astype(np.float64),
+                theta.grad.cpu().numpy().astype(np.float64))
 
 
 def _loss(hb, h, x, b):
