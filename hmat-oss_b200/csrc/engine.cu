@@ -1465,18 +1465,23 @@ class Engine : public EngineBase {
     return wide;
   }
 
-  // FP32 tensor-core units: the widest multiple of 8 columns whose piece (O x c) and X rows
-  // (c rows of 16 floats) fit one pipeline stage, the X rows right after the piece (16-byte
-  // aligned); *xoff is their offset in the stage.
+  // Tensor-core units (FP32, FP64): the widest multiple of the kernel's column step (8 for the
+  // TF32 MMA, 4 for the FP64 one) whose piece (O x c) and X rows (c rows of 16 scalars) fit
+  // one pipeline stage, the X rows right after the piece (16-byte aligned); *xoff is their
+  // offset in the stage.
   static int mma_unit_cols(int O, int* xoff) {
-    const int stage = warp_piece_bytes(4) + kWarpXBytes;
-    auto need = [&](int c) { return (((long long)O * c * 4 + 15) / 16) * 16 + (long long)c * 64; };
-    int c = 8;
-    while (need(c + 8) <= stage) c += 8;
+    const int s = (int)sizeof(T);
+    const int stage = warp_piece_bytes(s) + kWarpXBytes;
+    const int xrow = gemv_rhs_stride(s, 16) * s;
+    const int step = s == 4 ? 8 : 4;
+    auto need = [&](int c) { return (((long long)O * c * s + 15) / 16) * 16 + (long long)c * xrow; };
+    int c = step;
+    while (need(c + step) <= stage) c += step;
     if (need(c) > stage) throw Error("gemv plan: output too tall for a tensor-core unit");
-    *xoff = (int)(((long long)O * c * 4 + 15) / 16 * 16);
+    *xoff = (int)(((long long)O * c * s + 15) / 16 * 16);
     return c;
   }
+  static constexpr bool kTensorN = std::is_same<T, float>::value || std::is_same<T, double>::value;
 
   // Units of out(O rows) += P X for a column-major O x C block at `poff`, X rows from `xrow`,
   // `cols` columns per unit.
@@ -1522,7 +1527,10 @@ class Engine : public EngineBase {
                                      : stream_smem_bytes((int)sizeof(T), Rmax, RS16, omax, transposed);
     // warp-level kernels: 228 KB of shared memory an SM, 1 KB reserved a CTA (their launch
     // bounds guarantee the registers for that many CTAs)
-    int per_sm = (int)std::min<size_t>(8, ((warp_level ? 228 : 226) * 1024) / (smem + 1024));
+    // (shared memory is allocated in 128-byte granules)
+    const size_t alloc = (smem + 127) / 128 * 128;
+    int per_sm = (int)std::min<size_t>(8, ((warp_level ? 228 : 226) * 1024) / (alloc + 1024));
+    if (map == 3) per_sm = std::min(per_sm, mma_stream_blocks_per_sm(omax / 8, (int)sizeof(T)));  // registers
     per_sm = std::max(per_sm, 1);
     return persistent_grid(per_sm);
   }
@@ -1564,10 +1572,12 @@ class Engine : public EngineBase {
   static void warp_shape(GemvLaunch& L, int omax) {
     L.warp_level = true;
     L.ol = 32;
-    if (std::is_same<T, float>::value) {
-      // FP32: tensor-core tiles of 8 output rows (map 3, rpt = row tiles held per warp)
+    if (std::is_same<T, float>::value || std::is_same<T, double>::value) {
+      // FP32 and FP64: tensor-core tiles of 8 output rows (map 3, rpt = row tiles held per warp:
+      // exactly those of the tallest task up to 8, else 16)
       L.map = 3;
-      L.rpt = omax <= 16 ? 2 : (omax <= 32 ? 4 : (omax <= 64 ? 8 : 16));
+      const int tiles = (omax + 7) / 8;
+      L.rpt = tiles <= 8 ? tiles : 16;
       return;
     }
     L.map = omax <= 32 ? 2 : (omax <= 64 ? 1 : 0);
@@ -1671,7 +1681,7 @@ class Engine : public EngineBase {
       if (!trans) {
         // z = B^T x_J: B^T is k x n column-major
         int xoff = 0;
-        const int zc = std::is_same<T, float>::value ? mma_unit_cols(k.k, &xoff) : warp_unit_cols_wide(k.k, &xoff);
+        const int zc = kTensorN ? mma_unit_cols(k.k, &xoff) : warp_unit_cols_wide(k.k, &xoff);
         px_units(lu, layout_.bt[leaf], k.k, k.n, k.col_off, zc, xoff);
       } else {
         // z' = A^T x_I: each A panel (len x k) is a transposed piece
@@ -1748,7 +1758,7 @@ class Engine : public EngineBase {
         int xoff = warp_piece_bytes((int)sizeof(T)), cols;
         if (tc_y)
           cols = kTcCols;
-        else if (std::is_same<T, float>::value)
+        else if (kTensorN)
           cols = mma_unit_cols(O, &xoff);
         else
           cols = warp_unit_cols(O);
@@ -1794,7 +1804,7 @@ class Engine : public EngineBase {
       if (tc_y) probe.map = 4;
       else warp_shape(probe, maxlen);
       const int wpc = probe.map == 4 ? 1 : warp_stream_warps_per_cta();
-      const int G = launch_ctas(maxlen, false, probe.map != 4, probe.map) * wpc;
+      const int G = launch_ctas(probe.map == 3 ? 8 * probe.rpt : maxlen, false, probe.map != 4, probe.map) * wpc;
       const int nyu = (int)units.size() - first_y;
       std::vector<double> cum(nyu + 1, 0.0);
       for (int v = 0; v < nyu; ++v) {
@@ -1878,7 +1888,11 @@ class Engine : public EngineBase {
       class_shape(c, ol, rpt);
       GemvLaunch& L = side.z[side.nz];
       L = GemvLaunch();
-      if (!trans) warp_shape(L, kClassMax[c]);
+      if (!trans) {
+        int om = 1;  // the class's tallest task (FP32 launches hold exactly its tiles)
+        for (const GemvTask& t : zt[c]) om = std::max(om, t.O);
+        warp_shape(L, kTensorN ? om : kClassMax[c]);
+      }
       finish_launch(L, sb, side.nz, zt[c], units, ol, rpt, trans, false);
       side.nz++;
     }

@@ -160,10 +160,13 @@ __device__ inline void issue_x(unsigned char* dst, const T* xz, const GemvUnit& 
     return;
   }
   uint32_t off = 0;
-  for (int r = 0; r < U.nruns; ++r) {
-    const uint32_t b = (uint32_t)U.run_len[r] * RS * (uint32_t)sizeof(T);
-    bulk_g2s(dst + off, xz + (size_t)U.run_row[r] * RS, b, bar);
-    off += b;
+#pragma unroll
+  for (int r = 0; r < kUnitRuns; ++r) {  // constant indices: the descriptor stays in registers
+    if (r < U.nruns) {
+      const uint32_t b = (uint32_t)U.run_len[r] * RS * (uint32_t)sizeof(T);
+      bulk_g2s(dst + off, xz + (size_t)U.run_row[r] * RS, b, bar);
+      off += b;
+    }
   }
 }
 
@@ -424,10 +427,11 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char* wbase = smem_raw + (size_t)warp * kWarpStages * warp_stage_bytes((int)sizeof(T));
-  GemvUnit* uslot =
-      reinterpret_cast<GemvUnit*>(smem_raw + (size_t)kWarpCTA * kWarpStages * warp_stage_bytes((int)sizeof(T))) + warp * kWarpStages;
+  // per stage: the unit's column count and X offset (what the consumers read), then the barriers
+  int2* uslot =
+      reinterpret_cast<int2*>(smem_raw + (size_t)kWarpCTA * kWarpStages * warp_stage_bytes((int)sizeof(T))) + warp * kWarpStages;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWarpCTA * kWarpStages *
-                                                               (warp_stage_bytes((int)sizeof(T)) + sizeof(GemvUnit))) +
+                                                               (warp_stage_bytes((int)sizeof(T)) + sizeof(int2))) +
                    warp * kWarpStages;
   const int gw = blockIdx.x * kWarpCTA + warp;
   const int t0 = warp_begin[gw], t1 = warp_begin[gw + 1];
@@ -448,7 +452,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
   auto issue = [&](int u, const GemvUnit& U) {
     const int s = (u - u_begin) % kWarpStages;
     last_issued = u;
-    uslot[s] = U;
+    uslot[s] = make_int2(U.c, U.o0);
     const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(T));
     const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(T);
     unsigned char* st = wbase + (size_t)s * warp_stage_bytes((int)sizeof(T));
@@ -506,7 +510,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
         if (lane == 0) warp_give_up(err, bars, kWarpStages, u_begin, u, last_issued);
         return;
       }
-      const int c = uslot[s].c;
+      const int c = uslot[s].x;
       const T* P = reinterpret_cast<const T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)));
       const T* X = reinterpret_cast<const T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)) + warp_piece_bytes((int)sizeof(T)));
       // Rows of a lane past O read the next column (or, in the last column, the first
@@ -642,6 +646,32 @@ __device__ __forceinline__ void mma_kstep(const float* P, const float* X, int k0
   }
 }
 
+// FP64 products on the FP64 tensor cores (mma.sync m8n8k4, FP64 operands and sums): one
+// 4-column step k0 computes D (8 right-hand sides x 8 rows) += X^T (8 x 4) P^T (4 x 8) for
+// each half of the right-hand sides and each 8-row tile; the sums accumulate in the MMA itself
+// (FP64 fused multiply-adds), in acc[t][2 h + i] = out[8 t + 2 tg + i][8 h + g], the layout of
+// the TF32 kernel's accumulators.
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+template <int RS, int NT, int NTILE, bool TAIL>
+__device__ __forceinline__ void dmma_kstep(const double* P, const double* X, int k0, int c, int O, int g, int tg,
+                                           double (&acc)[NTILE][4]) {
+  const int ka = k0 + tg;
+  const bool va = !TAIL || ka < c;
+  const double a0 = (va && g < RS) ? X[ka * RS + g] : 0.0;
+  const double a1 = (va && g + 8 < RS) ? X[ka * RS + g + 8] : 0.0;
+  const double* pa = P + ka * O + g;
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {
+    const double b = va ? pa[t * 8] : 0.0;
+    dmma(acc[t][0], acc[t][1], a0, b);
+    if constexpr (RS > 8) dmma(acc[t][2], acc[t][3], a1, b);
+  }
+}
+
 // All steps of one unit with NT output tiles.
 template <int RS, int NT, int NTILE>
 __device__ __forceinline__ void mma_unit(const float* P, const float* X, int c, int O, int g, int tg,
@@ -658,34 +688,50 @@ __device__ __forceinline__ void mma_unit(const float* P, const float* X, int c, 
   }
   if (k0 < c) mma_kstep<RS, NT, NTILE, true>(P, X, k0, c, O, g, tg, acc);
 }
+template <int RS, int NT, int NTILE>
+__device__ __forceinline__ void mma_unit(const double* P, const double* X, int c, int O, int g, int tg,
+                                         double (&acc)[NTILE][4]) {
+  int k0 = 0;
+#pragma unroll 2
+  for (; k0 + 4 <= c; k0 += 4) dmma_kstep<RS, NT, NTILE, false>(P, X, k0, c, O, g, tg, acc);
+  if (k0 < c) dmma_kstep<RS, NT, NTILE, true>(P, X, k0, c, O, g, tg, acc);
+}
 
 // The unit with the task's tile count (1 .. NTILE) as a compile-time constant.
-template <int RS, int NTILE, int NT = 1>
-__device__ __forceinline__ void mma_unit_dispatch(int ntn, const float* P, const float* X, int c, int O, int g,
-                                                  int tg, float (&acc)[NTILE][4]) {
+template <typename T, int RS, int NTILE, int NT = 1>
+__device__ __forceinline__ void mma_unit_dispatch(int ntn, const T* P, const T* X, int c, int O, int g, int tg,
+                                                  T (&acc)[NTILE][4]) {
   if constexpr (NT < NTILE) {
     if (ntn == NT) {
       mma_unit<RS, NT, NTILE>(P, X, c, O, g, tg, acc);
       return;
     }
-    mma_unit_dispatch<RS, NTILE, NT + 1>(ntn, P, X, c, O, g, tg, acc);
+    mma_unit_dispatch<T, RS, NTILE, NT + 1>(ntn, P, X, c, O, g, tg, acc);
   } else {
     mma_unit<RS, NTILE, NTILE>(P, X, c, O, g, tg, acc);
   }
 }
 
-template <int R, int RS, int NTILE>
-__global__ void __launch_bounds__(kWarpCTA * 32, 5)
+// CTAs an SM the tensor-core kernel is compiled for: five (20 warps) while its sums fit the
+// register share of five, four for the tallest tasks (6 tiles and more: 28+ accumulators).
+// FP64 (2 x 4 KB-piece stages a warp): four by shared memory.
+__host__ __device__ constexpr int mma_min_blocks(int ntile, int elem_bytes) {
+  return elem_bytes == 8 ? 4 : (ntile >= 6 ? 4 : 5);
+}
+
+template <typename T, int R, int RS, int NTILE>
+__global__ void __launch_bounds__(kWarpCTA * 32, mma_min_blocks(NTILE, sizeof(T)))
     mma_stream_kernel(const GemvTask* __restrict__ tasks, const int* __restrict__ warp_begin,
-                      const GemvUnit* __restrict__ units, const float* __restrict__ arena, float* xz, GemvStatus* err) {
+                      const GemvUnit* __restrict__ units, const T* __restrict__ arena, T* xz, GemvStatus* err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, tg = lane & 3;
-  unsigned char* wbase = smem_raw + (size_t)warp * kWarpStages * warp_stage_bytes(4);
-  GemvUnit* uslot =
-      reinterpret_cast<GemvUnit*>(smem_raw + (size_t)kWarpCTA * kWarpStages * warp_stage_bytes(4)) + warp * kWarpStages;
+  unsigned char* wbase = smem_raw + (size_t)warp * kWarpStages * warp_stage_bytes((int)sizeof(T));
+  // per stage: the unit's column count and X offset (what the consumers read), then the barriers
+  int2* uslot =
+      reinterpret_cast<int2*>(smem_raw + (size_t)kWarpCTA * kWarpStages * warp_stage_bytes((int)sizeof(T))) + warp * kWarpStages;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kWarpCTA * kWarpStages *
-                                                               (warp_stage_bytes(4) + sizeof(GemvUnit))) +
+                                                               (warp_stage_bytes((int)sizeof(T)) + sizeof(int2))) +
                    warp * kWarpStages;
   const int gw = blockIdx.x * kWarpCTA + warp;
   const int t0 = warp_begin[gw], t1 = warp_begin[gw + 1];
@@ -704,13 +750,13 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 5)
   auto issue = [&](int u, const GemvUnit& U) {
     const int s = (u - u_begin) % kWarpStages;
     last_issued = u;
-    uslot[s] = U;
-    const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(float));
-    const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(float);
-    unsigned char* st = wbase + (size_t)s * warp_stage_bytes(4);
+    uslot[s] = make_int2(U.c, U.o0);
+    const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(T));
+    const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(T);
+    unsigned char* st = wbase + (size_t)s * warp_stage_bytes((int)sizeof(T));
     mbar_expect_tx(&bars[s], pbytes + xbytes);
     bulk_g2s(st, arena + U.poff, pbytes, &bars[s]);
-    issue_x<float, RS>(st + U.o0, xz, U, &bars[s]);
+    issue_x<T, RS>(st + U.o0, xz, U, &bars[s]);
   };
   auto issue_next = [&](int v) {
     issue(v, nxt);
@@ -729,11 +775,11 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 5)
     if (t + 1 < t1) task_next = tasks[t + 1];
     const int O = task.O;
     const int ntn = (O + 7) >> 3;  // 8-row tiles holding rows of this task (warp-uniform)
-    float acc[NTILE][4];
+    T acc[NTILE][4];
 #pragma unroll
     for (int i = 0; i < NTILE; ++i)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) acc[i][e] = 0.f;
+      for (int e = 0; e < 4; ++e) acc[i][e] = zero<T>();
 
     for (int kk = 0; kk < task.nunits; ++kk, ++u) {
       const int s = (u - u_begin) % kWarpStages;
@@ -742,17 +788,17 @@ __global__ void __launch_bounds__(kWarpCTA * 32, 5)
         if (lane == 0) warp_give_up(err, bars, kWarpStages, u_begin, u, last_issued);
         return;
       }
-      const int c = uslot[s].c;
-      const float* P = reinterpret_cast<const float*>(wbase + (size_t)s * warp_stage_bytes(4));
-      const float* X = reinterpret_cast<const float*>(wbase + (size_t)s * warp_stage_bytes(4) + uslot[s].o0);
-      mma_unit_dispatch<RS, NTILE>(ntn, P, X, c, O, g, tg, acc);
+      const int c = uslot[s].x;
+      const T* P = reinterpret_cast<const T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)));
+      const T* X = reinterpret_cast<const T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)) + uslot[s].y);
+      mma_unit_dispatch<T, RS, NTILE>(ntn, P, X, c, O, g, tg, acc);
       __syncwarp();  // every lane is done with stage s
       if (lane == 0 && u + kWarpStages < u_end) issue_next(u + kWarpStages);
     }
 
     // ---- epilogue: accumulator (rhs g (+8), rows 8 i + 2 t (+1)); right-hand sides past R
     // hold exact zeros (their X columns were zeros), which pads the row to RS ----
-    float* out = xz + (size_t)task.out_row * RS;
+    T* out = xz + (size_t)task.out_row * RS;
 #pragma unroll
     for (int i = 0; i < NTILE; ++i) {
       if (i < ntn) {
@@ -1083,11 +1129,11 @@ void launch_warp_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T
   kern<<<L.ncta, kWarpCTA * 32, smem, s>>>(L.tasks, L.cta_begin, units, arena, xz, err);
 }
 
-template <int R, int RS, int NTILE>
-void launch_mma_t(const GemvLaunch& L, const GemvUnit* units, const float* arena, float* xz, GemvStatus* err,
+template <typename T, int R, int RS, int NTILE>
+void launch_mma_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, GemvStatus* err,
                   cudaStream_t s) {
-  auto kern = mma_stream_kernel<R, RS, NTILE>;
-  const size_t smem = warp_stream_smem_bytes((int)sizeof(float));
+  auto kern = mma_stream_kernel<T, R, RS, NTILE>;
+  const size_t smem = warp_stream_smem_bytes((int)sizeof(T));
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1107,16 +1153,19 @@ void launch_stream(const GemvLaunch& L, const GemvUnit* units, const T* arena, T
     }
   }
   if (L.warp_level) {
-    if constexpr (std::is_same<T, float>::value) {
-      if (L.map == 3) {  // rpt = 8-row tiles per task
-        if (L.rpt <= 2)
-          launch_mma_t<R, RS, 2>(L, units, arena, xz, err, s);
-        else if (L.rpt <= 4)
-          launch_mma_t<R, RS, 4>(L, units, arena, xz, err, s);
-        else if (L.rpt <= 8)
-          launch_mma_t<R, RS, 8>(L, units, arena, xz, err, s);
-        else
-          launch_mma_t<R, RS, 16>(L, units, arena, xz, err, s);
+    if constexpr (std::is_same<T, float>::value || std::is_same<T, double>::value) {
+      if (L.map == 3) {  // rpt = 8-row tiles of the launch's tallest task (exact up to 8)
+        switch (L.rpt) {
+          case 1: launch_mma_t<T, R, RS, 1>(L, units, arena, xz, err, s); break;
+          case 2: launch_mma_t<T, R, RS, 2>(L, units, arena, xz, err, s); break;
+          case 3: launch_mma_t<T, R, RS, 3>(L, units, arena, xz, err, s); break;
+          case 4: launch_mma_t<T, R, RS, 4>(L, units, arena, xz, err, s); break;
+          case 5: launch_mma_t<T, R, RS, 5>(L, units, arena, xz, err, s); break;
+          case 6: launch_mma_t<T, R, RS, 6>(L, units, arena, xz, err, s); break;
+          case 7: launch_mma_t<T, R, RS, 7>(L, units, arena, xz, err, s); break;
+          case 8: launch_mma_t<T, R, RS, 8>(L, units, arena, xz, err, s); break;
+          default: launch_mma_t<T, R, RS, 16>(L, units, arena, xz, err, s); break;
+        }
         return;
       }
     }
@@ -1280,9 +1329,10 @@ size_t stream_smem_bytes(int elem_bytes, int R, int RS, int omax, bool transpose
 int gemv_rhs_stride(int elem_bytes, int R) { return R * elem_bytes >= 16 ? R : 16 / elem_bytes; }
 
 size_t warp_stream_smem_bytes(int elem_bytes) {
-  return (size_t)kWarpCTA * kWarpStages * (warp_stage_bytes(elem_bytes) + sizeof(GemvUnit) + sizeof(uint64_t));
+  return (size_t)kWarpCTA * kWarpStages * (warp_stage_bytes(elem_bytes) + sizeof(int2) + sizeof(uint64_t));
 }
 int warp_stream_warps_per_cta() { return kWarpCTA; }
+int mma_stream_blocks_per_sm(int ntile, int elem_bytes) { return mma_min_blocks(ntile, elem_bytes); }
 
 size_t umma_smem_bytes() {
   return (size_t)kTcStages * kTcStage + 2 * kTcSteps * (kTcTileA + kTcTileB) + (kTcStages + 1) * 8 + 16 +

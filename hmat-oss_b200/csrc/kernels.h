@@ -176,6 +176,9 @@ size_t stream_smem_bytes(int elem_bytes, int R, int RS, int omax, bool transpose
 size_t warp_stream_smem_bytes(int elem_bytes);
 size_t umma_smem_bytes();
 int warp_stream_warps_per_cta();
+// Resident CTAs an SM of the tensor-core gemv kernel (FP32 or FP64) with `ntile` 8-row tiles
+// (its register budget).
+int mma_stream_blocks_per_sm(int ntile, int elem_bytes);
 
 // Leaf-factor gradients of y = H x for the output gradient r (real types; x, r device,
 // client numbering, nrhs <= 16): dF = r_I x_J^T, dA = r_I (B^T x_J)^T, dB = x_J (A^T r_I)^T,
