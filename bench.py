@@ -345,11 +345,11 @@ def supplementary(args):
         one = 1.0
 
         def backward(s):
-            # r = H x - b, dx = H^T r, leaf gradients
+            # r = H x - b, then dx = H^T r and the leaf gradients in one pass
             rd.copy_(bd)
             h.gemv_device(xd.data_ptr(), rd.data_ptr(), 1, alpha=one, beta=-1.0, stream=s.cuda_stream)
-            h.gemv_device(rd.data_ptr(), dx.data_ptr(), 1, trans="T", stream=s.cuda_stream)
-            h.leaf_gradients(xd.data_ptr(), rd.data_ptr(), 1, g.data_ptr(), accumulate=False, stream=s.cuda_stream)
+            h.gemv_adjoint(xd.data_ptr(), rd.data_ptr(), 1, dx.data_ptr(), g.data_ptr(), accumulate=False,
+                           stream=s.cuda_stream)
 
         with torch.cuda.stream(stream):
             ms = _time_device(backward, args.steps, args.warmup, stream)

@@ -143,7 +143,7 @@ EXPORTED = [
     "hmat_b200_batch_create", "hmat_b200_batch_offsets", "hmat_b200_batch_assemble",
     "hmat_b200_leaf_count",
     "hmat_b200_leaf_table", "hmat_b200_leaf_payload", "hmat_b200_payload_layout", "hmat_b200_leaf_gradients",
-    "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_gemv_launches", "hmat_b200_aca_shapes",
+    "hmat_b200_gemv_adjoint", "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_gemv_launches", "hmat_b200_aca_shapes",
     "hmat_b200_last_error",
     "hmat_b200_clear_last_error",
 ]
@@ -189,6 +189,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "hmat_b200_leaf_payload": (C.c_longlong, [_P, C.c_int, _P]),
         "hmat_b200_payload_layout": (C.c_int, [_P, _P, C.POINTER(C.c_longlong)]),
         "hmat_b200_leaf_gradients": (C.c_int, [_P, _P, _P, C.c_int, _P, C.c_int, _P]),
+        "hmat_b200_gemv_adjoint": (C.c_int, [_P, _P, _P, C.c_int, _P, _P, C.c_int, _P]),
         "hmat_b200_phase_times": (C.c_int, [_P, _P]),
         "hmat_b200_gemv_profile": (C.c_int, [_P, C.c_char, _P, _P, C.c_int, _P, _P]),
         "hmat_b200_gemv_launches": (C.c_int, [_P, C.c_char, C.c_int]),
@@ -341,12 +342,13 @@ class HMatrix:
         return self.lib.hmat_b200_gemv_device_noalloc(self.m, trans.encode(), a.ctypes.data, C.c_void_p(x_ptr),
                                                       b.ctypes.data, C.c_void_p(y_ptr), nrhs, C.c_void_p(stream))
 
-    def gemv_status(self, stream=0) -> bool:
-        """True if a device product of this matrix stopped since the last query because a
-        kernel's wait for a bulk copy gave up (hmat_b200_gemv_status; clears the flag)."""
+    def gemv_status(self, stream=0) -> int:
+        """Non-zero if a device product of this matrix failed since the last query
+        (hmat_b200_gemv_status; clears the flag): 1 a kernel's wait for a bulk copy gave up, 2 a
+        unit failed the kernels' checks of its copies.  0 when all went well."""
         failed = C.c_int(0)
         _check(self.lib.hmat_b200_gemv_status(self.m, C.c_void_p(stream), C.byref(failed)), "hmat_b200_gemv_status")
-        return bool(failed.value)
+        return int(failed.value)
 
     def info(self) -> dict:
         return self.hi.get_info(self.m).as_dict()
@@ -457,6 +459,12 @@ class HMatrix:
         _check(self.lib.hmat_b200_leaf_gradients(self.m, C.c_void_p(x_ptr), C.c_void_p(r_ptr), nrhs,
                                                  C.c_void_p(grad_ptr), int(accumulate), C.c_void_p(stream)),
                "hmat_b200_leaf_gradients")
+
+    def gemv_adjoint(self, x_ptr, r_ptr, nrhs, dx_ptr, grad_ptr, accumulate=False, stream=0):
+        """dx = H^T r and the leaf gradients in one pass (hmat_b200_gemv_adjoint)."""
+        _check(self.lib.hmat_b200_gemv_adjoint(self.m, C.c_void_p(x_ptr), C.c_void_p(r_ptr), nrhs, C.c_void_p(dx_ptr),
+                                               C.c_void_p(grad_ptr), int(accumulate), C.c_void_p(stream)),
+               "hmat_b200_gemv_adjoint")
 
     def gemv_profile(self, x_ptr: int, y_ptr: int, nrhs: int, trans: str = "N"):
         ms = np.zeros(3)

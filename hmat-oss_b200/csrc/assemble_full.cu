@@ -67,14 +67,18 @@ void launch_full_from_canonical(const FullLeafDesc* d_leaves, const long long* g
   full_from_canonical_kernel<T><<<grid, 256, 0, s>>>(d_leaves, goff, nleaves, panels, src, arena);
 }
 
-// Segmented copy between two device buffers (relayout of stored leaves): segment g copies
-// count elements from src + src_off to dst + dst_off.  A CTA per segment, threads over elements.
+// Segmented copy between two device buffers (relayout of stored leaves): segment g copies a
+// rows x cols column-major block.  A CTA per segment, threads over elements.
 template <typename T>
 __global__ void __launch_bounds__(256) copy_segments_kernel(const CopySeg* __restrict__ segs, int nseg,
                                                             const T* __restrict__ src, T* __restrict__ dst) {
   for (int g = blockIdx.x; g < nseg; g += gridDim.x) {
     const CopySeg c = segs[g];
-    for (long long e = threadIdx.x; e < c.count; e += blockDim.x) dst[c.dst + e] = src[c.src + e];
+    const long long count = (long long)c.rows * c.cols;
+    for (long long e = threadIdx.x; e < count; e += blockDim.x) {
+      const long long r = e % c.rows, q = e / c.rows;
+      dst[c.dst + r + q * c.dst_ld] = src[c.src + r + q * c.src_ld];
+    }
   }
 }
 

@@ -1198,6 +1198,15 @@ int hmat_b200_leaf_gradients(hmat_matrix_t* m, const void* x, const void* r, int
   return 0;
 }
 
+int hmat_b200_gemv_adjoint(hmat_matrix_t* m, const void* x, const void* r, int nrhs, void* dx, void* grad,
+                           int accumulate, void* stream) {
+  HB_TRY("hmat_b200_gemv_adjoint", {
+    if (!m || !x || !r || !dx || !grad) throw Error("null argument");
+    engine_of(m).gemv_adjoint(x, r, nrhs, dx, grad, accumulate != 0, (cudaStream_t)stream);
+  });
+  return 0;
+}
+
 int hmat_b200_gemv_profile(hmat_matrix_t* m, char trans, const void* x_dev, void* y_dev, int nrhs, double* ms3,
                            double* bytes3) {
   HB_TRY("hmat_b200_gemv_profile", {

@@ -339,7 +339,8 @@ class Engine : public EngineBase {
     }
     if (L.type == 0) return (long long)L.m * L.n;
     h.resize((size_t)k * L.n);
-    HB_CUDA(cudaMemcpy(h.data(), arena_.p + layout_.bt[leaf], h.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    HB_CUDA(cudaMemcpy2D(h.data(), (size_t)k * sizeof(T), arena_.p + layout_.bt[leaf],
+                         (size_t)layout_.bt_ld[leaf] * sizeof(T), (size_t)k * sizeof(T), L.n, cudaMemcpyDeviceToHost));
     T* Bo = o + (size_t)L.m * k;  // B^T (k x n) -> B (n x k)
     for (int j = 0; j < L.n; ++j)
       for (int l = 0; l < k; ++l) Bo[j + (size_t)l * L.n] = h[l + (size_t)j * k];
@@ -368,6 +369,20 @@ class Engine : public EngineBase {
     cudaStream_t s = user_stream ? user_stream : stream_;
     launch_leaf_gradients<T>(plan_, nrhs, (const T*)x, (const T*)r, xz_.p, rz_.p, (T*)grad, (T*)grad, accumulate,
                              err_.p, s);
+    HB_CUDA(cudaGetLastError());
+  }
+
+  void gemv_adjoint(const void* x, const void* r, int nrhs, void* dx, void* grad, bool accumulate,
+                    cudaStream_t user_stream) override {
+    if (!assembled) throw Error("matrix is not assembled");
+    if (Traits<T>::is_complex) throw Error("the adjoint is implemented for real value types");
+    if (nrhs < 1 || nrhs > 16) throw Error("the adjoint takes 1 to 16 right-hand sides");
+    check_device();
+    xz_.ensure(xz_elems());
+    rz_.ensure(xz_elems());
+    cudaStream_t s = user_stream ? user_stream : stream_;
+    launch_gemv_adjoint<T>(plan_, nrhs, (const T*)x, (const T*)r, (T*)dx, xz_.p, rz_.p, (T*)grad, (T*)grad, accumulate,
+                           err_.p, s);
     HB_CUDA(cudaGetLastError());
   }
 
@@ -498,7 +513,7 @@ class Engine : public EngineBase {
       auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
       for (int b = br.first; b < br.second; ++b)
         segs.push_back(CopySeg{old.panel[old.first[i] + (b - br.first)], layout_.panel[layout_.first[i] + (b - br.first)],
-                               (long long)rblocks_[b].len * L[i].n});
+                               rblocks_[b].len * L[i].n, 1, 0, 0});
     }
     DevArray<CopySeg> d_segs;
     d_segs.upload(segs, stream_);
@@ -580,9 +595,11 @@ class Engine : public EngineBase {
   int gemv_status(cudaStream_t user_stream) override {
     check_device();
     cudaStream_t s = user_stream ? user_stream : stream_;
-    HB_CUDA(cudaMemcpyAsync(&h_err_->failed, &err_.p->failed, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaMemcpyAsync(&h_err_->failed, &err_.p->failed, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     HB_CUDA(cudaStreamSynchronize(s));
     const int failed = h_err_->failed;
+    if (failed == 2)  // a unit that failed its copy checks (index in the second word)
+      fprintf(stderr, "gemv: unit %d of the schedule failed its copy checks and was skipped\n", h_err_->pad);
     if (failed) clear_status(s);
     return failed;
   }
@@ -624,7 +641,8 @@ class Engine : public EngineBase {
 
   void clear_status(cudaStream_t s) {
     h_err_->failed = 0;
-    HB_CUDA(cudaMemsetAsync(&err_.p->failed, 0, sizeof(int), s));
+    h_err_->pad = 0;
+    HB_CUDA(cudaMemsetAsync(&err_.p->failed, 0, 2 * sizeof(int), s));
     HB_CUDA(cudaStreamSynchronize(s));
   }
 
@@ -1302,13 +1320,24 @@ class Engine : public EngineBase {
   // O_b x w chunk.  Region BT: per Rk leaf of rank k > 0, B^T (k x n, column-major), 16-byte
   // aligned.  The 'N' product streams each block's matrix in one pass; every piece of it and
   // every B^T starts on a 16-byte boundary (the TMA rule).
+  // A group of Rk leaves with one column range: their B^T stacked as one column-major h x n
+  // matrix (leaf order, at most kZGroupRows rows unless one leaf has more), so that one pass
+  // over its columns computes the z = B^T x of all of them with the x rows read once.
+  struct ZGroup {
+    long long base;
+    int h, col_off, n;
+    std::vector<int> leaves;  // member leaves, rows in this order
+  };
+  static constexpr int kZGroupRows = 32;
   struct Layout {
     std::vector<int> first;         // per leaf: its first entry in `panel`, -1 without storage
     std::vector<long long> panel;   // per (leaf, block of its rows): offset of the leaf's panel
     std::vector<int> pcol;          // its first column in the block's matrix
     std::vector<long long> bt;      // per leaf: offset of B^T, -1 unless Rk with rank > 0
+    std::vector<int> bt_ld;         // per leaf: leading dimension of B^T (its group's height)
     std::vector<long long> yblock;  // per output block: offset of its matrix
     std::vector<int> ywidth;        // per output block: columns (a multiple of kYColAlign)
+    std::vector<ZGroup> zgroups;    // the B^T groups, in the region's order
     long long total = 0;
   };
 
@@ -1352,11 +1381,44 @@ class Engine : public EngineBase {
         y.panel[e] = y.yblock[b] + (long long)y.pcol[e] * rblocks_[b].len;
       }
     }
+    // Region BT: Rk leaves with the same column range (in order of first appearance) stacked
+    // in groups of at most kZGroupRows rows
     pos = pad32(pos);
+    y.bt_ld.assign(nleaves, 0);
+    std::map<std::pair<int, int>, int> by_cols;
+    std::vector<std::vector<int>> members;
     for (int i = 0; i < nleaves; ++i) {
       if (L[i].type != 1 || y.first[i] < 0) continue;
-      y.bt[i] = pos;
-      pos += padded((long long)ranks[i] * L[i].n);
+      auto key = std::make_pair(L[i].col_off, L[i].n);
+      auto it = by_cols.find(key);
+      if (it == by_cols.end()) {
+        it = by_cols.emplace(key, (int)members.size()).first;
+        members.emplace_back();
+      }
+      members[it->second].push_back(i);
+    }
+    for (const auto& mem : members) {
+      ZGroup g{0, 0, L[mem[0]].col_off, L[mem[0]].n, {}};
+      auto close = [&]() {
+        if (g.leaves.empty()) return;
+        g.base = pos;
+        int r = 0;
+        for (int i : g.leaves) {
+          y.bt[i] = pos + r;
+          y.bt_ld[i] = g.h;
+          r += ranks[i];
+        }
+        pos += padded((long long)g.h * g.n);
+        y.zgroups.push_back(g);
+        g.leaves.clear();
+        g.h = 0;
+      };
+      for (int i : mem) {
+        if (g.h > 0 && g.h + ranks[i] > kZGroupRows) close();
+        g.leaves.push_back(i);
+        g.h += ranks[i];
+      }
+      close();
     }
     y.total = pad32(pos);
     layout_ = std::move(y);
@@ -1384,7 +1446,7 @@ class Engine : public EngineBase {
   // Where Rk leaf i's factors live in the current layout: its A panels appended to `panels`.
   RkStoreDesc rk_store(int i, std::vector<PanelDesc>& panels) const {
     const LeafInfo& l = bt_->leaves[i];
-    RkStoreDesc st{(int)panels.size(), 0, layout_.bt[i]};
+    RkStoreDesc st{(int)panels.size(), 0, layout_.bt[i], layout_.first[i] < 0 ? 0 : layout_.bt_ld[i], 0};
     if (layout_.first[i] < 0) return st;
     auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
     for (int b = br.first; b < br.second; ++b) {
@@ -1406,11 +1468,12 @@ class Engine : public EngineBase {
       auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
       long long p = piece_loff_[i];
       for (int b = br.first; b < br.second; ++b) {
-        const long long len = (long long)rblocks_[b].len * k;
-        segs[piece_of_[i]].push_back(CopySeg{p, layout_.panel[layout_.first[i] + (b - br.first)], len});
+        const int len = rblocks_[b].len * k;
+        segs[piece_of_[i]].push_back(CopySeg{p, layout_.panel[layout_.first[i] + (b - br.first)], len, 1, 0, 0});
         p += padded(len);
       }
-      segs[piece_of_[i]].push_back(CopySeg{p, layout_.bt[i], (long long)k * L[i].n});
+      // B^T: k x n in the piece, rows of its group's matrix in the arena
+      segs[piece_of_[i]].push_back(CopySeg{p, layout_.bt[i], k, L[i].n, k, layout_.bt_ld[i]});
     }
     std::vector<DevArray<CopySeg>> d_segs(pieces_.size());
     for (size_t q = 0; q < pieces_.size(); ++q) {
@@ -1481,7 +1544,7 @@ class Engine : public EngineBase {
     *xoff = (int)(((long long)O * c * s + 15) / 16 * 16);
     return c;
   }
-  static constexpr bool kTensorN = std::is_same<T, float>::value || std::is_same<T, double>::value;
+  static constexpr bool kTensorN = std::is_same<T, float>::value;  // 'N' products on the TF32 tensor-core kernel
 
   // Units of out(O rows) += P X for a column-major O x C block at `poff`, X rows from `xrow`,
   // `cols` columns per unit.
@@ -1572,9 +1635,9 @@ class Engine : public EngineBase {
   static void warp_shape(GemvLaunch& L, int omax) {
     L.warp_level = true;
     L.ol = 32;
-    if (std::is_same<T, float>::value || std::is_same<T, double>::value) {
-      // FP32 and FP64: tensor-core tiles of 8 output rows (map 3, rpt = row tiles held per warp:
-      // exactly those of the tallest task up to 8, else 16)
+    if (std::is_same<T, float>::value) {
+      // FP32: tensor-core tiles of 8 output rows (map 3, rpt = row tiles held per warp: exactly
+      // those of the tallest task up to 8, else 16)
       L.map = 3;
       const int tiles = (omax + 7) / 8;
       L.rpt = tiles <= 8 ? tiles : 16;
@@ -1669,46 +1732,56 @@ class Engine : public EngineBase {
     // FP32 'N' y-phase on the tensor-memory kernel when HMAT_B200_TC_Y=1
     const bool tc_y = !trans && std::is_same<T, float>::value && tc_y_enabled();
 
-    // ---- z-phase: one task per Rk leaf (or chunk), one launch per rank class ----
+    // ---- z-phase: 'N' one task per B^T group (z = B^T x_J of its leaves at once, the x rows
+    // read once), 'T' one per Rk leaf (z' = A^T x_I over its A panels); long ones cut into
+    // chunks; one launch per height class ----
     std::vector<GemvTask> zt[4];
     std::vector<GemvUnit> zunits[4];
     std::vector<GemvZred> zred;
     std::vector<GemvUnit> lu;
-    for (size_t t = 0; t < K.size(); ++t) {
-      const GemvRkLeaf& k = K[t];
-      const int leaf = rk_leaf[t];
+    const auto& G = layout_.zgroups;
+    const size_t nz = trans ? K.size() : G.size();
+    for (size_t t = 0; t < nz; ++t) {
       lu.clear();
+      int O, zrow;
       if (!trans) {
-        // z = B^T x_J: B^T is k x n column-major
+        // the group's stacked B^T: h x n column-major
+        const ZGroup& g = G[t];
         int xoff = 0;
-        const int zc = kTensorN ? mma_unit_cols(k.k, &xoff) : warp_unit_cols_wide(k.k, &xoff);
-        px_units(lu, layout_.bt[leaf], k.k, k.n, k.col_off, zc, xoff);
+        const int zc = kTensorN ? mma_unit_cols(g.h, &xoff) : warp_unit_cols_wide(g.h, &xoff);
+        px_units(lu, g.base, g.h, g.n, g.col_off, zc, xoff);
+        O = g.h;
+        zrow = zgroup_row_[0][t];
       } else {
+        const GemvRkLeaf& k = K[t];
+        const int leaf = rk_leaf[t];
         // z' = A^T x_I: each A panel (len x k) is a transposed piece
         auto br = block_range(rblocks_, rstarts_, k.row_off, k.m);
         for (int b = br.first; b < br.second; ++b)
           ptx_units(lu, layout_.panel[layout_.first[leaf] + (b - br.first)], rblocks_[b].len, k.k, 0,
                     rblocks_[b].off);
+        O = k.k;
+        zrow = k.zrow_t;
       }
-      if (k.k > 128) throw Error("gemv plan: ranks above 128 are not supported by the streamed kernels");
-      // 'N' launches take every rank up to 32 in one column-slice window launch
-      const int cls = trans ? rank_class(k.k) : std::max(1, rank_class(k.k));
-      const int zrow = trans ? k.zrow_t : k.zrow_n;
+      if (O > 128) throw Error("gemv plan: ranks above 128 are not supported by the streamed kernels");
+      // 'N' launches take every height up to 32 in one launch; the tensor-core kernel takes every
+      // height up to 64 in one (its tile count is a per-task constant), so one wave covers them
+      const int cls = trans ? rank_class(O) : (kTensorN && O <= 64 ? 2 : std::max(1, rank_class(O)));
       // units of one launch must be contiguous in task order: collect them per class
       std::vector<GemvUnit>& cu = zunits[cls];
       if ((int)lu.size() <= kMaxUnits) {
-        zt[cls].push_back(GemvTask{k.k, (int)cu.size(), (int)lu.size(), zrow});
+        zt[cls].push_back(GemvTask{O, (int)cu.size(), (int)lu.size(), zrow});
         cu.insert(cu.end(), lu.begin(), lu.end());
       } else {
         const int nparts = ((int)lu.size() + kMaxUnits - 1) / kMaxUnits;
         const int part_row = (int)next_row;
-        next_row += (long long)nparts * k.k;
+        next_row += (long long)nparts * O;
         for (int pidx = 0; pidx < nparts; ++pidx) {
           const int u0 = pidx * kMaxUnits, u1 = std::min((int)lu.size(), u0 + kMaxUnits);
-          zt[cls].push_back(GemvTask{k.k, (int)cu.size(), u1 - u0, part_row + pidx * k.k});
+          zt[cls].push_back(GemvTask{O, (int)cu.size(), u1 - u0, part_row + pidx * O});
           cu.insert(cu.end(), lu.begin() + u0, lu.begin() + u1);
         }
-        zred.push_back(GemvZred{zrow, k.k, part_row, nparts});
+        zred.push_back(GemvZred{zrow, O, part_row, nparts});
       }
     }
     for (int c = 0; c < 4; ++c) {
@@ -1848,25 +1921,31 @@ class Engine : public EngineBase {
     } else {
       // each output block is cut into chunks of at most kYChunkUnits units whose partial rows go
       // to xz; a final pass sums them into y (client order).  The chunks spread the blocks with
-      // many leaves over the grid.
+      // many leaves over the grid.  The Rk terms come per B^T group: the block's columns of the
+      // group's matrix times the group's z' rows.
       const int kYChunkUnits = 16;
+      std::vector<std::vector<int>> groups_of(oblocks.size());
+      for (size_t gi = 0; gi < G.size(); ++gi) {
+        auto br = block_range(oblocks, ostarts, G[gi].col_off, G[gi].n);
+        for (int b = br.first; b < br.second; ++b) groups_of[b].push_back((int)gi);
+      }
       for (size_t b = 0; b < oblocks.size(); ++b) {
         const Block& ob = oblocks[b];
         const int first = (int)units.size();
         for (int i : per_block[b]) {
           const LeafInfo& l = L[i];
-          if (l.type == 0) {
-            // columns of block b in every row panel of full leaf i
-            auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
-            for (int q = br.first; q < br.second; ++q) {
-              const int len = rblocks_[q].len;
-              ptx_units(units, layout_.panel[layout_.first[i] + (q - br.first)] + (long long)(ob.off - l.col_off) * len,
-                        len, ob.len, 0, rblocks_[q].off);
-            }
-          } else {
-            const int k = ranks[i];
-            ptx_units(units, layout_.bt[i] + (long long)(ob.off - l.col_off) * k, k, ob.len, 0, K[rk_index[i]].zrow_t);
+          if (l.type != 0) continue;
+          // columns of block b in every row panel of full leaf i
+          auto br = block_range(rblocks_, rstarts_, l.row_off, l.m);
+          for (int q = br.first; q < br.second; ++q) {
+            const int len = rblocks_[q].len;
+            ptx_units(units, layout_.panel[layout_.first[i] + (q - br.first)] + (long long)(ob.off - l.col_off) * len,
+                      len, ob.len, 0, rblocks_[q].off);
           }
+        }
+        for (int gi : groups_of[b]) {
+          const ZGroup& g = G[gi];
+          ptx_units(units, g.base + (long long)(ob.off - g.col_off) * g.h, g.h, ob.len, 0, zgroup_row_[1][gi]);
         }
         const int nu = (int)units.size() - first;
         const int nparts = (nu + kYChunkUnits - 1) / kYChunkUnits;
@@ -1931,16 +2010,25 @@ class Engine : public EngineBase {
       } else if (L[i].type == 1 && ranks[i] > 0) {
         GemvRkLeaf k{L[i].row_off, L[i].m, L[i].col_off, L[i].n, ranks[i], 0, goff, 0, 0};
         goff += (long long)ranks[i] * (L[i].m + L[i].n);
-        k.zrow_n = (int)next_row;
-        next_row += ranks[i];
         K.push_back(k);
         rk_leaf.push_back((int)i);
       }
     }
-    for (auto& k : K) {
-      k.zrow_t = (int)next_row;
-      next_row += k.k;
-    }
+    // z slots ('N', then 'T') in the order of the B^T groups: a group's z rows are contiguous
+    std::vector<int> kidx(L.size(), -1);
+    for (size_t t = 0; t < rk_leaf.size(); ++t) kidx[rk_leaf[t]] = (int)t;
+    const auto& G = layout_.zgroups;
+    zgroup_row_[0].assign(G.size(), 0);
+    zgroup_row_[1].assign(G.size(), 0);
+    for (int side = 0; side < 2; ++side)
+      for (size_t gi = 0; gi < G.size(); ++gi) {
+        zgroup_row_[side][gi] = (int)next_row;
+        for (int i : G[gi].leaves) {
+          GemvRkLeaf& k = K[kidx[i]];
+          (side == 0 ? k.zrow_n : k.zrow_t) = (int)next_row;
+          next_row += k.k;
+        }
+      }
     if (!d_perm_rows_.p || !d_perm_cols_.p) throw Error("gemv plan: cluster permutations are not on the device");
     plan_.perm_rows = d_perm_rows_.p;
     plan_.perm_cols = d_perm_cols_.p;
@@ -1993,6 +2081,7 @@ class Engine : public EngineBase {
   DevArray<GemvFullLeaf> g_full_;
   DevArray<GemvRkLeaf> g_rk_;
   SideBuf side_buf_[2];
+  std::vector<int> zgroup_row_[2];  // first z row of each B^T group, 'N' and 'T' 
   GemvPlan plan_;
   DevArray<T> xz_, rz_, stage_x_, stage_y_;
   DevArray<GemvStatus> err_;       // status block of this matrix's products (flag, wait bound)

@@ -43,6 +43,9 @@ class EngineBase {
   virtual void payload_layout(long long* offsets, long long* total) = 0;
   virtual void leaf_gradients(const void* x, const void* r, int nrhs, void* grad, bool accumulate,
                               cudaStream_t user_stream) = 0;
+  // dx = H^T r and the leaf gradients (leaf_gradients) in one pass.
+  virtual void gemv_adjoint(const void* x, const void* r, int nrhs, void* dx, void* grad, bool accumulate,
+                            cudaStream_t user_stream) = 0;
   virtual void retruncate(double eps) = 0;
   // Loads stored leaves: ranks[i] (-1 for full leaves) and the canonical payload of every
   // leaf (payload_layout order, host memory); the matrix is then assembled.

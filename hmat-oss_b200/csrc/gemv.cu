@@ -44,6 +44,9 @@ __device__ inline void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
 }
+__device__ inline void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ inline void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
@@ -74,10 +77,14 @@ __device__ inline bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long lo
 // A warp whose wait gave up: sets the status flag, then waits (bounded) for the copies of
 // the units it has issued and not consumed (u .. last_issued, one stage each) to land, so
 // that no bulk copy is still writing its shared memory when it exits.
+__device__ inline long long drain_limit(const GemvStatus* st) {
+  return st->wait_limit > 0 && st->wait_limit < kGemvDrainLimit ? st->wait_limit : kGemvDrainLimit;
+}
 __device__ inline void warp_give_up(GemvStatus* st, uint64_t* bars, int nstages, int u_begin, int u, int last_issued) {
-  atomicExch(&st->failed, 1);
+  atomicCAS(&st->failed, 0, 1);
+  const long long lim = drain_limit(st);
   for (int v = u; v <= last_issued; ++v)
-    mbar_wait_bounded(&bars[(v - u_begin) % nstages], (uint32_t)(((v - u_begin) / nstages) & 1), kGemvDrainLimit);
+    mbar_wait_bounded(&bars[(v - u_begin) % nstages], (uint32_t)(((v - u_begin) / nstages) & 1), lim);
 }
 
 __device__ inline uint32_t round16(uint64_t b) { return (uint32_t)((b + 15) & ~15ull); }
@@ -151,6 +158,32 @@ __global__ void __launch_bounds__(256) gather_kernel(const T* __restrict__ x, in
   }
 }
 inline unsigned gather_grid(int N) { return (unsigned)((N + kGatherRows - 1) / kGatherRows + 1); }
+
+// Checks a unit's copies into a warp-level stage before they are issued: 16-byte sizes and
+// addresses (the bulk-copy rule), the piece below the X rows, the X rows inside the stage, and
+// runs that cover exactly its columns.  A unit that fails is not copied: the stage's barrier
+// gets a plain arrival (so nothing waits for it), and the status block records code 2 and the
+// unit's index.
+template <typename T, int RS>
+__device__ inline bool unit_copies_ok(const GemvUnit& U, const T* arena, const T* xz, int stage_bytes, int xoff) {
+  const uint64_t pbytes = round16((uint64_t)U.pel * sizeof(T));
+  const uint64_t xbytes = (uint64_t)U.c * RS * sizeof(T);
+  if (U.c <= 0 || U.pel <= 0 || (reinterpret_cast<uintptr_t>(arena + U.poff) & 15) != 0) return false;
+  if (xoff < (int)pbytes || xoff % 16 != 0 || (uint64_t)xoff + xbytes > (uint64_t)stage_bytes) return false;
+  if (((size_t)RS * sizeof(T)) % 16 != 0) return false;
+  if (U.nruns < 0 || U.nruns > kUnitRuns) return false;
+  if (U.nruns > 0) {
+    int rows = 0;
+    for (int r = 0; r < kUnitRuns; ++r)
+      if (r < U.nruns) rows += U.run_len[r];
+    if (rows != U.c) return false;
+  }
+  return true;
+}
+__device__ inline void record_bad_unit(GemvStatus* st, int u) {
+  atomicExch(&st->failed, 2);
+  atomicExch(&st->pad, u);
+}
 
 // The X rows of a unit into a pipeline stage: one bulk copy, or one per run.
 template <typename T, int RS>
@@ -273,10 +306,10 @@ __global__ void __launch_bounds__(kThreads) stream_kernel(const GemvTask* __rest
       // the copies it has in flight (units u .. u + NSTAGE - 1) have landed
       if (__syncthreads_or(!ok)) {
         if (tid == 0) {
-          atomicExch(&err->failed, 1);
+          atomicCAS(&err->failed, 0, 1);
           for (int v = u; v < u_end && v < u + NSTAGE; ++v)
             mbar_wait_bounded(&bars[(v - u_begin) % NSTAGE], (uint32_t)(((v - u_begin) / NSTAGE) & 1),
-                              kGemvDrainLimit);
+                              drain_limit(err));
         }
         return;
       }
@@ -456,6 +489,11 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
     const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(T));
     const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(T);
     unsigned char* st = wbase + (size_t)s * warp_stage_bytes((int)sizeof(T));
+    if (!unit_copies_ok<T, RS>(U, arena, xz, warp_stage_bytes((int)sizeof(T)), warp_piece_bytes((int)sizeof(T)))) {
+      record_bad_unit(err, u);
+      mbar_arrive(&bars[s]);
+      return;
+    }
     mbar_expect_tx(&bars[s], pbytes + xbytes);
     bulk_g2s(st, arena + U.poff, pbytes, &bars[s]);
     issue_x<T, RS>(st + warp_piece_bytes((int)sizeof(T)), xz, U, &bars[s]);
@@ -646,32 +684,6 @@ __device__ __forceinline__ void mma_kstep(const float* P, const float* X, int k0
   }
 }
 
-// FP64 products on the FP64 tensor cores (mma.sync m8n8k4, FP64 operands and sums): one
-// 4-column step k0 computes D (8 right-hand sides x 8 rows) += X^T (8 x 4) P^T (4 x 8) for
-// each half of the right-hand sides and each 8-row tile; the sums accumulate in the MMA itself
-// (FP64 fused multiply-adds), in acc[t][2 h + i] = out[8 t + 2 tg + i][8 h + g], the layout of
-// the TF32 kernel's accumulators.
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-      : "+d"(d0), "+d"(d1)
-      : "d"(a), "d"(b));
-}
-template <int RS, int NT, int NTILE, bool TAIL>
-__device__ __forceinline__ void dmma_kstep(const double* P, const double* X, int k0, int c, int O, int g, int tg,
-                                           double (&acc)[NTILE][4]) {
-  const int ka = k0 + tg;
-  const bool va = !TAIL || ka < c;
-  const double a0 = (va && g < RS) ? X[ka * RS + g] : 0.0;
-  const double a1 = (va && g + 8 < RS) ? X[ka * RS + g + 8] : 0.0;
-  const double* pa = P + ka * O + g;
-#pragma unroll
-  for (int t = 0; t < NT; ++t) {
-    const double b = va ? pa[t * 8] : 0.0;
-    dmma(acc[t][0], acc[t][1], a0, b);
-    if constexpr (RS > 8) dmma(acc[t][2], acc[t][3], a1, b);
-  }
-}
-
 // All steps of one unit with NT output tiles.
 template <int RS, int NT, int NTILE>
 __device__ __forceinline__ void mma_unit(const float* P, const float* X, int c, int O, int g, int tg,
@@ -688,15 +700,6 @@ __device__ __forceinline__ void mma_unit(const float* P, const float* X, int c, 
   }
   if (k0 < c) mma_kstep<RS, NT, NTILE, true>(P, X, k0, c, O, g, tg, acc);
 }
-template <int RS, int NT, int NTILE>
-__device__ __forceinline__ void mma_unit(const double* P, const double* X, int c, int O, int g, int tg,
-                                         double (&acc)[NTILE][4]) {
-  int k0 = 0;
-#pragma unroll 2
-  for (; k0 + 4 <= c; k0 += 4) dmma_kstep<RS, NT, NTILE, false>(P, X, k0, c, O, g, tg, acc);
-  if (k0 < c) dmma_kstep<RS, NT, NTILE, true>(P, X, k0, c, O, g, tg, acc);
-}
-
 // The unit with the task's tile count (1 .. NTILE) as a compile-time constant.
 template <typename T, int RS, int NTILE, int NT = 1>
 __device__ __forceinline__ void mma_unit_dispatch(int ntn, const T* P, const T* X, int c, int O, int g, int tg,
@@ -714,9 +717,8 @@ __device__ __forceinline__ void mma_unit_dispatch(int ntn, const T* P, const T* 
 
 // CTAs an SM the tensor-core kernel is compiled for: five (20 warps) while its sums fit the
 // register share of five, four for the tallest tasks (6 tiles and more: 28+ accumulators).
-// FP64 (2 x 4 KB-piece stages a warp): four by shared memory.
 __host__ __device__ constexpr int mma_min_blocks(int ntile, int elem_bytes) {
-  return elem_bytes == 8 ? 4 : (ntile >= 6 ? 4 : 5);
+  return elem_bytes == 4 && ntile < 6 ? 5 : 4;
 }
 
 template <typename T, int R, int RS, int NTILE>
@@ -754,6 +756,11 @@ __global__ void __launch_bounds__(kWarpCTA * 32, mma_min_blocks(NTILE, sizeof(T)
     const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(T));
     const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(T);
     unsigned char* st = wbase + (size_t)s * warp_stage_bytes((int)sizeof(T));
+    if (!unit_copies_ok<T, RS>(U, arena, xz, warp_stage_bytes((int)sizeof(T)), U.o0)) {
+      record_bad_unit(err, u);
+      mbar_arrive(&bars[s]);
+      return;
+    }
     mbar_expect_tx(&bars[s], pbytes + xbytes);
     bulk_g2s(st, arena + U.poff, pbytes, &bars[s]);
     issue_x<T, RS>(st + U.o0, xz, U, &bars[s]);
@@ -1033,10 +1040,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // flag the product, then let the MMAs and copies in flight finish before the tensor
     // memory is freed and the CTA exits
     atomicExch(&err->failed, 1);
-    if (mma_pending) mbar_wait_bounded(mmab, mma_parity, kGemvDrainLimit);
+    if (mma_pending) mbar_wait_bounded(mmab, mma_parity, drain_limit(err));
     for (int v = pending; v <= last_issued; ++v)
       mbar_wait_bounded(&full[(v - u_begin) % kTcStages], (uint32_t)(((v - u_begin) / kTcStages) & 1),
-                        kGemvDrainLimit);
+                        drain_limit(err));
   }
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -1153,7 +1160,7 @@ void launch_stream(const GemvLaunch& L, const GemvUnit* units, const T* arena, T
     }
   }
   if (L.warp_level) {
-    if constexpr (std::is_same<T, float>::value || std::is_same<T, double>::value) {
+    if constexpr (std::is_same<T, float>::value) {
       if (L.map == 3) {  // rpt = 8-row tiles of the launch's tallest task (exact up to 8)
         switch (L.rpt) {
           case 1: launch_mma_t<T, R, RS, 1>(L, units, arena, xz, err, s); break;
@@ -1317,6 +1324,28 @@ void grads_tile(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* r
   if (p.nrk > 0 && grk) grad_rk_kernel<T, RS, R><<<grid, 256, 0, s>>>(p.rk, p.nrk, xz, rz, grk, accumulate);
 }
 
+// The adjoint of y = H x at the output gradient r in one pass: dx = H^T r (the 'T' product,
+// whose z' = A^T r stays in rz) and the leaf gradients, which reuse that z' as w; z = B^T x is
+// formed once in xz.
+template <typename T, int R>
+void adjoint_tile(const GemvPlan& p, int nrhs, const T* x, const T* r, T* dx, T* xz, T* rz, T* gfull, T* grk,
+                  bool accumulate, GemvStatus* err, cudaStream_t s) {
+  constexpr int RS = rs_of<T>(R);
+  const T* arena = (const T*)p.arena;
+  run_tile<T, R, true>(p, nrhs, 0, one<T>(), zero<T>(), r, dx, rz, 0, err, s, nullptr);
+  gather_kernel<T, R, RS><<<gather_grid(p.n_cols), 256, 0, s>>>(x, p.n_cols, p.n_cols, 0, nrhs, p.iperm_cols, xz,
+                                                                   p.n_in_max);
+  const GemvSide& sn = p.side[0];
+  for (int c = 0; c < sn.nz; ++c)
+    launch_stream<T, R, RS, false>(sn.z[c], sn.units, arena, xz, 0, nullptr, nullptr, 0, 0, 0, one<T>(), zero<T>(),
+                                   err, s);
+  if (sn.nzred > 0) zred_kernel<T, RS><<<sn.nzred, 128, 0, s>>>(sn.zred, xz);
+  const int grid = persistent_grid(4);
+  if (p.nfull > 0 && gfull)
+    grad_full_kernel<T, RS, R><<<grid, 256, 0, s>>>(p.full, p.nfull, xz, rz, gfull, accumulate);
+  if (p.nrk > 0 && grk) grad_rk_kernel<T, RS, R><<<grid, 256, 0, s>>>(p.rk, p.nrk, xz, rz, grk, accumulate);
+}
+
 }  // namespace
 
 size_t stream_smem_bytes(int elem_bytes, int R, int RS, int omax, bool transposed) {
@@ -1361,6 +1390,16 @@ void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, 
 }
 
 template <typename T>
+void launch_gemv_adjoint(const GemvPlan& p, int nrhs, const T* x, const T* r, T* dx, T* xz, T* rz, T* gfull, T* grk,
+                         bool accumulate, GemvStatus* err, cudaStream_t s) {
+  constexpr bool big = sizeof(T) < 16;
+  if (big && nrhs > 8) adjoint_tile<T, big ? 16 : 4>(p, nrhs, x, r, dx, xz, rz, gfull, grk, accumulate, err, s);
+  else if (big && nrhs > 4) adjoint_tile<T, big ? 8 : 4>(p, nrhs, x, r, dx, xz, rz, gfull, grk, accumulate, err, s);
+  else if (nrhs > 1) adjoint_tile<T, 4>(p, nrhs, x, r, dx, xz, rz, gfull, grk, accumulate, err, s);
+  else adjoint_tile<T, 1>(p, nrhs, x, r, dx, xz, rz, gfull, grk, accumulate, err, s);
+}
+
+template <typename T>
 void launch_gemv(const GemvPlan& p, char trans, int nrhs, T alpha, T beta, const T* x_client, T* y_client, T* xz,
                  GemvStatus* err, cudaStream_t s, const GemvTiming* tm) {
   if (trans == 'N') run_all<T, false>(p, nrhs, alpha, beta, x_client, y_client, xz, 0, err, s, tm);
@@ -1373,7 +1412,9 @@ void launch_gemv(const GemvPlan& p, char trans, int nrhs, T alpha, T beta, const
   template void launch_gemv<T>(const GemvPlan&, char, int, T, T, const T*, T*, T*, GemvStatus*, cudaStream_t,         \
                                const GemvTiming*);                                                             \
   template void launch_leaf_gradients<T>(const GemvPlan&, int, const T*, const T*, T*, T*, T*, T*, bool, GemvStatus*, \
-                                         cudaStream_t);
+                                         cudaStream_t);                                                                  \
+  template void launch_gemv_adjoint<T>(const GemvPlan&, int, const T*, const T*, T*, T*, T*, T*, T*, bool, GemvStatus*, \
+                                       cudaStream_t);
 HB_INST(float)
 HB_INST(double)
 HB_INST(cfloat)

@@ -34,9 +34,12 @@ struct FullLeafDesc {
   int panel_first, npanel;
 };
 
-// One contiguous copy of a segmented relayout (elements).
+// One piece of a segmented relayout (elements): a rows x cols column-major block, leading
+// dimensions src_ld and dst_ld (a contiguous run is cols = 1).
 struct CopySeg {
-  long long src, dst, count;
+  long long src, dst;
+  int rows, cols;
+  int src_ld, dst_ld;
 };
 template <typename T>
 void launch_copy_segments(const CopySeg* segs, int nseg, const T* src, T* dst, cudaStream_t s);
@@ -45,6 +48,8 @@ void launch_copy_segments(const CopySeg* segs, int nseg, const T* src, T* dst, c
 struct RkStoreDesc {
   int panel_first, npanel;
   long long bt_off;
+  int bt_ld;  // leading dimension of B^T (0: k, the leaf's own k x n block)
+  int pad;
 };
 
 // ---- assembly ----
@@ -186,6 +191,11 @@ int mma_stream_blocks_per_sm(int ntile, int elem_bytes);
 template <typename T>
 void launch_leaf_gradients(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* rz, T* gfull, T* grk,
                            bool accumulate, GemvStatus* err, cudaStream_t s);
+// dx = H^T r and the leaf gradients of y = H x at the output gradient r, in one pass (the
+// transposed product's z' = A^T r serves both); nrhs <= 16.
+template <typename T>
+void launch_gemv_adjoint(const GemvPlan& p, int nrhs, const T* x, const T* r, T* dx, T* xz, T* rz, T* gfull, T* grk,
+                         bool accumulate, GemvStatus* err, cudaStream_t s);
 
 // Load the assembly kernels of the storage type T ahead of the first assembly.
 template <typename T>

@@ -259,7 +259,8 @@ __global__ void __launch_bounds__(kTruncThreads) truncate_kernel(const RkLeafDes
   }
 }
 
-// Writes A as row panels (len x k column-major each) and B transposed (k x n column-major).
+// Writes A as row panels (len x k column-major each) and B transposed (k x n column-major,
+// leading dimension bt_ld: rows of a taller matrix of stacked B^T blocks).
 template <typename T>
 __global__ void compact_kernel(const RkLeafDesc* __restrict__ leaves, int nleaves, const T* __restrict__ ws,
                                const int* __restrict__ ranks, const RkStoreDesc* __restrict__ store,
@@ -281,9 +282,10 @@ __global__ void compact_kernel(const RkLeafDesc* __restrict__ leaves, int nleave
     }
   }
   T* bt = arena + st.bt_off;
+  const int ld = st.bt_ld > 0 ? st.bt_ld : k;
   for (int e = threadIdx.x; e < d.n * k; e += blockDim.x) {
     const int l = e % k, j = e / k;
-    bt[e] = B[(size_t)l * d.n + j];
+    bt[l + (size_t)j * ld] = B[(size_t)l * d.n + j];
   }
 }
 
@@ -310,9 +312,10 @@ __global__ void unpack_kernel(const RkLeafDesc* __restrict__ leaves, int nleaves
     }
   }
   const T* bt = arena + st.bt_off;
+  const int ld = st.bt_ld > 0 ? st.bt_ld : k;
   for (int e = threadIdx.x; e < d.n * k; e += blockDim.x) {
     const int l = e % k, j = e / k;
-    B[(size_t)l * d.n + j] = bt[e];
+    B[(size_t)l * d.n + j] = bt[l + (size_t)j * ld];
   }
 }
 

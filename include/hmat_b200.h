@@ -384,7 +384,9 @@ int hmat_b200_gemv_device(hmat_matrix_t* hmatrix, char trans, const void* alpha,
 /* Status of the device products of `hmatrix` (hmat_b200_gemv_device, _noalloc, and the
  * leaf gradients): synchronises `stream` (NULL: the matrix's own stream), then sets *failed
  * to 1 if one of them stopped since the last query because a kernel's wait for a bulk copy
- * gave up (their results are not valid), else 0, and clears the flag.  Allocates nothing.
+ * gave up, 2 if a unit of the product's schedule failed the kernels' own checks of its copies
+ * (sizes, alignment, stage bounds) and was skipped (in both cases the results are not valid),
+ * else 0, and clears the flag.  Allocates nothing.
  * The C table's gemv checks the same flag itself and returns 1.  Returns 0, or non-zero
  * on a bad argument.  No counterpart in the reference (its products run on the host). */
 int hmat_b200_gemv_status(hmat_matrix_t* hmatrix, void* stream, int* failed);
@@ -455,6 +457,15 @@ int hmat_b200_payload_layout(hmat_matrix_t* hmatrix, long long* offsets, long lo
  * The gradient with respect to x is gemv('T') of r.  Real value types only. */
 int hmat_b200_leaf_gradients(hmat_matrix_t* hmatrix, const void* x_dev, const void* r_dev, int nrhs, void* grad,
                              int accumulate, void* stream);
+
+/* The whole backward pass of y = H x at the output gradient r (device buffers, client
+ * numbering, 1 to 16 columns): dx = H^T r into dx_dev, and the leaf gradients of
+ * hmat_b200_leaf_gradients into grad (added when `accumulate`).  One pass: the transposed
+ * product's A^T r serves as the gradients' w, so it costs one transposed product plus the
+ * gradient kernels and one B^T x.  Real value types only.  No counterpart in the reference
+ * (its transposed product is RkMatrix::gemv 'T', rk_matrix.cpp:156-206). */
+int hmat_b200_gemv_adjoint(hmat_matrix_t* hmatrix, const void* x_dev, const void* r_dev, int nrhs, void* dx_dev,
+                           void* grad, int accumulate, void* stream);
 
 /* One eager product y = op(H) x on device buffers (1 to 16 right-hand sides), timed per
  * phase with CUDA events: ms3 = device ms of [gather, z-phase, y-phase], bytes3 = their

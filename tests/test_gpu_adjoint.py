@@ -2,8 +2,8 @@
 central finite differences and against the reference's own transposed product.
 
     forward:  y = H x                                   hmat_b200_gemv_device ('N')
-    backward: dx = H^T r                                hmat_b200_gemv_device ('T')
-              dF, dA, dB (canonical payload layout)     hmat_b200_leaf_gradients
+    backward: dx = H^T r and dF, dA, dB (canonical      hmat_b200_gemv_adjoint (one pass; the same as
+              payload layout)                           gemv_device 'T' + hmat_b200_leaf_gradients)
 for the loss L = 1/2 ||H x - b||^2, r = H x - b.  The leaf payload enters the function as a
 tensor `theta` holding the matrix's stored leaves (canonical layout: full m x n, Rk A m x k
 then B n x k, column-major, leaf order), so that autograd returns dL/dtheta beside dL/dx.
@@ -57,10 +57,10 @@ class HGemv:
                 nrhs = x.shape[0]
                 stream = torch.cuda.current_stream().cuda_stream
                 dx = torch.empty_like(x)
-                h.gemv_device(gy.data_ptr(), dx.data_ptr(), nrhs, trans="T", stream=stream)
                 dtheta = torch.empty(ctx.theta_shape, dtype=x.dtype, device=x.device)
-                h.leaf_gradients(x.data_ptr(), gy.data_ptr(), nrhs, dtheta.data_ptr(), accumulate=False,
-                                 stream=stream)
+                # dx = H^T r and the leaf gradients in one pass (hmat_b200_gemv_adjoint)
+                h.gemv_adjoint(x.data_ptr(), gy.data_ptr(), nrhs, dx.data_ptr(), dtheta.data_ptr(), accumulate=False,
+                               stream=stream)
                 assert not h.gemv_status(stream)
                 return dx, dtheta, None
 
@@ -189,5 +189,39 @@ def test_autograd_dx_matches_reference_transposed_gemv(hb, vt, tol):
         b = y - xg  # r = H x - b = x_g
         _, dx, _ = _loss_and_grads(torch, h, x, b)
         assert rel(dx, g["y_T"]) < tol
+    finally:
+        h.close()
+
+
+@pytest.mark.parametrize("vt", [1, 0])
+def test_fused_adjoint_equals_separate_calls(hb, vt):
+    """hmat_b200_gemv_adjoint gives bit for bit what the transposed device product and
+    hmat_b200_leaf_gradients give separately (same kernels, the transposed product's A^T r
+    reused as the gradients' w), also with accumulate."""
+    import torch
+    wl = _wl()
+    pts = wl.cube(2500, 4)
+    hb.set_parameters(compressionMinLeafSize=0)
+    h = hb.HMatrix(pts, hb.kernel(hb.EXP_COV, ell=0.3, nugget=1e-6), value_type=vt, leaf_size=32, eta=2.0,
+                   epsilon=1e-6)
+    try:
+        n = len(pts)
+        dt = torch.float64 if vt == 1 else torch.float32
+        rng = np.random.default_rng(12)
+        with torch.cuda.stream(torch.cuda.Stream()):
+            st = torch.cuda.current_stream().cuda_stream
+            x = torch.from_numpy(rng.standard_normal((3, n))).to("cuda", dt)
+            r = torch.from_numpy(rng.standard_normal((3, n))).to("cuda", dt)
+            _, total = h.payload_layout()
+            dx1, dx2 = torch.empty_like(x), torch.empty_like(x)
+            g1 = torch.full((total,), 0.5, device="cuda", dtype=dt)
+            g2 = g1.clone()
+            h.gemv_device(r.data_ptr(), dx1.data_ptr(), 3, trans="T", stream=st)
+            h.leaf_gradients(x.data_ptr(), r.data_ptr(), 3, g1.data_ptr(), accumulate=True, stream=st)
+            h.gemv_adjoint(x.data_ptr(), r.data_ptr(), 3, dx2.data_ptr(), g2.data_ptr(), accumulate=True, stream=st)
+            torch.cuda.current_stream().synchronize()
+            assert not h.gemv_status(st)
+        assert torch.equal(dx1, dx2)
+        assert torch.equal(g1, g2)
     finally:
         h.close()

@@ -63,7 +63,7 @@ def test_noalloc_gemv_matches_device_gemv_twice(hb, vt, tol):
         h.gemv_device(x.data_ptr(), y_ref.data_ptr(), 2, alpha=2.0, beta=0.5, stream=stream.cuda_stream)
         assert h.gemv_device_noalloc(x.data_ptr(), y_na.data_ptr(), 2, alpha=2.0, beta=0.5,
                                      stream=stream.cuda_stream) == 0
-        assert h.gemv_status(stream.cuda_stream) is False
+        assert h.gemv_status(stream.cuda_stream) == 0
         a = y_ref.cpu().numpy()
         b = y_na.cpu().numpy()
         assert np.linalg.norm(a - b) / np.linalg.norm(a) <= tol
