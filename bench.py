@@ -286,7 +286,7 @@ def supplementary(args):
             res[label] = {"assembly_device_ms": a_ms, "assembly_wall_s": wall, "phase_ms": parts,
                           "gemv_ms": ms, "gemv_gbs": h.gemv_bytes(c["nrhs"]) / (ms * 1e-3) / 1e9,
                           "rk_leaves": nrk, "aca_leaves_per_s": nrk / ((parts["aca_ms"] + parts["truncate_ms"]) * 1e-3),
-                          "y": y}
+                          "gemv_schedule": h.gemv_tuning(), "y": y}
             h.close()
         lo, hi = ("C", "Z") if cplx else ("S", "D")
         err = float(np.linalg.norm(res[lo]["y"] - res[hi]["y"]) / np.linalg.norm(res[hi]["y"]))
@@ -319,7 +319,7 @@ def supplementary(args):
                           "aca_leaves_per_s": rk / ((parts["aca_ms"] + parts["truncate_ms"]) * 1e-3),
                           "matrices_per_s": len(batch) / (a_ms * 1e-3), "gemv_ms": ms,
                           "gemv_gbs": b.gemv_bytes(nrhs) / (ms * 1e-3) / 1e9,
-                          "gemv_launches": b.gemv_launches(nrhs)}
+                          "gemv_launches": b.gemv_launches(nrhs), "gemv_schedule": b.gemv_tuning()}
             b.close()
         err = float(np.linalg.norm(ys["S"] - ys["D"]) / np.linalg.norm(ys["D"]))
         cpu = None
@@ -357,7 +357,8 @@ def supplementary(args):
         payload = total * 4
         out.update({"metric": "adjoint GB/s (forward bytes + written leaf gradients)", "n": n,
                     "backward_ms": ms, "bytes": fwd + payload,
-                    "gbs": (fwd + payload) / (ms * 1e-3) / 1e9, "assembly_device_ms": asm_ms(h)[0]})
+                    "gbs": (fwd + payload) / (ms * 1e-3) / 1e9, "assembly_device_ms": asm_ms(h)[0],
+                    "gemv_schedule": h.gemv_tuning()})
         h.close()
     print(json.dumps(out))
     return 0
@@ -513,7 +514,7 @@ def main():
                        f"{bytes32 / 1e9:.3f} GB)", "leaves": int(len(T32)), "rk_leaves": n_rk,
                        "bytes_per_step": bytes32, "assembly_device_ms": asm32, "assembly_wall_s": wall32,
                        "aca_leaves_per_s": n_rk / ((pt32["aca_ms"] + pt32["truncate_ms"]) * 1e-3),
-                       "phase_ms": pt32, "aca_shapes": aca32},
+                       "phase_ms": pt32, "aca_shapes": aca32, "gemv_schedule": h32.gemv_tuning()},
             "roofline": {"bound": "hbm", "kernel": f"gemv {dom}", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": measured_traffic(dom),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture "

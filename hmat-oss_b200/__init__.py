@@ -144,7 +144,7 @@ EXPORTED = [
     "hmat_b200_leaf_count",
     "hmat_b200_leaf_table", "hmat_b200_leaf_payload", "hmat_b200_payload_layout", "hmat_b200_leaf_gradients",
     "hmat_b200_gemv_adjoint", "hmat_b200_phase_times", "hmat_b200_gemv_profile", "hmat_b200_gemv_launches", "hmat_b200_aca_shapes",
-    "hmat_b200_last_error",
+    "hmat_b200_gemv_tuning", "hmat_b200_last_error",
     "hmat_b200_clear_last_error",
 ]
 
@@ -194,6 +194,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "hmat_b200_gemv_profile": (C.c_int, [_P, C.c_char, _P, _P, C.c_int, _P, _P]),
         "hmat_b200_gemv_launches": (C.c_int, [_P, C.c_char, C.c_int]),
         "hmat_b200_aca_shapes": (C.c_int, [_P, _P, _P, _P]),
+        "hmat_b200_gemv_tuning": (C.c_int, [_P, _P, _P, _P]),
         "hmat_b200_last_error": (C.c_char_p, []),
         "hmat_b200_clear_last_error": (None, []),
     }
@@ -560,6 +561,17 @@ class HMatrix:
             out[names[b]] = {"threads": int(shape[b]), "how": ("default", "measured", "cached")[int(tuned[b])],
                              "rates": {shapes[s]: float(rate[5 * b + s]) for s in range(5) if rate[5 * b + s] > 0}}
         return out
+
+    def gemv_tuning(self) -> dict:
+        """The gemv tuner's choice for this matrix's 'N' schedule (hmat_b200_gemv_tuning)."""
+        ch = np.zeros(2, np.int32)
+        how = C.c_int()
+        ms = np.zeros(5)
+        _check(self.lib.hmat_b200_gemv_tuning(self.m, ch.ctypes.data, C.byref(how), ms.ctypes.data),
+               "hmat_b200_gemv_tuning")
+        return {"z_chunk_units": int(ch[0]), "y_units": ("widest", "half")[int(ch[1])],
+                "how": ("default", "measured", "cached")[how.value],
+                "ms": {"z8": ms[0], "z16": ms[1], "z32": ms[2], "y_widest": ms[3], "y_half": ms[4]}}
 
     def gemv_bytes(self, nrhs: int) -> int:
         """Algorithmic bytes of one product: every stored leaf scalar read once, x read and

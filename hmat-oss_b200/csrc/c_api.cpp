@@ -1242,6 +1242,16 @@ int hmat_b200_aca_shapes(hmat_matrix_t* m, int* shape4, int* tuned4, double* rat
   return 0;
 }
 
+int hmat_b200_gemv_tuning(hmat_matrix_t* m, int* choice2, int* how, double* ms5) {
+  if (!m || !choice2 || !how || !ms5) return fail("hmat_b200_gemv_tuning", "null argument");
+  if (!m->engine || !m->engine->assembled) return fail("hmat_b200_gemv_tuning", "matrix is not assembled");
+  choice2[0] = m->engine->gemv_choice[0];
+  choice2[1] = m->engine->gemv_choice[1];
+  *how = m->engine->gemv_tuned;
+  for (int i = 0; i < 5; ++i) ms5[i] = m->engine->gemv_rate[i];
+  return 0;
+}
+
 const char* hmat_b200_last_error(void) { return g_last_error.c_str(); }
 void hmat_b200_clear_last_error(void) { g_last_error.clear(); }
 

@@ -110,6 +110,9 @@ int aca_tuning_mode() {
 // bucket).
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
+// Gemv tuner choices of the process: (z chunk units, half-width y units) by (scalar type,
+// height class of the output blocks).
+std::map<std::tuple<int, int, int, int>, std::pair<int, bool>> g_gemv_tune_cache;
 
 // Bound of each gemv kernel's wait for a bulk copy (polls of the stage barrier).
 // HMAT_B200_GEMV_WAIT_LIMIT changes it for the matrices created while it is set; a negative
@@ -259,6 +262,7 @@ class Engine : public EngineBase {
     times_ms[0] = ms;
     pieces_.clear();
     build_plan();
+    tune_gemv_plan();
     HB_CUDA(cudaStreamSynchronize(stream_));
     assembled = true;
   }
@@ -458,6 +462,7 @@ class Engine : public EngineBase {
     HB_CUDA(cudaGetLastError());
     HB_CUDA(cudaStreamSynchronize(stream_));
     build_plan();
+    tune_gemv_plan();
     HB_CUDA(cudaStreamSynchronize(stream_));
     for (int i = 0; i < 4; ++i) times_ms[i] = 0;
     assembled = true;
@@ -532,6 +537,7 @@ class Engine : public EngineBase {
       gexec_ = nullptr;
     }
     build_plan();
+    tune_gemv_plan();
     HB_CUDA(cudaStreamSynchronize(stream_));
     for (int i = 0; i < 4; ++i) times_ms[i] = saved[i];
   }
@@ -1728,7 +1734,9 @@ class Engine : public EngineBase {
     const std::vector<Block>& oblocks = trans ? cblocks_ : rblocks_;
     const std::vector<int>& ostarts = trans ? cstarts_ : rstarts_;
     std::vector<GemvUnit> units;
-    const int kMaxUnits = 16;  // a longer z task is cut into chunks summed afterwards (spreads long leaves over warps)
+    // a longer z task is cut into chunks summed afterwards (spreads long leaves over warps): the
+    // 'N' chunk size is the gemv tuner's choice
+    const int kMaxUnits = trans ? 16 : tune_zparts_;
     // FP32 'N' y-phase on the tensor-memory kernel when HMAT_B200_TC_Y=1
     const bool tc_y = !trans && std::is_same<T, float>::value && tc_y_enabled();
 
@@ -1835,6 +1843,10 @@ class Engine : public EngineBase {
           cols = mma_unit_cols(O, &xoff);
         else
           cols = warp_unit_cols(O);
+        if (tune_yhalf_ && !tc_y) {  // the tuner's narrower units: half the columns, kept aligned
+          const int step = kTensorN ? 8 : galign;
+          cols = std::max(step, cols / 2 / step * step);
+        }
         for (int j0 = 0; j0 < W;) {
           const int want = std::min(cols, W - j0);
           // the columns the unit can take with at most kUnitRuns runs of X rows
@@ -2052,6 +2064,108 @@ class Engine : public EngineBase {
     build_side(true, K, rk_leaf, next_row, plan_.side[1], side_buf_[1]);
     plan_.xz_rows = next_row;
     if (next_row >= (1LL << 31)) throw Error("gemv plan: z buffer too large");
+  }
+
+  // Gemv tuner.  Two knobs of the 'N' schedule: the size of the chunks long z tasks are cut into
+  // (8, 16 or 32 units: finer chunks spread long groups over more warps, coarser ones write
+  // fewer partial rows) and the width of the y-phase units (the widest that fit a stage, or
+  // half of it: more, shorter units).  For matrices whose leaves take at least 64 MB, each
+  // candidate schedule is built and its z- and y-phases timed on one product (CUDA events, the
+  // second of two runs); the fastest chunk size, then the fastest width, are kept and cached for
+  // the process by (scalar type, height class of the output blocks).  HMAT_B200_GEMV_TUNE=0
+  // keeps the defaults (16, widest); =2 samples any matrix and bypasses the cache (tests).
+  int tune_zparts_ = 16;
+  bool tune_yhalf_ = false;
+
+  static int gemv_tuning_mode() {
+    const char* s = getenv("HMAT_B200_GEMV_TUNE");
+    if (!s || !*s) return 1;
+    return s[0] == '0' ? 0 : (s[0] == '2' ? 2 : 1);
+  }
+
+  // Device ms of the z- and y-phases of one 'N' product with the current schedule.
+  void time_phases(double* zms, double* yms) {
+    const int nr = std::max(1, std::min(16, kTensorN ? 16 : (sizeof(T) >= 16 ? 4 : 16)));
+    DevArray<T> xb, yb;
+    xb.alloc((size_t)C_->n * nr);
+    yb.alloc((size_t)R_->n * nr);
+    HB_CUDA(cudaMemsetAsync(xb.p, 0, xb.n * sizeof(T), stream_));
+    xz_.ensure(xz_elems());
+    GemvTiming tm;
+    for (int i = 0; i < 4; ++i) HB_CUDA(cudaEventCreate(&tm.ev[i]));
+    for (int rep = 0; rep < 2; ++rep)
+      launch_gemv<T>(plan_, 'N', nr, one<T>(), zero<T>(), xb.p, yb.p, xz_.p, err_.p, stream_, &tm);
+    cudaError_t le = cudaGetLastError(), se = cudaStreamSynchronize(stream_);
+    float a = 0, b = 0;
+    if (le == cudaSuccess && se == cudaSuccess) {
+      cudaEventElapsedTime(&a, tm.ev[1], tm.ev[2]);
+      cudaEventElapsedTime(&b, tm.ev[2], tm.ev[3]);
+    }
+    for (int i = 0; i < 4; ++i) cudaEventDestroy(tm.ev[i]);
+    HB_CUDA(le);
+    HB_CUDA(se);
+    check_err_flag();
+    *zms = a;
+    *yms = b;
+  }
+
+  void tune_gemv_plan() {
+    gemv_tuned = 0;
+    gemv_choice[0] = tune_zparts_ = 16;
+    gemv_choice[1] = 0;
+    tune_yhalf_ = false;
+    for (double& v : gemv_rate) v = 0.0;
+    const int mode = gemv_tuning_mode();
+    if (mode == 0) return;
+    const long long bytes = layout_.total * (long long)sizeof(T);
+    if (mode == 1 && bytes < (64LL << 20)) return;
+    int maxlen = 1;
+    for (const Block& b : rblocks_) maxlen = std::max(maxlen, b.len);
+    const auto key = std::make_tuple((int)sizeof(T) * 2 + (Traits<T>::is_complex ? 1 : 0), (maxlen + 15) / 16, 0, 0);
+    if (mode == 1) {
+      std::lock_guard<std::mutex> g(g_tune_mu);
+      auto it = g_gemv_tune_cache.find(key);
+      if (it != g_gemv_tune_cache.end()) {
+        tune_zparts_ = it->second.first;
+        tune_yhalf_ = it->second.second;
+        gemv_choice[0] = tune_zparts_;
+        gemv_choice[1] = tune_yhalf_ ? 1 : 0;
+        gemv_tuned = 2;
+        build_plan();
+        return;
+      }
+    }
+    static const int kZparts[3] = {8, 16, 32};
+    double best_z = 1e300;
+    int zp = 16;
+    for (int i = 0; i < 3; ++i) {
+      tune_zparts_ = kZparts[i];
+      tune_yhalf_ = false;
+      build_plan();
+      double z, y;
+      time_phases(&z, &y);
+      gemv_rate[i] = z;
+      if (i == 0 || z < best_z) {
+        best_z = z;
+        zp = kZparts[i];
+      }
+      if (kZparts[i] == 16) gemv_rate[3] = y;  // the widest units' y-phase
+    }
+    tune_zparts_ = zp;
+    tune_yhalf_ = true;
+    build_plan();
+    double z, yh;
+    time_phases(&z, &yh);
+    gemv_rate[4] = yh;
+    tune_yhalf_ = yh < gemv_rate[3];
+    if (!tune_yhalf_) build_plan();
+    gemv_choice[0] = tune_zparts_;
+    gemv_choice[1] = tune_yhalf_ ? 1 : 0;
+    gemv_tuned = 1;
+    if (mode == 1) {
+      std::lock_guard<std::mutex> g(g_tune_mu);
+      g_gemv_tune_cache[key] = std::make_pair(tune_zparts_, tune_yhalf_);
+    }
   }
 
   const ClusterTree* R_;

@@ -74,6 +74,12 @@ class EngineBase {
   // no leaves), how it was chosen (0 default or forced, 1 measured now, 2 cached from an
   // earlier assembly of the process) and the measured leaf cost per ms of each shape (0 = not
   // run).
+  // Gemv tuner report of the last plan: the chosen z chunk size (units) and y unit width (0
+  // widest, 1 half), how (0 default, 1 measured now, 2 cached) and the measured device ms:
+  // z-phase with chunks of 8, 16, 32 units, y-phase with widest and half-width units.
+  int gemv_choice[2] = {16, 0};
+  int gemv_tuned = 0;
+  double gemv_rate[5] = {};
   int aca_shape[4] = {-1, -1, -1, -1};
   int aca_tuned[4] = {0, 0, 0, 0};
   double aca_rate[4][5] = {};

@@ -492,6 +492,14 @@ int hmat_b200_phase_times(hmat_matrix_t* hmatrix, double* out4);
  * reference. */
 int hmat_b200_aca_shapes(hmat_matrix_t* hmatrix, int* shape4, int* tuned4, double* rate20);
 
+/* The gemv tuner's choice for the matrix's 'N' product schedule (no counterpart in the
+ * reference): choice2[0] = units per chunk of long z tasks (8, 16 or 32), choice2[1] = y-phase
+ * unit width (0 the widest that fits a pipeline stage, 1 half of it); *how = 0 default, 1
+ * measured on this matrix, 2 taken from an earlier measurement of the process; ms5 = device ms
+ * of the z-phase with chunks of 8, 16 and 32 units, and of the y-phase with the widest and the
+ * half-width units (0 where not measured).  0, or non-zero before assembly. */
+int hmat_b200_gemv_tuning(hmat_matrix_t* hmatrix, int* choice2, int* how, double* ms5);
+
 /* Last error message of the calling thread ("" if none). */
 const char* hmat_b200_last_error(void);
 /* Clears the calling thread's last error (for the table entries that return no status,

@@ -345,6 +345,14 @@ def test_headline_cylinder_100k(hb, oracle):
         err = rel(y32, y64)
         print(f"mixed vs FP64 H-matrix, 16 RHS: {err:.3e}")
         assert err <= 1e-6
+        # size-independent properties at full size: repeated products bitwise identical (fixed
+        # summation orders), and linearity in x within rounding
+        x32 = x16.astype(np.float32)
+        assert np.array_equal(h32.gemv(x32), h32.gemv(x32))
+        assert np.array_equal(h64.gemv(x16), y64)
+        xa, xb = x16[:, :8], x16[:, 8:]
+        ylin = h64.gemv(np.asfortranarray(2.0 * xa - 0.5 * xb))
+        assert rel(ylin, 2.0 * y64[:, :8] - 0.5 * y64[:, 8:]) < 1e-13
     finally:
         h64.close()
         if h32 is not None:
@@ -371,5 +379,31 @@ def test_aca_capacity_retries_and_workspace_batches_match_reference(hb, name, mo
         tol = GEMV_TOL.get(name, 1e-12)
         assert rel(h.gemv(x, "N"), g["y"]) < tol
         assert rel(h.gemv(x, "T"), g["y_T"]) < tol
+    finally:
+        h.close()
+
+
+def test_gemv_tuner_schedules_give_the_same_products(hb, oracle, monkeypatch):
+    """The gemv tuner (HMAT_B200_GEMV_TUNE=2: every candidate schedule measured, whatever the
+    matrix size) picks a z chunk size and a y unit width; the product with its schedule equals
+    the oracle's like the default schedule's does (FP64, 1e-12), and the report names the
+    measured candidates."""
+    monkeypatch.setenv("HMAT_B200_GEMV_TUNE", "2")
+    h, pts, x, kern, tree = build_engine(hb, "cube_expcov")
+    try:
+        t = h.gemv_tuning()
+        assert t["how"] == "measured"
+        assert t["z_chunk_units"] in (8, 16, 32) and t["y_units"] in ("widest", "half")
+        assert all(t["ms"][k] > 0 for k in ("z8", "z16", "z32", "y_widest", "y_half"))
+        o = oracle.OracleHMatrix(pts, leaf=tree["leaf"], eta=tree["eta"])
+        o.assemble(eps=tree["eps"], **kern)
+        assert rel(h.gemv(x, "N"), o.gemv(x, "N")) < 1e-12
+        assert rel(h.gemv(x, "T"), o.gemv(x, "T")) < 1e-12
+    finally:
+        h.close()
+    monkeypatch.setenv("HMAT_B200_GEMV_TUNE", "0")
+    h, pts, x, kern, tree = build_engine(hb, "cube_expcov")
+    try:
+        assert h.gemv_tuning()["how"] == "default"
     finally:
         h.close()
