@@ -139,7 +139,7 @@ EXPORTED = [
     "hmat_create_compression_rrqr", "hmat_delete_compression", "hmat_default_progress",
     "hmat_assemble_context_init", "hmat_factorization_context_init", "hmat_solve_context_init",
     "hmat_init_default_interface", "hmat_get_parameters", "hmat_set_parameters", "hmat_get_version",
-    "hmat_b200_create_assembly", "hmat_b200_delete_assembly", "hmat_b200_gemv_device", "hmat_b200_gemv_device_noalloc", "hmat_b200_gemv_status",
+    "hmat_b200_create_assembly", "hmat_b200_create_assembly_strata", "hmat_b200_delete_assembly", "hmat_b200_gemv_device", "hmat_b200_gemv_device_noalloc", "hmat_b200_gemv_status",
     "hmat_b200_batch_create", "hmat_b200_batch_offsets", "hmat_b200_batch_assemble",
     "hmat_b200_leaf_count",
     "hmat_b200_leaf_table", "hmat_b200_leaf_payload", "hmat_b200_payload_layout", "hmat_b200_leaf_gradients",
@@ -177,6 +177,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "hmat_set_parameters": (C.c_int, [C.POINTER(Settings)]),
         "hmat_get_version": (C.c_char_p, []),
         "hmat_b200_create_assembly": (_P, [C.POINTER(KernelDesc), _P, C.c_int]),
+        "hmat_b200_create_assembly_strata": (_P, [C.POINTER(KernelDesc), _P, C.c_int, C.c_int, _P, _P]),
         "hmat_b200_delete_assembly": (None, [_P]),
         "hmat_b200_gemv_device": (C.c_int, [_P, C.c_char, _P, _P, _P, _P, C.c_int, _P]),
         "hmat_b200_gemv_device_noalloc": (C.c_int, [_P, C.c_char, _P, _P, _P, _P, C.c_int, _P]),
@@ -299,7 +300,14 @@ class HMatrix:
                 "svd": lib.hmat_create_compression_svd}[compression]
         self._comp = make(epsilon)
         self._kernel = kernel
-        self._assembly = lib.hmat_b200_create_assembly(C.byref(kernel), self.points.ctypes.data, self.n)
+        strata = getattr(kernel, "strata", None)
+        if strata is not None:
+            sp = np.ascontiguousarray(strata[0], dtype=np.float64)
+            sw = np.ascontiguousarray(strata[1], dtype=np.float64)
+            self._assembly = lib.hmat_b200_create_assembly_strata(C.byref(kernel), self.points.ctypes.data, self.n,
+                                                                  len(sp), sp.ctypes.data, sw.ctypes.data)
+        else:
+            self._assembly = lib.hmat_b200_create_assembly(C.byref(kernel), self.points.ctypes.data, self.n)
         if not self._assembly:
             raise HMatError("hmat_b200_create_assembly failed: " + lib.hmat_b200_last_error().decode())
         if assemble:
@@ -661,5 +669,14 @@ class HMatrixBatch(HMatrix):
         self.members = []
 
 
-def kernel(kind: int, delta: float = 0.01, ell: float = 0.3, nugget: float = 0.0, wavenumber: float = 0.0):
-    return KernelDesc(kind, delta, ell, nugget, wavenumber)
+def kernel(kind: int, delta: float = 0.01, ell: float = 0.3, nugget: float = 0.0, wavenumber: float = 0.0,
+           strata_param=None, strata_weight=None):
+    """Kernel descriptor.  With strata_param / strata_weight (same length, 1 to 8), a multi-strata
+    kernel: stratum q is strata_weight[q] times the kernel with its parameter (ell, delta or
+    wavenumber by kind) set to strata_param[q] (hmat_b200_create_assembly_strata)."""
+    k = KernelDesc(kind, delta, ell, nugget, wavenumber)
+    if strata_param is not None or strata_weight is not None:
+        if strata_param is None or strata_weight is None or len(strata_param) != len(strata_weight):
+            raise ValueError("strata_param and strata_weight: both, same length")
+        k.strata = (list(map(float, strata_param)), list(map(float, strata_weight)))
+    return k

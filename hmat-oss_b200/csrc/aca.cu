@@ -684,7 +684,9 @@ __global__ void dense_to_rk_kernel(const RkLeafDesc* __restrict__ leaves, const 
   }
   for (int e = threadIdx.x; e < m * n; e += blockDim.x) {
     const int i = e % m, j = e / m;
-    const T v = KernelEval<T>::eval(kp, pts, d.row_off + i, d.col_off + j);
+    // a multi-strata kernel: the sum of its strata (the SVD compression is not incremental)
+    const T v = kp.nstrata > 0 ? KernelEval<T>::eval_sum(kp, pts, d.row_off + i, d.col_off + j)
+                               : KernelEval<T>::eval(kp, pts, d.row_off + i, d.col_off + j);
     if (m >= n) A[(size_t)j * m + i] = v;  // A = M (m x n)
     else B[(size_t)i * n + j] = v;         // B = M^T (n x m)
   }

@@ -21,7 +21,9 @@ __global__ void __launch_bounds__(256) assemble_full_kernel(const FullLeafDesc* 
       const int mn = P.len * d.n;
       for (int e = threadIdx.x; e < mn; e += blockDim.x) {
         const int i = e % P.len, j = e / P.len;
-        F[e] = KernelEval<T>::eval(kp, pts, d.row_off + P.rs + i, d.col_off + j);
+        // a multi-strata kernel's full leaves hold the sum of its strata
+        F[e] = kp.nstrata > 0 ? KernelEval<T>::eval_sum(kp, pts, d.row_off + P.rs + i, d.col_off + j)
+                              : KernelEval<T>::eval(kp, pts, d.row_off + P.rs + i, d.col_off + j);
       }
     }
   }

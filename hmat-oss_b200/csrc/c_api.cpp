@@ -2,6 +2,7 @@
 // names, argument meaning and 0 / non-zero return convention as c_default_interface.cpp
 // and c_wrapping.hpp) plus the hmat_b200_* extensions declared in include/hmat_b200.h.
 #include <algorithm>
+#include <cmath>
 #include <complex>
 #include <cstdio>
 #include <cstring>
@@ -123,7 +124,7 @@ int assemble_generic(hmat_matrix_t* m, hmat_assemble_context_t* ctx) {
       throw Error("factorization is outside the B200 engine's path");
     if (ctx->simple_compute || ctx->block_compute || ctx->advanced_compute)
       throw Error("host interaction callbacks cannot run on the device; pass hmat_b200_create_assembly() in "
-                  "the 'assembly' field");
+                  "the 'assembly' field (hmat_b200_create_assembly_strata() for a multi-strata kernel)");
     const AssemblyObj* a = (const AssemblyObj*)ctx->assembly;
     if (!a || a->magic != kAssemblyMagic) throw Error("'assembly' is not a descriptor from hmat_b200_create_assembly");
     int method;
@@ -1026,6 +1027,32 @@ void* hmat_b200_create_assembly(const hmat_b200_kernel_t* k, const double* coord
   return a;
 }
 
+void* hmat_b200_create_assembly_strata(const hmat_b200_kernel_t* k, const double* coord, int n, int nstrata,
+                                       const double* param, const double* weight) {
+  if (!k || !coord || n <= 0 || !param || !weight || nstrata < 1 || nstrata > kMaxStrata) {
+    fail("hmat_b200_create_assembly_strata", "bad argument (1 to 8 strata, parameters and weights)");
+    return nullptr;
+  }
+  for (int q = 0; q < nstrata; ++q) {
+    if (k->kind == HMAT_B200_EXP_COV && !(param[q] > 0)) {
+      fail("hmat_b200_create_assembly_strata", "exp_cov strata need correlation lengths > 0");
+      return nullptr;
+    }
+    if (!std::isfinite(param[q]) || !std::isfinite(weight[q])) {
+      fail("hmat_b200_create_assembly_strata", "non-finite stratum parameter or weight");
+      return nullptr;
+    }
+  }
+  hmat_b200_kernel_t k1 = *k;
+  if (k1.kind == HMAT_B200_EXP_COV) k1.ell = param[0];  // the plain kernel's own check
+  AssemblyObj* a = (AssemblyObj*)hmat_b200_create_assembly(&k1, coord, n);
+  if (!a) return nullptr;
+  a->d.kp.ell = k->ell;
+  a->d.strata.assign(param, param + nstrata);
+  a->d.strata.insert(a->d.strata.end(), weight, weight + nstrata);
+  return a;
+}
+
 void hmat_b200_delete_assembly(void* a) {
   AssemblyObj* o = (AssemblyObj*)a;
   if (o && o->magic == kAssemblyMagic) {
@@ -1137,6 +1164,7 @@ int hmat_b200_batch_assemble(hmat_matrix_t* b, void* const* assemblies, const hm
       const int n = b->batch_rows[i + 1] - b->batch_rows[i];
       if ((long long)a->d.pts.size() != 3LL * n) throw Error("member assembly has another point count than its matrix");
       const KernelParams& k = a->d.kp;
+      if (!a->d.strata.empty()) throw Error("multi-strata kernels are not supported in batches");
       if (i == 0) d.kp = k;
       if (k.kind != d.kp.kind) throw Error("the members of a batch must share the kernel kind");
       if (k.nugget != d.kp.nugget) throw Error("the members of a batch must share the covariance nugget");

@@ -208,12 +208,23 @@ __device__ inline cdouble mul_rn(cdouble v, cdouble s) {
 
 enum KernelKind { kLaplaceReg = 0, kExpCov = 1, kHelmholtzReg = 2 };
 
+// Multi-strata kernels (the reference's advanced_compute callbacks with prepare's
+// number_of_strata, hmat.h:552-583): the kernel is the sum of its strata, stratum q being w_q
+// times the kernel with its parameter replaced by a_q (the correlation length of the
+// exponential covariance, with no nugget; the regularisation of the Laplace kernel; the
+// wavenumber of the Helmholtz kernel, whose amplitude keeps delta).  `strata` is a device array
+// a_0 .. a_{nstrata-1}, w_0 .. w_{nstrata-1}; eval_sum() evaluates the sum in stratum order.
+// The ACA of one stratum q runs eval() on the plain kernel with the parameter a_q and nugget 0;
+// w_q multiplies its A factor afterwards.
+constexpr int kMaxStrata = 8;
 struct KernelParams {
   int kind;
   double delta;       // r + delta regularisation
   double ell;         // correlation length
   double nugget;      // diagonal term of the covariance
   double wavenumber;  // Helmholtz k
+  int nstrata = 0;    // 0: a plain kernel
+  const double* strata = nullptr;
 };
 
 // Cluster-ordered coordinates of the row and column points (the same arrays when the
@@ -267,6 +278,19 @@ struct KernelEval<double> {
     if (p.rid[i] == p.cid[j]) v = __dadd_rn(v, k.nugget);
     return v;
   }
+  // The strata summed in order: w (1 / (4 pi (r + a))) or w exp(-r / a), FP64 operations in
+  // the order of the reference's strata callbacks.
+  __device__ static inline double eval_sum(const KernelParams& k, const Points& p, int i, int j) {
+    const double r = dist_fp64(p, i, j);
+    double sum = 0.0;
+    for (int q = 0; q < k.nstrata; ++q) {
+      const double a = k.strata[q], w = k.strata[k.nstrata + q];
+      const double v = k.kind == kLaplaceReg ? __ddiv_rn(1.0, __dmul_rn(HB_FOUR_PI, __dadd_rn(r, a)))
+                                             : exp(__ddiv_rn(-r, a));
+      sum = __dadd_rn(sum, __dmul_rn(w, v));
+    }
+    return sum;
+  }
 };
 
 template <>
@@ -278,6 +302,15 @@ struct KernelEval<float> {
     if (p.rid[i] == p.cid[j]) v += (float)k.nugget;
     return v;
   }
+  __device__ static inline float eval_sum(const KernelParams& k, const Points& p, int i, int j) {
+    const float r = dist_fp32(p, i, j);
+    float sum = 0.0f;
+    for (int q = 0; q < k.nstrata; ++q) {
+      const float a = (float)k.strata[q], w = (float)k.strata[k.nstrata + q];
+      sum += w * (k.kind == kLaplaceReg ? 1.0f / ((float)HB_FOUR_PI * (r + a)) : expf(-r / a));
+    }
+    return sum;
+  }
 };
 
 template <>
@@ -288,6 +321,20 @@ struct KernelEval<cdouble> {
     double sn, cs;
     sincos(__dmul_rn(param_of(p, i, k.wavenumber), r), &sn, &cs);
     return cdouble{cs * s, sn * s};
+  }
+  // w (cos(a r) s), w (sin(a r) s), real and imaginary parts summed in stratum order.
+  __device__ static inline cdouble eval_sum(const KernelParams& k, const Points& p, int i, int j) {
+    const double r = dist_fp64(p, i, j);
+    const double s = __ddiv_rn(1.0, __dmul_rn(HB_FOUR_PI, __dadd_rn(r, k.delta)));
+    double re = 0.0, im = 0.0;
+    for (int q = 0; q < k.nstrata; ++q) {
+      const double w = k.strata[k.nstrata + q];
+      double sn, cs;
+      sincos(__dmul_rn(k.strata[q], r), &sn, &cs);
+      re = __dadd_rn(re, __dmul_rn(w, __dmul_rn(cs, s)));
+      im = __dadd_rn(im, __dmul_rn(w, __dmul_rn(sn, s)));
+    }
+    return cdouble{re, im};
   }
 };
 
@@ -303,6 +350,20 @@ struct KernelEval<cfloat> {
     float sn, cs;
     sincosf(ph, &sn, &cs);
     return cfloat{cs * s, sn * s};
+  }
+  __device__ static inline cfloat eval_sum(const KernelParams& k, const Points& p, int i, int j) {
+    const double r = dist_fp64(p, i, j);
+    const float s = 1.0f / ((float)HB_FOUR_PI * ((float)r + (float)k.delta));
+    float re = 0.0f, im = 0.0f;
+    for (int q = 0; q < k.nstrata; ++q) {
+      const float w = (float)k.strata[k.nstrata + q];
+      const double kr = k.strata[q] * r;
+      float sn, cs;
+      sincosf((float)(kr - 6.283185307179586 * rint(kr * 0.15915494309189535)), &sn, &cs);
+      re += w * (cs * s);
+      im += w * (sn * s);
+    }
+    return cfloat{re, im};
   }
 };
 

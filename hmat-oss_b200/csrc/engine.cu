@@ -53,6 +53,10 @@ struct DevArray {
     alloc(v.size());
     if (n) HB_CUDA(cudaMemcpyAsync(p, v.data(), n * sizeof(X), cudaMemcpyHostToDevice, s));
   }
+  void swap(DevArray& o) {
+    std::swap(p, o.p);
+    std::swap(n, o.n);
+  }
 };
 
 inline long long pad32(long long x) { return (x + 31) & ~31LL; }
@@ -230,14 +234,29 @@ class Engine : public EngineBase {
       gexec_ = nullptr;
     }
     kp_ = a.kp;
+    // a multi-strata kernel: a_0 .. a_{S-1}, w_0 .. w_{S-1}
+    if (a.strata.size() % 2 || a.strata.size() > 2 * (size_t)kMaxStrata)
+      throw Error("multi-strata kernel: 1 to " + std::to_string(kMaxStrata) + " strata");
+    if (!a.strata.empty() && !a.param.empty())
+      throw Error("a multi-strata kernel cannot take per-point parameters");
+    strata_ = a.strata;
+    const int nstrata = (int)strata_.size() / 2;
+    kp_.nstrata = nstrata;
+    kp_.strata = nullptr;
+    if (nstrata) {
+      d_strata_.upload(strata_, stream_);
+      kp_.strata = d_strata_.p;
+    }
+    svd_below_ = svd_below;
     upload_points(a);
     const auto& L = bt_->leaves;
     const int nleaves = (int)L.size();
     piece_loff_.assign(nleaves, -1);
     times_ms[0] = times_ms[1] = times_ms[2] = 0;
 
-    // ---- admissible leaves: ACA / SVD, truncation, compaction into pieces ----
-    assemble_rk(method, eps_aca, eps_trunc, svd_below);
+    // ---- admissible leaves: ACA / SVD, truncation, compaction into pieces (stratum 0 of a
+    // multi-strata kernel) ----
+    assemble_rk(method, eps_aca, eps_trunc, svd_below, nstrata ? 0 : -1);
 
     // ---- final arena (the ranks fix the layout): full leaves evaluated in place, the Rk
     // factors moved from their pieces ----
@@ -261,6 +280,8 @@ class Engine : public EngineBase {
     HB_CUDA(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
     times_ms[0] = ms;
     pieces_.clear();
+    // ---- the further strata, each joined to the factors the leaves hold ----
+    for (int st = 1; st < nstrata; ++st) add_stratum(st, eps_aca, eps_trunc);
     build_plan();
     tune_gemv_plan();
     HB_CUDA(cudaStreamSynchronize(stream_));
@@ -505,33 +526,7 @@ class Engine : public EngineBase {
       run_batch(batch, eps, eps, retry, arena_.p);  // unpacks with the current layout
       if (!retry.empty()) throw Error("re-truncation: unexpected capacity retry");
     }
-    // new arena for the new ranks: the full leaves' panels moved, the re-truncated factors
-    // from their pieces
-    const Layout old = layout_;
-    compute_layout();
-    DevArray<T> na;
-    na.alloc((size_t)(layout_.total + 256));
-    HB_CUDA(cudaMemsetAsync(na.p, 0, (size_t)layout_.total * sizeof(T), stream_));
-    std::vector<CopySeg> segs;
-    for (int i = 0; i < nleaves; ++i) {
-      if (L[i].type != 0 || layout_.first[i] < 0) continue;
-      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
-      for (int b = br.first; b < br.second; ++b)
-        segs.push_back(CopySeg{old.panel[old.first[i] + (b - br.first)], layout_.panel[layout_.first[i] + (b - br.first)],
-                               rblocks_[b].len * L[i].n, 1, 0, 0});
-    }
-    DevArray<CopySeg> d_segs;
-    d_segs.upload(segs, stream_);
-    launch_copy_segments<T>(d_segs.p, (int)segs.size(), arena_.p, na.p, stream_);
-    HB_CUDA(cudaGetLastError());
-    scatter_pieces(na.p);
-    HB_CUDA(cudaStreamSynchronize(stream_));
-    arena_.release();
-    arena_.p = na.p;
-    arena_.n = na.n;
-    na.p = nullptr;
-    na.n = 0;
-    pieces_.clear();
+    rebuild_arena();
     if (gexec_) {
       cudaGraphExecDestroy(gexec_);
       gexec_ = nullptr;
@@ -702,7 +697,9 @@ class Engine : public EngineBase {
     int leaf;
     int kcap;
     bool svd;
-    bool cta = false;  // ACA on the CTA-per-leaf kernel (a retry after a capacity overflow)
+    bool cta = false;   // ACA on the CTA-per-leaf kernel (a retry after a capacity overflow)
+    int kcur = 0;       // a further stratum: the rank the leaf holds in the arena
+    bool pass = false;  // a further stratum: no ACA, the held factors kept as they are
   };
   struct Piece {
     DevArray<T> arena;
@@ -714,9 +711,19 @@ class Engine : public EngineBase {
   // compacted (A as row panels, B transposed) into a new piece.
   // With `src` set, the leaves are already assembled: their factors are unpacked from the
   // arena `src` (rank = kcap) instead of being computed, then truncated at eps_trunc.
-  void run_batch(const std::vector<RkJob>& jobs, double eps_aca, double eps_trunc, std::vector<RkJob>& retry,
-                 const T* src = nullptr) {
+  // With a multi-strata kernel, `stratum` >= 0 is the stratum whose ACA runs (the plain kernel
+  // with the stratum's parameter; A then scaled by its weight).  Stratum 0 is compressed as a
+  // plain kernel; a further stratum (src = the arena) is joined to the factors the leaves hold
+  // (kcur columns): concatenated and truncated, or, once the summed rank reaches min(m, n),
+  // summed as a full block and compressed by SVD, then truncated (compression.cpp:745-773,
+  // rk_matrix.cpp:846-1009).  The dense-SVD jobs compress the sum of the strata.
+  void run_batch(const std::vector<RkJob>& jobs_in, double eps_aca, double eps_trunc, std::vector<RkJob>& retry,
+                 const T* src = nullptr, int stratum = -1) {
     const auto& L = bt_->leaves;
+    std::vector<RkJob> jobs = jobs_in;  // a further stratum turns its dense sums into SVD jobs
+    const bool add_stratum = stratum >= 1;
+    if (add_stratum && !src) throw Error("stratum assembly without the arena");
+    const KernelParams kp_aca = stratum >= 0 ? stratum_kp(stratum) : kp_;
     const int nb = (int)jobs.size();
     std::vector<RkLeafDesc> desc(nb);
     long long ws = 0, fl = 0;
@@ -746,8 +753,9 @@ class Engine : public EngineBase {
       std::stable_sort(v.begin(), v.end(), [&](int x, int y) { return cost(x) > cost(y); });
     };
     const int forced = forced_aca_shape();
-    if (!src) {
+    if (!src || add_stratum) {
       for (int b = 0; b < nb; ++b) {
+        if (jobs[b].pass) continue;
         if (jobs[b].svd)
           svd_order.push_back(b);
         else if (jobs[b].cta)
@@ -873,7 +881,7 @@ class Engine : public EngineBase {
     if (runs.empty()) finish_shapes();
     HB_CUDA(cudaStreamSynchronize(stream_));
 
-    if (src) {
+    if (src && !add_stratum) {
       // rank = kcap: the stored factors, unpacked from their panels
       std::vector<int> k0(nb);
       std::vector<RkStoreDesc> ostore(nb);
@@ -894,10 +902,10 @@ class Engine : public EngineBase {
     auto launch_shape = [&](int shape, const int* order, int count, int* counter, cudaStream_t s) {
       if (count <= 0) return;
       if (shape == kShapeWarp)
-        launch_aca_warp<T>(d_desc.p, order, count, kp_, pts_, eps_aca, d_ws.p, d_ranks.p, d_status.p, counter,
+        launch_aca_warp<T>(d_desc.p, order, count, kp_aca, pts_, eps_aca, d_ws.p, d_ranks.p, d_status.p, counter,
                            max_cap, s);
       else
-        launch_aca<T>(d_desc.p, order, count, kp_, pts_, eps_aca, d_ws.p, d_flags.p, d_ranks.p, d_status.p,
+        launch_aca<T>(d_desc.p, order, count, kp_aca, pts_, eps_aca, d_ws.p, d_flags.p, d_ranks.p, d_status.p,
                       counter, max_cap, aca_concurrency<T>(kShapeThreads[shape], max_cap), s, kShapeThreads[shape]);
       HB_CUDA(cudaGetLastError());
     };
@@ -957,6 +965,7 @@ class Engine : public EngineBase {
     float ms = 0;
     HB_CUDA(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
     times_ms[1] += ms;
+    if (stratum >= 0) join_stratum(stratum, jobs, desc, d_desc, d_ws, d_ranks, h_status, h_ranks, src);
 
     std::vector<int> good;
     int max_k = 1;
@@ -972,7 +981,7 @@ class Engine : public EngineBase {
       }
       if (h_status[b] != kLeafOk)
         throw Error("device compression failed on a leaf (status " + std::to_string(h_status[b]) + ")");
-      if (h_ranks[b] > 0) good.push_back(b);
+      if (h_ranks[b] > 0 && !jobs[b].pass) good.push_back(b);
       max_k = std::max(max_k, h_ranks[b]);
     }
     auto tcost = [&](int b) { return (double)(desc[b].m + desc[b].n) * h_ranks[b] * h_ranks[b]; };
@@ -1172,9 +1181,11 @@ class Engine : public EngineBase {
     HB_CUDA(cudaEventRecord(ev_[4], stream_));
     if (!good.empty()) {
       if (!svd_good.empty()) {
-        // SVD of the dense blocks at the compression epsilon, then the regular truncation
+        // SVD of the dense blocks at the compression epsilon (a stratum's dense sum: at the
+        // low-rank epsilon, truncatedSvd in formattedAddParts), then the regular truncation
         HB_CUDA(cudaMemsetAsync(d_counter.p, 0, sizeof(int), stream_));
-        launch_truncate<T>(d_desc.p, d_svd_good.p, (int)svd_good.size(), eps_aca, d_ws.p, d_ranks.p, d_status.p,
+        launch_truncate<T>(d_desc.p, d_svd_good.p, (int)svd_good.size(), add_stratum ? eps_trunc : eps_aca, d_ws.p,
+                           d_ranks.p, d_status.p,
                            d_counter.p, d_scratch.p, slab, (int)grid, stream_);
         HB_CUDA(cudaGetLastError());
       }
@@ -1274,7 +1285,7 @@ class Engine : public EngineBase {
     pieces_.push_back(std::move(piece));
   }
 
-  void assemble_rk(int method, double eps_aca, double eps_trunc, int svd_below) {
+  void assemble_rk(int method, double eps_aca, double eps_trunc, int svd_below, int stratum) {
     HB_CUDA(set_jacobi_max_sweeps(jacobi_sweeps()));
     (void)method;
     const auto& L = bt_->leaves;
@@ -1312,10 +1323,196 @@ class Engine : public EngineBase {
           bytes += b;
           batch.push_back(queue[pos++]);
         }
-        run_batch(batch, eps_aca, eps_trunc, retry);
+        run_batch(batch, eps_aca, eps_trunc, retry, nullptr, stratum);
       }
       queue.swap(retry);
     }
+  }
+
+  // The plain kernel of stratum s: the stratum's parameter, no nugget (its weight scales A).
+  KernelParams stratum_kp(int s) const {
+    KernelParams k = kp_;
+    k.nstrata = 0;
+    k.strata = nullptr;
+    const double a = strata_[s];
+    if (k.kind == kExpCov) {
+      k.ell = a;
+      k.nugget = 0.0;
+    } else if (k.kind == kLaplaceReg) {
+      k.delta = a;
+    } else {
+      k.wavenumber = a;
+    }
+    return k;
+  }
+
+  // Stratum s after its ACA in run_batch (h_ranks: the stratum's ranks).  Stratum 0: A scaled
+  // by the stratum's weight, in place.  A further stratum: a new workspace whose slot b holds
+  // the factors leaf b holds (kcur columns, unpacked from the arena) followed by the stratum's
+  // (A scaled by its weight); a leaf whose summed rank reaches min(m, n) holds the exact
+  // factorisation of its full block instead and becomes an SVD job; a leaf with no new column
+  // keeps its factors and skips the truncation.  Leaves out of ACA capacity are left for the
+  // retry (their slots hold nothing).
+  void join_stratum(int s, std::vector<RkJob>& jobs, std::vector<RkLeafDesc>& desc, DevArray<RkLeafDesc>& d_desc,
+                    DevArray<T>& d_ws, DevArray<int>& d_ranks, const std::vector<int>& h_status,
+                    std::vector<int>& h_ranks, const T* src) {
+    const int nb = (int)jobs.size();
+    const double w = strata_[kp_.nstrata + s];
+    if (s == 0) {
+      if (w == 1.0) return;
+      std::vector<int> list;
+      for (int b = 0; b < nb; ++b)
+        if (!jobs[b].svd && !jobs[b].pass && h_status[b] == kLeafOk && h_ranks[b] > 0) list.push_back(b);
+      DevArray<int> d_list;
+      d_list.upload(list, stream_);
+      launch_scale_a<T>(d_desc.p, d_list.p, (int)list.size(), d_ranks.p, w, d_ws.p, stream_);
+      HB_CUDA(cudaGetLastError());
+      HB_CUDA(cudaStreamSynchronize(stream_));
+      return;
+    }
+    std::vector<RkLeafDesc> desc2(desc);
+    std::vector<int> kcur(nb, 0), ks(nb, 0), kcat(nb, 0), dense;
+    std::vector<long long> dof;
+    long long ws2 = 0, dsz = 0;
+    for (int b = 0; b < nb; ++b) {
+      const RkLeafDesc& d = desc[b];
+      int cap = 1;
+      if (h_status[b] == kLeafOk) {
+        kcur[b] = jobs[b].kcur;
+        ks[b] = jobs[b].pass ? 0 : h_ranks[b];
+        kcat[b] = kcur[b] + ks[b];
+        cap = std::max(1, kcat[b]);
+        if (ks[b] > 0 && kcat[b] >= std::min(d.m, d.n)) {
+          dense.push_back(b);
+          dof.push_back(dsz);
+          dsz += padded((long long)d.m * d.n);
+        }
+      }
+      desc2[b].kcap = cap;
+      desc2[b].ws_off = ws2;
+      ws2 += pad32(rk_slot_elems(d.m, d.n, cap));
+    }
+    std::vector<RkStoreDesc> ostore(nb);
+    std::vector<PanelDesc> opanels;
+    for (int b = 0; b < nb; ++b)
+      ostore[b] = kcur[b] > 0 ? rk_store(jobs[b].leaf, opanels) : RkStoreDesc{0, 0, 0, 0, 0};
+    DevArray<RkLeafDesc> d_desc2;
+    DevArray<T> ws_new;
+    DevArray<RkStoreDesc> d_ostore;
+    DevArray<PanelDesc> d_opanels;
+    DevArray<int> d_kcur, d_ks, d_kcat, d_dense;
+    DevArray<long long> d_dof;
+    DevArray<T> scratch;
+    d_desc2.upload(desc2, stream_);
+    ws_new.alloc((size_t)std::max(ws2, 1LL));
+    d_ostore.upload(ostore, stream_);
+    d_opanels.upload(opanels, stream_);
+    d_kcur.upload(kcur, stream_);
+    d_ks.upload(ks, stream_);
+    d_kcat.upload(kcat, stream_);
+    d_dense.upload(dense, stream_);
+    d_dof.upload(dof, stream_);
+    launch_unpack<T>(d_desc2.p, nb, d_kcur.p, d_ostore.p, d_opanels.p, src, ws_new.p, stream_);
+    launch_append_factors<T>(d_desc.p, d_desc2.p, nb, d_kcur.p, d_ks.p, w, d_ws.p, ws_new.p, stream_);
+    if (!dense.empty()) {
+      scratch.alloc((size_t)dsz);
+      launch_exact_factors<T>(d_desc2.p, d_dense.p, (int)dense.size(), d_kcur.p, d_kcat.p, d_dof.p, ws_new.p,
+                              scratch.p, stream_);
+    }
+    HB_CUDA(cudaGetLastError());
+    for (int b = 0; b < nb; ++b) {
+      if (h_status[b] != kLeafOk) continue;
+      h_ranks[b] = kcat[b];
+      if (ks[b] == 0) jobs[b].pass = true;  // nothing joined: kept as held
+    }
+    for (int b : dense) {
+      h_ranks[b] = std::min(desc[b].m, desc[b].n);
+      jobs[b].svd = true;
+    }
+    HB_CUDA(cudaMemcpyAsync(d_ranks.p, h_ranks.data(), nb * sizeof(int), cudaMemcpyHostToDevice, stream_));
+    HB_CUDA(cudaStreamSynchronize(stream_));
+    desc.swap(desc2);
+    d_desc.swap(d_desc2);
+    d_ws.swap(ws_new);
+  }
+
+  // Stratum s (>= 1) of a multi-strata kernel joined to the assembled leaves: every admissible
+  // leaf compressed by ACA runs the stratum's ACA (capacity retries as in assemble_rk), the
+  // dense-SVD leaves keep their factors (the SVD compression is not incremental:
+  // compression.hpp:103), then the arena is rebuilt for the new ranks.
+  void add_stratum(int s, double eps_aca, double eps_trunc) {
+    const auto& L = bt_->leaves;
+    const int nleaves = (int)L.size();
+    const int k0 = initial_kcap();
+    std::vector<RkJob> queue;
+    for (int i = 0; i < nleaves; ++i) {
+      if (L[i].type != 1) continue;
+      RkJob j;
+      j.leaf = i;
+      j.svd = false;
+      j.kcur = std::max(0, ranks[i]);
+      if (std::max(L[i].m, L[i].n) < svd_below_) {
+        if (j.kcur == 0) continue;
+        j.pass = true;
+        j.kcap = 1;
+      } else {
+        j.kcap = std::min(std::min(L[i].m, L[i].n), k0);
+      }
+      queue.push_back(j);
+    }
+    piece_of_.assign(nleaves, -1);
+    piece_loff_.assign(nleaves, -1);
+    pieces_.clear();
+    const size_t budget = workspace_budget();
+    while (!queue.empty()) {
+      std::vector<RkJob> retry;
+      size_t pos = 0;
+      while (pos < queue.size()) {
+        std::vector<RkJob> batch;
+        size_t bytes = 0;
+        while (pos < queue.size()) {
+          const RkJob& j = queue[pos];
+          const LeafInfo& l = L[j.leaf];
+          // the stratum's ACA slot and the joined slot
+          size_t b = (size_t)(pad32(rk_slot_elems(l.m, l.n, j.kcap)) + pad32(rk_slot_elems(l.m, l.n, j.kcur + j.kcap))) *
+                         sizeof(T) + l.m + l.n;
+          if (!batch.empty() && bytes + b > budget) break;
+          bytes += b;
+          batch.push_back(queue[pos++]);
+        }
+        run_batch(batch, eps_aca, eps_trunc, retry, arena_.p, s);
+      }
+      queue.swap(retry);
+    }
+    rebuild_arena();
+  }
+
+  // A new arena for new ranks: the full leaves' panels moved from the current one, the Rk
+  // factors from their pieces.
+  void rebuild_arena() {
+    const auto& L = bt_->leaves;
+    const int nleaves = (int)L.size();
+    const Layout old = layout_;
+    compute_layout();
+    DevArray<T> na;
+    na.alloc((size_t)(layout_.total + 256));
+    HB_CUDA(cudaMemsetAsync(na.p, 0, (size_t)layout_.total * sizeof(T), stream_));
+    std::vector<CopySeg> segs;
+    for (int i = 0; i < nleaves; ++i) {
+      if (L[i].type != 0 || layout_.first[i] < 0) continue;
+      auto br = block_range(rblocks_, rstarts_, L[i].row_off, L[i].m);
+      for (int b = br.first; b < br.second; ++b)
+        segs.push_back(CopySeg{old.panel[old.first[i] + (b - br.first)], layout_.panel[layout_.first[i] + (b - br.first)],
+                               rblocks_[b].len * L[i].n, 1, 0, 0});
+    }
+    DevArray<CopySeg> d_segs;
+    d_segs.upload(segs, stream_);
+    launch_copy_segments<T>(d_segs.p, (int)segs.size(), arena_.p, na.p, stream_);
+    HB_CUDA(cudaGetLastError());
+    scatter_pieces(na.p);
+    HB_CUDA(cudaStreamSynchronize(stream_));
+    arena_.swap(na);
+    pieces_.clear();
   }
 
   // ------------------------------------------------------------------------------
@@ -2182,6 +2379,9 @@ class Engine : public EngineBase {
   cudaEvent_t fork_[2 * kAcaShapes];
   cudaEvent_t tune_ev_[2 * kTuneRuns];  // brackets of the autotuner's sample runs
   KernelParams kp_{};
+  std::vector<double> strata_;  // a multi-strata kernel: a_0 .. a_{S-1}, w_0 .. w_{S-1}
+  DevArray<double> d_strata_;
+  int svd_below_ = 0;
   Points pts_{};
   DevArray<double> d_pts_;
   DevArray<double> d_prm_;  // per-point kernel parameter (cluster order), when the points carry one

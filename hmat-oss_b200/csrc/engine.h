@@ -24,6 +24,9 @@ struct AssemblyDesc {
   // regularisation of the Laplace kernels, the Helmholtz wavenumber).  Batches of independent
   // matrices with their own kernels use it: a block's rows and columns belong to one matrix.
   std::vector<double> param;
+  // Optional multi-strata kernel: a_0 .. a_{S-1} then w_0 .. w_{S-1} (stratum q is w_q times
+  // the kernel with its parameter set to a_q); empty for a plain kernel.
+  std::vector<double> strata;
 };
 
 struct LeafGrad;

@@ -92,6 +92,21 @@ template <typename T>
 void launch_dense_to_rk(const RkLeafDesc* d_leaves, const int* d_order, int nleaves, const KernelParams& kp,
                         Points pts, T* ws, int* ranks, int* status, cudaStream_t s);
 
+// Multi-strata assembly (strata.cu): A[:, 0 .. rank) *= w in the slots of the leaves in order;
+// the ks[b] columns of a stratum's factors (slot b of src, A scaled by w) appended after the
+// kcur[b] columns of slot b of dst; the full block A B^T of the kcat[b] columns of the leaves in
+// order (kcur[b] and the rest summed separately) written back as its exact rank-min(m, n)
+// factorisation, through scratch (m x n at dof[item]).
+template <typename T>
+void launch_scale_a(const RkLeafDesc* d_leaves, const int* d_order, int count, const int* ranks, double w, T* ws,
+                    cudaStream_t s);
+template <typename T>
+void launch_append_factors(const RkLeafDesc* src_desc, const RkLeafDesc* dst_desc, int nb, const int* kcur,
+                           const int* ks, double w, const T* src, T* dst, cudaStream_t s);
+template <typename T>
+void launch_exact_factors(const RkLeafDesc* d_leaves, const int* d_order, int count, const int* kcur,
+                          const int* kcat, const long long* dof, T* ws, T* scratch, cudaStream_t s);
+
 // Truncation (rk_matrix.cpp:490-585): replaces A, B in each slot by the recompressed
 // factors (first new-rank columns, same slot) and rewrites ranks.  `scratch` holds
 // `grid` per-CTA FP64 slabs of `slab_elems` wide elements each.

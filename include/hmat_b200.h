@@ -368,6 +368,17 @@ typedef struct {
 /* Assembly descriptor for hmat_assemble_context_t.assembly: kernel + the points it is
  * evaluated on (client numbering, point-major xyz, copied).  NULL on bad input. */
 void* hmat_b200_create_assembly(const hmat_b200_kernel_t* kernel, const double* coord, int n_points);
+/* Assembly descriptor of a multi-strata kernel: the sum of `nstrata` (1 to 8) strata, stratum q
+ * being weight[q] times `kernel` with its parameter replaced by param[q] (the correlation length
+ * of the exponential covariance, without the nugget; the regularisation delta of the Laplace
+ * kernel; the wavenumber of the Helmholtz kernel, whose amplitude keeps kernel->delta).  It
+ * replaces the reference's advanced_compute callback with prepare() setting number_of_strata
+ * (hmat.h:552-583): admissible blocks compressed by ACA+ or partial ACA are compressed stratum
+ * by stratum, each further stratum added to the truncated sum as compress() does
+ * (compression.cpp:745-773, RkMatrix::formattedAddParts rk_matrix.cpp:846-1009); full blocks
+ * and the dense-SVD compression of small blocks take the sum.  NULL on bad input. */
+void* hmat_b200_create_assembly_strata(const hmat_b200_kernel_t* kernel, const double* coord, int n_points,
+                                       int nstrata, const double* param, const double* weight);
 void hmat_b200_delete_assembly(void* assembly);
 
 /* gemv on device buffers (x, y column-major, client numbering, leading dimension = the

@@ -141,3 +141,28 @@ def test_gemv_status_rejects_bad_arguments(hb):
         lib.hmat_b200_clear_last_error()
     finally:
         h.close()
+
+
+def test_bad_strata_descriptors(hb):
+    """hmat_b200_create_assembly_strata: 1 to 8 strata, positive exp-cov lengths, finite values."""
+    lib = hb.load_library()
+    pts = np.zeros((10, 3))
+    k = hb.kernel(hb.EXP_COV)
+    par = np.array([0.1, 0.3, 1.0, 0.2, 0.2, 0.2, 0.2, 0.2, 0.2])
+    w = np.ones(9)
+    ok = lib.hmat_b200_create_assembly_strata(C.byref(k), pts.ctypes.data, 10, 3, par.ctypes.data, w.ctypes.data)
+    assert ok
+    lib.hmat_b200_delete_assembly(ok)
+    for n in (0, 9):
+        assert not lib.hmat_b200_create_assembly_strata(C.byref(k), pts.ctypes.data, 10, n, par.ctypes.data,
+                                                        w.ctypes.data)
+    neg = np.array([0.1, -0.3])
+    assert not lib.hmat_b200_create_assembly_strata(C.byref(k), pts.ctypes.data, 10, 2, neg.ctypes.data,
+                                                    w.ctypes.data)
+    assert b"correlation" in lib.hmat_b200_last_error()
+    inf = np.array([1.0, np.inf])
+    lap = hb.kernel(hb.LAPLACE_REG)
+    assert not lib.hmat_b200_create_assembly_strata(C.byref(lap), pts.ctypes.data, 10, 2, par.ctypes.data,
+                                                    inf.ctypes.data)
+    with pytest.raises(ValueError):
+        hb.kernel(hb.EXP_COV, strata_param=[0.1, 0.2], strata_weight=[1.0])
