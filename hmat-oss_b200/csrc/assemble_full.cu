@@ -70,16 +70,24 @@ void launch_full_from_canonical(const FullLeafDesc* d_leaves, const long long* g
 }
 
 // Segmented copy between two device buffers (relayout of stored leaves): segment g copies a
-// rows x cols column-major block.  A CTA per segment, threads over elements.
+// rows x cols column-major block (fewer than 2^31 elements).  A CTA per segment, threads over
+// elements: contiguous runs (cols = 1, or both leading dimensions equal to rows) as one flat
+// copy, other blocks with 32-bit index arithmetic.
 template <typename T>
 __global__ void __launch_bounds__(256) copy_segments_kernel(const CopySeg* __restrict__ segs, int nseg,
                                                             const T* __restrict__ src, T* __restrict__ dst) {
   for (int g = blockIdx.x; g < nseg; g += gridDim.x) {
     const CopySeg c = segs[g];
-    const long long count = (long long)c.rows * c.cols;
-    for (long long e = threadIdx.x; e < count; e += blockDim.x) {
-      const long long r = e % c.rows, q = e / c.rows;
-      dst[c.dst + r + q * c.dst_ld] = src[c.src + r + q * c.src_ld];
+    const T* s = src + c.src;
+    T* d = dst + c.dst;
+    const int count = c.rows * c.cols;
+    if (c.cols == 1 || (c.src_ld == c.rows && c.dst_ld == c.rows)) {
+      for (int e = threadIdx.x; e < count; e += blockDim.x) d[e] = s[e];
+    } else {
+      for (int e = threadIdx.x; e < count; e += blockDim.x) {
+        const int q = e / c.rows, r = e - q * c.rows;
+        d[r + (long long)q * c.dst_ld] = s[r + (long long)q * c.src_ld];
+      }
     }
   }
 }

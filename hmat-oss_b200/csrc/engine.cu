@@ -118,6 +118,13 @@ std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
 // height class of the output blocks).
 std::map<std::tuple<int, int, int, int>, std::pair<int, bool>> g_gemv_tune_cache;
 
+// HMAT_B200_GEMV_HALF_WARP_MAP=1 keeps the half-warp lane map (two column slices, 4 rows a lane)
+// for the FP64 and complex output blocks of 33 to 64 rows, in place of lanes over rows.
+bool gemv_half_warp_map() {
+  const char* s = getenv("HMAT_B200_GEMV_HALF_WARP_MAP");
+  return s && s[0] == '1';
+}
+
 // Bound of each gemv kernel's wait for a bulk copy (polls of the stage barrier).
 // HMAT_B200_GEMV_WAIT_LIMIT changes it for the matrices created while it is set; a negative
 // value makes every wait give up at once (a test hook: the kernels flag the product, let
@@ -274,10 +281,10 @@ class Engine : public EngineBase {
     launch_assemble_full<T>(d_fd.p, (int)fd.size(), d_fp.p, kp_, pts_, arena_.p, stream_);
     HB_CUDA(cudaGetLastError());
     HB_CUDA(cudaEventRecord(ev_[1], stream_));
-    scatter_pieces(arena_.p);
     HB_CUDA(cudaStreamSynchronize(stream_));
     float ms = 0;
     HB_CUDA(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
+    scatter_pieces(arena_.p, &ms);  // the compressed leaves placed in the arena, timed with them
     times_ms[0] = ms;
     pieces_.clear();
     // ---- the further strata, each joined to the factors the leaves hold ----
@@ -1484,12 +1491,14 @@ class Engine : public EngineBase {
       }
       queue.swap(retry);
     }
-    rebuild_arena();
+    float ms = 0;
+    rebuild_arena(&ms);
+    times_ms[0] += ms;
   }
 
   // A new arena for new ranks: the full leaves' panels moved from the current one, the Rk
-  // factors from their pieces.
-  void rebuild_arena() {
+  // factors from their pieces (with `timed`, the device time of the placement added to it).
+  void rebuild_arena(float* timed = nullptr) {
     const auto& L = bt_->leaves;
     const int nleaves = (int)L.size();
     const Layout old = layout_;
@@ -1509,8 +1518,7 @@ class Engine : public EngineBase {
     d_segs.upload(segs, stream_);
     launch_copy_segments<T>(d_segs.p, (int)segs.size(), arena_.p, na.p, stream_);
     HB_CUDA(cudaGetLastError());
-    scatter_pieces(na.p);
-    HB_CUDA(cudaStreamSynchronize(stream_));
+    scatter_pieces(na.p, timed);
     arena_.swap(na);
     pieces_.clear();
   }
@@ -1662,7 +1670,8 @@ class Engine : public EngineBase {
 
   // The compacted factors of every piece (A row panels, then B^T, per leaf at piece_loff_)
   // into their places in `dst` (laid out by layout_).
-  void scatter_pieces(T* dst) {
+  // With `timed`, the device time of the copies is added to *timed (ms).
+  void scatter_pieces(T* dst, float* timed = nullptr) {
     const auto& L = bt_->leaves;
     std::vector<std::vector<CopySeg>> segs(pieces_.size());
     for (int i = 0; i < (int)L.size(); ++i) {
@@ -1679,12 +1688,19 @@ class Engine : public EngineBase {
       segs[piece_of_[i]].push_back(CopySeg{p, layout_.bt[i], k, L[i].n, k, layout_.bt_ld[i]});
     }
     std::vector<DevArray<CopySeg>> d_segs(pieces_.size());
+    for (size_t q = 0; q < pieces_.size(); ++q) d_segs[q].upload(segs[q], stream_);
+    if (timed) HB_CUDA(cudaEventRecord(ev_[2], stream_));
     for (size_t q = 0; q < pieces_.size(); ++q) {
-      d_segs[q].upload(segs[q], stream_);
       launch_copy_segments<T>(d_segs[q].p, (int)segs[q].size(), pieces_[q].arena.p, dst, stream_);
       HB_CUDA(cudaGetLastError());
     }
+    if (timed) HB_CUDA(cudaEventRecord(ev_[3], stream_));
     HB_CUDA(cudaStreamSynchronize(stream_));
+    if (timed) {
+      float ms = 0;
+      HB_CUDA(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
+      *timed += ms;
+    }
   }
 
   // ------------------------------------------------------------------------------
@@ -1846,7 +1862,10 @@ class Engine : public EngineBase {
       L.rpt = tiles <= 8 ? tiles : 16;
       return;
     }
-    L.map = omax <= 32 ? 2 : (omax <= 64 ? 1 : 0);
+    // up to 32 rows: column-slice windows, 2 rows a lane; up to 64: lanes over rows, 2 rows a
+    // lane (map 5: half the accumulators of the half-warp map 1, so twice the resident warps
+    // with 16 FP64 right-hand sides); above: lanes over rows, 4 rows a lane
+    L.map = omax <= 32 ? 2 : (omax <= 64 ? (gemv_half_warp_map() ? 1 : 5) : 0);
     L.rpt = omax <= 32 ? 2 : 4;
   }
 
@@ -1880,7 +1899,7 @@ class Engine : public EngineBase {
       if (tasks[t].first_unit != tasks[t - 1].first_unit + tasks[t - 1].nunits)
         throw Error("gemv plan: units of a launch are not contiguous");
     const int omax = L.map == 4       ? 128
-                     : L.warp_level ? (L.map == 3 ? 8 * L.rpt : (L.map == 2 ? 32 : (L.map == 1 ? 64 : 128)))
+                     : L.warp_level ? (L.map == 3 ? 8 * L.rpt : (L.map == 2 ? 32 : (L.map == 1 || L.map == 5 ? 64 : 128)))
                                     : ol * rpt;
     for (auto& t : tasks)
       if (t.O > omax) throw Error("gemv plan: task taller than its launch shape");

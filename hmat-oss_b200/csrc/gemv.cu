@@ -457,6 +457,11 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
                        const GemvUnit* __restrict__ units, const T* __restrict__ arena, T* xz, GemvStatus* err) {
   using Ops = RowOps<T, R>;
   constexpr int OL = MODE == 0 ? 32 : 16;
+  // MODE 2: right-hand sides per round of the slice sums (a power of two)
+  constexpr int QC0 = warp_piece_bytes((int)sizeof(T)) / (32 * A2 * (int)sizeof(T));
+  constexpr int QC1 = QC0 >= 16 ? 16 : (QC0 >= 8 ? 8 : (QC0 >= 4 ? 4 : (QC0 >= 2 ? 2 : 1)));
+  constexpr int QC = QC1 < R ? QC1 : R;
+  static_assert(QC >= 1 && (R % QC) == 0, "reduction chunk");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char* wbase = smem_raw + (size_t)warp * kWarpStages * warp_stage_bytes((int)sizeof(T));
@@ -568,10 +573,6 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
     if constexpr (MODE == 2) {
       // slices summed in slice order through the stage just consumed, QC right-hand sides
       // per round: lane's partial of (its row a, q) at sc[(lane * A2 + a) * QC + q - q0]
-      constexpr int QC0 = warp_piece_bytes((int)sizeof(T)) / (32 * A2 * (int)sizeof(T));
-      constexpr int QC1 = QC0 >= 16 ? 16 : (QC0 >= 8 ? 8 : (QC0 >= 4 ? 4 : (QC0 >= 2 ? 2 : 1)));  // power of two
-      constexpr int QC = QC1 < R ? QC1 : R;
-      static_assert(QC >= 1 && (R % QC) == 0, "reduction chunk");
       T* sc = reinterpret_cast<T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)));
       if (task.nunits > 0) {
 #pragma unroll
@@ -1178,6 +1179,8 @@ void launch_stream(const GemvLaunch& L, const GemvUnit* units, const T* arena, T
     }
     if (L.map == 2)
       launch_warp_t<T, R, RS, 2, 2>(L, units, arena, xz, err, s);
+    else if (L.map == 5)
+      launch_warp_t<T, R, RS, 0, 2>(L, units, arena, xz, err, s);
     else if (L.map == 1)
       launch_warp_t<T, R, RS, 1, 4>(L, units, arena, xz, err, s);
     else

@@ -490,8 +490,9 @@ int hmat_b200_gemv_profile(hmat_matrix_t* hmatrix, char trans, const void* x_dev
  * (with hmat_b200_last_error set) on error.  No counterpart in the reference. */
 int hmat_b200_gemv_launches(hmat_matrix_t* hmatrix, char trans, int nrhs);
 
-/* Device time of the last phases on this matrix, milliseconds: [0] full assembly,
- * [1] ACA, [2] truncation (+ compaction), [3] last gemv. */
+/* Device time of the last phases on this matrix, milliseconds: [0] full leaves and the
+ * placement of the compressed leaves in the product's layout, [1] ACA, [2] truncation (+
+ * compaction), [3] last gemv. */
 int hmat_b200_phase_times(hmat_matrix_t* hmatrix, double* out4);
 
 /* ACA autotuner report of the last assembly, per leaf-size bucket b (0: m, n <= 64; 1: m + n
