@@ -386,6 +386,28 @@ class HMatrix:
             raise HMatError(err.decode())
         return st, b"".join(chunks)
 
+    def read_data(self, data_stream: bytes):
+        """The leaves of a data stream (hmat_interface_t.write_data of this library or of the
+        reference: both write the reference's data format) into this matrix, which must have
+        the writer's partition: hmat_interface_t.read_data.  The matrix is then assembled."""
+        pos, short = [0], []
+
+        def rd(buf, n, ud):
+            if n == 0:
+                return
+            take = data_stream[pos[0]:pos[0] + n]
+            pos[0] += n
+            if len(take) < n:
+                short.append(n)
+                take = take + bytes(n - len(take))
+            C.memmove(buf, take, n)
+        self.lib.hmat_b200_clear_last_error()
+        self.hi.fn("read_data")(self.m, _IOSTREAM(rd), None)
+        err = self.lib.hmat_b200_last_error()
+        if err or short or pos[0] != len(data_stream):
+            raise HMatError((err.decode() if err else "") + (" (stream too short)" if short else "") +
+                            (" (stream longer than the matrix's leaves)" if pos[0] < len(data_stream) else ""))
+
     @classmethod
     def load(cls, value_type: int, struct_stream: bytes, data_stream: bytes) -> "HMatrix":
         """A matrix read back with read_struct and read_data (no clustering, no assembly)."""

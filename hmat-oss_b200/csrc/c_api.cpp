@@ -546,18 +546,26 @@ int u_solve_lower_dense(hmat_matrix_t*, int, void*, int) { return unsupported("s
 int u_walk(hmat_matrix_t*, hmat_procedure_t*) { return unsupported("walk"); }
 int u_apply_on_leaf(hmat_matrix_t*, const hmat_leaf_procedure_t*) { return unsupported("apply_on_leaf"); }
 // ---- write_struct / read_struct / write_data / read_data (c_wrapping.hpp:921-946) ----
-// This library's own stream format (native byte order), through the caller's hmat_iostream:
+// Structure: this library's own stream format (native byte order), through the caller's
+// hmat_iostream (the reference's structure stream carries its internal node tree and the
+// cluster data classes, so structure streams are not exchangeable):
 //   struct: "HB2S", version, value type, rows tree, cols-tree flag (0: same as rows) [+ cols
 //           tree], leaf count, leaves (row node, col node, row offset, m, col offset, n, type),
-//           number of block clusters, low-rank epsilon
+//           number of block clusters, low-rank epsilon, end mark "HB2E"
 //   tree:   n, points (3 n doubles, client numbering), permutation (internal -> client),
 //           node count, nodes (offset, size, children, child count, depth, bounding box),
 //           tree-leaf count, tree leaves
-//   data:   "HB2D", version, value type, leaf count, ranks (-1 for full leaves), scalar
-//           count, the canonical payload of every leaf (full m x n; Rk A m x k then B n x k;
-//           column-major, leaf order)
-// Both end with the mark "HB2E".
-// The reference's own format carries its internal node tree; streams are not exchangeable.
+// Data: the reference's own data stream (MatrixDataMarshaller / MatrixDataUnmarshaller,
+// serialization.cpp:248-309 and 318-394), so that a matrix written by one library loads into
+// a matrix of the same partition built by the other: the non-empty leaves in depth-first order
+// (the leaf table's order), each as
+//   Rk leaf:   int rank; if rank > 0: A (m x k) then B (n x k), column-major scalars of the
+//              matrix's type, then the orthogonality flags of A and B (two ints, written 0)
+//   full leaf: int header (bit 0: null block, no data; bit 1: pivots; bit 2: diagonal: the
+//              factorised forms, refused here), then F (m x n, column-major)
+// The data stream has no header of its own: a matrix whose partition differs from the writer's
+// reads garbage, which the reader refuses where it can (ranks outside [0, min(m, n)], unknown
+// headers, a stream cut short).
 const int kStreamVersion = 1;
 struct StreamOut {
   hmat_iostream f;
@@ -733,25 +741,24 @@ void c_write_data(hmat_matrix_t* m, hmat_iostream f, void* ud) {
     EngineBase& e = engine_of(m);
     if (!e.assembled) throw Error("write_data needs an assembled matrix");
     const int nl = (int)m->bt.leaves.size();
-    long long total = 0;
-    e.payload_layout(nullptr, &total);
     StreamOut o{f, ud};
-    write_magic(o, 'D');
-    o.val<int>(VT);
-    o.val<int>(nl);
-    o.bytes(e.ranks.data(), (size_t)nl * sizeof(int));
-    o.val<long long>(total);
     std::vector<S> buf;
     for (int i = 0; i < nl; ++i) {
       const LeafInfo& l = m->bt.leaves[i];
-      const int k = e.ranks[i];
-      const size_t size = l.type == 0 ? (size_t)l.m * l.n : (k > 0 ? (size_t)k * (l.m + l.n) : 0);
-      if (!size) continue;
-      buf.resize(size);
-      e.leaf_payload(i, buf.data());
-      o.bytes(buf.data(), size * sizeof(S));
+      if (l.m == 0 || l.n == 0) continue;  // void blocks are not written (serialization.cpp:293-296)
+      const int k = l.type == 0 ? 0 : std::max(e.ranks[i], 0);
+      o.val<int>(l.type == 0 ? 0 : k);
+      const size_t size = l.type == 0 ? (size_t)l.m * l.n : (size_t)k * (l.m + l.n);
+      if (size) {
+        buf.resize(size);
+        e.leaf_payload(i, buf.data());
+        o.bytes(buf.data(), size * sizeof(S));
+      }
+      if (l.type == 1 && k > 0) {
+        o.val<int>(0);
+        o.val<int>(0);
+      }
     }
-    write_end(o);
   } catch (const std::exception& ex) {
     fail("write_data", ex.what());
   }
@@ -764,23 +771,41 @@ void c_read_data(hmat_matrix_t* m, hmat_iostream f, void* ud) {
     if (!m || !f) throw Error("null argument");
     if (m->vt != VT) throw Error("matrix value type does not match this interface");
     StreamIn in{f, ud};
-    read_magic(in, 'D');
-    if (in.val<int>() != VT) throw Error("Type mismatch between the stream and this interface");
-    const int nl = in.val<int>();
-    if (nl != (int)m->bt.leaves.size()) throw Error("stream and matrix have different leaves");
-    std::vector<int> rk(nl);
-    in.bytes(rk.data(), (size_t)nl * sizeof(int));
-    long long total = in.val<long long>();
-    long long want = 0;
+    const int nl = (int)m->bt.leaves.size();
+    std::vector<int> rk(nl, 0);
+    std::vector<S> payload;
     for (int i = 0; i < nl; ++i) {
       const LeafInfo& l = m->bt.leaves[i];
-      if (l.type == 0) want += (long long)l.m * l.n;
-      else if (rk[i] > 0) want += (long long)rk[i] * (l.m + l.n);
+      if (l.m == 0 || l.n == 0) {
+        rk[i] = l.type == 0 ? -1 : 0;
+        continue;
+      }
+      const int header = in.val<int>();
+      if (l.type == 1) {
+        if (header < 0 || header > std::min(l.m, l.n))
+          throw Error("corrupt stream or another partition (Rk leaf " + std::to_string(i) + " with rank " +
+                      std::to_string(header) + ")");
+        rk[i] = header;
+        if (header > 0) {
+          const size_t at = payload.size(), size = (size_t)header * (l.m + l.n);
+          payload.resize(at + size);
+          in.bytes(payload.data() + at, size * sizeof(S));
+          in.val<int>();  // orthogonality of A and B: not used by this library
+          in.val<int>();
+        }
+      } else {
+        rk[i] = -1;
+        if (header & ~7) throw Error("corrupt stream or another partition (full leaf " + std::to_string(i) + ")");
+        if (header & 6) throw Error("factorised full blocks (pivots or diagonal) are outside the B200 engine");
+        const size_t at = payload.size(), size = (size_t)l.m * l.n;
+        payload.resize(at + size, S(0));
+        if (!(header & 1)) in.bytes(payload.data() + at, size * sizeof(S));  // bit 0: a null block
+      }
     }
-    if (total != want) throw Error("corrupt stream (payload size)");
-    std::vector<S> payload((size_t)std::max(total, 1LL));
-    in.bytes(payload.data(), (size_t)total * sizeof(S));
-    read_end(in);
+    // the reference's reader ends with a read of 0 bytes (serialization.cpp:390-391)
+    S dummy;
+    f(&dummy, 0, ud);
+    payload.resize(std::max<size_t>(payload.size(), 1));
     engine_of(m).load_leaves(rk.data(), payload.data());
   } catch (const std::exception& e) {
     fail("read_data", e.what());

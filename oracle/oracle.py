@@ -186,10 +186,14 @@ def have_reference():
 
 def run_reference(points, kind, eps, leaf=64, eta=2.0, delta=0.01, ell=0.3, nugget=0.0, wavenumber=0.0, x=None,
                   nrhs=1, trans="N", scalar="D", dump_factors=False, gemv_reps=1, min_leaf=0, leaf_cols=0,
-                  gemv_warmup=0, retrunc=0.0, strata_param=None, strata_weight=None):
+                  gemv_warmup=0, retrunc=0.0, strata_param=None, strata_weight=None, read_data=None,
+                  write_data=None):
     """Runs the reference library (oracle/_ref/ref_driver) and returns its outputs.  With
     strata_param / strata_weight, the matrix is assembled through advanced_compute with one
-    stratum per entry (w_s times the kernel with parameter a_s: ell, delta or wavenumber)."""
+    stratum per entry (w_s times the kernel with parameter a_s: ell, delta or wavenumber).
+    read_data (bytes): the leaves are read from that data stream (hmat_interface_t.read_data)
+    into the matrix built on the points instead of being assembled; write_data=True returns the
+    assembled matrix's data stream (hmat_interface_t.write_data) as out["data"]."""
     if not have_reference():
         raise FileNotFoundError(REF_DRIVER)
     kname = {0: "laplace", 1: "expcov", 2: "helmholtz"}[kind]
@@ -202,6 +206,13 @@ def run_reference(points, kind, eps, leaf=64, eta=2.0, delta=0.01, ell=0.3, nugg
                  f"gemv_reps={gemv_reps}", f"gemv_warmup={gemv_warmup}", f"min_leaf={min_leaf}",
                  f"leaf_cols={leaf_cols}", f"retrunc={retrunc!r}",
                  f"out={os.path.join(d, 'out')}"]
+        if read_data is not None:
+            rp = os.path.join(d, "data_in.bin")
+            with open(rp, "wb") as f:
+                f.write(read_data)
+            lines.append(f"read_data={rp}")
+        if write_data:
+            lines.append(f"write_data={os.path.join(d, 'data_out.bin')}")
         if strata_param is not None:
             lines.append("strata_param=" + ",".join(repr(float(a)) for a in strata_param))
             lines.append("strata_weight=" + ",".join(repr(float(w)) for w in strata_weight))
@@ -225,4 +236,7 @@ def run_reference(points, kind, eps, leaf=64, eta=2.0, delta=0.01, ell=0.3, nugg
             out["y"] = np.fromfile(os.path.join(d, "out.y"), dt).reshape(x.shape, order="F")
         if dump_factors:
             out["payload"] = np.fromfile(os.path.join(d, "out.payload"), dt)
+        if write_data:
+            with open(os.path.join(d, "data_out.bin"), "rb") as f:
+                out["data"] = f.read()
         return out

@@ -34,6 +34,27 @@
 
 namespace {
 
+// hmat_iostream over a byte buffer (write_data appends, read_data consumes in order).
+struct StreamBuf {
+  std::vector<char> bytes;
+  size_t pos = 0;
+  bool overrun = false;
+};
+void stream_write(void* buf, size_t n, void* ud) {
+  StreamBuf* s = (StreamBuf*)ud;
+  s->bytes.insert(s->bytes.end(), (const char*)buf, (const char*)buf + n);
+}
+void stream_read(void* buf, size_t n, void* ud) {
+  StreamBuf* s = (StreamBuf*)ud;
+  if (s->pos + n > s->bytes.size()) {
+    s->overrun = true;
+    memset(buf, 0, n);
+    return;
+  }
+  memcpy(buf, s->bytes.data() + s->pos, n);
+  s->pos += n;
+}
+
 struct Params {
   std::map<std::string, std::string> kv;
   std::string get(const std::string& k, const std::string& d = "") const {
@@ -320,7 +341,22 @@ int run(const Params& p, hmat_value_t vt) {
   ctx.lower_symmetric = 0;
   ctx.factorization = hmat_factorization_none;
   t0 = now_s();
-  int rc = hi.assemble_generic(M, &ctx);
+  int rc = 0;
+  const std::string data_in = p.get("read_data");
+  if (!data_in.empty()) {
+    // the leaves from a data stream (write_data of this library or of another one) instead of
+    // an assembly: hmat_interface_t.read_data into the matrix just built
+    StreamBuf sb;
+    sb.bytes = read_file(data_in);
+    hi.read_data(M, stream_read, &sb);
+    if (sb.pos != sb.bytes.size() || sb.overrun) {
+      fprintf(stderr, "read_data consumed %zu of %zu bytes%s\n", sb.pos, sb.bytes.size(),
+              sb.overrun ? " and asked for more" : "");
+      return 3;
+    }
+  } else {
+    rc = hi.assemble_generic(M, &ctx);
+  }
   double t_assemble = now_s() - t0;
   if (rc) {
     fprintf(stderr, "assemble_generic failed\n");
@@ -335,6 +371,14 @@ int run(const Params& p, hmat_value_t vt) {
       fprintf(stderr, "truncate failed\n");
       return 4;
     }
+  }
+
+  // optional data stream of the assembled matrix (hmat_interface_t.write_data)
+  const std::string data_out = p.get("write_data");
+  if (!data_out.empty()) {
+    StreamBuf sb;
+    hi.write_data(M, stream_write, &sb);
+    write_file(data_out, sb.bytes.data(), sb.bytes.size());
   }
 
   // Cluster permutation (internal -> client).

@@ -10,7 +10,8 @@ then B n x k, column-major, leaf order), so that autograd returns dL/dtheta besi
 
 Finite differences perturb one entry of x, or one stored entry of a full leaf, of A or of B,
 by +-1e-6: a perturbed matrix is the original written with write_struct / write_data, the entry
-changed in the data stream, and read back with read_struct / read_data.
+changed in the data stream (the reference's data layout), and read back with read_struct /
+read_data.
 
 The reference's transposed gemv (RkMatrix::gemv 'T', rk_matrix.cpp:156-206, reached through
 HMatrix::gemv and getChildForGEMM, h_matrix.cpp:772-857) is the golden y_T = H^T x_g of the
@@ -100,15 +101,30 @@ def _loss(hb, h, x, b):
     return 0.5 * float(np.sum((y - b) ** 2))
 
 
+def _stream_offset(h, pos):
+    """Byte offset in the data stream (the reference's layout: per leaf a header int, its
+    entries, and two ints after the factors of an Rk leaf of rank > 0) of canonical payload
+    entry `pos`."""
+    offs, _ = h.payload_layout()
+    T = h.leaf_table()
+    s = np.dtype(h.dtype).itemsize
+    at = 0
+    for i, (r0, m, c0, n, t, k) in enumerate(T):
+        size = m * n if t == 0 else max(k, 0) * (m + n)
+        if offs[i] <= pos < offs[i] + size:
+            return at + 4 + (pos - offs[i]) * s
+        at += 4 + size * s + (8 if t == 1 and k > 0 else 0)
+    raise IndexError(pos)
+
+
 def _perturbed(hb, h, pos, delta):
     """The matrix with canonical payload entry `pos` changed by delta (through the streams)."""
     st, data = h.dump()
-    nl = len(h.leaf_table())
     s = np.dtype(h.dtype).itemsize
-    start = 24 + 4 * nl  # magic, version, value type, leaf count, ranks, scalar count
+    at = _stream_offset(h, pos)
     buf = bytearray(data)
-    v = np.frombuffer(bytes(buf[start + pos * s:start + (pos + 1) * s]), dtype=h.dtype)[0]
-    buf[start + pos * s:start + (pos + 1) * s] = np.array([v + delta], dtype=h.dtype).tobytes()
+    v = np.frombuffer(bytes(buf[at:at + s]), dtype=h.dtype)[0]
+    buf[at:at + s] = np.array([v + delta], dtype=h.dtype).tobytes()
     return hb.HMatrix.load(h.value_type, st, bytes(buf))
 
 

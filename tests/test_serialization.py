@@ -1,6 +1,9 @@
 """write_struct / read_struct / write_data / read_data (the reference's checkpoint entries,
-c_wrapping.hpp:921-946) on this library's own stream format: a matrix written and read
-back has the same cluster trees, leaves and products, without re-assembly."""
+c_wrapping.hpp:921-946): a matrix written and read back has the same cluster trees, leaves and
+products, without re-assembly.  The structure stream is this library's own format; the data
+stream is the reference's (MatrixDataMarshaller, serialization.cpp:248-309): the non-empty
+leaves in depth-first order, an Rk leaf as its rank, A, B and two orthogonality ints, a full
+leaf as a header int and its entries."""
 import ctypes as C
 
 import numpy as np
@@ -68,7 +71,16 @@ def test_checkpoint_round_trip(hb, name, vt):
     h, x = _build(hb, name, vt)
     try:
         st, data = h.dump()
-        assert data[:4] == b"HB2D"
+        # the reference's data layout, leaf by leaf
+        T = h.leaf_table()
+        sz = np.dtype(h.dtype).itemsize
+        full = T[:, 4] == 0
+        rk = (T[:, 4] == 1) & (T[:, 5] > 0)
+        want = 4 * len(T) + sz * int((T[full, 1].astype(np.int64) * T[full, 3]).sum() +
+                                     (T[rk, 5].astype(np.int64) * (T[rk, 1] + T[rk, 3])).sum()) + 8 * int(rk.sum())
+        assert len(data) == want
+        first = int(np.frombuffer(data[:4], np.int32)[0])
+        assert first == (0 if T[0, 4] == 0 else T[0, 5])
         g = hb.HMatrix.load(vt, st, data)
         try:
             assert np.array_equal(g.perm(), h.perm())
