@@ -1710,8 +1710,16 @@ class Engine : public EngineBase {
     DevArray<GemvTask> tasks[GemvSide::kMaxLaunch + 1];
     DevArray<int> begin[GemvSide::kMaxLaunch + 1];
     DevArray<GemvZred> zred;
+    DevArray<int> zcnt;
     DevArray<int2> yrows;
   };
+
+  // Whether the z kernels sum the chunks of long groups themselves (the warp finishing a sum's
+  // last chunk adds the parts) instead of a separate pass: the 'N' products in FP64 and complex
+  // (cylinder 100,000, 16 RHS, FP64: z-phase 0.385 -> 0.352 ms).  Not the FP32 tensor-core
+  // z-phase, whose short kernel ends later by the chunks' fences and the last warps' sums than
+  // the separate pass takes (0.134 -> 0.141 ms).
+  static bool zsum_in_kernel(bool trans) { return !trans && !kTensorN; }
 
   static int rank_class(int k) { return k <= 16 ? 0 : (k <= 32 ? 1 : (k <= 64 ? 2 : 3)); }
   static void class_shape(int c, int& ol, int& rpt) {
@@ -2002,7 +2010,9 @@ class Engine : public EngineBase {
         next_row += (long long)nparts * O;
         for (int pidx = 0; pidx < nparts; ++pidx) {
           const int u0 = pidx * kMaxUnits, u1 = std::min((int)lu.size(), u0 + kMaxUnits);
-          zt[cls].push_back(GemvTask{O, (int)cu.size(), u1 - u0, part_row + pidx * O});
+          GemvTask task{O, (int)cu.size(), u1 - u0, part_row + pidx * O};
+          if (zsum_in_kernel(trans)) task.red = (int)zred.size();
+          zt[cls].push_back(task);
           cu.insert(cu.end(), lu.begin() + u0, lu.begin() + u1);
         }
         zred.push_back(GemvZred{zrow, O, part_row, nparts});
@@ -2215,6 +2225,10 @@ class Engine : public EngineBase {
     sb.zred.upload(zred, stream_);
     side.nzred = (int)zred.size();
     side.zred = sb.zred.p;
+    side.zfused = zsum_in_kernel(trans);
+    sb.zcnt.alloc((size_t)std::max<size_t>(zred.size(), 1));
+    HB_CUDA(cudaMemsetAsync(sb.zcnt.p, 0, sb.zcnt.n * sizeof(int), stream_));
+    side.zcnt = sb.zcnt.p;
     sb.yrows.upload(yrows, stream_);
     side.nyrows = (int)yrows.size();
     side.yrows = sb.yrows.p;

@@ -133,15 +133,18 @@ constexpr int nstage_of() {
 // kGatherRows client rows: it reads each column of x along the rows (coalesced), transposes
 // through shared memory, and writes each client row's RS values as one contiguous xz row at
 // its cluster position iperm[j].  One more CTA clears the kZeroRows zero rows from row `zrow0`
-// (the X rows of the y matrices' padding columns).
+// (the X rows of the y matrices' padding columns) and the ncnt chunk counters of the fused z
+// sums, so that every product starts from zero (also after one that stopped early).
 constexpr int kGatherRows = 64;
 template <typename T, int R, int RS>
 __global__ void __launch_bounds__(256) gather_kernel(const T* __restrict__ x, int N, int ldx, int q0, int r,
-                                                     const int* __restrict__ iperm, T* __restrict__ xz, int zrow0) {
+                                                     const int* __restrict__ iperm, T* __restrict__ xz, int zrow0,
+                                                     int* zcnt, int ncnt) {
   __shared__ T tile[RS][kGatherRows + 1];
   const int nblk = (N + kGatherRows - 1) / kGatherRows;
   if ((int)blockIdx.x >= nblk) {
     for (int e = threadIdx.x; e < kZeroRows * RS; e += blockDim.x) xz[(size_t)zrow0 * RS + e] = zero<T>();
+    for (int e = threadIdx.x; e < ncnt; e += blockDim.x) zcnt[e] = 0;  // the z sums' chunk counters
     return;
   }
   const int j0 = blockIdx.x * kGatherRows;
@@ -158,6 +161,42 @@ __global__ void __launch_bounds__(256) gather_kernel(const T* __restrict__ x, in
   }
 }
 inline unsigned gather_grid(int N) { return (unsigned)((N + kGatherRows - 1) / kGatherRows + 1); }
+
+// Loads through L2 only (another SM's writes, made visible by its fence, are not in this
+// SM's L1).
+__device__ inline float ld_l2(const float* p) { return __ldcg(p); }
+__device__ inline double ld_l2(const double* p) { return __ldcg(p); }
+__device__ inline cfloat ld_l2(const cfloat* p) {
+  const float2 v = __ldcg(reinterpret_cast<const float2*>(p));
+  return cfloat{v.x, v.y};
+}
+__device__ inline cdouble ld_l2(const cdouble* p) {
+  const double2 v = __ldcg(reinterpret_cast<const double2*>(p));
+  return cdouble{v.x, v.y};
+}
+
+// End of a z task that is a chunk of a long group (task.red >= 0), after its partial slot is
+// written: the warp's writes are fenced, the sum's counter taken, and the warp that finishes
+// the sum's last chunk adds the partial slots in part order into the final slot (the order of
+// zred_kernel, so the result does not depend on which chunk finishes last).  No warp waits.
+template <typename T, int RS>
+__device__ inline void z_chunk_done(const GemvTask& task, const GemvZred* __restrict__ zred, int* zcnt, T* xz,
+                                    int lane) {
+  if (task.red < 0 || !zcnt) return;
+  __threadfence();
+  __syncwarp();
+  int last = 0;
+  if (lane == 0) last = atomicAdd(&zcnt[task.red], 1) == zred[task.red].nparts - 1;
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (!last) return;
+  __threadfence();
+  const GemvZred d = zred[task.red];
+  for (int e = lane; e < d.k * RS; e += 32) {
+    T v = zero<T>();
+    for (int p = 0; p < d.nparts; ++p) v = v + ld_l2(xz + ((size_t)d.part_row + (size_t)p * d.k) * RS + e);
+    xz[(size_t)d.final_row * RS + e] = v;
+  }
+}
 
 // Checks a unit's copies into a warp-level stage before they are issued: 16-byte sizes and
 // addresses (the bulk-copy rule), the piece below the X rows, the X rows inside the stage, and
@@ -454,7 +493,8 @@ constexpr int warp_min_blocks() {
 template <typename T, int R, int RS, int MODE, int A2>
 __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
     warp_stream_kernel(const GemvTask* __restrict__ tasks, const int* __restrict__ warp_begin,
-                       const GemvUnit* __restrict__ units, const T* __restrict__ arena, T* xz, GemvStatus* err) {
+                       const GemvUnit* __restrict__ units, const T* __restrict__ arena, T* xz, GemvStatus* err,
+                       const GemvZred* __restrict__ zred, int* zcnt) {
   using Ops = RowOps<T, R>;
   constexpr int OL = MODE == 0 ? 32 : 16;
   // MODE 2: right-hand sides per round of the slice sums (a power of two)
@@ -623,6 +663,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       issue_next(u - 1 + kWarpStages);
     }
+    z_chunk_done<T, RS>(task, zred, zcnt, xz, lane);
   }
 }
 
@@ -725,7 +766,8 @@ __host__ __device__ constexpr int mma_min_blocks(int ntile, int elem_bytes) {
 template <typename T, int R, int RS, int NTILE>
 __global__ void __launch_bounds__(kWarpCTA * 32, mma_min_blocks(NTILE, sizeof(T)))
     mma_stream_kernel(const GemvTask* __restrict__ tasks, const int* __restrict__ warp_begin,
-                      const GemvUnit* __restrict__ units, const T* __restrict__ arena, T* xz, GemvStatus* err) {
+                      const GemvUnit* __restrict__ units, const T* __restrict__ arena, T* xz, GemvStatus* err,
+                      const GemvZred* __restrict__ zred, int* zcnt) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, tg = lane & 3;
@@ -821,6 +863,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, mma_min_blocks(NTILE, sizeof(T)
         }
       }
     }
+    z_chunk_done<T, RS>(task, zred, zcnt, xz, lane);
   }
 }
 
@@ -1126,7 +1169,8 @@ void launch_stream_t(const GemvLaunch& L, const GemvUnit* units, const T* arena,
 }
 
 template <typename T, int R, int RS, int MODE, int A2>
-void launch_warp_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, GemvStatus* err, cudaStream_t s) {
+void launch_warp_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, GemvStatus* err, cudaStream_t s,
+                   const GemvZred* zred, int* zcnt) {
   auto kern = warp_stream_kernel<T, R, RS, MODE, A2>;
   const size_t smem = warp_stream_smem_bytes((int)sizeof(T));
   static bool attr = false;
@@ -1134,12 +1178,12 @@ void launch_warp_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = true;
   }
-  kern<<<L.ncta, kWarpCTA * 32, smem, s>>>(L.tasks, L.cta_begin, units, arena, xz, err);
+  kern<<<L.ncta, kWarpCTA * 32, smem, s>>>(L.tasks, L.cta_begin, units, arena, xz, err, zred, zcnt);
 }
 
 template <typename T, int R, int RS, int NTILE>
 void launch_mma_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, GemvStatus* err,
-                  cudaStream_t s) {
+                  cudaStream_t s, const GemvZred* zred, int* zcnt) {
   auto kern = mma_stream_kernel<T, R, RS, NTILE>;
   const size_t smem = warp_stream_smem_bytes((int)sizeof(T));
   static bool attr = false;
@@ -1147,12 +1191,15 @@ void launch_mma_t(const GemvLaunch& L, const GemvUnit* units, const T* arena, T*
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     attr = true;
   }
-  kern<<<L.ncta, kWarpCTA * 32, smem, s>>>(L.tasks, L.cta_begin, units, arena, xz, err);
+  kern<<<L.ncta, kWarpCTA * 32, smem, s>>>(L.tasks, L.cta_begin, units, arena, xz, err, zred, zcnt);
 }
 
+// zred / zcnt: the sums of the z chunks, done by the warp-level z kernels themselves
+// (z_chunk_done); null for the y launches and the CTA-level kernels.
 template <typename T, int R, int RS, bool TRANSP>
 void launch_stream(const GemvLaunch& L, const GemvUnit* units, const T* arena, T* xz, int conj, const int* perm_out,
-                   T* y, int ldy, int q0, int r, T alpha, T beta, GemvStatus* err, cudaStream_t s) {
+                   T* y, int ldy, int q0, int r, T alpha, T beta, GemvStatus* err, cudaStream_t s,
+                   const GemvZred* zred = nullptr, int* zcnt = nullptr) {
   if (L.ntasks <= 0) return;
   if constexpr (std::is_same<T, float>::value && !TRANSP) {
     if (L.map == 4) {
@@ -1164,27 +1211,27 @@ void launch_stream(const GemvLaunch& L, const GemvUnit* units, const T* arena, T
     if constexpr (std::is_same<T, float>::value) {
       if (L.map == 3) {  // rpt = 8-row tiles of the launch's tallest task (exact up to 8)
         switch (L.rpt) {
-          case 1: launch_mma_t<T, R, RS, 1>(L, units, arena, xz, err, s); break;
-          case 2: launch_mma_t<T, R, RS, 2>(L, units, arena, xz, err, s); break;
-          case 3: launch_mma_t<T, R, RS, 3>(L, units, arena, xz, err, s); break;
-          case 4: launch_mma_t<T, R, RS, 4>(L, units, arena, xz, err, s); break;
-          case 5: launch_mma_t<T, R, RS, 5>(L, units, arena, xz, err, s); break;
-          case 6: launch_mma_t<T, R, RS, 6>(L, units, arena, xz, err, s); break;
-          case 7: launch_mma_t<T, R, RS, 7>(L, units, arena, xz, err, s); break;
-          case 8: launch_mma_t<T, R, RS, 8>(L, units, arena, xz, err, s); break;
-          default: launch_mma_t<T, R, RS, 16>(L, units, arena, xz, err, s); break;
+          case 1: launch_mma_t<T, R, RS, 1>(L, units, arena, xz, err, s, zred, zcnt); break;
+          case 2: launch_mma_t<T, R, RS, 2>(L, units, arena, xz, err, s, zred, zcnt); break;
+          case 3: launch_mma_t<T, R, RS, 3>(L, units, arena, xz, err, s, zred, zcnt); break;
+          case 4: launch_mma_t<T, R, RS, 4>(L, units, arena, xz, err, s, zred, zcnt); break;
+          case 5: launch_mma_t<T, R, RS, 5>(L, units, arena, xz, err, s, zred, zcnt); break;
+          case 6: launch_mma_t<T, R, RS, 6>(L, units, arena, xz, err, s, zred, zcnt); break;
+          case 7: launch_mma_t<T, R, RS, 7>(L, units, arena, xz, err, s, zred, zcnt); break;
+          case 8: launch_mma_t<T, R, RS, 8>(L, units, arena, xz, err, s, zred, zcnt); break;
+          default: launch_mma_t<T, R, RS, 16>(L, units, arena, xz, err, s, zred, zcnt); break;
         }
         return;
       }
     }
     if (L.map == 2)
-      launch_warp_t<T, R, RS, 2, 2>(L, units, arena, xz, err, s);
+      launch_warp_t<T, R, RS, 2, 2>(L, units, arena, xz, err, s, zred, zcnt);
     else if (L.map == 5)
-      launch_warp_t<T, R, RS, 0, 2>(L, units, arena, xz, err, s);
+      launch_warp_t<T, R, RS, 0, 2>(L, units, arena, xz, err, s, zred, zcnt);
     else if (L.map == 1)
-      launch_warp_t<T, R, RS, 1, 4>(L, units, arena, xz, err, s);
+      launch_warp_t<T, R, RS, 1, 4>(L, units, arena, xz, err, s, zred, zcnt);
     else
-      launch_warp_t<T, R, RS, 0, 4>(L, units, arena, xz, err, s);
+      launch_warp_t<T, R, RS, 0, 4>(L, units, arena, xz, err, s, zred, zcnt);
     return;
   }
   if (L.ol == 16)
@@ -1208,12 +1255,14 @@ void run_tile(const GemvPlan& p, int nrhs, int q0, T alpha, T beta, const T* x, 
   const int ld_in = n_in, ld_out = TRANSP ? p.n_cols : p.n_rows;
   const T* arena = (const T*)p.arena;
   if (tm) cudaEventRecord(tm->ev[0], s);
-  gather_kernel<T, R, RS><<<gather_grid(n_in), 256, 0, s>>>(x, n_in, ld_in, q0, nrhs, iperm_in, xz, p.n_in_max);
+  const GemvSide& sn = p.side[0];
+  gather_kernel<T, R, RS><<<gather_grid(n_in), 256, 0, s>>>(x, n_in, ld_in, q0, nrhs, iperm_in, xz, p.n_in_max, sn.zcnt,
+                                                            sn.zfused ? sn.nzred : 0);
   if (tm) cudaEventRecord(tm->ev[1], s);
   for (int c = 0; c < side.nz; ++c)
     launch_stream<T, R, RS, TRANSP>(side.z[c], side.units, arena, xz, conj, nullptr, nullptr, 0, 0, 0, alpha, beta,
-                                    err, s);
-  if (side.nzred > 0) zred_kernel<T, RS><<<side.nzred, 128, 0, s>>>(side.zred, xz);
+                                    err, s, side.zfused ? side.zred : nullptr, side.zcnt);
+  if (side.nzred > 0 && !side.zfused) zred_kernel<T, RS><<<side.nzred, 128, 0, s>>>(side.zred, xz);
   if (tm) cudaEventRecord(tm->ev[2], s);
   launch_stream<T, R, RS, TRANSP>(side.y, side.units, arena, xz, conj, perm_out, y, ld_out, q0, nrhs, alpha, beta,
                                   err, s);
@@ -1306,16 +1355,16 @@ void grads_tile(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* r
   constexpr int RS = rs_of<T>(R);
   const T* arena = (const T*)p.arena;
   // x in cluster order (columns) and z = B^T x
-  gather_kernel<T, R, RS><<<gather_grid(p.n_cols), 256, 0, s>>>(x, p.n_cols, p.n_cols, 0, nrhs, p.iperm_cols, xz,
-                                                                   p.n_in_max);
   const GemvSide& sn = p.side[0];
+  gather_kernel<T, R, RS><<<gather_grid(p.n_cols), 256, 0, s>>>(x, p.n_cols, p.n_cols, 0, nrhs, p.iperm_cols, xz,
+                                                                   p.n_in_max, sn.zcnt, sn.zfused ? sn.nzred : 0);
   for (int c = 0; c < sn.nz; ++c)
     launch_stream<T, R, RS, false>(sn.z[c], sn.units, arena, xz, 0, nullptr, nullptr, 0, 0, 0, one<T>(), zero<T>(),
-                                   err, s);
-  if (sn.nzred > 0) zred_kernel<T, RS><<<sn.nzred, 128, 0, s>>>(sn.zred, xz);
+                                   err, s, sn.zfused ? sn.zred : nullptr, sn.zcnt);
+  if (sn.nzred > 0 && !sn.zfused) zred_kernel<T, RS><<<sn.nzred, 128, 0, s>>>(sn.zred, xz);
   // r in cluster order (rows) and w = A^T r
   gather_kernel<T, R, RS><<<gather_grid(p.n_rows), 256, 0, s>>>(r, p.n_rows, p.n_rows, 0, nrhs, p.iperm_rows, rz,
-                                                                   p.n_in_max);
+                                                                   p.n_in_max, sn.zcnt, sn.zfused ? sn.nzred : 0);
   const GemvSide& st = p.side[1];
   for (int c = 0; c < st.nz; ++c)
     launch_stream<T, R, RS, true>(st.z[c], st.units, arena, rz, 0, nullptr, nullptr, 0, 0, 0, one<T>(), zero<T>(),
@@ -1336,13 +1385,13 @@ void adjoint_tile(const GemvPlan& p, int nrhs, const T* x, const T* r, T* dx, T*
   constexpr int RS = rs_of<T>(R);
   const T* arena = (const T*)p.arena;
   run_tile<T, R, true>(p, nrhs, 0, one<T>(), zero<T>(), r, dx, rz, 0, err, s, nullptr);
-  gather_kernel<T, R, RS><<<gather_grid(p.n_cols), 256, 0, s>>>(x, p.n_cols, p.n_cols, 0, nrhs, p.iperm_cols, xz,
-                                                                   p.n_in_max);
   const GemvSide& sn = p.side[0];
+  gather_kernel<T, R, RS><<<gather_grid(p.n_cols), 256, 0, s>>>(x, p.n_cols, p.n_cols, 0, nrhs, p.iperm_cols, xz,
+                                                                   p.n_in_max, sn.zcnt, sn.zfused ? sn.nzred : 0);
   for (int c = 0; c < sn.nz; ++c)
     launch_stream<T, R, RS, false>(sn.z[c], sn.units, arena, xz, 0, nullptr, nullptr, 0, 0, 0, one<T>(), zero<T>(),
-                                   err, s);
-  if (sn.nzred > 0) zred_kernel<T, RS><<<sn.nzred, 128, 0, s>>>(sn.zred, xz);
+                                   err, s, sn.zfused ? sn.zred : nullptr, sn.zcnt);
+  if (sn.nzred > 0 && !sn.zfused) zred_kernel<T, RS><<<sn.nzred, 128, 0, s>>>(sn.zred, xz);
   const int grid = persistent_grid(4);
   if (p.nfull > 0 && gfull)
     grad_full_kernel<T, RS, R><<<grid, 256, 0, s>>>(p.full, p.nfull, xz, rz, gfull, accumulate);
@@ -1375,7 +1424,7 @@ int gemv_launch_count(const GemvPlan& p, char trans, int nrhs, int elem_bytes) {
   const GemvSide& side = p.side[(trans == 'N' || trans == 'n') ? 0 : 1];
   int per_tile = 1;  // gather
   for (int c = 0; c < side.nz; ++c) per_tile += side.z[c].ntasks > 0;
-  per_tile += side.nzred > 0;
+  per_tile += side.nzred > 0 && !side.zfused;
   per_tile += side.y.ntasks > 0;
   per_tile += side.nyrows > 0;  // final pass
   const int maxR = elem_bytes >= 16 ? 4 : 16;

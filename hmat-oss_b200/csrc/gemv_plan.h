@@ -41,6 +41,8 @@ struct GemvTask {
   int first_unit;  // units [first_unit, first_unit + nunits) in order
   int nunits;
   int out_row;     // y: first output row (cluster order); z: first xz row of the slot
+  int red = -1;    // 'N' z chunk of a long group: its z sum (GemvZred index); the last chunk of
+                   // the sum to finish adds the partial slots in part order
 };
 
 // One launch: tasks of one shape class, each CTA of a persistent grid takes a contiguous
@@ -100,6 +102,10 @@ struct GemvSide {
   GemvLaunch z[kMaxLaunch];
   int nzred = 0;
   const GemvZred* zred = nullptr;
+  // zfused: the z kernels sum the parts themselves (the 'N' side); zcnt[i]: chunks of sum i
+  // finished in the current product (cleared by the gather that opens every product)
+  bool zfused = false;
+  int* zcnt = nullptr;
   GemvLaunch y;
   const GemvUnit* units = nullptr;
   // The y launches write partial rows (chunks of the output blocks) into xz; the final pass
