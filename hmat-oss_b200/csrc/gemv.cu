@@ -1110,10 +1110,10 @@ void launch_umma_t(const GemvLaunch& L, const GemvUnit* units, const float* aren
 }
 
 // y in client order from the partial rows of the 'N' y tasks:
-// y[i, q0 + q] = alpha * sum_p xz[pos + p * O, q] + beta * y[i, q0 + q].  A CTA takes 32
+// y[i, q0 + q] = alpha * sum_p xz[pos + p * O, q] + beta * y[i, q0 + q].  A CTA takes 128
 // client rows: the partial rows are read along q (contiguous), transposed through shared
 // memory, and y is written along i (contiguous in each column of y).
-constexpr int kFinalRows = 32;
+constexpr int kFinalRows = 128;
 template <typename T, int R, int RS>
 __global__ void __launch_bounds__(256) yfinal_kernel(const int2* __restrict__ rows, int n, const T* __restrict__ xz,
                                                      T* __restrict__ y, int ldy, int q0, int r, T alpha, T beta) {
@@ -1141,16 +1141,34 @@ __global__ void __launch_bounds__(256) yfinal_kernel(const int2* __restrict__ ro
   }
 }
 
-// Sums the chunk partials of long leaves: xz[final + l] = sum_p xz[part + p k + l].
+// Sums the chunk partials of long leaves: xz[final + l] = sum_p xz[part + p k + l], the parts
+// added in part order.  A warp per sum (kZredWarps sums a CTA), lanes over 16-byte chunks of
+// the k x RS slot (a row of RS scalars is a multiple of 16 bytes).
+constexpr int kZredWarps = 8;
 template <typename T, int RS>
-__global__ void zred_kernel(const GemvZred* __restrict__ zr, T* xz) {
-  const GemvZred d = zr[blockIdx.x];
-  for (int e = threadIdx.x; e < d.k * RS; e += blockDim.x) {
-    T s = zero<T>();
-    for (int p = 0; p < d.nparts; ++p) s = s + xz[((size_t)d.part_row + (size_t)p * d.k) * RS + e];
-    xz[(size_t)d.final_row * RS + e] = s;
+__global__ void __launch_bounds__(kZredWarps * 32) zred_kernel(const GemvZred* __restrict__ zr, int n, T* xz) {
+  constexpr int V = sizeof(T) >= 16 ? 1 : 16 / (int)sizeof(T);  // scalars a 16-byte chunk
+  static_assert((RS * sizeof(T)) % 16 == 0, "xz rows are 16-byte multiples");
+  const int w = blockIdx.x * kZredWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (w >= n) return;
+  const GemvZred d = zr[w];
+  const int nchunk = d.k * RS / V;
+  const T* part = xz + (size_t)d.part_row * RS;
+  T* fin = xz + (size_t)d.final_row * RS;
+  for (int c = lane; c < nchunk; c += 32) {
+    T s[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) s[e] = zero<T>();
+    for (int p = 0; p < d.nparts; ++p) {
+      uint4 raw = *reinterpret_cast<const uint4*>(part + ((size_t)p * d.k * RS + (size_t)c * V));
+      const T* v = reinterpret_cast<const T*>(&raw);
+#pragma unroll
+      for (int e = 0; e < V; ++e) s[e] = s[e] + v[e];
+    }
+    *reinterpret_cast<uint4*>(fin + (size_t)c * V) = *reinterpret_cast<const uint4*>(s);
   }
 }
+inline unsigned zred_grid(int n) { return (unsigned)((n + kZredWarps - 1) / kZredWarps); }
 
 // ---------------------------------------------------------------------------------
 template <typename T, int R, int RS, int OL, int RPT, bool TRANSP>
@@ -1262,7 +1280,7 @@ void run_tile(const GemvPlan& p, int nrhs, int q0, T alpha, T beta, const T* x, 
   for (int c = 0; c < side.nz; ++c)
     launch_stream<T, R, RS, TRANSP>(side.z[c], side.units, arena, xz, conj, nullptr, nullptr, 0, 0, 0, alpha, beta,
                                     err, s, side.zfused ? side.zred : nullptr, side.zcnt);
-  if (side.nzred > 0 && !side.zfused) zred_kernel<T, RS><<<side.nzred, 128, 0, s>>>(side.zred, xz);
+  if (side.nzred > 0 && !side.zfused) zred_kernel<T, RS><<<zred_grid(side.nzred), kZredWarps * 32, 0, s>>>(side.zred, side.nzred, xz);
   if (tm) cudaEventRecord(tm->ev[2], s);
   launch_stream<T, R, RS, TRANSP>(side.y, side.units, arena, xz, conj, perm_out, y, ld_out, q0, nrhs, alpha, beta,
                                   err, s);
@@ -1361,7 +1379,7 @@ void grads_tile(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* r
   for (int c = 0; c < sn.nz; ++c)
     launch_stream<T, R, RS, false>(sn.z[c], sn.units, arena, xz, 0, nullptr, nullptr, 0, 0, 0, one<T>(), zero<T>(),
                                    err, s, sn.zfused ? sn.zred : nullptr, sn.zcnt);
-  if (sn.nzred > 0 && !sn.zfused) zred_kernel<T, RS><<<sn.nzred, 128, 0, s>>>(sn.zred, xz);
+  if (sn.nzred > 0 && !sn.zfused) zred_kernel<T, RS><<<zred_grid(sn.nzred), kZredWarps * 32, 0, s>>>(sn.zred, sn.nzred, xz);
   // r in cluster order (rows) and w = A^T r
   gather_kernel<T, R, RS><<<gather_grid(p.n_rows), 256, 0, s>>>(r, p.n_rows, p.n_rows, 0, nrhs, p.iperm_rows, rz,
                                                                    p.n_in_max, sn.zcnt, sn.zfused ? sn.nzred : 0);
@@ -1369,7 +1387,7 @@ void grads_tile(const GemvPlan& p, int nrhs, const T* x, const T* r, T* xz, T* r
   for (int c = 0; c < st.nz; ++c)
     launch_stream<T, R, RS, true>(st.z[c], st.units, arena, rz, 0, nullptr, nullptr, 0, 0, 0, one<T>(), zero<T>(),
                                   err, s);
-  if (st.nzred > 0) zred_kernel<T, RS><<<st.nzred, 128, 0, s>>>(st.zred, rz);
+  if (st.nzred > 0) zred_kernel<T, RS><<<zred_grid(st.nzred), kZredWarps * 32, 0, s>>>(st.zred, st.nzred, rz);
   const int grid = persistent_grid(4);
   if (p.nfull > 0 && gfull)
     grad_full_kernel<T, RS, R><<<grid, 256, 0, s>>>(p.full, p.nfull, xz, rz, gfull, accumulate);
@@ -1391,7 +1409,7 @@ void adjoint_tile(const GemvPlan& p, int nrhs, const T* x, const T* r, T* dx, T*
   for (int c = 0; c < sn.nz; ++c)
     launch_stream<T, R, RS, false>(sn.z[c], sn.units, arena, xz, 0, nullptr, nullptr, 0, 0, 0, one<T>(), zero<T>(),
                                    err, s, sn.zfused ? sn.zred : nullptr, sn.zcnt);
-  if (sn.nzred > 0 && !sn.zfused) zred_kernel<T, RS><<<sn.nzred, 128, 0, s>>>(sn.zred, xz);
+  if (sn.nzred > 0 && !sn.zfused) zred_kernel<T, RS><<<zred_grid(sn.nzred), kZredWarps * 32, 0, s>>>(sn.zred, sn.nzred, xz);
   const int grid = persistent_grid(4);
   if (p.nfull > 0 && gfull)
     grad_full_kernel<T, RS, R><<<grid, 256, 0, s>>>(p.full, p.nfull, xz, rz, gfull, accumulate);
