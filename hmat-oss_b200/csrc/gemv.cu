@@ -757,11 +757,10 @@ __device__ __forceinline__ void mma_unit_dispatch(int ntn, const T* P, const T* 
   }
 }
 
-// CTAs an SM the tensor-core kernel is compiled for: five (20 warps) while its sums fit the
-// register share of five, four for the tallest tasks (6 tiles and more: 28+ accumulators).
-__host__ __device__ constexpr int mma_min_blocks(int ntile, int elem_bytes) {
-  return elem_bytes == 4 && ntile < 6 ? 5 : 4;
-}
+// CTAs an SM the tensor-core kernel is compiled for: four, the number its shared memory allows
+// (two stages of warp_stage_bytes(4) for each of its four warps), so every tile count gets the
+// registers of four CTAs.
+__host__ __device__ constexpr int mma_min_blocks(int /*ntile*/, int /*elem_bytes*/) { return 4; }
 
 template <typename T, int R, int RS, int NTILE>
 __global__ void __launch_bounds__(kWarpCTA * 32, mma_min_blocks(NTILE, sizeof(T)))

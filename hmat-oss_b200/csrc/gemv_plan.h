@@ -81,10 +81,14 @@ constexpr int kTcPieceBytes = 128 * kTcCols * 4;
 constexpr int kTcXBytes = kTcCols * 16 * 4;
 
 // Per-stage capacities of the warp-level pipeline (bytes): one P piece and its X rows.  FP32
-// pieces are 3,584 B so that five CTAs of the tensor-core kernel (4 warps, two stages of
-// 3,584 + 2,048 B a warp, 45.4 KB a CTA) share an SM's 228 KB: 20 resident warps instead of 16
-// measured 8 % faster than 4 KB pieces, the kernel being issue-bound.
-__host__ __device__ constexpr int warp_piece_bytes(int elem_bytes) { return elem_bytes == 4 ? 3584 : 4096; }
+// pieces are 5,088 B: four CTAs of the tensor-core kernel (4 warps, two stages of 5,088 +
+// 2,048 B a warp, 57.2 KB a CTA, 1 KB reserved) fill an SM's 228 KB, and the kernel's output
+// tiles get the registers of four CTAs.  Against 3,584-B pieces at five CTAs an SM for the
+// z-phase (the y-phase's 6 to 8 tiles already ran at four), fewer and larger units took the
+// y-phase of the 100,000-point cylinder from 0.148 to 0.132 ms with the z-phase unchanged: per
+// unit the kernel pays its barrier wait, descriptor and copy issue, and the larger pieces also
+// keep more bytes in flight a warp.
+__host__ __device__ constexpr int warp_piece_bytes(int elem_bytes) { return elem_bytes == 4 ? 5088 : 4096; }
 constexpr int kWarpXBytes = 2048;
 // FP32 units of short pieces (the z-phase's k x c blocks of B^T) may split the same stage the
 // other way, kWarpXBytesWide bytes of X rows after a piece of the rest.
