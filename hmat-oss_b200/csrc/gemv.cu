@@ -1117,15 +1117,19 @@ template <typename T, int R, int RS>
 __global__ void __launch_bounds__(256) yfinal_kernel(const int2* __restrict__ rows, int n, const T* __restrict__ xz,
                                                      T* __restrict__ y, int ldy, int q0, int r, T alpha, T beta) {
   __shared__ T tile[R][kFinalRows + 1];
+  __shared__ int2 rd[kFinalRows];
   const int i0 = blockIdx.x * kFinalRows;
+  // the rows' part descriptors first, so that the loads of the partial rows below do not wait
+  // on them one by one
+  for (int il = threadIdx.x; il < kFinalRows; il += blockDim.x) rd[il] = i0 + il < n ? rows[i0 + il] : int2{0, 0};
+  __syncthreads();
+#pragma unroll 4
   for (int e = threadIdx.x; e < kFinalRows * R; e += blockDim.x) {
-    const int il = e / R, q = e % R, i = i0 + il;
+    const int il = e / R, q = e % R;
+    const int2 d = rd[il];
+    const int O = d.y & 255, np = d.y >> 8;
     T v = zero<T>();
-    if (i < n) {
-      const int2 d = rows[i];
-      const int O = d.y & 255, np = d.y >> 8;
-      for (int p = 0; p < np; ++p) v = v + xz[((size_t)d.x + (size_t)p * O) * RS + q];
-    }
+    for (int p = 0; p < np; ++p) v = v + xz[((size_t)d.x + (size_t)p * O) * RS + q];
     tile[q][il] = v;
   }
   __syncthreads();
@@ -1154,15 +1158,24 @@ __global__ void __launch_bounds__(kZredWarps * 32) zred_kernel(const GemvZred* _
   const int nchunk = d.k * RS / V;
   const T* part = xz + (size_t)d.part_row * RS;
   T* fin = xz + (size_t)d.final_row * RS;
+  constexpr int kBatch = 8;  // parts loaded before they are added (loads in flight together)
   for (int c = lane; c < nchunk; c += 32) {
     T s[V];
 #pragma unroll
     for (int e = 0; e < V; ++e) s[e] = zero<T>();
-    for (int p = 0; p < d.nparts; ++p) {
-      uint4 raw = *reinterpret_cast<const uint4*>(part + ((size_t)p * d.k * RS + (size_t)c * V));
-      const T* v = reinterpret_cast<const T*>(&raw);
+    for (int p0 = 0; p0 < d.nparts; p0 += kBatch) {
+      uint4 raw[kBatch];
 #pragma unroll
-      for (int e = 0; e < V; ++e) s[e] = s[e] + v[e];
+      for (int i = 0; i < kBatch; ++i)
+        if (p0 + i < d.nparts)
+          raw[i] = *reinterpret_cast<const uint4*>(part + ((size_t)(p0 + i) * d.k * RS + (size_t)c * V));
+#pragma unroll
+      for (int i = 0; i < kBatch; ++i)
+        if (p0 + i < d.nparts) {
+          const T* v = reinterpret_cast<const T*>(&raw[i]);
+#pragma unroll
+          for (int e = 0; e < V; ++e) s[e] = s[e] + v[e];
+        }
     }
     *reinterpret_cast<uint4*>(fin + (size_t)c * V) = *reinterpret_cast<const uint4*>(s);
   }
