@@ -56,11 +56,33 @@ __device__ inline void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 __device__ inline void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-__device__ inline void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+// L2 policies of the streamed copies: a leaf piece is read once per product (evict first), the
+// x / z rows by every unit over their columns (evict last), so that the stream of pieces does
+// not push the vector rows out of L2 and the units read them from DRAM again (100,000-point
+// cylinder, 16 right-hand sides: FP32 product 0.248 -> 0.2435 ms, FP64 0.750 -> 0.743 ms).
+__device__ inline uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ inline uint64_t policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ inline void bulk_g2s_hint(void* dst, const void* src, uint32_t bytes, uint64_t* bar, uint64_t pol) {
   asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
       : "memory");
+}
+// A leaf piece, and the X rows of a unit.
+__device__ inline void bulk_piece(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  bulk_g2s_hint(dst, src, bytes, bar, policy_evict_first());
+}
+__device__ inline void bulk_xrows(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  bulk_g2s_hint(dst, src, bytes, bar, policy_evict_last());
 }
 __device__ inline bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
@@ -237,7 +259,7 @@ __device__ inline void record_bad_unit(GemvStatus* st, int u) {
 template <typename T, int RS>
 __device__ inline void issue_x(unsigned char* dst, const T* xz, const GemvUnit& U, uint64_t* bar) {
   if (U.nruns == 0) {
-    bulk_g2s(dst, xz + (size_t)U.xrow * RS, (uint32_t)U.c * RS * (uint32_t)sizeof(T), bar);
+    bulk_xrows(dst, xz + (size_t)U.xrow * RS, (uint32_t)U.c * RS * (uint32_t)sizeof(T), bar);
     return;
   }
   uint32_t off = 0;
@@ -245,7 +267,7 @@ __device__ inline void issue_x(unsigned char* dst, const T* xz, const GemvUnit& 
   for (int r = 0; r < kUnitRuns; ++r) {  // constant indices: the descriptor stays in registers
     if (r < U.nruns) {
       const uint32_t b = (uint32_t)U.run_len[r] * RS * (uint32_t)sizeof(T);
-      bulk_g2s(dst + off, xz + (size_t)U.run_row[r] * RS, b, bar);
+      bulk_xrows(dst + off, xz + (size_t)U.run_row[r] * RS, b, bar);
       off += b;
     }
   }
@@ -294,8 +316,8 @@ __global__ void __launch_bounds__(kThreads) stream_kernel(const GemvTask* __rest
     const uint32_t pbytes = round16((uint64_t)(U.pel + U.shift) * sizeof(T));
     const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(T);
     mbar_expect_tx(&bars[s], pbytes + xbytes);
-    bulk_g2s(Ps + (size_t)s * PCAP, arena + (U.poff - U.shift), pbytes, &bars[s]);
-    bulk_g2s(Xs + (size_t)s * XCAP, xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
+    bulk_piece(Ps + (size_t)s * PCAP, arena + (U.poff - U.shift), pbytes, &bars[s]);
+    bulk_xrows(Xs + (size_t)s * XCAP, xz + (size_t)U.xrow * RS, xbytes, &bars[s]);
   };
   if (tid == 0)
     for (int u = u_begin; u < u_end && u < u_begin + NSTAGE; ++u) issue(u);
@@ -550,7 +572,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
       return;
     }
     mbar_expect_tx(&bars[s], pbytes + xbytes);
-    bulk_g2s(st, arena + U.poff, pbytes, &bars[s]);
+    bulk_piece(st, arena + U.poff, pbytes, &bars[s]);
     issue_x<T, RS>(st + warp_piece_bytes((int)sizeof(T)), xz, U, &bars[s]);
   };
   auto issue_next = [&](int v) {  // nxt holds units[v]
@@ -815,7 +837,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, mma_min_blocks(NTILE, sizeof(T)
       return;
     }
     mbar_expect_tx(&bars[s], pbytes + xbytes);
-    bulk_g2s(st, arena + U.poff, pbytes, &bars[s]);
+    bulk_piece(st, arena + U.poff, pbytes, &bars[s]);
     issue_x<T, RS>(st + U.o0, xz, U, &bars[s]);
   };
   auto issue_next = [&](int v) {
@@ -987,7 +1009,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(float);
     unsigned char* st = ring + (size_t)s * kTcStage;
     mbar_expect_tx(&full[s], pbytes + xbytes);
-    bulk_g2s(st, arena + U.poff, pbytes, &full[s]);
+    bulk_piece(st, arena + U.poff, pbytes, &full[s]);
     issue_x<float, RS>(st + kTcPieceBytes, xz, U, &full[s]);
   };
   if (tid == 0)
