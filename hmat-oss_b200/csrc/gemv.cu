@@ -426,6 +426,58 @@ __global__ void __launch_bounds__(kThreads) stream_kernel(const GemvTask* __rest
 }
 
 // ---------------------------------------------------------------------------------
+// The descriptors of the next unit and the next task a warp-level kernel issues, prefetched one
+// issue ahead.  LANES = true spreads each over the warp's lanes, one 32-bit word a lane, and
+// gathers it with shuffles when it is used (every lane calls get()), instead of holding it whole
+// in every lane's registers through the unit's sums.  The FP64 y-phase kernel then keeps its
+// accumulators without spilling (100,000-point cylinder, 16 right-hand sides: y-phase 0.393 ->
+// 0.340 ms) and the FP32 one with up to 8 tiles schedules better (0.128 -> 0.1245 ms); the
+// column-slice z kernels keep the whole copy (the FP64 one is slower with the shuffles, 0.349 ->
+// 0.362 ms), and so does the 16-tile FP32 kernel (it spills more with them).
+constexpr int kUnitWords = (int)(sizeof(GemvUnit) / 4);
+constexpr int kTaskWords = (int)(sizeof(GemvTask) / 4);
+static_assert(sizeof(GemvUnit) % 4 == 0 && kUnitWords <= 32, "unit descriptor words");
+static_assert(sizeof(GemvTask) % 4 == 0 && kTaskWords <= 32, "task descriptor words");
+template <typename D, int W>
+__device__ __forceinline__ D from_lanes(uint32_t w) {
+  D d;
+  uint32_t* p = reinterpret_cast<uint32_t*>(&d);
+#pragma unroll
+  for (int i = 0; i < W; ++i) p[i] = __shfl_sync(0xffffffffu, w, i);
+  return d;
+}
+template <bool LANES>
+struct NextUnit {  // lane 0 holds the descriptor
+  GemvUnit d;
+  __device__ void load(const GemvUnit* units, int v, int lane) {
+    if (lane == 0) d = units[v];
+  }
+  __device__ GemvUnit get() const { return d; }
+};
+template <>
+struct NextUnit<true> {  // lane l < kUnitWords holds word l
+  uint32_t w = 0;
+  __device__ void load(const GemvUnit* units, int v, int lane) {
+    w = lane < kUnitWords ? __ldg(reinterpret_cast<const uint32_t*>(units + v) + lane) : 0u;
+  }
+  __device__ GemvUnit get() const { return from_lanes<GemvUnit, kUnitWords>(w); }
+};
+template <bool LANES>
+struct NextTask {  // every lane holds the descriptor
+  GemvTask d;
+  __device__ void load(const GemvTask* tasks, int t, int /*lane*/) { d = tasks[t]; }
+  __device__ GemvTask get() const { return d; }
+};
+template <>
+struct NextTask<true> {  // lane l < kTaskWords holds word l
+  uint32_t w = 0;
+  __device__ void load(const GemvTask* tasks, int t, int lane) {
+    w = lane < kTaskWords ? __ldg(reinterpret_cast<const uint32_t*>(tasks + t) + lane) : 0u;
+  }
+  __device__ GemvTask get() const { return from_lanes<GemvTask, kTaskWords>(w); }
+};
+
+// ---------------------------------------------------------------------------------
 // Warp-level streamed tasks (the 'N' products).  Every warp owns a contiguous range of whole
 // tasks and runs its own two-stage TMA pipeline: lane 0 copies the unit descriptor into the
 // stage and issues the unit's two bulk copies (P piece, X rows), completion on the stage's
@@ -557,7 +609,8 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
   __syncwarp();
   // lane 0: descriptor into the stage, then the unit's two bulk copies.  The descriptor of
   // the next unit to issue is loaded one issue ahead, off the critical path.
-  GemvUnit nxt;
+  constexpr bool kLanes = MODE != 2;
+  NextUnit<kLanes> nxt;
   int last_issued = u_begin - 1;  // lane 0: the last unit whose copies were issued
   auto issue = [&](int u, const GemvUnit& U) {
     const int s = (u - u_begin) % kWarpStages;
@@ -575,21 +628,21 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
     bulk_piece(st, arena + U.poff, pbytes, &bars[s]);
     issue_x<T, RS>(st + warp_piece_bytes((int)sizeof(T)), xz, U, &bars[s]);
   };
-  auto issue_next = [&](int v) {  // nxt holds units[v]
-    issue(v, nxt);
-    if (v + 1 < u_end) nxt = units[v + 1];
+  auto issue_next = [&](int v) {  // nxt holds units[v]; kLanes: every lane calls it, else lane 0
+    const GemvUnit U = nxt.get();
+    if (lane == 0) issue(v, U);
+    if (v + 1 < u_end) nxt.load(units, v + 1, lane);
   };
-  if (lane == 0) {
-    int v = u_begin;
-    for (; v < u_end && v < u_begin + kWarpStages; ++v) issue(v, units[v]);
-    if (v < u_end) nxt = units[v];
-  }
+  if (lane == 0)
+    for (int v = u_begin; v < u_end && v < u_begin + kWarpStages; ++v) issue(v, units[v]);
+  if (u_begin + kWarpStages < u_end) nxt.load(units, u_begin + kWarpStages, lane);
 
   int u = u_begin;
-  GemvTask task_next = tasks[t0];
+  NextTask<kLanes> task_next;
+  task_next.load(tasks, t0, lane);
   for (int t = t0; t < t1; ++t) {
-    const GemvTask task = task_next;
-    if (t + 1 < t1) task_next = tasks[t + 1];
+    const GemvTask task = task_next.get();
+    if (t + 1 < t1) task_next.load(tasks, t + 1, lane);
     const int O = task.O;
     int row0, js, SL, Og = O;
     float inv = 1.f;
@@ -637,7 +690,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
       }
       __syncwarp();  // every lane is done with stage s
       // the last unit's stage stays free until the epilogue has used it as scratch
-      if (lane == 0 && kk + 1 < task.nunits && u + kWarpStages < u_end) issue_next(u + kWarpStages);
+      if ((kLanes || lane == 0) && kk + 1 < task.nunits && u + kWarpStages < u_end) issue_next(u + kWarpStages);
     }
 
     // ---- epilogue: the task's rows go to xz[out_row + l], zero-padded to RS ----
@@ -690,9 +743,9 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
         }
       }
     }
-    if (task.nunits > 0 && lane == 0 && (u - 1) + kWarpStages < u_end) {
+    if (task.nunits > 0 && (kLanes || lane == 0) && (u - 1) + kWarpStages < u_end) {
       // the scratch writes (generic proxy) are ordered before the copy that reuses the stage
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      if (lane == 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       issue_next(u - 1 + kWarpStages);
     }
     z_chunk_done<T, RS>(task, zred, zcnt, xz, lane);
@@ -822,7 +875,8 @@ __global__ void __launch_bounds__(kWarpCTA * 32, mma_min_blocks(NTILE, sizeof(T)
     mbar_fence_init();
   }
   __syncwarp();
-  GemvUnit nxt;
+  constexpr bool kLanes = NTILE <= 8;  // descriptors spread over the lanes (NextUnit)
+  NextUnit<kLanes> nxt;
   int last_issued = u_begin - 1;  // lane 0: the last unit whose copies were issued
   auto issue = [&](int u, const GemvUnit& U) {
     const int s = (u - u_begin) % kWarpStages;
@@ -840,21 +894,21 @@ __global__ void __launch_bounds__(kWarpCTA * 32, mma_min_blocks(NTILE, sizeof(T)
     bulk_piece(st, arena + U.poff, pbytes, &bars[s]);
     issue_x<T, RS>(st + U.o0, xz, U, &bars[s]);
   };
-  auto issue_next = [&](int v) {
-    issue(v, nxt);
-    if (v + 1 < u_end) nxt = units[v + 1];
+  auto issue_next = [&](int v) {  // nxt holds units[v]; kLanes: every lane calls it, else lane 0
+    const GemvUnit U = nxt.get();
+    if (lane == 0) issue(v, U);
+    if (v + 1 < u_end) nxt.load(units, v + 1, lane);
   };
-  if (lane == 0) {
-    int v = u_begin;
-    for (; v < u_end && v < u_begin + kWarpStages; ++v) issue(v, units[v]);
-    if (v < u_end) nxt = units[v];
-  }
+  if (lane == 0)
+    for (int v = u_begin; v < u_end && v < u_begin + kWarpStages; ++v) issue(v, units[v]);
+  if (u_begin + kWarpStages < u_end) nxt.load(units, u_begin + kWarpStages, lane);
 
   int u = u_begin;
-  GemvTask task_next = tasks[t0];
+  NextTask<kLanes> task_next;
+  task_next.load(tasks, t0, lane);
   for (int t = t0; t < t1; ++t) {
-    const GemvTask task = task_next;
-    if (t + 1 < t1) task_next = tasks[t + 1];
+    const GemvTask task = task_next.get();
+    if (t + 1 < t1) task_next.load(tasks, t + 1, lane);
     const int O = task.O;
     const int ntn = (O + 7) >> 3;  // 8-row tiles holding rows of this task (warp-uniform)
     T acc[NTILE][4];
@@ -875,7 +929,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, mma_min_blocks(NTILE, sizeof(T)
       const T* X = reinterpret_cast<const T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)) + uslot[s].y);
       mma_unit_dispatch<T, RS, NTILE>(ntn, P, X, c, O, g, tg, acc);
       __syncwarp();  // every lane is done with stage s
-      if (lane == 0 && u + kWarpStages < u_end) issue_next(u + kWarpStages);
+      if ((kLanes || lane == 0) && u + kWarpStages < u_end) issue_next(u + kWarpStages);
     }
 
     // ---- epilogue: accumulator (rhs g (+8), rows 8 i + 2 t (+1)); right-hand sides past R
