@@ -1739,13 +1739,29 @@ class Engine : public EngineBase {
     if (cols < g) throw Error("gemv plan: output too tall for a warp-level unit");
     return cols;
   }
-  // Columns and X offset of the FP32 units of a short piece (O rows): the stage split the
-  // other way (kWarpXBytesWide of X rows) when that gives wider units, as for B^T blocks of
-  // ranks below 16 (40 columns at rank 12 instead of 32).  Other types keep the fixed split.
+  // Columns and X offset of the units of a piece of O rows.  FP32: the stage split the other
+  // way (kWarpXBytesWide of X rows) when that gives wider units, as for B^T blocks of ranks
+  // below 16 (40 columns at rank 12 instead of 32).  Other types: the widest aligned unit whose
+  // piece and X rows fit the stage together, the X rows right after the piece (16-byte
+  // aligned), instead of the fixed split whose X part held 16 FP64 rows whatever O: the FP64
+  // z-phase units of a rank-12 group take 30 columns instead of 16, the y-phase's 64-row
+  // blocks 10 instead of 8.
   static int warp_unit_cols_wide(int O, int* xoff) {
     const int cols = warp_unit_cols(O);
     *xoff = warp_piece_bytes((int)sizeof(T));
-    if (!std::is_same<T, float>::value) return cols;
+    if (!std::is_same<T, float>::value) {
+      const int s = (int)sizeof(T);
+      const int Rmax = s >= 16 ? 4 : 16;
+      const long long xrow = (long long)gemv_rhs_stride(s, Rmax) * s;
+      const int g = s >= 16 ? 1 : 16 / s;  // the next piece starts 16-byte aligned
+      const long long stage = warp_piece_bytes(s) + kWarpXBytes;
+      auto need = [&](long long c) { return ((long long)O * c * s + 15) / 16 * 16 + c * xrow; };
+      long long c = cols;
+      while (need(c + g) <= stage) c += g;
+      if (need(c) > stage) throw Error("gemv plan: output too tall for a warp-level unit");
+      *xoff = (int)(((long long)O * c * s + 15) / 16 * 16);
+      return (int)c;
+    }
     const int stage = warp_piece_bytes(4) + kWarpXBytes;
     const int xrow_bytes = gemv_rhs_stride(4, 16) * 4;
     int wide = std::min(kWarpXBytesWide / xrow_bytes, (stage - kWarpXBytesWide) / (O * 4));
@@ -1918,11 +1934,11 @@ class Engine : public EngineBase {
       for (auto& t : tasks)
         for (int u = t.first_unit; u < t.first_unit + t.nunits; ++u) {
           const GemvUnit& g = units[u];
-          // FP32 tensor-core units carry their stage split; the other kernels use the fixed one
+          // every unit carries its stage split: the X rows at byte o0, after the piece
           const long long stage = warp_piece_bytes((int)sizeof(T)) + kWarpXBytes;
-          const long long xoff = L.map == 3 ? g.o0 : warp_piece_bytes((int)sizeof(T));
+          const long long xoff = g.o0;
           if (xoff % 16 != 0 || xoff <= 0 || xoff > stage || (long long)g.pel * sizeof(T) > xoff || g.shift != 0 ||
-              (L.map != 3 && g.o0 != xoff) || g.c * xrow_bytes > stage - xoff)
+              g.c * xrow_bytes > stage - xoff)
             throw Error("gemv plan: unit above the warp-level stage capacity");
         }
     }
@@ -2068,7 +2084,7 @@ class Engine : public EngineBase {
         else if (kTensorN)
           cols = mma_unit_cols(O, &xoff);
         else
-          cols = warp_unit_cols(O);
+          cols = warp_unit_cols_wide(O, &xoff);
         if (tune_yhalf_ && !tc_y) {  // the tuner's narrower units: half the columns, kept aligned
           const int step = kTensorN ? 8 : galign;
           cols = std::max(step, cols / 2 / step * step);

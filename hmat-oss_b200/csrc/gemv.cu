@@ -480,7 +480,8 @@ struct NextTask<true> {  // lane l < kTaskWords holds word l
 // ---------------------------------------------------------------------------------
 // Warp-level streamed tasks (the 'N' products).  Every warp owns a contiguous range of whole
 // tasks and runs its own two-stage TMA pipeline: lane 0 copies the unit descriptor into the
-// stage and issues the unit's two bulk copies (P piece, X rows), completion on the stage's
+// stage and issues the unit's bulk copies (P piece; X rows at the unit's byte offset o0 in the
+// stage, right after the piece), completion on the stage's
 // mbarrier, so warps never wait for one another.  Lane maps (output rows O of the task):
 //   MODE 2 (O <= 32): the warp is a window of floor(32 / O) column slices x O rows, lane =
 //          slice * O + row; P is read as one contiguous run per step (no bank conflicts);
@@ -619,14 +620,14 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
     const uint32_t pbytes = round16((uint64_t)U.pel * sizeof(T));
     const uint32_t xbytes = (uint32_t)U.c * RS * (uint32_t)sizeof(T);
     unsigned char* st = wbase + (size_t)s * warp_stage_bytes((int)sizeof(T));
-    if (!unit_copies_ok<T, RS>(U, arena, xz, warp_stage_bytes((int)sizeof(T)), warp_piece_bytes((int)sizeof(T)))) {
+    if (!unit_copies_ok<T, RS>(U, arena, xz, warp_stage_bytes((int)sizeof(T)), U.o0)) {
       record_bad_unit(err, u);
       mbar_arrive(&bars[s]);
       return;
     }
     mbar_expect_tx(&bars[s], pbytes + xbytes);
     bulk_piece(st, arena + U.poff, pbytes, &bars[s]);
-    issue_x<T, RS>(st + warp_piece_bytes((int)sizeof(T)), xz, U, &bars[s]);
+    issue_x<T, RS>(st + U.o0, xz, U, &bars[s]);
   };
   auto issue_next = [&](int v) {  // nxt holds units[v]; kLanes: every lane calls it, else lane 0
     const GemvUnit U = nxt.get();
@@ -680,7 +681,7 @@ __global__ void __launch_bounds__(kWarpCTA * 32, (warp_min_blocks<T, R, A2>()))
       }
       const int c = uslot[s].x;
       const T* P = reinterpret_cast<const T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)));
-      const T* X = reinterpret_cast<const T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)) + warp_piece_bytes((int)sizeof(T)));
+      const T* X = reinterpret_cast<const T*>(wbase + (size_t)s * warp_stage_bytes((int)sizeof(T)) + uslot[s].y);
       // Rows of a lane past O read the next column (or, in the last column, the first
       // elements of the X rows of the same stage); they are never written.
       if constexpr (MODE == 2) {
