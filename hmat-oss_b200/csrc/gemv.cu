@@ -820,9 +820,11 @@ template <int RS, int NT, int NTILE>
 __device__ __forceinline__ void mma_unit(const float* P, const float* X, int c, int O, int g, int tg,
                                          float (&acc)[NTILE][4]) {
   int k0 = 0;
-  if constexpr (NT <= 3) {
+  if constexpr (NT <= 4) {
     // two steps per iteration: their MMA chains are independent and overlap (wider tasks
-    // have enough independent tiles in one step, and the registers go to their sums)
+    // have enough independent tiles in one step, and the registers go to their sums; with
+    // two steps for 5-7 tiles the y-phase took 0.1213 -> 0.1235 ms, and with them for 4 tiles
+    // the z-phase 0.1145 -> 0.111 ms, on the 100,000-point cylinder)
 #pragma unroll 2
     for (; k0 + 8 <= c; k0 += 8) mma_kstep<RS, NT, NTILE, false>(P, X, k0, c, O, g, tg, acc);
   } else {
